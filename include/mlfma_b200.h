@@ -1,0 +1,169 @@
+/*
+ * mlfma_b200: C ABI of the B200 MLFMA operator and GMRES solver.
+ *
+ * The reference (ellilu11/MLFMA) has no foreign-function interface; its
+ * operator API is a C++ object protocol driven from main() with global
+ * state.  Each entry point below replaces one step of that protocol; the
+ * reference file:line it stands in for is given beside it.
+ *
+ * Conventions:
+ *   - every call returns an int status (MLFMA_OK or MLFMA_ERR_*); nothing throws
+ *     across the boundary; mlfma_last_error() gives a message (per thread);
+ *   - complex vectors are interleaved (re, im) doubles, length 2*N, in the
+ *     caller's source order (the order sources were passed in);
+ *   - host buffers are caller-owned; device state is owned by the handle;
+ *   - a handle is used from one thread at a time; many handles may coexist.
+ */
+#ifndef MLFMA_B200_H
+#define MLFMA_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    MLFMA_OK = 0,
+    MLFMA_ERR_ARG = 1,            /* invalid argument or input geometry */
+    MLFMA_ERR_CUDA = 2,           /* CUDA runtime error (no device, launch failure, ...) */
+    MLFMA_ERR_STATE = 3,          /* call out of order (e.g. matvec before setup) */
+    MLFMA_ERR_NOT_CONVERGED = 4,  /* solver hit its iteration limit */
+    MLFMA_ERR_NONFINITE = 5,      /* NaN or Inf in an input or the solver state */
+    MLFMA_ERR_INTERNAL = 6
+};
+
+enum { MLFMA_DIPOLE = 0, MLFMA_RWG = 1 };
+
+/* Precision enum of the reference (src/config.h:7): triangle quadrature rule. */
+enum { MLFMA_QUAD_1PT = 0, MLFMA_QUAD_3PT = 1, MLFMA_QUAD_7PT = 2, MLFMA_QUAD_13PT = 3 };
+
+typedef struct mlfma_op_s* mlfma_handle;
+
+/* Operator configuration.  The first six fields are the reference Config
+ * (src/config.h:50-73) with the same meaning; the rest are extensions. */
+typedef struct {
+    int quad_prec;       /* MLFMA_QUAD_*; RWG only */
+    int digits;          /* excess-bandwidth digits of the angular sampling */
+    int interp_order;    /* Lagrange half-width: 2*interp_order points */
+    double over_interp;  /* psi oversampling of the transfer functions */
+    double root_leng;    /* side of the root box, centred at the origin */
+    int max_node_srcs;   /* a box splits while it holds more sources than this */
+    int max_level;       /* >0: do not split below this level (0 = reference rule) */
+    int ref_compat;      /* 1: reproduce the reference's stale-local rule (default) */
+    int device;          /* CUDA device ordinal */
+} mlfma_config;
+
+/* Incident plane wave (src/excite.h:6-28; file format src/fileio.h:8-27). */
+typedef struct {
+    double amplitude;
+    double pol[3];
+    double khat[3];
+    double wavenum;
+} mlfma_planewave;
+
+typedef struct {
+    int num_nodes, num_leaves, max_level, num_levels_far;
+    long long list2, list4, near_pairs, near_entries, pattern_elems;
+    long long device_bytes;
+} mlfma_stats;
+
+/* Per-stage device time of one matvec, ms (the reference's ClockTimes stages,
+ * src/clock.h:8-17, plus the near field). */
+typedef struct {
+    float gather, s2m, m2m, m2l, l2l, l2t, near_field, finish, total;
+} mlfma_stage_times;
+
+/* Algorithmic HBM bytes of one matvec per stage (roofline accounting). */
+typedef struct {
+    double s2m, m2m, m2l, l2l, l2t, near_field, total;
+} mlfma_traffic;
+
+typedef struct {
+    int max_iter;        /* iteration limit (reference: 500, src/mlfma.cpp:69) */
+    double tol;          /* relative residual target (reference: 1e-6, src/mlfma.cpp:70) */
+    int restart;         /* 0 = no restart (reference), else GMRES(restart) */
+    int ref_givens;      /* 1: complex-symmetric Givens of the reference (src/math.h:168-172) */
+} mlfma_solver_opts;
+
+typedef struct {
+    int iterations;
+    double residual;       /* final |g_{k+1}| / g0 estimate */
+    double true_residual;  /* ||b - A x|| / ||b||, recomputed */
+    double seconds;
+} mlfma_solve_info;
+
+/* Fill *cfg with the defaults (digits 3, order 3, overInterp 2, rootLeng 4, 64 per box). */
+int mlfma_config_default(mlfma_config* cfg);
+
+/* Dipole sources: pos and mom are n x 3 (row-major).  Builds the host plan:
+ * tree, lists, angular grids and tables (replaces Node::initStatic,
+ * src/fmm/node.cpp:13-26, the Stem/Leaf constructors, src/mlfma.cpp:26-30,
+ * buildLists, src/fmm/stem.cpp:48-57, and Node::buildTables,
+ * src/fmm/node.cpp:46-56, after importDipoles, src/fileio.h:110-131). */
+int mlfma_create_dipoles(const mlfma_config* cfg, const mlfma_planewave* pw, int n,
+                         const double* pos, const double* mom, mlfma_handle* out);
+
+/* RWG sources on a triangle mesh: verts nv x 3, faces nf x 3, rwgs ne x 4
+ * (v0, v1, t+, t-), 0-based (importRWG, src/fileio.h:174-202, then the same
+ * setup steps as mlfma_create_dipoles). */
+int mlfma_create_rwg(const mlfma_config* cfg, const mlfma_planewave* pw, int nv, const double* verts,
+                     int nf, const int* faces, int ne, const int* rwgs, mlfma_handle* out);
+
+/* Upload to the GPU and assemble radiation patterns and near-field blocks
+ * there (Leaf::buildNearRads, src/fmm/leaf.cpp:108-180; root->resizeCoeffs;
+ * Leaf::buildRadPats, src/fmm/leaf.cpp:185-207). */
+int mlfma_setup(mlfma_handle h);
+
+int mlfma_num_unknowns(mlfma_handle h, int* n);
+int mlfma_get_stats(mlfma_handle h, mlfma_stats* st);
+
+/* b = -V, the GMRES right-hand side (Solver ctor, src/solver.cpp:31-32;
+ * Source::buildVoltage, src/sources/dipole.h:29-32, src/sources/rwg.h:18-21). */
+int mlfma_rhs(mlfma_handle h, double* b);
+
+/* y = A x (accumulate = 0) or y += A x (accumulate = 1), host buffers
+ * (Solver::evalRvec, src/solver.cpp:41-57: rvec += A lvec).  Copies in and
+ * out through the handle's stream. */
+int mlfma_matvec(mlfma_handle h, const double* x, double* y, int accumulate);
+
+/* Same on device buffers (cudaStream_t passed as void*, NULL = handle's stream).
+ * Asynchronous with respect to the host. */
+int mlfma_matvec_device(mlfma_handle h, const void* d_x, void* d_y, int accumulate, void* stream);
+
+/* Solve A x = b with GMRES on the device; b and x host buffers (Solver::solve,
+ * src/solver.cpp:116-146).  x is overwritten (initial guess 0). */
+int mlfma_gmres(mlfma_handle h, const double* b, double* x, const mlfma_solver_opts* opts,
+                mlfma_solve_info* info);
+
+/* CUDA-event time of each stage of one matvec on the handle's stream. */
+int mlfma_time_stages(mlfma_handle h, mlfma_stage_times* t);
+int mlfma_get_traffic(mlfma_handle h, mlfma_traffic* t);
+
+/* Diagnostics: angular grid of a level (sizes: nth, nph, L) and the
+ * outgoing (which = 0) or local (which = 1) patterns of every box of a level
+ * after the last matvec, as [box][dir][2] complex, plus each box's integer
+ * coordinates (3 ints per box). */
+int mlfma_level_info(mlfma_handle h, int level, int* sizes, double* thetas, double* weights,
+                     double* phis);
+int mlfma_level_boxes(mlfma_handle h, int level, int* nbox, int* coords);
+int mlfma_level_patterns(mlfma_handle h, int level, int which, double* out, long long count);
+/* Transfer functions of a level: 316 x ndir complex in the order of
+ * Math::getINodeDistVecs (src/math.cpp:106-122). */
+int mlfma_level_transl(mlfma_handle h, int level, double* out);
+
+/* Far-field leaves in tree order: count, then per leaf (level, box, first
+ * source in tree order, source count) and the tree-order -> caller-order
+ * permutation (n ints). */
+int mlfma_far_leaves(mlfma_handle h, int* count, int* info, int* perm);
+/* Reference-rounded RWG radiation patterns computed on the host, laid out as
+ * the device array: per far leaf, per source, per direction, 2 complex. */
+int mlfma_rwg_patterns_host(mlfma_handle h, double* out, long long count);
+
+int mlfma_destroy(mlfma_handle h);
+
+const char* mlfma_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MLFMA_B200_H */

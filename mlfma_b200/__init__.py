@@ -1,0 +1,216 @@
+"""B200 MLFMA operator and GMRES solver (Python front end over the C ABI).
+
+    from mlfma_b200 import MLFMA, inputs
+    op = MLFMA.dipoles(inputs.make_dipoles(8192), inputs.PlaneWave())
+    op.setup()                 # GPU: patterns + near field
+    y = op.matvec(x)           # y = A x   (Solver::evalRvec)
+    x, info = op.solve(op.rhs())   # GMRES  (Solver::solve)
+
+Every numerical step runs in libmlfma_b200.so; this module only marshals
+arrays.  The reference's setup steps map onto create (tree, lists, tables)
+and setup (patterns and near field on the device).
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import inputs
+from ._lib import (Config, MlfmaError, NotConverged, PlaneWaveC, SolveInfo, SolverOpts, StageTimes, Stats,
+                   Traffic, check, lib)
+
+__all__ = ["MLFMA", "MlfmaError", "NotConverged", "inputs", "default_config"]
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int)
+
+
+def default_config(**overrides) -> Config:
+    c = Config()
+    check(lib().mlfma_config_default(ctypes.byref(c)))
+    for k, v in overrides.items():
+        if not hasattr(c, k):
+            raise KeyError(k)
+        setattr(c, k, v)
+    return c
+
+
+def _pw(p: inputs.PlaneWave) -> PlaneWaveC:
+    c = PlaneWaveC()
+    c.amplitude = p.amplitude
+    for i in range(3):
+        c.pol[i] = p.pol[i]
+        c.khat[i] = p.khat[i]
+    c.wavenum = p.wavenum
+    return c
+
+
+def _cvec(x, n):
+    a = np.ascontiguousarray(np.asarray(x, dtype=np.complex128).reshape(-1))
+    if a.shape[0] != n:
+        raise ValueError(f"expected {n} entries, got {a.shape[0]}")
+    return a
+
+
+@dataclass
+class SolveResult:
+    iterations: int
+    residual: float
+    true_residual: float
+    seconds: float
+    converged: bool
+
+
+class MLFMA:
+    """One operator instance (one handle)."""
+
+    def __init__(self, handle: ctypes.c_void_p, n: int, kind: str):
+        self._h = handle
+        self.n = n
+        self.kind = kind
+        self._ready = False
+
+    # ---------------------------------------------------------------- create
+    @classmethod
+    def dipoles(cls, d: inputs.Dipoles, pw: inputs.PlaneWave, config: Config | None = None, **kw) -> "MLFMA":
+        cfg = config or default_config(**kw)
+        pos = np.ascontiguousarray(d.pos, dtype=np.float64)
+        mom = np.ascontiguousarray(d.mom, dtype=np.float64)
+        h = ctypes.c_void_p()
+        p = _pw(pw)
+        check(lib().mlfma_create_dipoles(ctypes.byref(cfg), ctypes.byref(p), d.n, pos.ctypes.data_as(_dp),
+                                         mom.ctypes.data_as(_dp), ctypes.byref(h)))
+        return cls(h, d.n, "dipole")
+
+    @classmethod
+    def rwg(cls, m: inputs.RWGMesh, pw: inputs.PlaneWave, config: Config | None = None, **kw) -> "MLFMA":
+        cfg = config or default_config(**kw)
+        V = np.ascontiguousarray(m.vertices, dtype=np.float64)
+        F = np.ascontiguousarray(m.faces, dtype=np.int32)
+        E = np.ascontiguousarray(m.rwgs, dtype=np.int32)
+        h = ctypes.c_void_p()
+        p = _pw(pw)
+        check(lib().mlfma_create_rwg(ctypes.byref(cfg), ctypes.byref(p), V.shape[0], V.ctypes.data_as(_dp),
+                                     F.shape[0], F.ctypes.data_as(_ip), E.shape[0], E.ctypes.data_as(_ip),
+                                     ctypes.byref(h)))
+        return cls(h, m.n, "rwg")
+
+    def setup(self) -> "MLFMA":
+        check(lib().mlfma_setup(self._h))
+        self._ready = True
+        return self
+
+    def close(self) -> None:
+        if self._h:
+            lib().mlfma_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # ---------------------------------------------------------------- host queries
+    def stats(self) -> dict:
+        s = Stats()
+        check(lib().mlfma_get_stats(self._h, ctypes.byref(s)))
+        return {k: getattr(s, k) for k, _ in Stats._fields_}
+
+    def rhs(self) -> np.ndarray:
+        b = np.zeros(self.n, dtype=np.complex128)
+        check(lib().mlfma_rhs(self._h, b.view(np.float64).ctypes.data_as(_dp)))
+        return b
+
+    def level_info(self, level: int) -> dict:
+        sz = np.zeros(3, dtype=np.int32)
+        check(lib().mlfma_level_info(self._h, level, sz.ctypes.data_as(_ip), None, None, None))
+        nth, nph, L = (int(v) for v in sz)
+        th, w, ph = np.zeros(nth), np.zeros(nth), np.zeros(nph)
+        check(lib().mlfma_level_info(self._h, level, sz.ctypes.data_as(_ip), th.ctypes.data_as(_dp),
+                                     w.ctypes.data_as(_dp), ph.ctypes.data_as(_dp)))
+        return dict(thetas=th, weights=w, phis=ph, L=L, nth=nth, nph=nph)
+
+    def level_boxes(self, level: int) -> np.ndarray:
+        nb = ctypes.c_int()
+        check(lib().mlfma_level_boxes(self._h, level, ctypes.byref(nb), None))
+        c = np.zeros((max(nb.value, 1), 3), dtype=np.int32)
+        check(lib().mlfma_level_boxes(self._h, level, ctypes.byref(nb), c.ctypes.data_as(_ip)))
+        return c[: nb.value]
+
+    def level_transl(self, level: int) -> np.ndarray:
+        info = self.level_info(level)
+        ndir = info["nth"] * info["nph"]
+        out = np.zeros(316 * ndir, dtype=np.complex128)
+        check(lib().mlfma_level_transl(self._h, level, out.view(np.float64).ctypes.data_as(_dp)))
+        return out.reshape(316, ndir)
+
+    def far_leaves(self):
+        """(info[:, (level, box, src0, nsrc)], perm) with perm[tree slot] = caller index."""
+        cnt = ctypes.c_int()
+        check(lib().mlfma_far_leaves(self._h, ctypes.byref(cnt), None, None))
+        info = np.zeros((max(cnt.value, 1), 4), dtype=np.int32)
+        perm = np.zeros(self.n, dtype=np.int32)
+        check(lib().mlfma_far_leaves(self._h, ctypes.byref(cnt), info.ctypes.data_as(_ip),
+                                     perm.ctypes.data_as(_ip)))
+        return info[: cnt.value], perm
+
+    def rwg_patterns_host(self) -> np.ndarray:
+        n = self.stats()["pattern_elems"]
+        out = np.zeros(2 * n, dtype=np.complex128)
+        check(lib().mlfma_rwg_patterns_host(self._h, out.view(np.float64).ctypes.data_as(_dp), out.size * 2))
+        return out
+
+    # ---------------------------------------------------------------- device
+    def matvec(self, x, accumulate: bool = False, out: np.ndarray | None = None) -> np.ndarray:
+        xv = _cvec(x, self.n)
+        y = out if out is not None else np.zeros(self.n, dtype=np.complex128)
+        if y.dtype != np.complex128 or not y.flags.c_contiguous or y.shape[0] != self.n:
+            raise ValueError("out must be a contiguous complex128 vector of length n")
+        check(lib().mlfma_matvec(self._h, xv.view(np.float64).ctypes.data_as(_dp),
+                                 y.view(np.float64).ctypes.data_as(_dp), int(accumulate)))
+        return y
+
+    def matvec_device(self, x_ptr: int, y_ptr: int, accumulate: bool = False, stream: int = 0) -> None:
+        check(lib().mlfma_matvec_device(self._h, ctypes.c_void_p(x_ptr), ctypes.c_void_p(y_ptr),
+                                        int(accumulate), ctypes.c_void_p(stream)))
+
+    def solve(self, b=None, max_iter: int = 500, tol: float = 1e-6, restart: int = 0,
+              ref_givens: bool = True, raise_on_fail: bool = False):
+        bv = self.rhs() if b is None else _cvec(b, self.n)
+        x = np.zeros(self.n, dtype=np.complex128)
+        o = SolverOpts(max_iter=max_iter, tol=tol, restart=restart, ref_givens=int(ref_givens))
+        info = SolveInfo()
+        code = lib().mlfma_gmres(self._h, bv.view(np.float64).ctypes.data_as(_dp),
+                                 x.view(np.float64).ctypes.data_as(_dp), ctypes.byref(o), ctypes.byref(info))
+        converged = code == 0
+        if code not in (0, 4) or (raise_on_fail and code != 0):
+            check(code)
+        return x, SolveResult(info.iterations, info.residual, info.true_residual, info.seconds, converged)
+
+    def stage_times(self) -> dict:
+        t = StageTimes()
+        check(lib().mlfma_time_stages(self._h, ctypes.byref(t)))
+        return {k: float(getattr(t, k)) for k, _ in StageTimes._fields_}
+
+    def traffic(self) -> dict:
+        t = Traffic()
+        check(lib().mlfma_get_traffic(self._h, ctypes.byref(t)))
+        return {k: float(getattr(t, k)) for k, _ in Traffic._fields_}
+
+    def level_patterns(self, level: int, which: int = 0) -> np.ndarray:
+        info = self.level_info(level)
+        nb = self.level_boxes(level).shape[0]
+        ndir = info["nth"] * info["nph"]
+        out = np.zeros(nb * ndir * 2, dtype=np.complex128)
+        check(lib().mlfma_level_patterns(self._h, level, which, out.view(np.float64).ctypes.data_as(_dp),
+                                         out.size))
+        return out.reshape(nb, ndir, 2)

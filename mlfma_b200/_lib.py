@@ -1,0 +1,127 @@
+"""ctypes binding of libmlfma_b200.so (declarations in include/mlfma_b200.h).
+
+The library is loaded from the package directory.  A missing library raises
+immediately: there is no fallback implementation.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmlfma_b200.so")
+
+MLFMA_OK = 0
+MLFMA_ERR_ARG = 1
+MLFMA_ERR_CUDA = 2
+MLFMA_ERR_STATE = 3
+MLFMA_ERR_NOT_CONVERGED = 4
+MLFMA_ERR_NONFINITE = 5
+MLFMA_ERR_INTERNAL = 6
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int)
+
+
+class Config(ctypes.Structure):
+    _fields_ = [("quad_prec", ctypes.c_int), ("digits", ctypes.c_int), ("interp_order", ctypes.c_int),
+                ("over_interp", ctypes.c_double), ("root_leng", ctypes.c_double),
+                ("max_node_srcs", ctypes.c_int), ("max_level", ctypes.c_int),
+                ("ref_compat", ctypes.c_int), ("device", ctypes.c_int)]
+
+
+class PlaneWaveC(ctypes.Structure):
+    _fields_ = [("amplitude", ctypes.c_double), ("pol", ctypes.c_double * 3),
+                ("khat", ctypes.c_double * 3), ("wavenum", ctypes.c_double)]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [("num_nodes", ctypes.c_int), ("num_leaves", ctypes.c_int), ("max_level", ctypes.c_int),
+                ("num_levels_far", ctypes.c_int), ("list2", ctypes.c_longlong),
+                ("list4", ctypes.c_longlong), ("near_pairs", ctypes.c_longlong),
+                ("near_entries", ctypes.c_longlong), ("pattern_elems", ctypes.c_longlong),
+                ("device_bytes", ctypes.c_longlong)]
+
+
+class StageTimes(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_float) for k in
+                ("gather", "s2m", "m2m", "m2l", "l2l", "l2t", "near_field", "finish", "total")]
+
+
+class Traffic(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_double) for k in ("s2m", "m2m", "m2l", "l2l", "l2t", "near_field", "total")]
+
+
+class SolverOpts(ctypes.Structure):
+    _fields_ = [("max_iter", ctypes.c_int), ("tol", ctypes.c_double), ("restart", ctypes.c_int),
+                ("ref_givens", ctypes.c_int)]
+
+
+class SolveInfo(ctypes.Structure):
+    _fields_ = [("iterations", ctypes.c_int), ("residual", ctypes.c_double),
+                ("true_residual", ctypes.c_double), ("seconds", ctypes.c_double)]
+
+
+# name -> (restype, argtypes); every symbol the header declares.
+SIGNATURES = {
+    "mlfma_config_default": (ctypes.c_int, [ctypes.POINTER(Config)]),
+    "mlfma_create_dipoles": (ctypes.c_int, [ctypes.POINTER(Config), ctypes.POINTER(PlaneWaveC), ctypes.c_int,
+                                            _dp, _dp, ctypes.POINTER(ctypes.c_void_p)]),
+    "mlfma_create_rwg": (ctypes.c_int, [ctypes.POINTER(Config), ctypes.POINTER(PlaneWaveC), ctypes.c_int, _dp,
+                                        ctypes.c_int, _ip, ctypes.c_int, _ip, ctypes.POINTER(ctypes.c_void_p)]),
+    "mlfma_setup": (ctypes.c_int, [ctypes.c_void_p]),
+    "mlfma_num_unknowns": (ctypes.c_int, [ctypes.c_void_p, _ip]),
+    "mlfma_get_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Stats)]),
+    "mlfma_rhs": (ctypes.c_int, [ctypes.c_void_p, _dp]),
+    "mlfma_matvec": (ctypes.c_int, [ctypes.c_void_p, _dp, _dp, ctypes.c_int]),
+    "mlfma_matvec_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                           ctypes.c_void_p]),
+    "mlfma_gmres": (ctypes.c_int, [ctypes.c_void_p, _dp, _dp, ctypes.POINTER(SolverOpts),
+                                   ctypes.POINTER(SolveInfo)]),
+    "mlfma_time_stages": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(StageTimes)]),
+    "mlfma_get_traffic": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Traffic)]),
+    "mlfma_level_info": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _ip, _dp, _dp, _dp]),
+    "mlfma_level_boxes": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _ip, _ip]),
+    "mlfma_level_patterns": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp, ctypes.c_longlong]),
+    "mlfma_level_transl": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _dp]),
+    "mlfma_far_leaves": (ctypes.c_int, [ctypes.c_void_p, _ip, _ip, _ip]),
+    "mlfma_rwg_patterns_host": (ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_longlong]),
+    "mlfma_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "mlfma_last_error": (ctypes.c_char_p, []),
+}
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"mlfma_b200 native library not built: {LIB_PATH} "
+                               "(run `python -m mlfma_b200.build`)")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+class MlfmaError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+class NotConverged(MlfmaError):
+    pass
+
+
+def check(code: int) -> None:
+    if code == MLFMA_OK:
+        return
+    msg = lib().mlfma_last_error().decode(errors="replace")
+    if code == MLFMA_ERR_NOT_CONVERGED:
+        raise NotConverged(code, msg)
+    raise MlfmaError(code, msg)

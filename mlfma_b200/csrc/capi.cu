@@ -1,0 +1,343 @@
+// C ABI of the operator (include/mlfma_b200.h).
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <exception>
+#include <memory>
+#include <string>
+
+#include "../../include/mlfma_b200.h"
+#include "device.cuh"
+#include "gmres.hpp"
+#include "plan.hpp"
+
+struct mlfma_op_s {
+    mlfma::Plan plan;
+    int device = 0;
+    std::unique_ptr<mlfma::DeviceOp> dev;
+    std::unique_ptr<mlfma::Gmres> gmres;
+    double2* d_x = nullptr;  // staging for host-buffer calls
+    double2* d_y = nullptr;
+    ~mlfma_op_s() {
+        if (d_x || d_y) {
+            cudaSetDevice(device);
+            if (d_x) cudaFree(d_x);
+            if (d_y) cudaFree(d_y);
+        }
+    }
+};
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+    g_err = msg;
+    return code;
+}
+
+int from_msg(const std::string& msg) {
+    if (msg.empty()) return MLFMA_OK;
+    if (msg.rfind("nonfinite", 0) == 0) return fail(MLFMA_ERR_NONFINITE, msg);
+    return fail(MLFMA_ERR_CUDA, msg);
+}
+
+mlfma::Config to_cfg(const mlfma_config* c) {
+    mlfma::Config o;
+    o.quad_prec = c->quad_prec;
+    o.digits = c->digits;
+    o.interp_order = c->interp_order;
+    o.over_interp = c->over_interp;
+    o.root_leng = c->root_leng;
+    o.max_node_srcs = c->max_node_srcs;
+    o.max_level = c->max_level;
+    o.ref_compat = c->ref_compat;
+    return o;
+}
+
+mlfma::PlaneWave to_pw(const mlfma_planewave* p) {
+    mlfma::PlaneWave o;
+    o.amplitude = p->amplitude;
+    for (int k = 0; k < 3; ++k) {
+        o.pol[k] = p->pol[k];
+        o.khat[k] = p->khat[k];
+    }
+    o.wavenum = p->wavenum;
+    return o;
+}
+
+bool ready(mlfma_handle h) { return h && h->dev; }
+
+}  // namespace
+
+extern "C" {
+
+const char* mlfma_last_error(void) { return g_err.c_str(); }
+
+int mlfma_config_default(mlfma_config* cfg) {
+    if (!cfg) return fail(MLFMA_ERR_ARG, "null config");
+    cfg->quad_prec = MLFMA_QUAD_7PT;
+    cfg->digits = 3;
+    cfg->interp_order = 3;
+    cfg->over_interp = 2.0;
+    cfg->root_leng = 4.0;
+    cfg->max_node_srcs = 64;
+    cfg->max_level = 0;
+    cfg->ref_compat = 1;
+    cfg->device = 0;
+    return MLFMA_OK;
+}
+
+int mlfma_create_dipoles(const mlfma_config* cfg, const mlfma_planewave* pw, int n, const double* pos,
+                         const double* mom, mlfma_handle* out) {
+    if (!cfg || !pw || !pos || !mom || !out || n <= 0) return fail(MLFMA_ERR_ARG, "null argument or n <= 0");
+    try {
+        auto h = std::make_unique<mlfma_op_s>();
+        h->device = cfg->device;
+        const std::string e = h->plan.build_dipoles(to_cfg(cfg), to_pw(pw), n, pos, mom);
+        if (!e.empty()) return fail(MLFMA_ERR_ARG, e);
+        *out = h.release();
+        return MLFMA_OK;
+    } catch (const std::exception& e) {
+        return fail(MLFMA_ERR_INTERNAL, e.what());
+    }
+}
+
+int mlfma_create_rwg(const mlfma_config* cfg, const mlfma_planewave* pw, int nv, const double* verts, int nf,
+                     const int* faces, int ne, const int* rwgs, mlfma_handle* out) {
+    if (!cfg || !pw || !verts || !faces || !rwgs || !out) return fail(MLFMA_ERR_ARG, "null argument");
+    try {
+        auto h = std::make_unique<mlfma_op_s>();
+        h->device = cfg->device;
+        const std::string e = h->plan.build_rwg(to_cfg(cfg), to_pw(pw), nv, verts, nf, faces, ne, rwgs);
+        if (!e.empty()) return fail(MLFMA_ERR_ARG, e);
+        *out = h.release();
+        return MLFMA_OK;
+    } catch (const std::exception& e) {
+        return fail(MLFMA_ERR_INTERNAL, e.what());
+    }
+}
+
+int mlfma_setup(mlfma_handle h) {
+    if (!h) return fail(MLFMA_ERR_ARG, "null handle");
+    if (h->dev) return fail(MLFMA_ERR_STATE, "already set up");
+    try {
+        auto dev = std::make_unique<mlfma::DeviceOp>();
+        std::string e = dev->setup(h->plan, h->device);
+        if (!e.empty()) return fail(MLFMA_ERR_CUDA, e);
+        if (cudaMalloc(&h->d_x, sizeof(double2) * h->plan.n) != cudaSuccess ||
+            cudaMalloc(&h->d_y, sizeof(double2) * h->plan.n) != cudaSuccess)
+            return fail(MLFMA_ERR_CUDA, "cudaMalloc failed");
+        h->dev = std::move(dev);
+        h->gmres = std::make_unique<mlfma::Gmres>();
+        return MLFMA_OK;
+    } catch (const std::exception& e) {
+        return fail(MLFMA_ERR_INTERNAL, e.what());
+    }
+}
+
+int mlfma_num_unknowns(mlfma_handle h, int* n) {
+    if (!h || !n) return fail(MLFMA_ERR_ARG, "null argument");
+    *n = h->plan.n;
+    return MLFMA_OK;
+}
+
+int mlfma_get_stats(mlfma_handle h, mlfma_stats* st) {
+    if (!h || !st) return fail(MLFMA_ERR_ARG, "null argument");
+    const mlfma::Plan& p = h->plan;
+    std::memset(st, 0, sizeof(*st));
+    st->num_nodes = static_cast<int>(p.nodes.size());
+    st->num_leaves = static_cast<int>(p.leaves.size());
+    st->max_level = p.max_level;
+    st->num_levels_far = p.max_level >= p.lmin ? p.max_level - p.lmin + 1 : 0;
+    st->list2 = p.n_list2;
+    st->list4 = p.n_list4;
+    st->near_pairs = p.n_near_pairs;
+    st->near_entries = p.near_entries;
+    st->pattern_elems = p.pat_elems;
+    st->device_bytes = h->dev ? h->dev->bytes_allocated() : 0;
+    return MLFMA_OK;
+}
+
+int mlfma_rhs(mlfma_handle h, double* b) {
+    if (!h || !b) return fail(MLFMA_ERR_ARG, "null argument");
+    h->plan.rhs(reinterpret_cast<mlfma::cplx*>(b));
+    return MLFMA_OK;
+}
+
+int mlfma_matvec(mlfma_handle h, const double* x, double* y, int accumulate) {
+    if (!h || !x || !y) return fail(MLFMA_ERR_ARG, "null argument");
+    if (!ready(h)) return fail(MLFMA_ERR_STATE, "mlfma_setup has not run");
+    const size_t bytes = sizeof(double2) * h->plan.n;
+    cudaStream_t s = h->dev->stream();
+    if (cudaSetDevice(h->device) != cudaSuccess) return fail(MLFMA_ERR_CUDA, "cudaSetDevice failed");
+    if (cudaMemcpyAsync(h->d_x, x, bytes, cudaMemcpyHostToDevice, s) != cudaSuccess)
+        return fail(MLFMA_ERR_CUDA, "copy of x failed");
+    if (accumulate && cudaMemcpyAsync(h->d_y, y, bytes, cudaMemcpyHostToDevice, s) != cudaSuccess)
+        return fail(MLFMA_ERR_CUDA, "copy of y failed");
+    std::string e = h->dev->matvec_device(h->d_x, h->d_y, accumulate != 0, s);
+    if (!e.empty()) return fail(MLFMA_ERR_CUDA, e);
+    if (cudaMemcpyAsync(y, h->d_y, bytes, cudaMemcpyDeviceToHost, s) != cudaSuccess)
+        return fail(MLFMA_ERR_CUDA, "copy of y failed");
+    const cudaError_t ce = cudaStreamSynchronize(s);
+    if (ce != cudaSuccess) return fail(MLFMA_ERR_CUDA, cudaGetErrorString(ce));
+    return MLFMA_OK;
+}
+
+int mlfma_matvec_device(mlfma_handle h, const void* d_x, void* d_y, int accumulate, void* stream) {
+    if (!h || !d_x || !d_y) return fail(MLFMA_ERR_ARG, "null argument");
+    if (!ready(h)) return fail(MLFMA_ERR_STATE, "mlfma_setup has not run");
+    std::string e = h->dev->matvec_device(static_cast<const double2*>(d_x), static_cast<double2*>(d_y),
+                                          accumulate != 0, static_cast<cudaStream_t>(stream));
+    if (!e.empty()) return fail(MLFMA_ERR_CUDA, e);
+    return MLFMA_OK;
+}
+
+int mlfma_gmres(mlfma_handle h, const double* b, double* x, const mlfma_solver_opts* opts,
+                mlfma_solve_info* info) {
+    if (!h || !b || !x) return fail(MLFMA_ERR_ARG, "null argument");
+    if (!ready(h)) return fail(MLFMA_ERR_STATE, "mlfma_setup has not run");
+    mlfma::SolveOpts o;
+    if (opts) {
+        o.max_iter = opts->max_iter;
+        o.tol = opts->tol;
+        o.restart = opts->restart;
+        o.ref_givens = opts->ref_givens;
+    }
+    const size_t bytes = sizeof(double2) * h->plan.n;
+    cudaStream_t s = h->dev->stream();
+    cudaSetDevice(h->device);
+    if (cudaMemcpyAsync(h->d_x, b, bytes, cudaMemcpyHostToDevice, s) != cudaSuccess)
+        return fail(MLFMA_ERR_CUDA, "copy of b failed");
+    mlfma::SolveResult r;
+    std::string e = h->gmres->solve(*h->dev, h->d_x, h->d_y, o, &r);
+    if (!e.empty()) return from_msg(e);
+    if (cudaMemcpyAsync(x, h->d_y, bytes, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+        return fail(MLFMA_ERR_CUDA, "copy of x failed");
+    if (info) {
+        info->iterations = r.iterations;
+        info->residual = r.residual;
+        info->true_residual = r.true_residual;
+        info->seconds = r.seconds;
+    }
+    if (!r.converged) return fail(MLFMA_ERR_NOT_CONVERGED, "iteration limit reached");
+    return MLFMA_OK;
+}
+
+int mlfma_time_stages(mlfma_handle h, mlfma_stage_times* t) {
+    if (!h || !t) return fail(MLFMA_ERR_ARG, "null argument");
+    if (!ready(h)) return fail(MLFMA_ERR_STATE, "mlfma_setup has not run");
+    mlfma::StageTimes st{};
+    std::string e = h->dev->time_stages(&st);
+    if (!e.empty()) return fail(MLFMA_ERR_CUDA, e);
+    t->gather = st.gather;
+    t->s2m = st.s2m;
+    t->m2m = st.m2m;
+    t->m2l = st.m2l;
+    t->l2l = st.l2l;
+    t->l2t = st.l2t;
+    t->near_field = st.near;
+    t->finish = st.finish;
+    t->total = st.total;
+    return MLFMA_OK;
+}
+
+int mlfma_get_traffic(mlfma_handle h, mlfma_traffic* t) {
+    if (!h || !t) return fail(MLFMA_ERR_ARG, "null argument");
+    if (!ready(h)) return fail(MLFMA_ERR_STATE, "mlfma_setup has not run");
+    const auto tr = h->dev->traffic();
+    t->s2m = tr.s2m;
+    t->m2m = tr.m2m;
+    t->m2l = tr.m2l;
+    t->l2l = tr.l2l;
+    t->l2t = tr.l2t;
+    t->near_field = tr.near;
+    t->total = tr.total;
+    return MLFMA_OK;
+}
+
+int mlfma_level_info(mlfma_handle h, int level, int* sizes, double* thetas, double* weights, double* phis) {
+    if (!h || !sizes) return fail(MLFMA_ERR_ARG, "null argument");
+    const mlfma::Plan& p = h->plan;
+    if (level < p.lmin || level > p.max_level) return fail(MLFMA_ERR_ARG, "level has no far field");
+    const mlfma::Level& L = p.levels[level];
+    sizes[0] = L.nth;
+    sizes[1] = L.nph;
+    sizes[2] = L.L;
+    if (thetas) std::memcpy(thetas, L.thetas.data(), sizeof(double) * L.nth);
+    if (weights) std::memcpy(weights, L.weights.data(), sizeof(double) * L.nth);
+    if (phis) std::memcpy(phis, L.phis.data(), sizeof(double) * L.nph);
+    return MLFMA_OK;
+}
+
+int mlfma_level_boxes(mlfma_handle h, int level, int* nbox, int* coords) {
+    if (!h || !nbox) return fail(MLFMA_ERR_ARG, "null argument");
+    const mlfma::Plan& p = h->plan;
+    if (level < p.lmin || level > p.max_level) return fail(MLFMA_ERR_ARG, "level has no far field");
+    const mlfma::Level& L = p.levels[level];
+    *nbox = static_cast<int>(L.boxes.size());
+    if (coords)
+        for (size_t b = 0; b < L.boxes.size(); ++b) {
+            const mlfma::Node& nd = p.nodes[L.boxes[b]];
+            coords[3 * b] = nd.ix;
+            coords[3 * b + 1] = nd.iy;
+            coords[3 * b + 2] = nd.iz;
+        }
+    return MLFMA_OK;
+}
+
+int mlfma_level_patterns(mlfma_handle h, int level, int which, double* out, long long count) {
+    if (!h || !out) return fail(MLFMA_ERR_ARG, "null argument");
+    if (!ready(h)) return fail(MLFMA_ERR_STATE, "mlfma_setup has not run");
+    std::string e = h->dev->copy_level(level, which, reinterpret_cast<double2*>(out), count);
+    if (!e.empty()) return fail(MLFMA_ERR_ARG, e);
+    return MLFMA_OK;
+}
+
+int mlfma_level_transl(mlfma_handle h, int level, double* out) {
+    if (!h || !out) return fail(MLFMA_ERR_ARG, "null argument");
+    const mlfma::Plan& p = h->plan;
+    if (level < p.lmin || level > p.max_level) return fail(MLFMA_ERR_ARG, "level has no far field");
+    const mlfma::Level& L = p.levels[level];
+    std::memcpy(out, L.transl.data(), sizeof(double) * 2 * L.transl.size());
+    return MLFMA_OK;
+}
+
+int mlfma_far_leaves(mlfma_handle h, int* count, int* info, int* perm) {
+    if (!h || !count) return fail(MLFMA_ERR_ARG, "null argument");
+    const mlfma::Plan& p = h->plan;
+    *count = static_cast<int>(p.far_leaves.size());
+    if (info)
+        for (size_t i = 0; i < p.far_leaves.size(); ++i) {
+            const mlfma::FarLeaf& f = p.far_leaves[i];
+            info[4 * i] = f.level;
+            info[4 * i + 1] = f.box;
+            info[4 * i + 2] = f.src0;
+            info[4 * i + 3] = f.nsrc;
+        }
+    if (perm) std::memcpy(perm, p.perm.data(), sizeof(int) * p.perm.size());
+    return MLFMA_OK;
+}
+
+int mlfma_rwg_patterns_host(mlfma_handle h, double* out, long long count) {
+    if (!h || !out) return fail(MLFMA_ERR_ARG, "null argument");
+    const mlfma::Plan& p = h->plan;
+    if (p.kind != mlfma::kRwg) return fail(MLFMA_ERR_ARG, "not an RWG operator");
+    if (count < p.pat_elems * 2) return fail(MLFMA_ERR_ARG, "buffer too small");
+    try {
+        std::vector<mlfma::cplx> pat;
+        p.rwg_patterns_host(pat);
+        std::memcpy(out, pat.data(), sizeof(mlfma::cplx) * pat.size());
+    } catch (const std::exception& e) {
+        return fail(MLFMA_ERR_INTERNAL, e.what());
+    }
+    return MLFMA_OK;
+}
+
+int mlfma_destroy(mlfma_handle h) {
+    delete h;
+    return MLFMA_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,56 @@
+// Device GMRES driver (see gmres.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "device.cuh"
+
+namespace mlfma {
+
+struct SolveOpts {
+    int max_iter = 500;
+    double tol = 1e-6;
+    int restart = 0;     // 0: no restart (reference)
+    int ref_givens = 1;  // complex-symmetric rotations of the reference
+};
+
+struct SolveResult {
+    int iterations = 0;
+    double residual = 0;
+    double true_residual = 0;
+    double seconds = 0;
+    bool converged = false;
+};
+
+class Gmres {
+public:
+    Gmres() = default;
+    ~Gmres();
+    Gmres(const Gmres&) = delete;
+    Gmres& operator=(const Gmres&) = delete;
+
+    // b and x are device vectors in the caller's source order.
+    std::string solve(DeviceOp& op, const double2* d_b_user, double2* d_x_user, const SolveOpts& o,
+                      SolveResult* res);
+
+private:
+    std::string ensure(int n, int ncols);
+    void release();
+    std::string norm(const double2* v, cudaStream_t s, double* out);
+    std::string cgs_pass(int ncols, cudaStream_t s, bool add);
+
+    int n_ = 0, cap_ = 0, nchunks_ = 0;
+    double2* Q_ = nullptr;
+    double2* w_ = nullptr;
+    double2* b_ = nullptr;
+    double2* x_ = nullptr;
+    double2* r_ = nullptr;
+    double2* h_ = nullptr;
+    double2* y_ = nullptr;
+    double2* partial_ = nullptr;
+    double* npartial_ = nullptr;
+};
+
+}  // namespace mlfma
