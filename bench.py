@@ -1,0 +1,318 @@
+#!/usr/bin/env python
+"""MLFMA matvec throughput on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Workload: the PEC sphere of radius 2 wavelengths meshed as a level-5
+subdivided icosahedron (20,480 triangles, 30,720 RWG unknowns), 7-point
+triangle quadrature, root box 4 wavelengths, boxes split while they hold more
+than 54 RWGs (every 0.25-wavelength box is a leaf), 3-digit angular sampling,
+6-point interpolation, plain complex FP64.  One step is one MLFMA
+matrix-vector product y = A x on one right-hand side.
+
+`value` is device-resident throughput (x and y already in HBM), timed with
+CUDA events on the launching stream; `e2e` is the same product through the
+public host-buffer call mlfma_matvec, with the host->device copy of x and the
+device->host copy of y (pinned buffers) inside the timed region.  The operator
+reads 0.54 GB per matvec, more than the 126 MB L2, so no flush runs between
+steps.  With N > 1 every rank runs an independent replica of the product
+(there is no data exchange on this path); rank 0 reports N * K / max time.
+
+`--impl reference` times the reference's own CPU code (oracle/_ref, built from
+its sources, single-threaded by construction) on the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+METRIC = "MLFMA matvecs/s, GMRES solve s @1e-4 resid: mixed/batched vs FP64 on 1 B200"
+UNIT = "matvecs/s"
+WORKLOAD = dict(name="rwg_sphere_r2lambda_ico5", kind="rwg", level=5, radius=2.0, root_leng=4.0,
+                max_node_srcs=54, quad_prec=2, digits=3, interp_order=3, over_interp=2.0)
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def make_problem():
+    sys.path.insert(0, HERE)
+    from mlfma_b200 import inputs
+    mesh = inputs.make_icosphere(WORKLOAD["level"], radius=WORKLOAD["radius"])
+    pw = inputs.PlaneWave(amplitude=1.0, pol=(1.0, 0.0, 0.0), khat=(0.0, 0.0, -1.0), wavenum=2.0 * np.pi)
+    return mesh, pw
+
+
+def config_dict(extra=None):
+    c = {"workload": WORKLOAD["name"], "unknowns": 30720, "triangles": 20480,
+         "radius_lambda": WORKLOAD["radius"], "root_box_lambda": WORKLOAD["root_leng"],
+         "max_node_srcs": WORKLOAD["max_node_srcs"], "quadrature": "7-point",
+         "digits": WORKLOAD["digits"], "interp_points": 2 * WORKLOAD["interp_order"],
+         "precision": "complex fp64", "rhs_per_step": 1,
+         "l2": "no flush: operator data read per step 0.54 GB > 126 MB L2"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+# ------------------------------------------------------------------ clocks
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clock and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-f", self.path], stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        try:
+            with open(self.path) as f:
+                for line in f:
+                    p = [v.strip() for v in line.split(",")]
+                    if len(p) < 9:
+                        continue
+                    try:
+                        sm.append(float(p[1]))
+                        smax.append(float(p[2]))
+                    except ValueError:
+                        continue
+                    for nm, v in zip(names, p[5:9]):
+                        if v.lower().startswith("active"):
+                            reasons.add(nm)
+            os.unlink(self.path)
+        except OSError:
+            pass
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+# ------------------------------------------------------------------ reference arm
+
+def run_reference(steps: int, warmup: int, quiet=False) -> dict:
+    sys.path.insert(0, HERE)
+    from oracle import ref_lib
+    mesh, pw = make_problem()
+    t0 = time.perf_counter()
+    P = ref_lib.RefProblem("rwg", mesh, pw, digits=WORKLOAD["digits"], interp_order=WORKLOAD["interp_order"],
+                           over_interp=WORKLOAD["over_interp"], root_leng=WORKLOAD["root_leng"],
+                           max_node_srcs=WORKLOAD["max_node_srcs"], quad_prec=WORKLOAD["quad_prec"])
+    setup_s = time.perf_counter() - t0
+    x = np.random.default_rng(7).standard_normal(P.n) + 1j * np.random.default_rng(8).standard_normal(P.n)
+    for _ in range(warmup):
+        P.matvec(x)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        P.matvec(x)
+    dt = time.perf_counter() - t0
+    return {"value": steps / dt, "ms_per_step": dt / steps * 1e3, "setup_s": setup_s, "steps": steps}
+
+
+# ------------------------------------------------------------------ our arm
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-steps", type=int, default=3)
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        r = run_reference(args.steps, max(args.warmup, 0))
+        line = {"metric": METRIC, "value": r["value"], "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms_per_step"],
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
+                "data": "synthetic (seeded icosphere mesh)",
+                "config": config_dict({"reference_setup_s": r["setup_s"]}),
+                "cpu_baseline": {"value": r["value"], "unit": UNIT, "cores": 1, "kind": "reference",
+                                 "sample": f"{args.steps} full matvecs of the workload after {args.warmup} "
+                                           "warm-up matvecs; the reference is single-threaded"},
+                "e2e": {"value": r["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return 0
+
+    if args.warmup < 3:
+        print("warm-up must be >= 3", file=sys.stderr)
+        args.warmup = 3
+    import torch
+    import torch.distributed as dist
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+
+    # CPU baseline in a child process (rank 0, N = 1), overlapping GPU setup.
+    cpu_proc = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu_proc = subprocess.Popen([sys.executable, os.path.abspath(__file__), "--impl", "reference",
+                                     "--steps", str(args.cpu_steps), "--warmup", "1"],
+                                    stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+
+    sys.path.insert(0, HERE)
+    from mlfma_b200 import MLFMA, default_config
+    mesh, pw = make_problem()
+    cfg = default_config(quad_prec=WORKLOAD["quad_prec"], digits=WORKLOAD["digits"],
+                         interp_order=WORKLOAD["interp_order"], over_interp=WORKLOAD["over_interp"],
+                         root_leng=WORKLOAD["root_leng"], max_node_srcs=WORKLOAD["max_node_srcs"],
+                         device=local_rank)
+    t0 = time.perf_counter()
+    op = MLFMA.rwg(mesh, pw, config=cfg)
+    op.setup()
+    setup_s = time.perf_counter() - t0
+    st = op.stats()
+    n = op.n
+    g = torch.Generator(device="cpu").manual_seed(1234 + rank)
+    xh = torch.complex(torch.randn(n, generator=g, dtype=torch.float64), torch.randn(n, generator=g, dtype=torch.float64))
+    x = xh.to(dev)
+    y = torch.zeros(n, dtype=torch.complex128, device=dev)
+    torch.cuda.synchronize(dev)
+    # Every product runs on the operator's own stream; events are recorded there.
+    stream = torch.cuda.ExternalStream(op.stream(), device=dev)
+
+    def step():
+        op.matvec_device(x.data_ptr(), y.data_ptr(), False, stream.cuda_stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    time.sleep(0.3)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    ms = e0.elapsed_time(e1) / args.steps
+
+    # End to end through the public host-buffer call (pinned buffers).
+    xp = torch.empty(n, dtype=torch.complex128, pin_memory=True)
+    yp = torch.empty(n, dtype=torch.complex128, pin_memory=True)
+    xp.copy_(xh)
+    xn, yn = xp.numpy(), yp.numpy()
+    ostream = stream
+    for _ in range(args.warmup):
+        op.matvec(xn, out=yn)
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record(ostream)
+    for _ in range(args.steps):
+        op.matvec(xn, out=yn)
+    f1.record(ostream)
+    torch.cuda.synchronize(dev)
+    e2e_ms = f0.elapsed_time(f1) / args.steps
+    clk = clocks.stop()
+
+    # Per-stage device times (stages launched back to back on the operator's stream).
+    stages = [op.stage_times() for _ in range(max(5, min(args.steps, 50)))]
+    avg = {k: float(np.mean([s[k] for s in stages])) for k in stages[0]}
+    traffic = op.traffic()
+    stage_keys = ["s2m", "m2m", "m2l", "l2l", "l2t", "near_field"]
+    dom = max(stage_keys, key=lambda k: avg[k])
+    peaks = {}
+    try:
+        with open(os.path.join(HERE, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except OSError:
+        pass
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    achieved = traffic[dom] / (avg[dom] * 1e-3) / 1e9
+    ncu_traffic = None
+    try:
+        with open(os.path.join(HERE, "profiles", "traffic.json")) as f:
+            ncu_traffic = json.load(f).get(WORKLOAD["name"], {}).get(dom)
+    except (OSError, ValueError):
+        pass
+
+    if world > 1:
+        t = torch.tensor([ms, e2e_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, e2e_ms = float(t[0]), float(t[1])
+
+    if rank == 0:
+        cpu = None
+        if cpu_proc is not None:
+            try:
+                out, _ = cpu_proc.communicate(timeout=900)
+                r = json.loads(out.strip().splitlines()[-1])
+                cpu = {"value": r["value"], "unit": UNIT, "cores": 1, "kind": "reference",
+                       "sample": f"{args.cpu_steps} full matvecs of this workload by the reference built from its "
+                                 f"sources (oracle/_ref), after 1 warm-up matvec and a "
+                                 f"{r['config'].get('reference_setup_s', 0):.0f} s setup"}
+            except Exception as e:  # noqa: BLE001
+                cpu = {"value": None, "unit": UNIT, "cores": 1, "kind": "reference", "sample": f"failed: {e}"}
+        launches = int(st.get("launches_per_matvec", 0)) * args.steps
+        line = {
+            "metric": METRIC, "value": world * 1000.0 / ms, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic (seeded icosphere mesh)",
+            "config": config_dict({"parallelism": f"replicas{world}", "levels": st["max_level"],
+                                   "near_entries": st["near_entries"], "setup_s": setup_s}),
+            "e2e": {"value": world * 1000.0 / e2e_ms, "unit": UNIT, "h2d_bytes_per_step": n * 16,
+                    "d2h_bytes_per_step": n * 16},
+            "gpu_launches": launches,
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                         "frac": achieved / hbm_peak, "peak_source": peak_src,
+                         "traffic": ncu_traffic, "algorithmic_bytes": traffic[dom],
+                         "avg_launch_ms": avg[dom]},
+            "stage_ms": avg,
+            "matvec_alg_bytes": traffic["total"],
+            "clocks": clk,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    op.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

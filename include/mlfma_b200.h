@@ -64,6 +64,7 @@ typedef struct {
     int num_nodes, num_leaves, max_level, num_levels_far;
     long long list2, list4, near_pairs, near_entries, pattern_elems;
     long long device_bytes;
+    int launches_per_matvec;  /* kernels this library launches per matvec */
 } mlfma_stats;
 
 /* Per-stage device time of one matvec, ms (the reference's ClockTimes stages,
@@ -133,6 +134,10 @@ int mlfma_matvec_device(mlfma_handle h, const void* d_x, void* d_y, int accumula
  * src/solver.cpp:116-146).  x is overwritten (initial guess 0). */
 int mlfma_gmres(mlfma_handle h, const double* b, double* x, const mlfma_solver_opts* opts,
                 mlfma_solve_info* info);
+
+/* The handle's own CUDA stream (cudaStream_t as void*), on which mlfma_matvec
+ * and mlfma_gmres run; callers may record events on it. */
+int mlfma_get_stream(mlfma_handle h, void** stream);
 
 /* CUDA-event time of each stage of one matvec on the handle's stream. */
 int mlfma_time_stages(mlfma_handle h, mlfma_stage_times* t);

@@ -196,6 +196,11 @@ class MLFMA:
             check(code)
         return x, SolveResult(info.iterations, info.residual, info.true_residual, info.seconds, converged)
 
+    def stream(self) -> int:
+        s = ctypes.c_void_p()
+        check(lib().mlfma_get_stream(self._h, ctypes.byref(s)))
+        return s.value or 0
+
     def stage_times(self) -> dict:
         t = StageTimes()
         check(lib().mlfma_time_stages(self._h, ctypes.byref(t)))

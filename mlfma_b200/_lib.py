@@ -40,7 +40,7 @@ class Stats(ctypes.Structure):
                 ("num_levels_far", ctypes.c_int), ("list2", ctypes.c_longlong),
                 ("list4", ctypes.c_longlong), ("near_pairs", ctypes.c_longlong),
                 ("near_entries", ctypes.c_longlong), ("pattern_elems", ctypes.c_longlong),
-                ("device_bytes", ctypes.c_longlong)]
+                ("device_bytes", ctypes.c_longlong), ("launches_per_matvec", ctypes.c_int)]
 
 
 class StageTimes(ctypes.Structure):
@@ -78,6 +78,7 @@ SIGNATURES = {
                                            ctypes.c_void_p]),
     "mlfma_gmres": (ctypes.c_int, [ctypes.c_void_p, _dp, _dp, ctypes.POINTER(SolverOpts),
                                    ctypes.POINTER(SolveInfo)]),
+    "mlfma_get_stream": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]),
     "mlfma_time_stages": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(StageTimes)]),
     "mlfma_get_traffic": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Traffic)]),
     "mlfma_level_info": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _ip, _dp, _dp, _dp]),

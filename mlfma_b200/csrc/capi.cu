@@ -156,6 +156,7 @@ int mlfma_get_stats(mlfma_handle h, mlfma_stats* st) {
     st->near_entries = p.near_entries;
     st->pattern_elems = p.pat_elems;
     st->device_bytes = h->dev ? h->dev->bytes_allocated() : 0;
+    st->launches_per_matvec = h->dev ? h->dev->launches_per_matvec() : 0;
     return MLFMA_OK;
 }
 
@@ -222,6 +223,13 @@ int mlfma_gmres(mlfma_handle h, const double* b, double* x, const mlfma_solver_o
         info->seconds = r.seconds;
     }
     if (!r.converged) return fail(MLFMA_ERR_NOT_CONVERGED, "iteration limit reached");
+    return MLFMA_OK;
+}
+
+int mlfma_get_stream(mlfma_handle h, void** stream) {
+    if (!h || !stream) return fail(MLFMA_ERR_ARG, "null argument");
+    if (!ready(h)) return fail(MLFMA_ERR_STATE, "mlfma_setup has not run");
+    *stream = static_cast<void*>(h->dev->stream());
     return MLFMA_OK;
 }
 

@@ -96,6 +96,7 @@ public:
     const int* perm() const { return perm_; }
     int device() const { return device_; }
     long long bytes_allocated() const { return bytes_; }
+    int launches_per_matvec() const;
     const std::vector<DevFarLeaf>& far_leaves_host() const { return h_leaves_; }
 
     // Diagnostic copies of per-level patterns (level, which: 0 outgoing, 1 local).

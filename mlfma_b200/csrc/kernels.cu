@@ -655,6 +655,19 @@ std::string DeviceOp::setup(const Plan& plan, int device) {
     }
 }
 
+int DeviceOp::launches_per_matvec() const {
+    int n = 2;  // gather + finish
+    if (n_leaves_) {
+        n += 2;  // S2M + L2T
+        for (int p = lv_.lmin; p < lv_.lmax; ++p)
+            if (trans_[p].npar) n += 2;  // M2M + L2L
+        for (int l = lv_.lmin; l <= lv_.lmax; ++l)
+            if (m2l_nbox_[l]) n += 1;
+    }
+    if (n_near_blocks_) n += 1;
+    return n;
+}
+
 int DeviceOp::m2m_rows(int nth, int nph) {
     const int rows = (kM2MThreads * kM2MOut) / std::max(nph, 1);
     return std::max(1, std::min(nth, rows));

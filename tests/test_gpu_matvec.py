@@ -1,0 +1,115 @@
+"""Parity of the CUDA matvec with the reference: golden fixtures, the reference
+library on fresh seeded problems, and the numpy oracle; plus size-independent
+properties at the benchmark size.
+
+Tolerance: 1e-10 relative (the plain-FP64 contract), for dipoles and RWGs."""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import needs_ref
+from mlfma_b200 import MLFMA, inputs
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+PW = inputs.PlaneWave()
+TOL = 1e-10
+
+
+def rel(a, b):
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+def cvec(n, seed):
+    r = np.random.default_rng(seed)
+    return r.standard_normal(n) + 1j * r.standard_normal(n)
+
+
+@pytest.mark.parametrize("name", ["dipole_n600", "dipole_n2000", "rwg_ico2_r1", "rwg_ico3_r1"])
+def test_matvec_matches_golden(cuda_device, name):
+    import make_golden as mg
+    case = mg.CASES[name]
+    f = np.load(os.path.join(GOLD, name + ".npz"))
+    g = mg.geometry(case)
+    op = (MLFMA.dipoles if case["kind"] == "dipole" else MLFMA.rwg)(g, PW, max_node_srcs=case["max_node_srcs"])
+    op.setup()
+    assert rel(op.matvec(f["x"]), f["y"]) <= TOL
+    op.close()
+
+
+CASES = [("dipole", dict(n=3000, seed=31), 16), ("dipole", dict(n=8192, seed=1), 64),
+         ("rwg", dict(level=3, radius=1.0), 16), ("rwg", dict(level=4, radius=1.5), 24)]
+
+
+def build(kind, geo, mns):
+    from oracle import ref_lib
+    g = inputs.make_dipoles(geo["n"], seed=geo["seed"]) if kind == "dipole" else \
+        inputs.make_icosphere(geo["level"], radius=geo["radius"])
+    op = (MLFMA.dipoles if kind == "dipole" else MLFMA.rwg)(g, PW, max_node_srcs=mns).setup()
+    return op, ref_lib.RefProblem(kind, g, PW, max_node_srcs=mns)
+
+
+@needs_ref
+@pytest.mark.parametrize("kind,geo,mns", CASES)
+def test_matvec_matches_reference(cuda_device, kind, geo, mns):
+    op, P = build(kind, geo, mns)
+    x = cvec(op.n, 5)
+    assert rel(op.matvec(x), P.matvec(x)) <= TOL
+    # state carried between products (the reference's stale-local rule) stays in step
+    x2 = cvec(op.n, 6)
+    assert rel(op.matvec(x2), P.matvec(x2)) <= TOL
+    op.close()
+
+
+def test_matvec_matches_numpy_oracle(cuda_device):
+    from oracle import mlfma_oracle as O
+    d = inputs.make_dipoles(1800, seed=8)
+    op = MLFMA.dipoles(d, PW, max_node_srcs=20).setup()
+    orc = O.Oracle(O.DipoleSources(d.pos, d.mom, PW), max_node_srcs=20)
+    x = cvec(op.n, 9)
+    assert rel(op.matvec(x), orc.matvec(x)) <= 1e-12
+    op.close()
+
+
+@pytest.fixture(scope="module")
+def bench_op():
+    m = inputs.make_icosphere(5, radius=2.0)
+    op = MLFMA.rwg(m, PW, max_node_srcs=54).setup()
+    yield op
+    op.close()
+
+
+def test_linearity_at_benchmark_size(cuda_device, bench_op):
+    op = bench_op
+    x1, x2 = cvec(op.n, 1), cvec(op.n, 2)
+    a, b = 0.3 - 1.1j, -2.0 + 0.5j
+    y = op.matvec(a * x1 + b * x2)
+    assert rel(y, a * op.matvec(x1) + b * op.matvec(x2)) <= 1e-13
+
+
+def test_accumulate_and_device_pointer_api(cuda_device, bench_op):
+    import torch
+    op = bench_op
+    x, y0 = cvec(op.n, 3), cvec(op.n, 4)
+    ax = op.matvec(x)
+    acc = op.matvec(x, accumulate=True, out=y0.copy())
+    assert rel(acc, y0 + ax) <= 1e-14
+    xd = torch.from_numpy(x).cuda()
+    yd = torch.zeros_like(xd)
+    op.matvec_device(xd.data_ptr(), yd.data_ptr(), False, torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    assert rel(yd.cpu().numpy(), ax) <= 1e-14
+
+
+def test_repeatable(cuda_device, bench_op):
+    op = bench_op
+    x = cvec(op.n, 7)
+    assert rel(op.matvec(x), op.matvec(x)) <= 1e-14
+
+
+def test_stage_times_and_traffic(cuda_device, bench_op):
+    t = bench_op.stage_times()
+    assert t["total"] > 0 and all(t[k] >= 0 for k in t)
+    tr = bench_op.traffic()
+    assert tr["total"] > 4e8  # ~0.54 GB of operator data per matvec
