@@ -127,7 +127,10 @@ int mlfma_rhs(mlfma_handle h, double* b);
 int mlfma_matvec(mlfma_handle h, const double* x, double* y, int accumulate);
 
 /* Same on device buffers (cudaStream_t passed as void*, NULL = handle's stream).
- * Asynchronous with respect to the host. */
+ * Asynchronous with respect to the host.  The product runs as one CUDA graph
+ * (captured on the first call) between a gather and a scatter kernel, using
+ * the handle's internal work buffers: products on one handle must not overlap
+ * on the GPU (issue them on one stream, or order the streams). */
 int mlfma_matvec_device(mlfma_handle h, const void* d_x, void* d_y, int accumulate, void* stream);
 
 /* Solve A x = b with GMRES on the device; b and x host buffers (Solver::solve,

@@ -37,8 +37,11 @@ struct DevLevels {
     int ref_compat;
 };
 
+// Stencil rows padded to a fixed width (padding entries have coefficient 0):
+// entry k of row r is at r * width + k.  The sign of a pole-reflected tap is
+// folded into its coefficient.
 struct DevStencil {
-    const int* ptr;
+    int width;
     const int* src;
     const int* refl;
     const double* coef;
@@ -63,6 +66,11 @@ struct DevNearBlock {
     int row0, nrow, col0, ncol;
     long long off;
     int self, pad;
+};
+
+struct DevNearRow {
+    int row0, nrow, ncol, pad;
+    long long off, col_off;
 };
 
 struct StageTimes {
@@ -121,12 +129,30 @@ private:
     long long bytes_ = 0;
 
     static int m2m_rows(int nth, int nph);
+    void stage_s2m(const double2* xt, cudaStream_t s);
+    void stage_m2m(cudaStream_t s);
+    void stage_m2l(cudaStream_t s);
+    void stage_l2l(cudaStream_t s);
+    void stage_l2t(cudaStream_t s);
+    void enqueue_core(cudaStream_t s);   // xt_ -> yfar_, ynear_
+    std::string ensure_graph();
+
+    cudaGraph_t graph_ = nullptr;
+    cudaGraphExec_t graph_exec_ = nullptr;
+    bool use_graph_ = true;
 
     DevLevels lv_{};
     DevLevel* lv_dev_ = nullptr;        // device copy of lv_.lv
     std::vector<DevTrans> trans_;       // index = parent level
-    std::vector<int*> m2l_boxes_;       // per level: target boxes to process
-    std::vector<int> m2l_nbox_;
+    int4* m2l_items_ = nullptr;         // (level, box, first direction, count)
+    int n_m2l_items_ = 0;
+    std::vector<int2*> l2l_pairs_;      // per parent level: (parent, child entry)
+    std::vector<int> n_l2l_pairs_;
+    int4* s2m_items_ = nullptr;          // (leaf, first element, element count)
+    int n_s2m_items_ = 0;
+    int4* l2t_items_ = nullptr;          // (leaf, first source, source count)
+    int n_l2t_items_ = 0;
+    int max_src_ = 0;                    // largest far leaf
     DevFarLeaf* leaves_ = nullptr;
     std::vector<DevFarLeaf> h_leaves_;
     int n_leaves_ = 0;
@@ -135,6 +161,11 @@ private:
     int n_near_blocks_ = 0;
     double2* near_z_ = nullptr;
     long long near_entries_ = 0;
+    DevNearRow* near_rows_ = nullptr;   // block rows (device storage of the near field)
+    int n_near_rows_ = 0;
+    int* near_cols_ = nullptr;
+    int4* near_items_ = nullptr;        // (row block, first row, row count)
+    int n_near_items_ = 0;
     int* perm_ = nullptr;
     double2* xt_ = nullptr;    // tree-ordered input
     double2* yfar_ = nullptr;  // tree-ordered far result (before C k)

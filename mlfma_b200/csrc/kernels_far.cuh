@@ -1,0 +1,246 @@
+// Far-field kernels of the MLFMA matvec (FP64): aggregation (S2M),
+// interpolation (M2M), translation (M2L), anterpolation (L2L) and
+// disaggregation (L2T).  Included once, by kernels.cu.
+//
+// Layout: per level, patterns are [box][direction][2 components] complex;
+// element e = 2*direction + component runs contiguously, so a box's
+// pattern is one contiguous run of 2*ndir double2 values.
+#pragma once
+
+#include "device.cuh"
+#include "zmath.cuh"
+
+namespace mlfma {
+namespace {
+
+// ------------------------------------------------------------ S2M
+// a_B[e] = sum_n x_n R_n[e]  (Leaf::buildMpoleCoeffs, src/fmm/leaf.cpp:212-230).
+// One block per work item (leaf, run of at most kS2MThreads elements), all leaf
+// levels in one launch; one thread per element e (direction, component), so
+// every pattern row is read once with 16-byte coalesced loads; eight sources
+// are in flight per thread.
+constexpr int kS2MThreads = 352;
+constexpr int kL2TThreads = 256;
+constexpr int kL2TSrcPerBlock = kL2TThreads / 32;
+
+__global__ void __launch_bounds__(kS2MThreads)
+k_s2m(const DevLevel* __restrict__ lvs, const int4* __restrict__ items, const DevFarLeaf* __restrict__ leaves,
+      const double2* __restrict__ pat, const double2* __restrict__ x) {
+    extern __shared__ double2 xs[];
+    const int4 it = items[blockIdx.x];  // leaf, first element, element count
+    const DevFarLeaf lf = leaves[it.x];
+    const int ne = 2 * lvs[lf.level].ndir;
+    double2* A = lvs[lf.level].A + static_cast<size_t>(lf.box) * ne;
+    for (int i = threadIdx.x; i < lf.nsrc; i += blockDim.x) xs[i] = x[lf.src0 + i];
+    __syncthreads();
+    if (static_cast<int>(threadIdx.x) >= it.z) return;
+    const int e = it.y + threadIdx.x;
+    const double2* r = pat + lf.pat_off * 2 + e;
+    double2 a0 = z0(), a1 = z0(), a2 = z0(), a3 = z0();
+    int s = 0;
+    for (; s + 8 <= lf.nsrc; s += 8) {
+        double2 v[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) v[u] = ldg_stream(r + static_cast<size_t>(s + u) * ne);
+        a0 = cfma(xs[s], v[0], a0);
+        a1 = cfma(xs[s + 1], v[1], a1);
+        a2 = cfma(xs[s + 2], v[2], a2);
+        a3 = cfma(xs[s + 3], v[3], a3);
+        a0 = cfma(xs[s + 4], v[4], a0);
+        a1 = cfma(xs[s + 5], v[5], a1);
+        a2 = cfma(xs[s + 6], v[6], a2);
+        a3 = cfma(xs[s + 7], v[7], a3);
+    }
+    for (; s < lf.nsrc; ++s) a0 = cfma(xs[s], ldg_stream(r + static_cast<size_t>(s) * ne), a0);
+    A[e] = cadd(cadd(a0, a1), cadd(a2, a3));
+}
+
+// ------------------------------------------------------------ L2T
+// y_m = sum_e conj(R_m[e]) b_B[e]  (Leaf::evalFarSols, src/fmm/leaf.cpp:257-280;
+// C k is applied when the result is written out).  One block per work item
+// (leaf, run of up to eight sources), one warp per source, eight loads in
+// flight per lane.
+__global__ void __launch_bounds__(kL2TThreads)
+k_l2t(const DevLevel* __restrict__ lvs, const int4* __restrict__ items, const DevFarLeaf* __restrict__ leaves,
+      const double2* __restrict__ pat, double2* __restrict__ yfar) {
+    const int4 it = items[blockIdx.x];  // leaf, first source, source count
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (warp >= it.z) return;
+    const DevFarLeaf lf = leaves[it.x];
+    const int ndir = lvs[lf.level].ndir, ne = 2 * ndir;
+    const double2* Bb = lvs[lf.level].B + static_cast<size_t>(lf.box) * ne;
+    const int s = it.y + warp;
+    const double2* r = pat + (lf.pat_off + static_cast<long long>(s) * ndir) * 2;
+    double2 a0 = z0(), a1 = z0(), a2 = z0(), a3 = z0();
+    int e = lane;
+    for (; e + 224 < ne; e += 256) {
+        double2 v[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) v[u] = ldg_stream(r + e + 32 * u);
+        a0 = cjfma(v[0], Bb[e], a0);
+        a1 = cjfma(v[1], Bb[e + 32], a1);
+        a2 = cjfma(v[2], Bb[e + 64], a2);
+        a3 = cjfma(v[3], Bb[e + 96], a3);
+        a0 = cjfma(v[4], Bb[e + 128], a0);
+        a1 = cjfma(v[5], Bb[e + 160], a1);
+        a2 = cjfma(v[6], Bb[e + 192], a2);
+        a3 = cjfma(v[7], Bb[e + 224], a3);
+    }
+    for (; e < ne; e += 32) a0 = cjfma(ldg_stream(r + e), Bb[e], a0);
+    const double2 acc = warp_sum(cadd(cadd(a0, a1), cadd(a2, a3)));
+    if (lane == 0) yfar[lf.src0 + s] = acc;
+}
+
+// ------------------------------------------------------------ M2M
+// Parent outgoing pattern = sum over non-empty children of Interp[shift(child)]:
+// shift on the child grid, theta pass with pole reflection, periodic phi pass
+// (Stem::buildMpoleCoeffs and addInterpCoeffs, src/fmm/stem.cpp:72-184).
+// Block = (parent, tile of `rows` parent theta rows).  Phase 1 computes the
+// theta pass of every child into shared memory at once (all loads
+// independent); phase 2 forms each parent output from the children's rows.
+__global__ void __launch_bounds__(128)
+k_m2m(const DevLevel* __restrict__ lvs, DevTrans T, int rows) {
+    extern __shared__ double2 sm[];
+    const int par = blockIdx.x;
+    const DevLevel P = lvs[T.plevel];
+    const DevLevel C = lvs[T.plevel + 1];
+    const int nph = P.nph, mph = C.nph, halfm = C.nph / 2;
+    const int r0 = blockIdx.y * rows;
+    const int nrow = min(P.nth, r0 + rows) - r0;
+    if (nrow <= 0) return;
+    const int c0 = T.child_ptr[par], nch = T.child_ptr[par + 1] - c0;
+    const int per_child = nrow * mph;
+    for (int it = threadIdx.x; it < nch * per_child; it += blockDim.x) {
+        const int c = it / per_child, e = it - c * per_child;
+        const int jr = e / mph, iph = e - jr * mph;
+        const int jth = r0 + jr;
+        const double2* Ac = C.A + static_cast<size_t>(T.child_box[c0 + c]) * C.ndir * 2;
+        const double2* sh = C.shift_up + static_cast<size_t>(T.child_oct[c0 + c]) * C.ndir;
+        double2 v0 = z0(), v1 = z0();
+        const int w = T.up_th.width;
+        for (int q = jth * w; q < jth * w + w; ++q) {
+            const bool rf = T.up_th.refl[q];
+            const int sp = rf ? (iph < halfm ? iph + halfm : iph - halfm) : iph;
+            const double cf = T.up_th.coef[q];
+            const int d = T.up_th.src[q] * mph + sp;
+            const double2 ph = sh[d];
+            v0 = cfma(make_double2(cf, 0.0), cmul(ph, Ac[2 * d]), v0);
+            v1 = cfma(make_double2(cf, 0.0), cmul(ph, Ac[2 * d + 1]), v1);
+        }
+        sm[2 * it] = v0;
+        sm[2 * it + 1] = v1;
+    }
+    __syncthreads();
+    double2* Ap = P.A + (static_cast<size_t>(T.par_box[par]) * P.ndir + static_cast<size_t>(r0) * nph) * 2;
+    for (int o = threadIdx.x; o < nrow * nph; o += blockDim.x) {
+        const int jr = o / nph, jph = o - jr * nph;
+        double2 a0 = z0(), a1 = z0();
+        const int w = T.up_ph.width;
+        for (int c = 0; c < nch; ++c) {
+            const double2* row = sm + (static_cast<size_t>(c) * per_child + static_cast<size_t>(jr) * mph) * 2;
+            for (int q = jph * w; q < jph * w + w; ++q) {
+                const int s = T.up_ph.src[q];
+                const double cf = T.up_ph.coef[q];
+                a0 = cadd(a0, cscale(cf, row[2 * s]));
+                a1 = cadd(a1, cscale(cf, row[2 * s + 1]));
+            }
+        }
+        Ap[2 * o] = a0;
+        Ap[2 * o + 1] = a1;
+    }
+}
+
+// ------------------------------------------------------------ M2L
+// b_B = w_theta (2 pi / nph) sum_{S in list 2} T[c_B - c_S] a_S
+// (Node::buildMpoleToLocalCoeffs, src/fmm/node.cpp:105-134).  One block per
+// (level, box, direction chunk) item, all levels in one launch; two list
+// entries in flight per thread.
+__global__ void __launch_bounds__(128)
+k_m2l(const DevLevel* __restrict__ lvs, const int4* __restrict__ items, int zero_empty) {
+    const int4 it = items[blockIdx.x];  // level, box, first direction, count
+    if (static_cast<int>(threadIdx.x) >= it.w) return;
+    const DevLevel lv = lvs[it.x];
+    const int b = it.y, d = it.z + threadIdx.x, ndir = lv.ndir;
+    const int p0 = lv.m2l_ptr[b], p1 = lv.m2l_ptr[b + 1];
+    double2* Bo = lv.B + (static_cast<size_t>(b) * ndir + d) * 2;
+    if (p0 == p1) {
+        if (zero_empty) { Bo[0] = z0(); Bo[1] = z0(); }
+        return;
+    }
+    double2 a0 = z0(), a1 = z0(), c0 = z0(), c1 = z0();
+    int p = p0;
+    for (; p + 2 <= p1; p += 2) {
+        const int s0 = lv.m2l_src[p], o0 = lv.m2l_off[p];
+        const int s1 = lv.m2l_src[p + 1], o1 = lv.m2l_off[p + 1];
+        const double2 t0 = lv.transl[static_cast<size_t>(o0) * ndir + d];
+        const double2 t1 = lv.transl[static_cast<size_t>(o1) * ndir + d];
+        const double2* A0 = lv.A + (static_cast<size_t>(s0) * ndir + d) * 2;
+        const double2* A1 = lv.A + (static_cast<size_t>(s1) * ndir + d) * 2;
+        const double2 x00 = A0[0], x01 = A0[1], x10 = A1[0], x11 = A1[1];
+        a0 = cfma(t0, x00, a0);
+        a1 = cfma(t0, x01, a1);
+        c0 = cfma(t1, x10, c0);
+        c1 = cfma(t1, x11, c1);
+    }
+    if (p < p1) {
+        const int s0 = lv.m2l_src[p], o0 = lv.m2l_off[p];
+        const double2 t0 = lv.transl[static_cast<size_t>(o0) * ndir + d];
+        const double2* A0 = lv.A + (static_cast<size_t>(s0) * ndir + d) * 2;
+        a0 = cfma(t0, A0[0], a0);
+        a1 = cfma(t0, A0[1], a1);
+    }
+    const double w = lv.w[d];
+    Bo[0] = cscale(w, cadd(a0, c0));
+    Bo[1] = cscale(w, cadd(a1, c1));
+}
+
+// ------------------------------------------------------------ L2L
+// child local += Anterp[shift(parent local)]: shift on the parent grid, then
+// the transposed phi pass, then the transposed theta pass with pole
+// reflection (Stem::getShiftedLocalCoeffs and addAnterpCoeffs,
+// src/fmm/stem.cpp:109-244).  One block per (parent, child) pair; the
+// pair list already omits parents that pass nothing down.
+__global__ void __launch_bounds__(256)
+k_l2l(const DevLevel* __restrict__ lvs, DevTrans T, const int2* __restrict__ pairs) {
+    extern __shared__ double2 sm[];
+    const int2 pc = pairs[blockIdx.x];  // parent index, child entry
+    const DevLevel P = lvs[T.plevel];
+    const DevLevel C = lvs[T.plevel + 1];
+    const int pth = P.nth, pph = P.nph, cth = C.nth, cph = C.nph, halfc = C.nph / 2;
+    const double2* Bp = P.B + static_cast<size_t>(T.par_box[pc.x]) * P.ndir * 2;
+    const double2* sh = P.shift_down + static_cast<size_t>(T.child_oct[pc.y]) * P.ndir;
+    for (int e = threadIdx.x; e < pth * cph; e += blockDim.x) {
+        const int ith = e / cph, jph = e - ith * cph;
+        double2 v0 = z0(), v1 = z0();
+        const int w = T.dn_ph.width;
+        for (int q = jph * w; q < jph * w + w; ++q) {
+            const int d = ith * pph + T.dn_ph.src[q];
+            const double cf = T.dn_ph.coef[q];
+            const double2 ph = sh[d];
+            v0 = cfma(make_double2(cf, 0.0), cmul(ph, Bp[2 * d]), v0);
+            v1 = cfma(make_double2(cf, 0.0), cmul(ph, Bp[2 * d + 1]), v1);
+        }
+        sm[2 * e] = v0;
+        sm[2 * e + 1] = v1;
+    }
+    __syncthreads();
+    double2* Bc = C.B + static_cast<size_t>(T.child_box[pc.y]) * C.ndir * 2;
+    for (int e = threadIdx.x; e < cth * cph; e += blockDim.x) {
+        const int jth = e / cph, jph = e - jth * cph;
+        double2 v0 = z0(), v1 = z0();
+        const int w = T.dn_th.width;
+        for (int q = jth * w; q < jth * w + w; ++q) {
+            const bool rf = T.dn_th.refl[q];
+            const int sp = rf ? (jph < halfc ? jph + halfc : jph - halfc) : jph;
+            const double cf = T.dn_th.coef[q];
+            const double2* row = sm + (static_cast<size_t>(T.dn_th.src[q]) * cph + sp) * 2;
+            v0 = cadd(v0, cscale(cf, row[0]));
+            v1 = cadd(v1, cscale(cf, row[1]));
+        }
+        Bc[2 * e] = cadd(Bc[2 * e], v0);
+        Bc[2 * e + 1] = cadd(Bc[2 * e + 1], v1);
+    }
+}
+
+}  // namespace
+}  // namespace mlfma

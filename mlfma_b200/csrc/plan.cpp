@@ -915,6 +915,38 @@ void Plan::build_near_plan() {
         const Node& A = nodes[a];
         add(A.src_begin, A.src_count, A.src_begin, A.src_count, 1);
     }
+
+    // Block rows: every stored block in both orientations.
+    std::vector<int> leaf_of(n, -1);  // tree slot -> leaf node
+    for (int a : leaves)
+        for (int s = 0; s < nodes[a].src_count; ++s) leaf_of[nodes[a].src_begin + s] = a;
+    std::unordered_map<int, std::vector<std::pair<int, int>>> ranges;  // leaf -> column ranges
+    for (const NearBlock& b : near_blocks) {
+        const int ra = leaf_of[b.row0];
+        ranges[ra].emplace_back(b.col0, b.ncol);
+        if (b.self) continue;
+        // transpose: every leaf holding rows of the column range sees the row range
+        for (int s = b.col0; s < b.col0 + b.ncol;) {
+            const int lb = leaf_of[s];
+            ranges[lb].emplace_back(b.row0, b.nrow);
+            s = nodes[lb].src_begin + nodes[lb].src_count;
+        }
+    }
+    near_rows.clear();
+    near_cols.clear();
+    near_row_entries = 0;
+    for (int a : leaves) {
+        const Node& A = nodes[a];
+        if (A.src_count == 0) continue;
+        auto it = ranges.find(a);
+        if (it == ranges.end()) continue;
+        NearRow r{A.src_begin, A.src_count, 0, near_row_entries, static_cast<long long>(near_cols.size())};
+        for (const auto& rg : it->second)
+            for (int c = 0; c < rg.second; ++c) near_cols.push_back(rg.first + c);
+        r.ncol = static_cast<int>(near_cols.size() - r.col_off);
+        near_row_entries += static_cast<long long>(r.nrow) * r.ncol;
+        near_rows.push_back(r);
+    }
 }
 
 }  // namespace mlfma

@@ -95,6 +95,16 @@ struct NearBlock {
     int self;                    // 1: strict-lower packed self block (nrow == ncol)
 };
 
+// The near field of one leaf as a dense block row: every source of the leaf
+// against the concatenated source ranges it interacts with directly (its own
+// leaf, list-1 leaves, list-3/4 partners in either role).  Entries are stored
+// row-major; col_off indexes the shared column list near_cols.
+struct NearRow {
+    int row0, nrow, ncol;
+    long long off;      // entry offset
+    long long col_off;  // offset into near_cols
+};
+
 struct FarLeaf {
     int level, box, src0, nsrc;
     long long pat_off;  // offset in units of (direction, 2 components)
@@ -128,8 +138,11 @@ struct Plan {
     std::vector<FarLeaf> far_leaves;
     long long pat_elems = 0;         // total (direction, 2 comp) slots
     // Near field
-    std::vector<NearBlock> near_blocks;
+    std::vector<NearBlock> near_blocks;   // each interaction once (reference storage)
     long long near_entries = 0;
+    std::vector<NearRow> near_rows;       // both orientations, per leaf (device storage)
+    std::vector<int> near_cols;
+    long long near_row_entries = 0;
     // Stats
     long long n_list2 = 0, n_list4 = 0, n_near_pairs = 0;
 
