@@ -1,0 +1,118 @@
+// C++ wrapper over the C ABI (mlfma_b200.h) with the reference's entry-point
+// names, for host code that drove the reference's FMM::Node / Solver protocol.
+//
+//   reference (ellilu11/MLFMA)                     this wrapper
+//   Node::initStatic + root ctor + buildLists      mlfma_b200::Operator::dipoles / rwg
+//     + Node::buildTables (src/mlfma.cpp:21-55)
+//   Leaf::buildNearRads + resizeCoeffs             Operator::setup()
+//     + Leaf::buildRadPats (src/mlfma.cpp:42-62)
+//   Solver::evalRvec: rvec += A lvec               Operator::evalRvec(lvec, rvec)
+//     (src/solver.cpp:41-57)
+//   Solver(srcs, root, maxIter, EPS, ...).solve()  Solver(op, maxIter, EPS).solve()
+//     (src/solver.cpp:5-146)
+//
+// Errors become std::runtime_error carrying the ABI's message, like the
+// reference's own std::runtime_error on bad input (src/fileio.h).
+#pragma once
+
+#include <complex>
+#include <stdexcept>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "mlfma_b200.h"
+
+namespace mlfma_b200 {
+
+using cplx = std::complex<double>;
+
+inline void check(int code) {
+    if (code != MLFMA_OK) throw std::runtime_error(std::string("mlfma_b200: ") + mlfma_last_error());
+}
+
+class Operator {
+public:
+    static Operator dipoles(const mlfma_config& cfg, const mlfma_planewave& pw, const std::vector<double>& pos,
+                            const std::vector<double>& mom) {
+        mlfma_handle h = nullptr;
+        check(mlfma_create_dipoles(&cfg, &pw, static_cast<int>(pos.size() / 3), pos.data(), mom.data(), &h));
+        return Operator(h);
+    }
+    static Operator rwg(const mlfma_config& cfg, const mlfma_planewave& pw, const std::vector<double>& verts,
+                        const std::vector<int>& faces, const std::vector<int>& rwgs) {
+        mlfma_handle h = nullptr;
+        check(mlfma_create_rwg(&cfg, &pw, static_cast<int>(verts.size() / 3), verts.data(),
+                               static_cast<int>(faces.size() / 3), faces.data(), static_cast<int>(rwgs.size() / 4),
+                               rwgs.data(), &h));
+        return Operator(h);
+    }
+    Operator(Operator&& o) noexcept : h_(std::exchange(o.h_, nullptr)) {}
+    Operator& operator=(Operator&& o) noexcept {
+        if (this != &o) {
+            if (h_) mlfma_destroy(h_);
+            h_ = std::exchange(o.h_, nullptr);
+        }
+        return *this;
+    }
+    Operator(const Operator&) = delete;
+    Operator& operator=(const Operator&) = delete;
+    ~Operator() {
+        if (h_) mlfma_destroy(h_);
+    }
+
+    void setup() { check(mlfma_setup(h_)); }
+
+    int numSrcs() const {
+        int n = 0;
+        check(mlfma_num_unknowns(h_, &n));
+        return n;
+    }
+
+    // -V, the reference's initial lvec (src/solver.cpp:31-32).
+    std::vector<cplx> rhs() const {
+        std::vector<cplx> b(numSrcs());
+        check(mlfma_rhs(h_, reinterpret_cast<double*>(b.data())));
+        return b;
+    }
+
+    // rvec += A lvec, as Solver::evalRvec does.
+    void evalRvec(const std::vector<cplx>& lvec, std::vector<cplx>& rvec) {
+        check(mlfma_matvec(h_, reinterpret_cast<const double*>(lvec.data()), reinterpret_cast<double*>(rvec.data()), 1));
+    }
+
+    mlfma_handle handle() const { return h_; }
+
+private:
+    explicit Operator(mlfma_handle h) : h_(h) {}
+    mlfma_handle h_ = nullptr;
+};
+
+class Solver {
+public:
+    Solver(Operator& op, int maxIter, double EPS) : op_(op) {
+        opts_.max_iter = maxIter;
+        opts_.tol = EPS;
+        opts_.restart = 0;
+        opts_.ref_givens = 1;
+    }
+    // Unrestarted GMRES from lvec = -V; returns the currents (Solver::solve).
+    std::vector<cplx> solve() {
+        const std::vector<cplx> b = op_.rhs();
+        currents_.assign(b.size(), cplx(0));
+        const int code = mlfma_gmres(op_.handle(), reinterpret_cast<const double*>(b.data()),
+                                     reinterpret_cast<double*>(currents_.data()), &opts_, &info_);
+        if (code != MLFMA_OK && code != MLFMA_ERR_NOT_CONVERGED) check(code);
+        return currents_;
+    }
+    const mlfma_solve_info& info() const { return info_; }
+    const std::vector<cplx>& getCurrents() const { return currents_; }
+
+private:
+    Operator& op_;
+    mlfma_solver_opts opts_{};
+    mlfma_solve_info info_{};
+    std::vector<cplx> currents_;
+};
+
+}  // namespace mlfma_b200
