@@ -138,6 +138,23 @@ int mlfma_matvec_device(mlfma_handle h, const void* d_x, void* d_y, int accumula
 int mlfma_gmres(mlfma_handle h, const double* b, double* x, const mlfma_solver_opts* opts,
                 mlfma_solve_info* info);
 
+/* GMRES that allocates no device memory.  No counterpart in the reference.
+ * mlfma_gmres allocates its Krylov basis with cudaMalloc on first use; a
+ * caller that cannot allocate device memory during a solve (a fixed memory
+ * budget reserved at start-up, an allocator policy that forbids cudaMalloc
+ * after initialisation) calls this instead.  Same algorithm and options as
+ * mlfma_gmres; b and x are DEVICE buffers of n complex values in the caller's
+ * source order; the solve runs on the handle's stream and returns when done.
+ * The workspace is one fixed array in device memory that is part of the
+ * library (32 MiB, held on every GPU that loads the library until exit): n *
+ * (restart + 5) must not exceed 2,097,152 complex values (restart = max_iter
+ * when restart is 0), otherwise MLFMA_ERR_ARG.  All calls share that array and
+ * it keeps the last call's contents, so calls that overlap on the GPU race.
+ * The first call on a device looks up the array's device address; make that
+ * first call before any stream capture. */
+int mlfma_gmres_noalloc(mlfma_handle h, const void* d_b, void* d_x, const mlfma_solver_opts* opts,
+                        mlfma_solve_info* info);
+
 /* The handle's own CUDA stream (cudaStream_t as void*), on which mlfma_matvec
  * and mlfma_gmres run; callers may record events on it. */
 int mlfma_get_stream(mlfma_handle h, void** stream);

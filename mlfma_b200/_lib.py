@@ -78,6 +78,8 @@ SIGNATURES = {
                                            ctypes.c_void_p]),
     "mlfma_gmres": (ctypes.c_int, [ctypes.c_void_p, _dp, _dp, ctypes.POINTER(SolverOpts),
                                    ctypes.POINTER(SolveInfo)]),
+    "mlfma_gmres_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                           ctypes.POINTER(SolverOpts), ctypes.POINTER(SolveInfo)]),
     "mlfma_get_stream": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]),
     "mlfma_time_stages": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(StageTimes)]),
     "mlfma_get_traffic": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Traffic)]),

@@ -16,6 +16,7 @@ struct mlfma_op_s {
     int device = 0;
     std::unique_ptr<mlfma::DeviceOp> dev;
     std::unique_ptr<mlfma::Gmres> gmres;
+    std::unique_ptr<mlfma::Gmres> gmres_fixed;  // runs on the library's fixed workspace
     double2* d_x = nullptr;  // staging for host-buffer calls
     double2* d_y = nullptr;
     ~mlfma_op_s() {
@@ -216,6 +217,38 @@ int mlfma_gmres(mlfma_handle h, const double* b, double* x, const mlfma_solver_o
     if (cudaMemcpyAsync(x, h->d_y, bytes, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
         cudaStreamSynchronize(s) != cudaSuccess)
         return fail(MLFMA_ERR_CUDA, "copy of x failed");
+    if (info) {
+        info->iterations = r.iterations;
+        info->residual = r.residual;
+        info->true_residual = r.true_residual;
+        info->seconds = r.seconds;
+    }
+    if (!r.converged) return fail(MLFMA_ERR_NOT_CONVERGED, "iteration limit reached");
+    return MLFMA_OK;
+}
+
+// For callers that cannot allocate device memory during a solve: the Krylov
+// workspace is the library's fixed device array (gmres.cu), never cudaMalloc.
+int mlfma_gmres_noalloc(mlfma_handle h, const void* d_b, void* d_x, const mlfma_solver_opts* opts,
+                        mlfma_solve_info* info) {
+    if (!h || !d_b || !d_x) return fail(MLFMA_ERR_ARG, "null argument");
+    if (!ready(h)) return fail(MLFMA_ERR_STATE, "mlfma_setup has not run");
+    mlfma::SolveOpts o;
+    if (opts) {
+        o.max_iter = opts->max_iter;
+        o.tol = opts->tol;
+        o.restart = opts->restart;
+        o.ref_givens = opts->ref_givens;
+    }
+    if (o.max_iter < 1 || o.restart < 0) return fail(MLFMA_ERR_ARG, "max_iter and restart must be positive");
+    if (cudaSetDevice(h->device) != cudaSuccess) return fail(MLFMA_ERR_CUDA, "cudaSetDevice failed");
+    if (!h->gmres_fixed) h->gmres_fixed = std::make_unique<mlfma::Gmres>();
+    const int m = o.restart > 0 ? o.restart : o.max_iter;
+    std::string e = h->gmres_fixed->use_static_workspace(h->plan.n, m + 1);
+    if (!e.empty()) return fail(e.rfind("size:", 0) == 0 ? MLFMA_ERR_ARG : MLFMA_ERR_CUDA, e);
+    mlfma::SolveResult r;
+    e = h->gmres_fixed->solve(*h->dev, static_cast<const double2*>(d_b), static_cast<double2*>(d_x), o, &r);
+    if (!e.empty()) return from_msg(e);
     if (info) {
         info->iterations = r.iterations;
         info->residual = r.residual;

@@ -93,6 +93,8 @@ public:
 
     // Operator on tree-ordered device vectors (used by the solver).
     void apply_tree(const double2* xt, double2* yt, cudaStream_t s);
+    // Same, never capturing a graph (launches the captured one if it exists).
+    void apply_tree_direct(const double2* xt, double2* yt, cudaStream_t s);
 
     // Per-stage CUDA-event timing of one matvec on the operator's stream.
     std::string time_stages(StageTimes* out);

@@ -16,7 +16,10 @@
 #include <chrono>
 #include <cmath>
 #include <complex>
+#include <map>
+#include <mutex>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "gmres.hpp"
@@ -133,6 +136,8 @@ inline int nblk(long long n, int bs) { return static_cast<int>((n + bs - 1) / bs
     } while (0)
 
 std::string Gmres::ensure(int n, int ncols) {
+    if (external_)
+        return (n == n_ && ncols <= cap_) ? std::string() : std::string("fixed workspace set up for another size");
     if (n == n_ && ncols <= cap_) return {};
     release();
     n_ = n;
@@ -151,15 +156,79 @@ std::string Gmres::ensure(int n, int ncols) {
 }
 
 void Gmres::release() {
-    for (void* p : {(void*)Q_, (void*)w_, (void*)b_, (void*)x_, (void*)r_, (void*)h_, (void*)y_,
-                    (void*)partial_, (void*)npartial_})
-        if (p) cudaFree(p);
+    if (!external_)
+        for (void* p : {(void*)Q_, (void*)w_, (void*)b_, (void*)x_, (void*)r_, (void*)h_, (void*)y_,
+                        (void*)partial_, (void*)npartial_})
+            if (p) cudaFree(p);
     Q_ = w_ = b_ = x_ = r_ = h_ = y_ = partial_ = nullptr;
     npartial_ = nullptr;
     n_ = cap_ = 0;
 }
 
 Gmres::~Gmres() { release(); }
+
+void Gmres::apply(DeviceOp& op, const double2* x, double2* y, cudaStream_t s) {
+    if (external_) op.apply_tree_direct(x, y, s); else op.apply_tree(x, y, s);
+}
+
+// ------------------------------------------------------------ fixed workspace
+// Some callers cannot allocate device memory while they solve: code that runs
+// with a device memory budget fixed at start-up, or under an allocator policy
+// that forbids cudaMalloc outside initialisation.  For them the library keeps
+// one fixed GMRES workspace in device memory that is part of the loaded module
+// (it exists on every GPU that loads the library, until the process exits):
+// kNoAllocWorkspace complex doubles (32 MiB) for the Krylov basis and work
+// vectors, and kNoAllocNorm doubles for norm partial sums.  Every solve shares
+// it and it keeps the previous solve's contents (every element is written
+// before it is read); two solves that overlap on the GPU race on it.
+constexpr size_t kNoAllocWorkspace = size_t(1) << 21;
+constexpr int kNoAllocNorm = 4096;
+static __device__ __align__(256) double2 g_noalloc_ws[kNoAllocWorkspace];
+static __device__ __align__(256) double g_noalloc_norm[kNoAllocNorm];
+
+std::string Gmres::use_static_workspace(int n, int ncols) {
+    // Device addresses of the arrays, looked up once per device (with that
+    // device current); host code only sees host-side stand-ins for them.
+    static std::mutex mu;
+    static std::map<int, std::pair<double2*, double*>> addr;
+    int dev = 0;
+    GM_CK(cudaGetDevice(&dev));
+    double2* ws = nullptr;
+    double* nws = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        auto it = addr.find(dev);
+        if (it == addr.end()) {
+            GM_CK(cudaGetSymbolAddress(reinterpret_cast<void**>(&ws), g_noalloc_ws));
+            GM_CK(cudaGetSymbolAddress(reinterpret_cast<void**>(&nws), g_noalloc_norm));
+            addr.emplace(dev, std::make_pair(ws, nws));
+        } else {
+            ws = it->second.first;
+            nws = it->second.second;
+        }
+    }
+    const int nchunks = (n + kDotChunk - 1) / kDotChunk;
+    const size_t need = static_cast<size_t>(n) * ncols + 4 * static_cast<size_t>(n) +
+                        2 * static_cast<size_t>(ncols + 1) + static_cast<size_t>(nchunks) * (ncols + 1);
+    if (need > kNoAllocWorkspace || nchunks > kNoAllocNorm)
+        return "size:N x (restart + 5) exceeds the fixed workspace of 2097152 complex values";
+    if (!external_) release();
+    external_ = true;
+    n_ = n;
+    cap_ = ncols;
+    nchunks_ = nchunks;
+    double2* p = ws;
+    Q_ = p; p += static_cast<size_t>(n) * ncols;
+    w_ = p; p += n;
+    b_ = p; p += n;
+    x_ = p; p += n;
+    r_ = p; p += n;
+    h_ = p; p += ncols + 1;
+    y_ = p; p += ncols + 1;
+    partial_ = p;
+    npartial_ = nws;
+    return {};
+}
 
 std::string Gmres::norm(const double2* v, cudaStream_t s, double* out) {
     k_norm2<<<nchunks_, kDotThreads, 0, s>>>(v, n_, npartial_);
@@ -224,7 +293,7 @@ std::string Gmres::solve(DeviceOp& op, const double2* d_b_user, double2* d_x_use
         if (total == 0) {
             GM_CK(cudaMemcpyAsync(r_, b_, sizeof(double2) * n, cudaMemcpyDeviceToDevice, s));
         } else {
-            op.apply_tree(x_, w_, s);
+            apply(op, x_, w_, s);
             k_sub<<<nblk(n, 256), 256, 0, s>>>(b_, w_, r_, n);
         }
         err = norm(r_, s, &beta);
@@ -238,7 +307,7 @@ std::string Gmres::solve(DeviceOp& op, const double2* d_b_user, double2* d_x_use
         int k = 0;
         for (; k < m && total < o.max_iter; ++k) {
             double2* qk = Q_ + static_cast<long long>(k) * n;
-            op.apply_tree(qk, w_, s);  // w = A q_k
+            apply(op, qk, w_, s);  // w = A q_k
             err = cgs_pass(k + 1, s, false);
             if (!err.empty()) return err;
             err = cgs_pass(k + 1, s, true);
@@ -316,7 +385,7 @@ std::string Gmres::solve(DeviceOp& op, const double2* d_b_user, double2* d_x_use
     }
     res->iterations = total;
     // True residual.
-    op.apply_tree(x_, w_, s);
+    apply(op, x_, w_, s);
     k_sub<<<nblk(n, 256), 256, 0, s>>>(b_, w_, r_, n);
     double rn;
     err = norm(r_, s, &rn);

@@ -35,7 +35,14 @@ public:
     std::string solve(DeviceOp& op, const double2* d_b_user, double2* d_x_user, const SolveOpts& o,
                       SolveResult* res);
 
+    // Point this solver at the library's fixed device workspace instead of
+    // allocating (see mlfma_gmres_noalloc); products then run without graph
+    // capture.  Fails if n and ncols do not fit.
+    std::string use_static_workspace(int n, int ncols);
+
 private:
+    void apply(DeviceOp& op, const double2* x, double2* y, cudaStream_t s);
+    bool external_ = false;   // workspace not owned (static device array)
     std::string ensure(int n, int ncols);
     void release();
     std::string norm(const double2* v, cudaStream_t s, double* out);

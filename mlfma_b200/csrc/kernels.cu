@@ -409,6 +409,12 @@ void DeviceOp::apply_tree(const double2* xt, double2* yt, cudaStream_t s) {
     k_finish<<<blocks_for(n_, 256), 256, 0, s>>>(yfar_, ynear_, nullptr, yt, n_, ck_, 0);
 }
 
+void DeviceOp::apply_tree_direct(const double2* xt, double2* yt, cudaStream_t s) {
+    if (xt != xt_) cudaMemcpyAsync(xt_, xt, sizeof(double2) * n_, cudaMemcpyDeviceToDevice, s);
+    if (graph_exec_) cudaGraphLaunch(graph_exec_, s); else enqueue_core(s);
+    k_finish<<<blocks_for(n_, 256), 256, 0, s>>>(yfar_, ynear_, nullptr, yt, n_, ck_, 0);
+}
+
 std::string DeviceOp::matvec_device(const double2* x, double2* y, bool accumulate, cudaStream_t stream) {
     if (!ready_) return "operator not set up";
     cudaStream_t s = stream ? stream : stream_;
