@@ -173,11 +173,24 @@ std::string DeviceOp::setup(const Plan& plan, int device) {
         for (int p = plan.lmin; p < plan.max_level; ++p) {
             const Transition& T = plan.trans[p];
             DevTrans& d = trans_[p];
-            auto st = [&](const Stencil& s) {
+            auto width_of = [](const Stencil& s) {
+                int w = 1;
+                for (size_t r = 0; r + 1 < s.ptr.size(); ++r) w = std::max(w, s.ptr[r + 1] - s.ptr[r]);
+                return w;
+            };
+            // The kernels are instantiated for fixed tap counts (fully unrolled).
+            const int w_up = width_of(T.up_th);
+            if (w_up != width_of(T.up_ph) || w_up % 2 || w_up < 2 || w_up > 10)
+                return "interp_order must be 1..5";
+            const int w_dn_need = std::max(width_of(T.dn_ph), width_of(T.dn_th));
+            int w_dn = 0;
+            for (int c : {8, 12, 16, 24, 32})
+                if (!w_dn && w_dn_need <= c) w_dn = c;
+            if (!w_dn) return "anterpolation stencil wider than 32 taps";
+            auto st = [&](const Stencil& s, int wpad) {
                 // pad rows to a fixed width; fold the reflection sign into the coefficient
                 const int rows = static_cast<int>(s.ptr.size()) - 1;
-                int w = 1;
-                for (int r = 0; r < rows; ++r) w = std::max(w, s.ptr[r + 1] - s.ptr[r]);
+                const int w = wpad;
                 std::vector<int> src(static_cast<size_t>(rows) * w, 0), refl(static_cast<size_t>(rows) * w, 0);
                 std::vector<double> coef(static_cast<size_t>(rows) * w, 0.0);
                 for (int r = 0; r < rows; ++r)
@@ -189,10 +202,10 @@ std::string DeviceOp::setup(const Plan& plan, int device) {
                     }
                 return DevStencil{w, upload(src), upload(refl), upload(coef)};
             };
-            d.up_th = st(T.up_th);
-            d.up_ph = st(T.up_ph);
-            d.dn_ph = st(T.dn_ph);
-            d.dn_th = st(T.dn_th);
+            d.up_th = st(T.up_th, w_up);
+            d.up_ph = st(T.up_ph, w_up);
+            d.dn_ph = st(T.dn_ph, w_dn);
+            d.dn_th = st(T.dn_th, w_dn);
             d.plevel = p;
             d.npar = static_cast<int>(T.par_box.size());
             d.par_box = upload(T.par_box);
@@ -302,10 +315,21 @@ std::string DeviceOp::setup(const Plan& plan, int device) {
         if (m2m_smem > static_cast<size_t>(dev_smem) || l2l_smem > static_cast<size_t>(dev_smem) ||
             s2m_smem > static_cast<size_t>(dev_smem))
             return "angular grid or leaf too large for the kernels' shared memory";
-        MLFMA_CK(cudaFuncSetAttribute(k_m2m, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      static_cast<int>(std::max<size_t>(m2m_smem, 1))));
-        MLFMA_CK(cudaFuncSetAttribute(k_l2l, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      static_cast<int>(std::max<size_t>(l2l_smem, 1))));
+        {
+            const int a = static_cast<int>(std::max<size_t>(m2m_smem, 1));
+            const int b = static_cast<int>(std::max<size_t>(l2l_smem, 1));
+            const auto attr = cudaFuncAttributeMaxDynamicSharedMemorySize;
+            MLFMA_CK(cudaFuncSetAttribute(k_m2m<2>, attr, a));
+            MLFMA_CK(cudaFuncSetAttribute(k_m2m<4>, attr, a));
+            MLFMA_CK(cudaFuncSetAttribute(k_m2m<6>, attr, a));
+            MLFMA_CK(cudaFuncSetAttribute(k_m2m<8>, attr, a));
+            MLFMA_CK(cudaFuncSetAttribute(k_m2m<10>, attr, a));
+            MLFMA_CK(cudaFuncSetAttribute(k_l2l<8>, attr, b));
+            MLFMA_CK(cudaFuncSetAttribute(k_l2l<12>, attr, b));
+            MLFMA_CK(cudaFuncSetAttribute(k_l2l<16>, attr, b));
+            MLFMA_CK(cudaFuncSetAttribute(k_l2l<24>, attr, b));
+            MLFMA_CK(cudaFuncSetAttribute(k_l2l<32>, attr, b));
+        }
         MLFMA_CK(cudaFuncSetAttribute(k_s2m, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       static_cast<int>(std::max<size_t>(s2m_smem, 1))));
         MLFMA_CK(cudaStreamSynchronize(stream_));
@@ -346,7 +370,13 @@ void DeviceOp::stage_m2m(cudaStream_t s) {
         const int rows = m2m_rows(P.nth, P.nph);
         const dim3 grid(T.npar, (P.nth + rows - 1) / rows);
         const size_t smem = static_cast<size_t>(8) * rows * C.nph * 2 * sizeof(double2);
-        k_m2m<<<grid, 128, smem, s>>>(lv_dev_, T, rows);
+        switch (T.up_th.width) {
+            case 2: k_m2m<2><<<grid, 128, smem, s>>>(lv_dev_, T, rows); break;
+            case 4: k_m2m<4><<<grid, 128, smem, s>>>(lv_dev_, T, rows); break;
+            case 6: k_m2m<6><<<grid, 128, smem, s>>>(lv_dev_, T, rows); break;
+            case 8: k_m2m<8><<<grid, 128, smem, s>>>(lv_dev_, T, rows); break;
+            default: k_m2m<10><<<grid, 128, smem, s>>>(lv_dev_, T, rows); break;
+        }
     }
 }
 
@@ -358,7 +388,14 @@ void DeviceOp::stage_l2l(cudaStream_t s) {
     for (int p = lv_.lmin; p < lv_.lmax; ++p) {
         if (!n_l2l_pairs_[p]) continue;
         const size_t smem = static_cast<size_t>(lv_.lv[p].nth) * lv_.lv[p + 1].nph * 2 * sizeof(double2);
-        k_l2l<<<n_l2l_pairs_[p], 256, smem, s>>>(lv_dev_, trans_[p], l2l_pairs_[p]);
+        const int g = n_l2l_pairs_[p];
+        switch (trans_[p].dn_ph.width) {
+            case 8: k_l2l<8><<<g, 256, smem, s>>>(lv_dev_, trans_[p], l2l_pairs_[p]); break;
+            case 12: k_l2l<12><<<g, 256, smem, s>>>(lv_dev_, trans_[p], l2l_pairs_[p]); break;
+            case 16: k_l2l<16><<<g, 256, smem, s>>>(lv_dev_, trans_[p], l2l_pairs_[p]); break;
+            case 24: k_l2l<24><<<g, 256, smem, s>>>(lv_dev_, trans_[p], l2l_pairs_[p]); break;
+            default: k_l2l<32><<<g, 256, smem, s>>>(lv_dev_, trans_[p], l2l_pairs_[p]); break;
+        }
     }
 }
 

@@ -98,6 +98,7 @@ k_l2t(const DevLevel* __restrict__ lvs, const int4* __restrict__ items, const De
 // Block = (parent, tile of `rows` parent theta rows).  Phase 1 computes the
 // theta pass of every child into shared memory at once (all loads
 // independent); phase 2 forms each parent output from the children's rows.
+template <int W>  // taps per row: 2 * interp_order (both passes)
 __global__ void __launch_bounds__(128)
 k_m2m(const DevLevel* __restrict__ lvs, DevTrans T, int rows) {
     extern __shared__ double2 sm[];
@@ -117,8 +118,9 @@ k_m2m(const DevLevel* __restrict__ lvs, DevTrans T, int rows) {
         const double2* Ac = C.A + static_cast<size_t>(T.child_box[c0 + c]) * C.ndir * 2;
         const double2* sh = C.shift_up + static_cast<size_t>(T.child_oct[c0 + c]) * C.ndir;
         double2 v0 = z0(), v1 = z0();
-        const int w = T.up_th.width;
-        for (int q = jth * w; q < jth * w + w; ++q) {
+#pragma unroll
+        for (int k = 0; k < W; ++k) {
+            const int q = jth * W + k;
             const bool rf = T.up_th.refl[q];
             const int sp = rf ? (iph < halfm ? iph + halfm : iph - halfm) : iph;
             const double cf = T.up_th.coef[q];
@@ -135,10 +137,11 @@ k_m2m(const DevLevel* __restrict__ lvs, DevTrans T, int rows) {
     for (int o = threadIdx.x; o < nrow * nph; o += blockDim.x) {
         const int jr = o / nph, jph = o - jr * nph;
         double2 a0 = z0(), a1 = z0();
-        const int w = T.up_ph.width;
         for (int c = 0; c < nch; ++c) {
             const double2* row = sm + (static_cast<size_t>(c) * per_child + static_cast<size_t>(jr) * mph) * 2;
-            for (int q = jph * w; q < jph * w + w; ++q) {
+#pragma unroll
+            for (int k = 0; k < W; ++k) {
+                const int q = jph * W + k;
                 const int s = T.up_ph.src[q];
                 const double cf = T.up_ph.coef[q];
                 a0 = cadd(a0, cscale(cf, row[2 * s]));
@@ -169,20 +172,28 @@ k_m2l(const DevLevel* __restrict__ lvs, const int4* __restrict__ items, int zero
     }
     double2 a0 = z0(), a1 = z0(), c0 = z0(), c1 = z0();
     int p = p0;
-    for (; p + 2 <= p1; p += 2) {
-        const int s0 = lv.m2l_src[p], o0 = lv.m2l_off[p];
-        const int s1 = lv.m2l_src[p + 1], o1 = lv.m2l_off[p + 1];
-        const double2 t0 = lv.transl[static_cast<size_t>(o0) * ndir + d];
-        const double2 t1 = lv.transl[static_cast<size_t>(o1) * ndir + d];
-        const double2* A0 = lv.A + (static_cast<size_t>(s0) * ndir + d) * 2;
-        const double2* A1 = lv.A + (static_cast<size_t>(s1) * ndir + d) * 2;
-        const double2 x00 = A0[0], x01 = A0[1], x10 = A1[0], x11 = A1[1];
-        a0 = cfma(t0, x00, a0);
-        a1 = cfma(t0, x01, a1);
-        c0 = cfma(t1, x10, c0);
-        c1 = cfma(t1, x11, c1);
+    for (; p + 4 <= p1; p += 4) {
+        int sb[4], ob[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) { sb[u] = lv.m2l_src[p + u]; ob[u] = lv.m2l_off[p + u]; }
+        double2 t[4], xa[4], xb[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            t[u] = lv.transl[static_cast<size_t>(ob[u]) * ndir + d];
+            const double2* As = lv.A + (static_cast<size_t>(sb[u]) * ndir + d) * 2;
+            xa[u] = As[0];
+            xb[u] = As[1];
+        }
+        a0 = cfma(t[0], xa[0], a0);
+        a1 = cfma(t[0], xb[0], a1);
+        c0 = cfma(t[1], xa[1], c0);
+        c1 = cfma(t[1], xb[1], c1);
+        a0 = cfma(t[2], xa[2], a0);
+        a1 = cfma(t[2], xb[2], a1);
+        c0 = cfma(t[3], xa[3], c0);
+        c1 = cfma(t[3], xb[3], c1);
     }
-    if (p < p1) {
+    for (; p < p1; ++p) {
         const int s0 = lv.m2l_src[p], o0 = lv.m2l_off[p];
         const double2 t0 = lv.transl[static_cast<size_t>(o0) * ndir + d];
         const double2* A0 = lv.A + (static_cast<size_t>(s0) * ndir + d) * 2;
@@ -200,6 +211,7 @@ k_m2l(const DevLevel* __restrict__ lvs, const int4* __restrict__ items, int zero
 // reflection (Stem::getShiftedLocalCoeffs and addAnterpCoeffs,
 // src/fmm/stem.cpp:109-244).  One block per (parent, child) pair; the
 // pair list already omits parents that pass nothing down.
+template <int W>  // both transposed stencils padded to W taps per row
 __global__ void __launch_bounds__(256)
 k_l2l(const DevLevel* __restrict__ lvs, DevTrans T, const int2* __restrict__ pairs) {
     extern __shared__ double2 sm[];
@@ -212,8 +224,9 @@ k_l2l(const DevLevel* __restrict__ lvs, DevTrans T, const int2* __restrict__ pai
     for (int e = threadIdx.x; e < pth * cph; e += blockDim.x) {
         const int ith = e / cph, jph = e - ith * cph;
         double2 v0 = z0(), v1 = z0();
-        const int w = T.dn_ph.width;
-        for (int q = jph * w; q < jph * w + w; ++q) {
+#pragma unroll
+        for (int k = 0; k < W; ++k) {
+            const int q = jph * W + k;
             const int d = ith * pph + T.dn_ph.src[q];
             const double cf = T.dn_ph.coef[q];
             const double2 ph = sh[d];
@@ -228,8 +241,9 @@ k_l2l(const DevLevel* __restrict__ lvs, DevTrans T, const int2* __restrict__ pai
     for (int e = threadIdx.x; e < cth * cph; e += blockDim.x) {
         const int jth = e / cph, jph = e - jth * cph;
         double2 v0 = z0(), v1 = z0();
-        const int w = T.dn_th.width;
-        for (int q = jth * w; q < jth * w + w; ++q) {
+#pragma unroll
+        for (int k = 0; k < W; ++k) {
+            const int q = jth * W + k;
             const bool rf = T.dn_th.refl[q];
             const int sp = rf ? (jph < halfc ? jph + halfc : jph - halfc) : jph;
             const double cf = T.dn_th.coef[q];
