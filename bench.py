@@ -141,6 +141,106 @@ def run_reference(steps: int, warmup: int, quiet=False) -> dict:
 
 # ------------------------------------------------------------------ our arm
 
+def measure(torch, dev, rank, world, args, precision: int, clocks=None) -> dict:
+    """Time one operator: device-resident products (value), host-buffer products
+    (e2e) and per-stage CUDA-event times."""
+    import torch.distributed as dist
+    from mlfma_b200 import MLFMA, default_config
+    mesh, pw = make_problem()
+    cfg = default_config(quad_prec=WORKLOAD["quad_prec"], digits=WORKLOAD["digits"],
+                         interp_order=WORKLOAD["interp_order"], over_interp=WORKLOAD["over_interp"],
+                         root_leng=WORKLOAD["root_leng"], max_node_srcs=WORKLOAD["max_node_srcs"],
+                         device=dev.index, precision=precision)
+    t0 = time.perf_counter()
+    op = MLFMA.rwg(mesh, pw, config=cfg)
+    op.setup()
+    setup_s = time.perf_counter() - t0
+    st = op.stats()
+    n = op.n
+    g = torch.Generator(device="cpu").manual_seed(1234 + rank)
+    xh = torch.complex(torch.randn(n, generator=g, dtype=torch.float64),
+                       torch.randn(n, generator=g, dtype=torch.float64))
+    x = xh.to(dev)
+    y = torch.zeros(n, dtype=torch.complex128, device=dev)
+    torch.cuda.synchronize(dev)
+    # Every product runs on the operator's own stream; events are recorded there.
+    stream = torch.cuda.ExternalStream(op.stream(), device=dev)
+
+    def step():
+        op.matvec_device(x.data_ptr(), y.data_ptr(), False, stream.cuda_stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    if clocks is not None:
+        clocks.start()
+        time.sleep(0.3)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    ms = e0.elapsed_time(e1) / args.steps
+    y_dev = y.cpu().numpy().copy()
+
+    # End to end through the public host-buffer call (pinned buffers).
+    xp = torch.empty(n, dtype=torch.complex128, pin_memory=True)
+    yp = torch.empty(n, dtype=torch.complex128, pin_memory=True)
+    xp.copy_(xh)
+    xn, yn = xp.numpy(), yp.numpy()
+    for _ in range(args.warmup):
+        op.matvec(xn, out=yn)
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for _ in range(args.steps):
+        op.matvec(xn, out=yn)
+    f1.record(stream)
+    torch.cuda.synchronize(dev)
+    e2e_ms = f0.elapsed_time(f1) / args.steps
+    clk = clocks.stop() if clocks is not None else None
+
+    # Per-stage device times (stages launched back to back on the operator's stream).
+    stages = [op.stage_times() for _ in range(max(5, min(args.steps, 50)))]
+    avg = {k: float(np.mean([s[k] for s in stages])) for k in stages[0]}
+    traffic = op.traffic()
+    op.close()
+    if world > 1:
+        t = torch.tensor([ms, e2e_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, e2e_ms = float(t[0]), float(t[1])
+    return dict(ms=ms, e2e_ms=e2e_ms, stages=avg, traffic=traffic, stats=st, setup_s=setup_s, n=n, y=y_dev,
+                clocks=clk)
+
+
+def roofline(avg, traffic, precision_name):
+    stage_keys = ["s2m", "m2m", "m2l", "l2l", "l2t", "near_field"]
+    dom = max(stage_keys, key=lambda k: avg[k])
+    peaks = {}
+    try:
+        with open(os.path.join(HERE, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except OSError:
+        pass
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    achieved = traffic[dom] / (avg[dom] * 1e-3) / 1e9
+    ncu_traffic = None
+    try:
+        with open(os.path.join(HERE, "profiles", "traffic.json")) as f:
+            ncu_traffic = json.load(f).get(WORKLOAD["name"] + precision_name, {}).get(dom)
+    except (OSError, ValueError):
+        pass
+    return {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+            "frac": achieved / hbm_peak, "peak_source": peak_src, "traffic": ncu_traffic,
+            "algorithmic_bytes": traffic[dom], "avg_launch_ms": avg[dom]}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -148,6 +248,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=3)
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
@@ -186,94 +287,10 @@ def main():
         cpu_proc = subprocess.Popen([sys.executable, os.path.abspath(__file__), "--impl", "reference",
                                      "--steps", str(args.cpu_steps), "--warmup", "1"],
                                     stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-
     sys.path.insert(0, HERE)
-    from mlfma_b200 import MLFMA, default_config
-    mesh, pw = make_problem()
-    cfg = default_config(quad_prec=WORKLOAD["quad_prec"], digits=WORKLOAD["digits"],
-                         interp_order=WORKLOAD["interp_order"], over_interp=WORKLOAD["over_interp"],
-                         root_leng=WORKLOAD["root_leng"], max_node_srcs=WORKLOAD["max_node_srcs"],
-                         device=local_rank)
-    t0 = time.perf_counter()
-    op = MLFMA.rwg(mesh, pw, config=cfg)
-    op.setup()
-    setup_s = time.perf_counter() - t0
-    st = op.stats()
-    n = op.n
-    g = torch.Generator(device="cpu").manual_seed(1234 + rank)
-    xh = torch.complex(torch.randn(n, generator=g, dtype=torch.float64), torch.randn(n, generator=g, dtype=torch.float64))
-    x = xh.to(dev)
-    y = torch.zeros(n, dtype=torch.complex128, device=dev)
-    torch.cuda.synchronize(dev)
-    # Every product runs on the operator's own stream; events are recorded there.
-    stream = torch.cuda.ExternalStream(op.stream(), device=dev)
 
-    def step():
-        op.matvec_device(x.data_ptr(), y.data_ptr(), False, stream.cuda_stream)
-
-    for _ in range(args.warmup):
-        step()
-    torch.cuda.synchronize(dev)
-
-    clocks = ClockSampler(local_rank)
-    clocks.start()
-    time.sleep(0.3)
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize(dev)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
-        step()
-    e1.record(stream)
-    torch.cuda.synchronize(dev)
-    if world > 1:
-        dist.barrier()
-    ms = e0.elapsed_time(e1) / args.steps
-
-    # End to end through the public host-buffer call (pinned buffers).
-    xp = torch.empty(n, dtype=torch.complex128, pin_memory=True)
-    yp = torch.empty(n, dtype=torch.complex128, pin_memory=True)
-    xp.copy_(xh)
-    xn, yn = xp.numpy(), yp.numpy()
-    ostream = stream
-    for _ in range(args.warmup):
-        op.matvec(xn, out=yn)
-    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    f0.record(ostream)
-    for _ in range(args.steps):
-        op.matvec(xn, out=yn)
-    f1.record(ostream)
-    torch.cuda.synchronize(dev)
-    e2e_ms = f0.elapsed_time(f1) / args.steps
-    clk = clocks.stop()
-
-    # Per-stage device times (stages launched back to back on the operator's stream).
-    stages = [op.stage_times() for _ in range(max(5, min(args.steps, 50)))]
-    avg = {k: float(np.mean([s[k] for s in stages])) for k in stages[0]}
-    traffic = op.traffic()
-    stage_keys = ["s2m", "m2m", "m2l", "l2l", "l2t", "near_field"]
-    dom = max(stage_keys, key=lambda k: avg[k])
-    peaks = {}
-    try:
-        with open(os.path.join(HERE, "MEASURED_PEAKS.json")) as f:
-            peaks = json.load(f)
-    except OSError:
-        pass
-    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
-    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
-    achieved = traffic[dom] / (avg[dom] * 1e-3) / 1e9
-    ncu_traffic = None
-    try:
-        with open(os.path.join(HERE, "profiles", "traffic.json")) as f:
-            ncu_traffic = json.load(f).get(WORKLOAD["name"], {}).get(dom)
-    except (OSError, ValueError):
-        pass
-
-    if world > 1:
-        t = torch.tensor([ms, e2e_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms, e2e_ms = float(t[0]), float(t[1])
+    r64 = measure(torch, dev, rank, world, args, precision=0, clocks=ClockSampler(local_rank))
+    rmx = None if args.no_mixed else measure(torch, dev, rank, world, args, precision=1)
 
     if rank == 0:
         cpu = None
@@ -287,27 +304,30 @@ def main():
                                  f"{r['config'].get('reference_setup_s', 0):.0f} s setup"}
             except Exception as e:  # noqa: BLE001
                 cpu = {"value": None, "unit": UNIT, "cores": 1, "kind": "reference", "sample": f"failed: {e}"}
-        launches = int(st.get("launches_per_matvec", 0)) * args.steps
+        st, n, ms, e2e_ms = r64["stats"], r64["n"], r64["ms"], r64["e2e_ms"]
         line = {
             "metric": METRIC, "value": world * 1000.0 / ms, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic (seeded icosphere mesh)",
             "config": config_dict({"parallelism": f"replicas{world}", "levels": st["max_level"],
-                                   "near_entries": st["near_entries"], "setup_s": setup_s}),
+                                   "near_entries": st["near_entries"], "setup_s": r64["setup_s"]}),
             "e2e": {"value": world * 1000.0 / e2e_ms, "unit": UNIT, "h2d_bytes_per_step": n * 16,
                     "d2h_bytes_per_step": n * 16},
-            "gpu_launches": launches,
-            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                         "frac": achieved / hbm_peak, "peak_source": peak_src,
-                         "traffic": ncu_traffic, "algorithmic_bytes": traffic[dom],
-                         "avg_launch_ms": avg[dom]},
-            "stage_ms": avg,
-            "matvec_alg_bytes": traffic["total"],
-            "clocks": clk,
+            "gpu_launches": int(st.get("launches_per_matvec", 0)) * args.steps,
+            "roofline": roofline(r64["stages"], r64["traffic"], ""),
+            "stage_ms": r64["stages"],
+            "matvec_alg_bytes": r64["traffic"]["total"],
+            "clocks": r64["clocks"],
             "cpu_baseline": cpu,
         }
+        if rmx is not None:
+            err = float(np.linalg.norm(rmx["y"] - r64["y"]) / np.linalg.norm(r64["y"]))
+            line["mixed"] = {"value": world * 1000.0 / rmx["ms"], "ms_per_step": rmx["ms"],
+                             "e2e": world * 1000.0 / rmx["e2e_ms"], "speedup_vs_fp64": ms / rmx["ms"],
+                             "rel_diff_vs_fp64": err, "dtype": "c64 far field, c128 near field",
+                             "stage_ms": rmx["stages"], "roofline": roofline(rmx["stages"], rmx["traffic"], "_mixed"),
+                             "matvec_alg_bytes": rmx["traffic"]["total"]}
         print(json.dumps(line), flush=True)
-    op.close()
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()

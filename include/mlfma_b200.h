@@ -50,7 +50,12 @@ typedef struct {
     int max_level;       /* >0: do not split below this level (0 = reference rule) */
     int ref_compat;      /* 1: reproduce the reference's stale-local rule (default) */
     int device;          /* CUDA device ordinal */
+    int precision;       /* MLFMA_FP64 (default) or MLFMA_MIXED: far field in complex
+                            float with float accumulation, near field and vectors in
+                            complex double */
 } mlfma_config;
+
+enum { MLFMA_FP64 = 0, MLFMA_MIXED = 1 };
 
 /* Incident plane wave (src/excite.h:6-28; file format src/fileio.h:8-27). */
 typedef struct {
@@ -137,6 +142,13 @@ int mlfma_matvec_device(mlfma_handle h, const void* d_x, void* d_y, int accumula
  * src/solver.cpp:116-146).  x is overwritten (initial guess 0). */
 int mlfma_gmres(mlfma_handle h, const double* b, double* x, const mlfma_solver_opts* opts,
                 mlfma_solve_info* info);
+
+/* Far field of the currents x (host, n complex, caller order) along ndir unit
+ * directions khat (host, ndir x 3): out (host, ndir x 3 complex) =
+ * C k (I - khat khat^T) sum_n x_n f_n(k khat), the sum of Node::printFarSols
+ * (src/fmm/node.cpp:147-178) for any direction list (the reference prints it
+ * on the root's angular grid).  Allocates device scratch for the directions. */
+int mlfma_farfield(mlfma_handle h, const double* x, int ndir, const double* khat, double* out);
 
 /* GMRES that allocates no device memory.  No counterpart in the reference.
  * mlfma_gmres allocates its Krylov basis with cudaMalloc on first use; a

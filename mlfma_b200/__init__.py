@@ -196,6 +196,21 @@ class MLFMA:
             check(code)
         return x, SolveResult(info.iterations, info.residual, info.true_residual, info.seconds, converged)
 
+    def farfield(self, currents, khat) -> np.ndarray:
+        """Far field (ndir x 3 complex) of `currents` along unit directions `khat` (ndir x 3)."""
+        cur = _cvec(currents, self.n)
+        kh = np.ascontiguousarray(np.asarray(khat, dtype=np.float64).reshape(-1, 3))
+        out = np.zeros((kh.shape[0], 3), dtype=np.complex128)
+        check(lib().mlfma_farfield(self._h, cur.view(np.float64).ctypes.data_as(_dp), kh.shape[0],
+                                   kh.ctypes.data_as(_dp), out.view(np.float64).ctypes.data_as(_dp)))
+        return out
+
+    @staticmethod
+    def phi_cut(n: int = 360, theta: float = np.pi / 2) -> np.ndarray:
+        """Unit directions of a phi cut at fixed theta (n equally spaced phi)."""
+        ph = 2.0 * np.pi * np.arange(n) / n
+        return np.stack([np.sin(theta) * np.cos(ph), np.sin(theta) * np.sin(ph), np.full(n, np.cos(theta))], -1)
+
     def stream(self) -> int:
         s = ctypes.c_void_p()
         check(lib().mlfma_get_stream(self._h, ctypes.byref(s)))

@@ -27,7 +27,7 @@ class Config(ctypes.Structure):
     _fields_ = [("quad_prec", ctypes.c_int), ("digits", ctypes.c_int), ("interp_order", ctypes.c_int),
                 ("over_interp", ctypes.c_double), ("root_leng", ctypes.c_double),
                 ("max_node_srcs", ctypes.c_int), ("max_level", ctypes.c_int),
-                ("ref_compat", ctypes.c_int), ("device", ctypes.c_int)]
+                ("ref_compat", ctypes.c_int), ("device", ctypes.c_int), ("precision", ctypes.c_int)]
 
 
 class PlaneWaveC(ctypes.Structure):
@@ -78,6 +78,7 @@ SIGNATURES = {
                                            ctypes.c_void_p]),
     "mlfma_gmres": (ctypes.c_int, [ctypes.c_void_p, _dp, _dp, ctypes.POINTER(SolverOpts),
                                    ctypes.POINTER(SolveInfo)]),
+    "mlfma_farfield": (ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_int, _dp, _dp]),
     "mlfma_gmres_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                            ctypes.POINTER(SolverOpts), ctypes.POINTER(SolveInfo)]),
     "mlfma_get_stream": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]),

@@ -14,6 +14,7 @@
 struct mlfma_op_s {
     mlfma::Plan plan;
     int device = 0;
+    int precision = 0;
     std::unique_ptr<mlfma::DeviceOp> dev;
     std::unique_ptr<mlfma::Gmres> gmres;
     std::unique_ptr<mlfma::Gmres> gmres_fixed;  // runs on the library's fixed workspace
@@ -86,6 +87,7 @@ int mlfma_config_default(mlfma_config* cfg) {
     cfg->max_level = 0;
     cfg->ref_compat = 1;
     cfg->device = 0;
+    cfg->precision = MLFMA_FP64;
     return MLFMA_OK;
 }
 
@@ -95,6 +97,7 @@ int mlfma_create_dipoles(const mlfma_config* cfg, const mlfma_planewave* pw, int
     try {
         auto h = std::make_unique<mlfma_op_s>();
         h->device = cfg->device;
+        h->precision = cfg->precision;
         const std::string e = h->plan.build_dipoles(to_cfg(cfg), to_pw(pw), n, pos, mom);
         if (!e.empty()) return fail(MLFMA_ERR_ARG, e);
         *out = h.release();
@@ -110,6 +113,7 @@ int mlfma_create_rwg(const mlfma_config* cfg, const mlfma_planewave* pw, int nv,
     try {
         auto h = std::make_unique<mlfma_op_s>();
         h->device = cfg->device;
+        h->precision = cfg->precision;
         const std::string e = h->plan.build_rwg(to_cfg(cfg), to_pw(pw), nv, verts, nf, faces, ne, rwgs);
         if (!e.empty()) return fail(MLFMA_ERR_ARG, e);
         *out = h.release();
@@ -124,7 +128,7 @@ int mlfma_setup(mlfma_handle h) {
     if (h->dev) return fail(MLFMA_ERR_STATE, "already set up");
     try {
         auto dev = std::make_unique<mlfma::DeviceOp>();
-        std::string e = dev->setup(h->plan, h->device);
+        std::string e = dev->setup(h->plan, h->device, h->precision);
         if (!e.empty()) return fail(MLFMA_ERR_CUDA, e);
         if (cudaMalloc(&h->d_x, sizeof(double2) * h->plan.n) != cudaSuccess ||
             cudaMalloc(&h->d_y, sizeof(double2) * h->plan.n) != cudaSuccess)
@@ -224,6 +228,33 @@ int mlfma_gmres(mlfma_handle h, const double* b, double* x, const mlfma_solver_o
         info->seconds = r.seconds;
     }
     if (!r.converged) return fail(MLFMA_ERR_NOT_CONVERGED, "iteration limit reached");
+    return MLFMA_OK;
+}
+
+int mlfma_farfield(mlfma_handle h, const double* x, int ndir, const double* khat, double* out) {
+    if (!h || !x || (ndir > 0 && (!khat || !out)) || ndir < 0) return fail(MLFMA_ERR_ARG, "null argument");
+    if (!ready(h)) return fail(MLFMA_ERR_STATE, "mlfma_setup has not run");
+    if (ndir == 0) return MLFMA_OK;
+    if (cudaSetDevice(h->device) != cudaSuccess) return fail(MLFMA_ERR_CUDA, "cudaSetDevice failed");
+    cudaStream_t s = h->dev->stream();
+    double* d_k = nullptr;
+    double2* d_o = nullptr;
+    if (cudaMalloc(&d_k, sizeof(double) * 3 * ndir) != cudaSuccess ||
+        cudaMalloc(&d_o, sizeof(double2) * 3 * ndir) != cudaSuccess) {
+        cudaFree(d_k);
+        return fail(MLFMA_ERR_CUDA, "cudaMalloc failed");
+    }
+    std::string e;
+    if (cudaMemcpyAsync(h->d_x, x, sizeof(double2) * h->plan.n, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+        cudaMemcpyAsync(d_k, khat, sizeof(double) * 3 * ndir, cudaMemcpyHostToDevice, s) != cudaSuccess)
+        e = "copy failed";
+    if (e.empty()) e = h->dev->farfield(h->d_x, ndir, d_k, d_o, s);
+    if (e.empty() && (cudaMemcpyAsync(out, d_o, sizeof(double2) * 3 * ndir, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+                      cudaStreamSynchronize(s) != cudaSuccess))
+        e = "copy of the far field failed";
+    cudaFree(d_k);
+    cudaFree(d_o);
+    if (!e.empty()) return fail(MLFMA_ERR_CUDA, e);
     return MLFMA_OK;
 }
 

@@ -1,5 +1,11 @@
 // Device-side plan: flat arrays in HBM that the kernels read, and the launch
 // wrappers.  One DeviceOp per operator handle.
+//
+// The far field exists in one of two precisions, chosen at setup:
+//   * FP64: complex double everywhere (the reference's arithmetic);
+//   * mixed: outgoing/local patterns, radiation patterns, transfer functions,
+//     shifts and interpolation weights in complex float, accumulated in float;
+//     the near field, x, y and the combination stay complex double.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -12,43 +18,42 @@
 namespace mlfma {
 
 constexpr int kMaxLevels = 20;
-constexpr int kM2MThreads = 256;  // threads per M2M block
-constexpr int kM2MOut = 8;        // parent outputs per thread (registers)
 
-struct DevLevel {
+enum Precision { kFp64 = 0, kMixed = 1 };
+
+template <class R> struct Cx;
+template <> struct Cx<double> { using T = double2; };
+template <> struct Cx<float> { using T = float2; };
+
+template <class R>
+struct DevLevelT {
+    using C = typename Cx<R>::T;
     int nth, nph, ndir, nbox;
-    double2* A;                  // outgoing patterns [nbox][ndir][2]
-    double2* B;                  // local (incoming) patterns [nbox][ndir][2]
-    const double2* transl;       // [316][ndir]
-    const double* w;             // [ndir] quadrature weight applied after M2L
-    const double2* shift_up;     // [8][ndir]
-    const double2* shift_down;   // [8][ndir]
-    const double* thph;          // [ndir][6]
-    const double* khat;          // [ndir][3]
+    C* A;                        // outgoing patterns [nbox][ndir][2]
+    C* B;                        // local (incoming) patterns [nbox][ndir][2]
+    const C* transl;             // [316][ndir]
+    const R* w;                  // [ndir] quadrature weight applied after M2L
+    const C* shift_up;           // [8][ndir]
+    const C* shift_down;         // [8][ndir]
     const int* m2l_ptr;          // [nbox+1]
     const int* m2l_src;
     const int* m2l_off;
 };
 
-struct DevLevels {
-    DevLevel lv[kMaxLevels];
-    int lmin, lmax;
-    double k;
-    int ref_compat;
-};
-
 // Stencil rows padded to a fixed width (padding entries have coefficient 0):
 // entry k of row r is at r * width + k.  The sign of a pole-reflected tap is
 // folded into its coefficient.
-struct DevStencil {
+template <class R>
+struct DevStencilT {
     int width;
     const int* src;
     const int* refl;
-    const double* coef;
+    const R* coef;
 };
 
-struct DevTrans {
-    DevStencil up_th, up_ph, dn_ph, dn_th;
+template <class R>
+struct DevTransT {
+    DevStencilT<R> up_th, up_ph, dn_ph, dn_th;
     int plevel, npar;
     const int* par_box;
     const int* par_ilist;
@@ -62,19 +67,43 @@ struct DevFarLeaf {
     long long pat_off;
 };
 
-struct DevNearBlock {
-    int row0, nrow, col0, ncol;
-    long long off;
-    int self, pad;
-};
-
 struct DevNearRow {
     int row0, nrow, ncol, pad;
     long long off, col_off;
 };
 
+// Source geometry on the device, tree order (patterns, near field, far field).
+struct DevSources {
+    int kind;
+    double k;
+    const double* pos;      // dipole positions
+    const double* phat;     // dipole unit moments
+    const RwgGeom* rwg;     // RWG geometry
+    const TriGeom* tris;    // triangles (input order)
+    const double* tri_quad; // [tri][nq][3]
+    const double* quad_w;   // [nq]
+    int nq;
+};
+
+// Geometry the setup kernels need (patterns, near-field entries).
+struct DevGeomLevel {
+    const double* thph;  // [ndir][6]
+    const double* khat;  // [ndir][3]
+    int ndir;
+};
+
 struct StageTimes {
     float gather, s2m, m2m, m2l, l2l, l2t, near, finish, total;
+};
+
+// Far-field data in one precision.
+template <class R>
+struct FarField {
+    using C = typename Cx<R>::T;
+    DevLevelT<R> lv[kMaxLevels] = {};
+    DevLevelT<R>* lv_dev = nullptr;
+    std::vector<DevTransT<R>> trans;  // index = parent level
+    C* pat = nullptr;                 // radiation patterns [pat_elems][2]
 };
 
 class DeviceOp {
@@ -85,7 +114,7 @@ public:
     DeviceOp& operator=(const DeviceOp&) = delete;
 
     // Uploads the plan and assembles radiation patterns and near-field blocks.
-    std::string setup(const Plan& plan, int device);
+    std::string setup(const Plan& plan, int device, int precision);
 
     // y (user order) = (accumulate ? y : 0) + A x, device pointers, on `stream`
     // (0 = the operator's own stream).  Interleaved complex FP64.
@@ -99,17 +128,20 @@ public:
     // Per-stage CUDA-event timing of one matvec on the operator's stream.
     std::string time_stages(StageTimes* out);
 
+    // Far field of currents (caller order, device) along ndir unit directions
+    // (device, ndir x 3); out: ndir x 3 complex (device).
+    std::string farfield(const double2* cur, int ndir, const double* khat, double2* out, cudaStream_t s);
+
     int n() const { return n_; }
+    int precision() const { return precision_; }
     cudaStream_t stream() const { return stream_; }
-    double2* scratch_x() { return xt_; }
-    double2* scratch_y() { return yfar_; }
     const int* perm() const { return perm_; }
     int device() const { return device_; }
     long long bytes_allocated() const { return bytes_; }
     int launches_per_matvec() const;
-    const std::vector<DevFarLeaf>& far_leaves_host() const { return h_leaves_; }
 
-    // Diagnostic copies of per-level patterns (level, which: 0 outgoing, 1 local).
+    // Diagnostic copies of per-level patterns (level, which: 0 outgoing, 1 local),
+    // widened to complex double.
     std::string copy_level(int level, int which, double2* host, long long count);
 
     // Algorithmic byte counts per stage for one matvec (roofline accounting).
@@ -119,62 +151,58 @@ public:
 private:
     template <class T> T* alloc(size_t count);
     template <class T> T* upload(const std::vector<T>& v);
-    void run_far(const double2* xt, cudaStream_t s);
+    template <class R> std::string setup_far(const Plan& plan, FarField<R>& F, const double2* pat64);
+    template <class R> void run_far_t(FarField<R>& F, const double2* xt, cudaStream_t s, int stage);
+    void run_far(const double2* xt, cudaStream_t s, int stage = -1);
     void run_near(const double2* xt, cudaStream_t s);
+    void enqueue_core(cudaStream_t s);   // xt_ -> yfar_, ynear_
+    std::string ensure_graph();
+    static int m2m_rows(int nth, int nph);
 
     int device_ = 0;
     int n_ = 0;
+    int precision_ = kFp64;
     bool ready_ = false;
     cudaStream_t stream_ = nullptr, side_ = nullptr;
     cudaEvent_t ev_fork_ = nullptr, ev_join_ = nullptr;
     std::vector<void*> allocs_;
     long long bytes_ = 0;
-
-    static int m2m_rows(int nth, int nph);
-    void stage_s2m(const double2* xt, cudaStream_t s);
-    void stage_m2m(cudaStream_t s);
-    void stage_m2l(cudaStream_t s);
-    void stage_l2l(cudaStream_t s);
-    void stage_l2t(cudaStream_t s);
-    void enqueue_core(cudaStream_t s);   // xt_ -> yfar_, ynear_
-    std::string ensure_graph();
-
     cudaGraph_t graph_ = nullptr;
     cudaGraphExec_t graph_exec_ = nullptr;
     bool use_graph_ = true;
 
-    DevLevels lv_{};
-    DevLevel* lv_dev_ = nullptr;        // device copy of lv_.lv
-    std::vector<DevTrans> trans_;       // index = parent level
-    int4* m2l_items_ = nullptr;         // (level, box, first direction, count)
+    // Shared by both precisions.
+    int lmin_ = 2, lmax_ = 0, ref_compat_ = 1;
+    int nbox_[kMaxLevels] = {}, ndir_[kMaxLevels] = {}, nth_[kMaxLevels] = {}, nph_[kMaxLevels] = {};
+    int4* m2l_items_ = nullptr;          // (level, box, first direction, count)
     int n_m2l_items_ = 0;
-    std::vector<int2*> l2l_pairs_;      // per parent level: (parent, child entry)
-    std::vector<int> n_l2l_pairs_;
+    std::vector<int2*> l2l_pairs_;       // per parent level: (parent, child entry)
+    std::vector<int> n_l2l_pairs_, npar_, up_w_, dn_w_;
     int4* s2m_items_ = nullptr;          // (leaf, first element, element count)
     int n_s2m_items_ = 0;
     int4* l2t_items_ = nullptr;          // (leaf, first source, source count)
     int n_l2t_items_ = 0;
     int max_src_ = 0;                    // largest far leaf
     DevFarLeaf* leaves_ = nullptr;
-    std::vector<DevFarLeaf> h_leaves_;
     int n_leaves_ = 0;
-    double2* pat_ = nullptr;            // [pat_elems][2]
-    DevNearBlock* near_blocks_ = nullptr;
-    int n_near_blocks_ = 0;
-    double2* near_z_ = nullptr;
-    long long near_entries_ = 0;
-    DevNearRow* near_rows_ = nullptr;   // block rows (device storage of the near field)
+    FarField<double> f64_;
+    FarField<float> f32_;
+
+    DevNearRow* near_rows_ = nullptr;    // block rows (device storage of the near field)
     int n_near_rows_ = 0;
     int* near_cols_ = nullptr;
-    int4* near_items_ = nullptr;        // (row block, first row, row count)
+    int4* near_items_ = nullptr;         // (row block, first row, row count)
     int n_near_items_ = 0;
+    double2* near_z_ = nullptr;
+    long long near_entries_ = 0;
+
     int* perm_ = nullptr;
+    DevSources src_{};         // source geometry (setup kernels, far field)
     double2* xt_ = nullptr;    // tree-ordered input
     double2* yfar_ = nullptr;  // tree-ordered far result (before C k)
     double2* ynear_ = nullptr; // tree-ordered near result (before C k)
-    double2* yt_ = nullptr;    // tree-ordered total (solver use)
+    double2* yt_ = nullptr;    // tree-ordered total (stage timing)
     double2 ck_{};             // Phys::C * k
-    int max_ndir_ = 0;
     Traffic traffic_{};
 };
 

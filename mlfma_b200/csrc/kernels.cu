@@ -2,15 +2,17 @@
 // patterns and near-field blocks, and launches the MLFMA matvec
 // (kernels in kernels_far.cuh and kernels_near.cuh).
 //
-// Data layout in HBM (all complex values interleaved re/im, double2):
+// Data layout in HBM (complex values interleaved re/im):
 //   * sources are permuted into tree order so every octree box owns a
 //     contiguous range; x and y are gathered/scattered at the boundary;
 //   * per level l: outgoing patterns A_l and local patterns B_l as
 //     [box][direction][2 polarisation components];
 //   * radiation patterns as [source][direction of its leaf level][2];
 //   * transfer functions as [316 offsets][direction] per level;
-//   * near-field blocks dense row-major (list 1 and list 3/4 pairs) or
-//     strict-lower packed (self blocks), each applied as Z and Z^T.
+//   * the near field as block rows (both orientations of each reference
+//     block) with a shared column list per leaf.
+// The far-field arrays are complex double (FP64 path) or complex float (mixed
+// path); x, y and the near field are complex double in both.
 //
 // One matvec: the near field runs on a side stream while the far-field chain
 // S2M -> M2M (fine to coarse) -> M2L (all levels) -> L2L (coarse to fine) ->
@@ -22,6 +24,7 @@
 #include <cstring>
 #include <stdexcept>
 #include <string>
+#include <type_traits>
 
 #include "device.cuh"
 #include "kernels_far.cuh"
@@ -58,6 +61,24 @@ __global__ void k_finish(const double2* __restrict__ yfar, const double2* __rest
 
 inline int blocks_for(long long n, int bs) { return static_cast<int>((n + bs - 1) / bs); }
 
+template <class C> C host_c(const cplx& v);
+template <> double2 host_c<double2>(const cplx& v) { return make_double2(v.real(), v.imag()); }
+template <> float2 host_c<float2>(const cplx& v) {
+    return make_float2(static_cast<float>(v.real()), static_cast<float>(v.imag()));
+}
+template <class C> std::vector<C> conv_c(const std::vector<cplx>& v) {
+    std::vector<C> o(v.size());
+    for (size_t i = 0; i < v.size(); ++i) o[i] = host_c<C>(v[i]);
+    return o;
+}
+template <class R> std::vector<R> conv_r(const std::vector<double>& v) {
+    return std::vector<R>(v.begin(), v.end());
+}
+
+// Tap counts for which the interpolation kernels are instantiated.
+constexpr int kUpWidths[] = {2, 4, 6, 8, 10};
+constexpr int kDnWidths[] = {8, 12, 16, 24, 32};
+
 }  // namespace
 
 // ================================================================= DeviceOp
@@ -91,20 +112,106 @@ T* DeviceOp::upload(const std::vector<T>& v) {
     return p;
 }
 
-static std::vector<double2> to_d2(const std::vector<cplx>& v) {
-    std::vector<double2> o(v.size());
-    for (size_t i = 0; i < v.size(); ++i) o[i] = make_double2(v[i].real(), v[i].imag());
-    return o;
-}
-
 int DeviceOp::m2m_rows(int nth, int nph) {
     // about one parent output per thread of a 128-thread block
     return std::max(1, std::min(nth, 128 / std::max(nph, 1)));
 }
 
-std::string DeviceOp::setup(const Plan& plan, int device) {
+// Far-field arrays in precision R (levels, transitions, patterns).
+template <class R>
+std::string DeviceOp::setup_far(const Plan& plan, FarField<R>& F, const double2* pat64) {
+    using C = typename Cx<R>::T;
+    for (int l = lmin_; l <= lmax_; ++l) {
+        const Level& L = plan.levels[l];
+        DevLevelT<R>& d = F.lv[l];
+        d.nth = L.nth;
+        d.nph = L.nph;
+        d.ndir = L.ndir;
+        d.nbox = static_cast<int>(L.boxes.size());
+        const size_t cnt = static_cast<size_t>(d.nbox) * L.ndir * 2;
+        d.A = alloc<C>(cnt);
+        d.B = alloc<C>(cnt);
+        MLFMA_CK(cudaMemset(d.A, 0, cnt * sizeof(C)));
+        MLFMA_CK(cudaMemset(d.B, 0, cnt * sizeof(C)));
+        d.transl = upload(conv_c<C>(L.transl));
+        d.w = upload(conv_r<R>(L.m2l_w));
+        d.shift_up = upload(conv_c<C>(L.shift_up));
+        d.shift_down = upload(conv_c<C>(L.shift_down));
+        d.m2l_ptr = upload(L.m2l_ptr);
+        d.m2l_src = upload(L.m2l_src);
+        d.m2l_off = upload(L.m2l_off);
+    }
+    F.lv_dev = upload(std::vector<DevLevelT<R>>(F.lv, F.lv + kMaxLevels));
+    F.trans.assign(std::max(lmax_, 0) + 1, DevTransT<R>{});
+    for (int p = lmin_; p < lmax_; ++p) {
+        const Transition& T = plan.trans[p];
+        DevTransT<R>& d = F.trans[p];
+        auto st = [&](const Stencil& s, int w) {
+            // pad rows to a fixed width; fold the reflection sign into the coefficient
+            const int rows = static_cast<int>(s.ptr.size()) - 1;
+            std::vector<int> src(static_cast<size_t>(rows) * w, 0), refl(static_cast<size_t>(rows) * w, 0);
+            std::vector<R> coef(static_cast<size_t>(rows) * w, R(0));
+            for (int r = 0; r < rows; ++r)
+                for (int q = s.ptr[r]; q < s.ptr[r + 1]; ++q) {
+                    const size_t at = static_cast<size_t>(r) * w + (q - s.ptr[r]);
+                    src[at] = s.src[q];
+                    refl[at] = s.refl[q];
+                    coef[at] = static_cast<R>(s.refl[q] ? -s.coef[q] : s.coef[q]);
+                }
+            return DevStencilT<R>{w, upload(src), upload(refl), upload(coef)};
+        };
+        d.up_th = st(T.up_th, up_w_[p]);
+        d.up_ph = st(T.up_ph, up_w_[p]);
+        d.dn_ph = st(T.dn_ph, dn_w_[p]);
+        d.dn_th = st(T.dn_th, dn_w_[p]);
+        d.plevel = p;
+        d.npar = static_cast<int>(T.par_box.size());
+        d.par_box = upload(T.par_box);
+        d.par_ilist = upload(T.par_ilist);
+        d.child_ptr = upload(T.child_ptr);
+        d.child_box = upload(T.child_box);
+        d.child_oct = upload(T.child_oct);
+    }
+    if (std::is_same<R, double>::value) {
+        F.pat = reinterpret_cast<C*>(const_cast<double2*>(pat64));
+    } else {
+        const long long cnt = plan.pat_elems * 2;
+        F.pat = alloc<C>(static_cast<size_t>(cnt));
+        if (cnt) k_narrow<C><<<blocks_for(cnt, 256), 256, 0, stream_>>>(pat64, F.pat, cnt);
+        MLFMA_CK(cudaGetLastError());
+    }
+    // Shared-memory limits.
+    size_t m2m_smem = 1, l2l_smem = 1;
+    for (int p = lmin_; p < lmax_; ++p) {
+        m2m_smem = std::max(m2m_smem, static_cast<size_t>(8) * m2m_rows(nth_[p], nph_[p]) * nph_[p + 1] * 2 * sizeof(C));
+        l2l_smem = std::max(l2l_smem, static_cast<size_t>(nth_[p]) * nph_[p + 1] * 2 * sizeof(C));
+    }
+    int dev_smem = 0;
+    MLFMA_CK(cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, device_));
+    const size_t s2m_smem = static_cast<size_t>(std::max(1, max_src_)) * sizeof(C);
+    if (m2m_smem > static_cast<size_t>(dev_smem) || l2l_smem > static_cast<size_t>(dev_smem) ||
+        s2m_smem > static_cast<size_t>(dev_smem))
+        return "angular grid or leaf too large for the kernels' shared memory";
+    const auto attr = cudaFuncAttributeMaxDynamicSharedMemorySize;
+    MLFMA_CK(cudaFuncSetAttribute(k_m2m<R, 2>, attr, static_cast<int>(m2m_smem)));
+    MLFMA_CK(cudaFuncSetAttribute(k_m2m<R, 4>, attr, static_cast<int>(m2m_smem)));
+    MLFMA_CK(cudaFuncSetAttribute(k_m2m<R, 6>, attr, static_cast<int>(m2m_smem)));
+    MLFMA_CK(cudaFuncSetAttribute(k_m2m<R, 8>, attr, static_cast<int>(m2m_smem)));
+    MLFMA_CK(cudaFuncSetAttribute(k_m2m<R, 10>, attr, static_cast<int>(m2m_smem)));
+    MLFMA_CK(cudaFuncSetAttribute(k_l2l<R, 8>, attr, static_cast<int>(l2l_smem)));
+    MLFMA_CK(cudaFuncSetAttribute(k_l2l<R, 12>, attr, static_cast<int>(l2l_smem)));
+    MLFMA_CK(cudaFuncSetAttribute(k_l2l<R, 16>, attr, static_cast<int>(l2l_smem)));
+    MLFMA_CK(cudaFuncSetAttribute(k_l2l<R, 24>, attr, static_cast<int>(l2l_smem)));
+    MLFMA_CK(cudaFuncSetAttribute(k_l2l<R, 32>, attr, static_cast<int>(l2l_smem)));
+    MLFMA_CK(cudaFuncSetAttribute(k_s2m<R>, attr, static_cast<int>(s2m_smem)));
+    return {};
+}
+
+std::string DeviceOp::setup(const Plan& plan, int device, int precision) {
     try {
         device_ = device;
+        precision_ = precision;
+        if (precision != kFp64 && precision != kMixed) return "precision must be 0 (FP64) or 1 (mixed)";
         MLFMA_CK(cudaSetDevice(device));
         MLFMA_CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
         MLFMA_CK(cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking));
@@ -119,125 +226,80 @@ std::string DeviceOp::setup(const Plan& plan, int device) {
         yfar_ = alloc<double2>(n_);
         ynear_ = alloc<double2>(n_);
         yt_ = alloc<double2>(n_);
-
-        // ---- levels
-        std::memset(&lv_, 0, sizeof(lv_));
-        lv_.lmin = plan.lmin;
-        lv_.lmax = plan.max_level;
-        lv_.k = plan.pw.wavenum;
-        lv_.ref_compat = plan.cfg.ref_compat;
+        lmin_ = plan.lmin;
+        lmax_ = plan.max_level;
+        ref_compat_ = plan.cfg.ref_compat;
         traffic_ = Traffic{};
+        const double cbytes = precision == kFp64 ? 16.0 : 8.0;  // one far-field complex value
+
+        // ---- level sizes and M2L work items: direction chunks of at most 128
         std::vector<int4> items;
-        for (int l = plan.lmin; l <= plan.max_level; ++l) {
+        for (int l = lmin_; l <= lmax_; ++l) {
             const Level& L = plan.levels[l];
-            DevLevel& d = lv_.lv[l];
-            d.nth = L.nth;
-            d.nph = L.nph;
-            d.ndir = L.ndir;
-            d.nbox = static_cast<int>(L.boxes.size());
-            const size_t cnt = static_cast<size_t>(d.nbox) * L.ndir * 2;
-            d.A = alloc<double2>(cnt);
-            d.B = alloc<double2>(cnt);
-            MLFMA_CK(cudaMemset(d.A, 0, cnt * sizeof(double2)));
-            MLFMA_CK(cudaMemset(d.B, 0, cnt * sizeof(double2)));
-            d.transl = upload(to_d2(L.transl));
-            d.w = upload(L.m2l_w);
-            d.shift_up = upload(to_d2(L.shift_up));
-            d.shift_down = upload(to_d2(L.shift_down));
-            d.thph = upload(L.thph);
-            d.khat = upload(L.khat);
-            d.m2l_ptr = upload(L.m2l_ptr);
-            d.m2l_src = upload(L.m2l_src);
-            d.m2l_off = upload(L.m2l_off);
-            max_ndir_ = std::max(max_ndir_, L.ndir);
+            nbox_[l] = static_cast<int>(L.boxes.size());
+            ndir_[l] = L.ndir;
+            nth_[l] = L.nth;
+            nph_[l] = L.nph;
+            const double cnt = static_cast<double>(nbox_[l]) * L.ndir * 2;
             // M2L reads every source box's pattern and the transfer table once
             // (repeats hit L2) and writes every local pattern once.
-            traffic_.m2l += static_cast<double>(cnt) * 16.0 * 2.0 + 316.0 * L.ndir * 16.0;
-            // M2L work items: direction chunks of at most 128 of equal size.
+            traffic_.m2l += cnt * cbytes * 2.0 + 316.0 * L.ndir * cbytes;
             const int nchunk = (L.ndir + 127) / 128;
             const int chunk = (L.ndir + nchunk - 1) / nchunk;
-            for (int b = 0; b < d.nbox; ++b) {
-                if (plan.cfg.ref_compat && L.m2l_ptr[b + 1] == L.m2l_ptr[b]) continue;
-                for (int d0 = 0; d0 < L.ndir; d0 += chunk) items.push_back(make_int4(l, b, d0, std::min(chunk, L.ndir - d0)));
+            for (int b = 0; b < nbox_[l]; ++b) {
+                if (ref_compat_ && L.m2l_ptr[b + 1] == L.m2l_ptr[b]) continue;
+                for (int d0 = 0; d0 < L.ndir; d0 += chunk)
+                    items.push_back(make_int4(l, b, d0, std::min(chunk, L.ndir - d0)));
             }
         }
-        lv_dev_ = upload(std::vector<DevLevel>(lv_.lv, lv_.lv + kMaxLevels));
         n_m2l_items_ = static_cast<int>(items.size());
         m2l_items_ = upload(items);
 
-        // ---- transitions
-        trans_.assign(std::max(plan.max_level, 0) + 1, DevTrans{});
-        l2l_pairs_.assign(std::max(plan.max_level, 0) + 1, nullptr);
-        n_l2l_pairs_.assign(std::max(plan.max_level, 0) + 1, 0);
-        size_t m2m_smem = 0, l2l_smem = 0;
-        for (int p = plan.lmin; p < plan.max_level; ++p) {
+        // ---- transitions: L2L pairs and stencil widths
+        l2l_pairs_.assign(std::max(lmax_, 0) + 1, nullptr);
+        n_l2l_pairs_.assign(std::max(lmax_, 0) + 1, 0);
+        npar_.assign(std::max(lmax_, 0) + 1, 0);
+        up_w_.assign(std::max(lmax_, 0) + 1, 0);
+        dn_w_.assign(std::max(lmax_, 0) + 1, 0);
+        for (int p = lmin_; p < lmax_; ++p) {
             const Transition& T = plan.trans[p];
-            DevTrans& d = trans_[p];
             auto width_of = [](const Stencil& s) {
                 int w = 1;
                 for (size_t r = 0; r + 1 < s.ptr.size(); ++r) w = std::max(w, s.ptr[r + 1] - s.ptr[r]);
                 return w;
             };
-            // The kernels are instantiated for fixed tap counts (fully unrolled).
             const int w_up = width_of(T.up_th);
-            if (w_up != width_of(T.up_ph) || w_up % 2 || w_up < 2 || w_up > 10)
+            if (w_up != width_of(T.up_ph) || std::find(std::begin(kUpWidths), std::end(kUpWidths), w_up) ==
+                                                 std::end(kUpWidths))
                 return "interp_order must be 1..5";
-            const int w_dn_need = std::max(width_of(T.dn_ph), width_of(T.dn_th));
+            const int need = std::max(width_of(T.dn_ph), width_of(T.dn_th));
             int w_dn = 0;
-            for (int c : {8, 12, 16, 24, 32})
-                if (!w_dn && w_dn_need <= c) w_dn = c;
+            for (int c : kDnWidths)
+                if (!w_dn && need <= c) w_dn = c;
             if (!w_dn) return "anterpolation stencil wider than 32 taps";
-            auto st = [&](const Stencil& s, int wpad) {
-                // pad rows to a fixed width; fold the reflection sign into the coefficient
-                const int rows = static_cast<int>(s.ptr.size()) - 1;
-                const int w = wpad;
-                std::vector<int> src(static_cast<size_t>(rows) * w, 0), refl(static_cast<size_t>(rows) * w, 0);
-                std::vector<double> coef(static_cast<size_t>(rows) * w, 0.0);
-                for (int r = 0; r < rows; ++r)
-                    for (int q = s.ptr[r]; q < s.ptr[r + 1]; ++q) {
-                        const size_t at = static_cast<size_t>(r) * w + (q - s.ptr[r]);
-                        src[at] = s.src[q];
-                        refl[at] = s.refl[q];
-                        coef[at] = s.refl[q] ? -s.coef[q] : s.coef[q];
-                    }
-                return DevStencil{w, upload(src), upload(refl), upload(coef)};
-            };
-            d.up_th = st(T.up_th, w_up);
-            d.up_ph = st(T.up_ph, w_up);
-            d.dn_ph = st(T.dn_ph, w_dn);
-            d.dn_th = st(T.dn_th, w_dn);
-            d.plevel = p;
-            d.npar = static_cast<int>(T.par_box.size());
-            d.par_box = upload(T.par_box);
-            d.par_ilist = upload(T.par_ilist);
-            d.child_ptr = upload(T.child_ptr);
-            d.child_box = upload(T.child_box);
-            d.child_oct = upload(T.child_oct);
+            up_w_[p] = w_up;
+            dn_w_[p] = w_dn;
+            npar_[p] = static_cast<int>(T.par_box.size());
             std::vector<int2> pairs;
-            for (int q = 0; q < d.npar; ++q) {
-                if (plan.cfg.ref_compat && !T.par_ilist[q]) continue;  // stem.cpp:115
+            for (int q = 0; q < npar_[p]; ++q) {
+                if (ref_compat_ && !T.par_ilist[q]) continue;  // stem.cpp:115
                 for (int c = T.child_ptr[q]; c < T.child_ptr[q + 1]; ++c) pairs.push_back(make_int2(q, c));
             }
             n_l2l_pairs_[p] = static_cast<int>(pairs.size());
             l2l_pairs_[p] = upload(pairs);
-            const Level& Lp = plan.levels[p];
-            const Level& Lc = plan.levels[p + 1];
             const double nch = static_cast<double>(T.child_box.size());
-            traffic_.m2m += nch * Lc.ndir * 32.0 + d.npar * Lp.ndir * 32.0;
-            traffic_.l2l += d.npar * Lp.ndir * 32.0 + nch * Lc.ndir * 32.0 * 2.0;
-            m2m_smem = std::max(m2m_smem, static_cast<size_t>(8) * m2m_rows(Lp.nth, Lp.nph) * Lc.nph * 2 * sizeof(double2));
-            l2l_smem = std::max(l2l_smem, static_cast<size_t>(Lp.nth) * Lc.nph * 2 * sizeof(double2));
+            traffic_.m2m += (nch * ndir_[p + 1] + npar_[p] * ndir_[p]) * 2.0 * cbytes;
+            traffic_.l2l += (npar_[p] * ndir_[p] + nch * ndir_[p + 1] * 2.0) * 2.0 * cbytes;
         }
 
-        // ---- far leaves (grouped by level for S2M/L2T) and radiation patterns
-        h_leaves_.clear();
+        // ---- far leaves and work items
+        std::vector<DevFarLeaf> h_leaves;
         std::vector<DevFarLeafGeom> geo;
         std::vector<int4> s2m_items, l2t_items;
         max_src_ = 0;
         for (const FarLeaf& f : plan.far_leaves) {
-            const DevFarLeaf dl{f.level, f.box, f.src0, f.nsrc, f.pat_off};
-            h_leaves_.push_back(dl);
-            const int li = static_cast<int>(h_leaves_.size()) - 1;
+            h_leaves.push_back(DevFarLeaf{f.level, f.box, f.src0, f.nsrc, f.pat_off});
+            const int li = static_cast<int>(h_leaves.size()) - 1;
             const int ne = 2 * plan.levels[f.level].ndir;
             const int nchunk = (ne + kS2MThreads - 1) / kS2MThreads;
             const int chunk = (ne + nchunk - 1) / nchunk;
@@ -248,17 +310,16 @@ std::string DeviceOp::setup(const Plan& plan, int device) {
             const Node& nd = plan.nodes[plan.levels[f.level].boxes[f.box]];
             geo.push_back(DevFarLeafGeom{{nd.center[0], nd.center[1], nd.center[2]}});
         }
+        n_leaves_ = static_cast<int>(h_leaves.size());
+        leaves_ = upload(h_leaves);
         n_s2m_items_ = static_cast<int>(s2m_items.size());
         s2m_items_ = upload(s2m_items);
         n_l2t_items_ = static_cast<int>(l2t_items.size());
         l2t_items_ = upload(l2t_items);
-        n_leaves_ = static_cast<int>(h_leaves_.size());
-        leaves_ = upload(h_leaves_);
-        DevFarLeafGeom* d_geo = upload(geo);
-        pat_ = alloc<double2>(static_cast<size_t>(plan.pat_elems) * 2);
-        traffic_.s2m = plan.pat_elems * 32.0 + n_ * 16.0;
-        traffic_.l2t = plan.pat_elems * 32.0 + n_ * 16.0;
+        traffic_.s2m = plan.pat_elems * 2.0 * cbytes + n_ * 16.0;
+        traffic_.l2t = plan.pat_elems * 2.0 * cbytes + n_ * 16.0;
 
+        // ---- radiation patterns (complex double first)
         DevSources S{};
         S.kind = plan.kind;
         S.k = plan.pw.wavenum;
@@ -272,26 +333,47 @@ std::string DeviceOp::setup(const Plan& plan, int device) {
             S.quad_w = upload(plan.quad_w);
             S.nq = plan.nq;
         }
+        src_ = S;
+        double2* pat64 = nullptr;
+        if (precision == kFp64) {
+            pat64 = alloc<double2>(static_cast<size_t>(plan.pat_elems) * 2);
+        } else {
+            MLFMA_CK(cudaMalloc(&pat64, sizeof(double2) * std::max<long long>(1, plan.pat_elems * 2)));
+        }
         if (n_leaves_ > 0 && plan.kind == kRwg && plan.cfg.ref_compat) {
             // Reference-compatible RWG patterns: the closed-form integral is
             // ill-conditioned near alpha, beta, gamma = 0, so it is evaluated on
             // the host with the reference's exact rounding and uploaded.
             std::vector<cplx> hp;
             plan.rwg_patterns_host(hp);
-            MLFMA_CK(cudaMemcpy(pat_, hp.data(), hp.size() * sizeof(cplx), cudaMemcpyHostToDevice));
+            MLFMA_CK(cudaMemcpy(pat64, hp.data(), hp.size() * sizeof(cplx), cudaMemcpyHostToDevice));
         } else if (n_leaves_ > 0) {
-            k_patterns<<<n_leaves_, 256, 0, stream_>>>(lv_dev_, leaves_, d_geo, S, pat_);
+            std::vector<DevGeomLevel> gl(kMaxLevels, DevGeomLevel{nullptr, nullptr, 0});
+            for (int l = lmin_; l <= lmax_; ++l)
+                gl[l] = DevGeomLevel{upload(plan.levels[l].thph), upload(plan.levels[l].khat), plan.levels[l].ndir};
+            DevGeomLevel* d_gl = upload(gl);
+            DevFarLeafGeom* d_geo = upload(geo);
+            k_patterns<<<n_leaves_, 256, 0, stream_>>>(d_gl, leaves_, d_geo, S, pat64);
             MLFMA_CK(cudaGetLastError());
         }
 
-        // ---- near field
-        // Stored as block rows (both orientations): gather-only application.
+        // ---- far field in the chosen precision
+        std::string err = precision == kFp64 ? setup_far<double>(plan, f64_, pat64)
+                                             : setup_far<float>(plan, f32_, pat64);
+        if (!err.empty()) return err;
+        if (precision != kFp64) {
+            MLFMA_CK(cudaStreamSynchronize(stream_));
+            cudaFree(pat64);
+        }
+
+        // ---- near field: block rows (both orientations), gather-only application
         std::vector<DevNearRow> nr;
         std::vector<int4> nitems;
         for (const NearRow& r : plan.near_rows) {
             nr.push_back(DevNearRow{r.row0, r.nrow, r.ncol, 0, r.off, r.col_off});
             for (int i0 = 0; i0 < r.nrow; i0 += kNearRowsPerBlock)
-                nitems.push_back(make_int4(static_cast<int>(nr.size()) - 1, i0, std::min(kNearRowsPerBlock, r.nrow - i0), 0));
+                nitems.push_back(
+                    make_int4(static_cast<int>(nr.size()) - 1, i0, std::min(kNearRowsPerBlock, r.nrow - i0), 0));
         }
         n_near_rows_ = static_cast<int>(nr.size());
         near_rows_ = upload(nr);
@@ -307,31 +389,6 @@ std::string DeviceOp::setup(const Plan& plan, int device) {
         }
         traffic_.near = near_entries_ * 16.0 + n_ * 16.0 * 2.0;
         traffic_.total = traffic_.s2m + traffic_.m2m + traffic_.m2l + traffic_.l2l + traffic_.l2t + traffic_.near;
-
-        // Shared-memory limits.
-        int dev_smem = 0;
-        MLFMA_CK(cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
-        const size_t s2m_smem = static_cast<size_t>(std::max(1, max_src_)) * sizeof(double2);
-        if (m2m_smem > static_cast<size_t>(dev_smem) || l2l_smem > static_cast<size_t>(dev_smem) ||
-            s2m_smem > static_cast<size_t>(dev_smem))
-            return "angular grid or leaf too large for the kernels' shared memory";
-        {
-            const int a = static_cast<int>(std::max<size_t>(m2m_smem, 1));
-            const int b = static_cast<int>(std::max<size_t>(l2l_smem, 1));
-            const auto attr = cudaFuncAttributeMaxDynamicSharedMemorySize;
-            MLFMA_CK(cudaFuncSetAttribute(k_m2m<2>, attr, a));
-            MLFMA_CK(cudaFuncSetAttribute(k_m2m<4>, attr, a));
-            MLFMA_CK(cudaFuncSetAttribute(k_m2m<6>, attr, a));
-            MLFMA_CK(cudaFuncSetAttribute(k_m2m<8>, attr, a));
-            MLFMA_CK(cudaFuncSetAttribute(k_m2m<10>, attr, a));
-            MLFMA_CK(cudaFuncSetAttribute(k_l2l<8>, attr, b));
-            MLFMA_CK(cudaFuncSetAttribute(k_l2l<12>, attr, b));
-            MLFMA_CK(cudaFuncSetAttribute(k_l2l<16>, attr, b));
-            MLFMA_CK(cudaFuncSetAttribute(k_l2l<24>, attr, b));
-            MLFMA_CK(cudaFuncSetAttribute(k_l2l<32>, attr, b));
-        }
-        MLFMA_CK(cudaFuncSetAttribute(k_s2m, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      static_cast<int>(std::max<size_t>(s2m_smem, 1))));
         MLFMA_CK(cudaStreamSynchronize(stream_));
         MLFMA_CK(cudaGetLastError());
         ready_ = true;
@@ -345,9 +402,9 @@ int DeviceOp::launches_per_matvec() const {
     int n = 2;  // gather + finish
     if (n_leaves_) {
         n += 2;  // S2M + L2T
-        for (int p = lv_.lmin; p < lv_.lmax; ++p) {
-            if (trans_[p].npar) n += 1;    // M2M
-            if (n_l2l_pairs_[p]) n += 1;   // L2L
+        for (int p = lmin_; p < lmax_; ++p) {
+            if (npar_[p]) n += 1;           // M2M
+            if (n_l2l_pairs_[p]) n += 1;    // L2L
         }
         if (n_m2l_items_) n += 1;
     }
@@ -355,61 +412,51 @@ int DeviceOp::launches_per_matvec() const {
     return n;
 }
 
-void DeviceOp::stage_s2m(const double2* xt, cudaStream_t s) {
-    if (n_s2m_items_)
-        k_s2m<<<n_s2m_items_, kS2MThreads, sizeof(double2) * std::max(1, max_src_), s>>>(lv_dev_, s2m_items_, leaves_,
-                                                                                         pat_, xt);
-}
-
-void DeviceOp::stage_m2m(cudaStream_t s) {
-    for (int p = lv_.lmax - 1; p >= lv_.lmin; --p) {
-        const DevTrans& T = trans_[p];
-        if (T.npar == 0) continue;
-        const DevLevel& P = lv_.lv[p];
-        const DevLevel& C = lv_.lv[p + 1];
-        const int rows = m2m_rows(P.nth, P.nph);
-        const dim3 grid(T.npar, (P.nth + rows - 1) / rows);
-        const size_t smem = static_cast<size_t>(8) * rows * C.nph * 2 * sizeof(double2);
-        switch (T.up_th.width) {
-            case 2: k_m2m<2><<<grid, 128, smem, s>>>(lv_dev_, T, rows); break;
-            case 4: k_m2m<4><<<grid, 128, smem, s>>>(lv_dev_, T, rows); break;
-            case 6: k_m2m<6><<<grid, 128, smem, s>>>(lv_dev_, T, rows); break;
-            case 8: k_m2m<8><<<grid, 128, smem, s>>>(lv_dev_, T, rows); break;
-            default: k_m2m<10><<<grid, 128, smem, s>>>(lv_dev_, T, rows); break;
-        }
-    }
-}
-
-void DeviceOp::stage_m2l(cudaStream_t s) {
-    if (n_m2l_items_) k_m2l<<<n_m2l_items_, 128, 0, s>>>(lv_dev_, m2l_items_, lv_.ref_compat ? 0 : 1);
-}
-
-void DeviceOp::stage_l2l(cudaStream_t s) {
-    for (int p = lv_.lmin; p < lv_.lmax; ++p) {
-        if (!n_l2l_pairs_[p]) continue;
-        const size_t smem = static_cast<size_t>(lv_.lv[p].nth) * lv_.lv[p + 1].nph * 2 * sizeof(double2);
-        const int g = n_l2l_pairs_[p];
-        switch (trans_[p].dn_ph.width) {
-            case 8: k_l2l<8><<<g, 256, smem, s>>>(lv_dev_, trans_[p], l2l_pairs_[p]); break;
-            case 12: k_l2l<12><<<g, 256, smem, s>>>(lv_dev_, trans_[p], l2l_pairs_[p]); break;
-            case 16: k_l2l<16><<<g, 256, smem, s>>>(lv_dev_, trans_[p], l2l_pairs_[p]); break;
-            case 24: k_l2l<24><<<g, 256, smem, s>>>(lv_dev_, trans_[p], l2l_pairs_[p]); break;
-            default: k_l2l<32><<<g, 256, smem, s>>>(lv_dev_, trans_[p], l2l_pairs_[p]); break;
-        }
-    }
-}
-
-void DeviceOp::stage_l2t(cudaStream_t s) {
-    if (n_l2t_items_) k_l2t<<<n_l2t_items_, kL2TThreads, 0, s>>>(lv_dev_, l2t_items_, leaves_, pat_, yfar_);
-}
-
-void DeviceOp::run_far(const double2* xt, cudaStream_t s) {
+// stage: -1 all, 0 S2M, 1 M2M, 2 M2L, 3 L2L, 4 L2T.
+template <class R>
+void DeviceOp::run_far_t(FarField<R>& F, const double2* xt, cudaStream_t s, int stage) {
+    using C = typename Cx<R>::T;
     if (n_leaves_ == 0) return;
-    stage_s2m(xt, s);
-    stage_m2m(s);
-    stage_m2l(s);
-    stage_l2l(s);
-    stage_l2t(s);
+    if ((stage < 0 || stage == 0) && n_s2m_items_)
+        k_s2m<R><<<n_s2m_items_, kS2MThreads, sizeof(C) * std::max(1, max_src_), s>>>(F.lv_dev, s2m_items_, leaves_,
+                                                                                        F.pat, xt);
+    if (stage < 0 || stage == 1)
+        for (int p = lmax_ - 1; p >= lmin_; --p) {
+            if (npar_[p] == 0) continue;
+            const int rows = m2m_rows(nth_[p], nph_[p]);
+            const dim3 grid(npar_[p], (nth_[p] + rows - 1) / rows);
+            const size_t smem = static_cast<size_t>(8) * rows * nph_[p + 1] * 2 * sizeof(C);
+            const DevTransT<R>& T = F.trans[p];
+            switch (up_w_[p]) {
+                case 2: k_m2m<R, 2><<<grid, 128, smem, s>>>(F.lv_dev, T, rows); break;
+                case 4: k_m2m<R, 4><<<grid, 128, smem, s>>>(F.lv_dev, T, rows); break;
+                case 6: k_m2m<R, 6><<<grid, 128, smem, s>>>(F.lv_dev, T, rows); break;
+                case 8: k_m2m<R, 8><<<grid, 128, smem, s>>>(F.lv_dev, T, rows); break;
+                default: k_m2m<R, 10><<<grid, 128, smem, s>>>(F.lv_dev, T, rows); break;
+            }
+        }
+    if ((stage < 0 || stage == 2) && n_m2l_items_)
+        k_m2l<R><<<n_m2l_items_, 128, 0, s>>>(F.lv_dev, m2l_items_, ref_compat_ ? 0 : 1);
+    if (stage < 0 || stage == 3)
+        for (int p = lmin_; p < lmax_; ++p) {
+            const int g = n_l2l_pairs_[p];
+            if (!g) continue;
+            const size_t smem = static_cast<size_t>(nth_[p]) * nph_[p + 1] * 2 * sizeof(C);
+            const DevTransT<R>& T = F.trans[p];
+            switch (dn_w_[p]) {
+                case 8: k_l2l<R, 8><<<g, 256, smem, s>>>(F.lv_dev, T, l2l_pairs_[p]); break;
+                case 12: k_l2l<R, 12><<<g, 256, smem, s>>>(F.lv_dev, T, l2l_pairs_[p]); break;
+                case 16: k_l2l<R, 16><<<g, 256, smem, s>>>(F.lv_dev, T, l2l_pairs_[p]); break;
+                case 24: k_l2l<R, 24><<<g, 256, smem, s>>>(F.lv_dev, T, l2l_pairs_[p]); break;
+                default: k_l2l<R, 32><<<g, 256, smem, s>>>(F.lv_dev, T, l2l_pairs_[p]); break;
+            }
+        }
+    if ((stage < 0 || stage == 4) && n_l2t_items_)
+        k_l2t<R><<<n_l2t_items_, kL2TThreads, 0, s>>>(F.lv_dev, l2t_items_, leaves_, F.pat, yfar_);
+}
+
+void DeviceOp::run_far(const double2* xt, cudaStream_t s, int stage) {
+    if (precision_ == kFp64) run_far_t(f64_, xt, s, stage); else run_far_t(f32_, xt, s, stage);
 }
 
 void DeviceOp::run_near(const double2* xt, cudaStream_t s) {
@@ -475,16 +522,10 @@ std::string DeviceOp::time_stages(StageTimes* out) {
     cudaMemsetAsync(yfar_, 0, sizeof(double2) * n_, s);
     cudaMemsetAsync(ynear_, 0, sizeof(double2) * n_, s);
     cudaEventRecord(ev[1], s);
-    if (n_leaves_) stage_s2m(xt_, s);
-    cudaEventRecord(ev[2], s);
-    if (n_leaves_) stage_m2m(s);
-    cudaEventRecord(ev[3], s);
-    if (n_leaves_) stage_m2l(s);
-    cudaEventRecord(ev[4], s);
-    if (n_leaves_) stage_l2l(s);
-    cudaEventRecord(ev[5], s);
-    if (n_leaves_) stage_l2t(s);
-    cudaEventRecord(ev[6], s);
+    for (int st = 0; st < 5; ++st) {
+        run_far(xt_, s, st);
+        cudaEventRecord(ev[2 + st], s);
+    }
     run_near(xt_, s);
     cudaEventRecord(ev[7], s);
     k_finish<<<blocks_for(n_, 256), 256, 0, s>>>(yfar_, ynear_, nullptr, yt_, n_, ck_, 0);
@@ -506,14 +547,42 @@ std::string DeviceOp::time_stages(StageTimes* out) {
     return {};
 }
 
+std::string DeviceOp::farfield(const double2* cur, int ndir, const double* khat, double2* out, cudaStream_t s) {
+    if (!ready_) return "operator not set up";
+    if (ndir <= 0) return {};
+    MLFMA_CK(cudaSetDevice(device_));
+    k_farfield<<<ndir, kFarThreads, 0, s>>>(src_, perm_, cur, n_, khat, ck_, out);
+    MLFMA_CK(cudaGetLastError());
+    return {};
+}
+
+namespace {
+template <class C>
+__global__ void k_widen(const C* __restrict__ src, double2* __restrict__ dst, long long n) {
+    const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = to_d2(src[i]);
+}
+}  // namespace
+
 std::string DeviceOp::copy_level(int level, int which, double2* host, long long count) {
-    if (level < lv_.lmin || level > lv_.lmax) return "level out of range";
-    const DevLevel& d = lv_.lv[level];
-    const long long cnt = static_cast<long long>(d.nbox) * d.ndir * 2;
+    if (level < lmin_ || level > lmax_) return "level out of range";
+    const long long cnt = static_cast<long long>(nbox_[level]) * ndir_[level] * 2;
     if (count < cnt) return "buffer too small";
     MLFMA_CK(cudaSetDevice(device_));
     MLFMA_CK(cudaStreamSynchronize(stream_));
-    MLFMA_CK(cudaMemcpy(host, which ? d.B : d.A, cnt * sizeof(double2), cudaMemcpyDeviceToHost));
+    if (precision_ == kFp64) {
+        const DevLevelT<double>& d = f64_.lv[level];
+        MLFMA_CK(cudaMemcpy(host, which ? d.B : d.A, cnt * sizeof(double2), cudaMemcpyDeviceToHost));
+        return {};
+    }
+    const DevLevelT<float>& d = f32_.lv[level];
+    double2* tmp = yt_;  // reuse work space in chunks of n
+    for (long long o = 0; o < cnt; o += n_) {
+        const long long m = std::min<long long>(n_, cnt - o);
+        k_widen<float2><<<blocks_for(m, 256), 256, 0, stream_>>>((which ? d.B : d.A) + o, tmp, m);
+        MLFMA_CK(cudaMemcpyAsync(host + o, tmp, m * sizeof(double2), cudaMemcpyDeviceToHost, stream_));
+        MLFMA_CK(cudaStreamSynchronize(stream_));
+    }
     return {};
 }
 

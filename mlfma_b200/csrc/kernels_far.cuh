@@ -1,10 +1,12 @@
-// Far-field kernels of the MLFMA matvec (FP64): aggregation (S2M),
-// interpolation (M2M), translation (M2L), anterpolation (L2L) and
-// disaggregation (L2T).  Included once, by kernels.cu.
+// Far-field kernels of the MLFMA matvec: aggregation (S2M), interpolation
+// (M2M), translation (M2L), anterpolation (L2L) and disaggregation (L2T).
+// Templated on the real type R of the far field (double: FP64 path; float:
+// mixed path, complex float storage with float accumulation).  Included once,
+// by kernels.cu.
 //
 // Layout: per level, patterns are [box][direction][2 components] complex;
 // element e = 2*direction + component runs contiguously, so a box's
-// pattern is one contiguous run of 2*ndir double2 values.
+// pattern is one contiguous run of 2*ndir values.
 #pragma once
 
 #include "device.cuh"
@@ -17,29 +19,32 @@ namespace {
 // a_B[e] = sum_n x_n R_n[e]  (Leaf::buildMpoleCoeffs, src/fmm/leaf.cpp:212-230).
 // One block per work item (leaf, run of at most kS2MThreads elements), all leaf
 // levels in one launch; one thread per element e (direction, component), so
-// every pattern row is read once with 16-byte coalesced loads; eight sources
-// are in flight per thread.
+// every pattern row is read once with coalesced loads; eight sources are in
+// flight per thread.
 constexpr int kS2MThreads = 352;
 constexpr int kL2TThreads = 256;
 constexpr int kL2TSrcPerBlock = kL2TThreads / 32;
 
+template <class R>
 __global__ void __launch_bounds__(kS2MThreads)
-k_s2m(const DevLevel* __restrict__ lvs, const int4* __restrict__ items, const DevFarLeaf* __restrict__ leaves,
-      const double2* __restrict__ pat, const double2* __restrict__ x) {
-    extern __shared__ double2 xs[];
+k_s2m(const DevLevelT<R>* __restrict__ lvs, const int4* __restrict__ items, const DevFarLeaf* __restrict__ leaves,
+      const typename Cx<R>::T* __restrict__ pat, const double2* __restrict__ x) {
+    using C = typename Cx<R>::T;
+    extern __shared__ unsigned char smraw[];
+    C* xs = reinterpret_cast<C*>(smraw);
     const int4 it = items[blockIdx.x];  // leaf, first element, element count
     const DevFarLeaf lf = leaves[it.x];
     const int ne = 2 * lvs[lf.level].ndir;
-    double2* A = lvs[lf.level].A + static_cast<size_t>(lf.box) * ne;
-    for (int i = threadIdx.x; i < lf.nsrc; i += blockDim.x) xs[i] = x[lf.src0 + i];
+    C* A = lvs[lf.level].A + static_cast<size_t>(lf.box) * ne;
+    for (int i = threadIdx.x; i < lf.nsrc; i += blockDim.x) xs[i] = from_d2<C>(x[lf.src0 + i]);
     __syncthreads();
     if (static_cast<int>(threadIdx.x) >= it.z) return;
     const int e = it.y + threadIdx.x;
-    const double2* r = pat + lf.pat_off * 2 + e;
-    double2 a0 = z0(), a1 = z0(), a2 = z0(), a3 = z0();
+    const C* r = pat + lf.pat_off * 2 + e;
+    C a0 = zero<C>(), a1 = zero<C>(), a2 = zero<C>(), a3 = zero<C>();
     int s = 0;
     for (; s + 8 <= lf.nsrc; s += 8) {
-        double2 v[8];
+        C v[8];
 #pragma unroll
         for (int u = 0; u < 8; ++u) v[u] = ldg_stream(r + static_cast<size_t>(s + u) * ne);
         a0 = cfma(xs[s], v[0], a0);
@@ -59,22 +64,24 @@ k_s2m(const DevLevel* __restrict__ lvs, const int4* __restrict__ items, const De
 // y_m = sum_e conj(R_m[e]) b_B[e]  (Leaf::evalFarSols, src/fmm/leaf.cpp:257-280;
 // C k is applied when the result is written out).  One block per work item
 // (leaf, run of up to eight sources), one warp per source, eight loads in
-// flight per lane.
+// flight per lane; the sum is widened to complex double on output.
+template <class R>
 __global__ void __launch_bounds__(kL2TThreads)
-k_l2t(const DevLevel* __restrict__ lvs, const int4* __restrict__ items, const DevFarLeaf* __restrict__ leaves,
-      const double2* __restrict__ pat, double2* __restrict__ yfar) {
+k_l2t(const DevLevelT<R>* __restrict__ lvs, const int4* __restrict__ items, const DevFarLeaf* __restrict__ leaves,
+      const typename Cx<R>::T* __restrict__ pat, double2* __restrict__ yfar) {
+    using C = typename Cx<R>::T;
     const int4 it = items[blockIdx.x];  // leaf, first source, source count
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (warp >= it.z) return;
     const DevFarLeaf lf = leaves[it.x];
     const int ndir = lvs[lf.level].ndir, ne = 2 * ndir;
-    const double2* Bb = lvs[lf.level].B + static_cast<size_t>(lf.box) * ne;
+    const C* Bb = lvs[lf.level].B + static_cast<size_t>(lf.box) * ne;
     const int s = it.y + warp;
-    const double2* r = pat + (lf.pat_off + static_cast<long long>(s) * ndir) * 2;
-    double2 a0 = z0(), a1 = z0(), a2 = z0(), a3 = z0();
+    const C* r = pat + (lf.pat_off + static_cast<long long>(s) * ndir) * 2;
+    C a0 = zero<C>(), a1 = zero<C>(), a2 = zero<C>(), a3 = zero<C>();
     int e = lane;
     for (; e + 224 < ne; e += 256) {
-        double2 v[8];
+        C v[8];
 #pragma unroll
         for (int u = 0; u < 8; ++u) v[u] = ldg_stream(r + e + 32 * u);
         a0 = cjfma(v[0], Bb[e], a0);
@@ -87,8 +94,8 @@ k_l2t(const DevLevel* __restrict__ lvs, const int4* __restrict__ items, const De
         a3 = cjfma(v[7], Bb[e + 224], a3);
     }
     for (; e < ne; e += 32) a0 = cjfma(ldg_stream(r + e), Bb[e], a0);
-    const double2 acc = warp_sum(cadd(cadd(a0, a1), cadd(a2, a3)));
-    if (lane == 0) yfar[lf.src0 + s] = acc;
+    const C acc = warp_sum(cadd(cadd(a0, a1), cadd(a2, a3)));
+    if (lane == 0) yfar[lf.src0 + s] = to_d2(acc);
 }
 
 // ------------------------------------------------------------ M2M
@@ -98,14 +105,16 @@ k_l2t(const DevLevel* __restrict__ lvs, const int4* __restrict__ items, const De
 // Block = (parent, tile of `rows` parent theta rows).  Phase 1 computes the
 // theta pass of every child into shared memory at once (all loads
 // independent); phase 2 forms each parent output from the children's rows.
-template <int W>  // taps per row: 2 * interp_order (both passes)
+template <class R, int W>  // taps per row: 2 * interp_order (both passes)
 __global__ void __launch_bounds__(128)
-k_m2m(const DevLevel* __restrict__ lvs, DevTrans T, int rows) {
-    extern __shared__ double2 sm[];
+k_m2m(const DevLevelT<R>* __restrict__ lvs, DevTransT<R> T, int rows) {
+    using C = typename Cx<R>::T;
+    extern __shared__ unsigned char smraw[];
+    C* sm = reinterpret_cast<C*>(smraw);
     const int par = blockIdx.x;
-    const DevLevel P = lvs[T.plevel];
-    const DevLevel C = lvs[T.plevel + 1];
-    const int nph = P.nph, mph = C.nph, halfm = C.nph / 2;
+    const DevLevelT<R> P = lvs[T.plevel];
+    const DevLevelT<R> Cl = lvs[T.plevel + 1];
+    const int nph = P.nph, mph = Cl.nph, halfm = Cl.nph / 2;
     const int r0 = blockIdx.y * rows;
     const int nrow = min(P.nth, r0 + rows) - r0;
     if (nrow <= 0) return;
@@ -115,37 +124,37 @@ k_m2m(const DevLevel* __restrict__ lvs, DevTrans T, int rows) {
         const int c = it / per_child, e = it - c * per_child;
         const int jr = e / mph, iph = e - jr * mph;
         const int jth = r0 + jr;
-        const double2* Ac = C.A + static_cast<size_t>(T.child_box[c0 + c]) * C.ndir * 2;
-        const double2* sh = C.shift_up + static_cast<size_t>(T.child_oct[c0 + c]) * C.ndir;
-        double2 v0 = z0(), v1 = z0();
+        const C* Ac = Cl.A + static_cast<size_t>(T.child_box[c0 + c]) * Cl.ndir * 2;
+        const C* sh = Cl.shift_up + static_cast<size_t>(T.child_oct[c0 + c]) * Cl.ndir;
+        C v0 = zero<C>(), v1 = zero<C>();
 #pragma unroll
         for (int k = 0; k < W; ++k) {
             const int q = jth * W + k;
             const bool rf = T.up_th.refl[q];
             const int sp = rf ? (iph < halfm ? iph + halfm : iph - halfm) : iph;
-            const double cf = T.up_th.coef[q];
+            const R cf = T.up_th.coef[q];
             const int d = T.up_th.src[q] * mph + sp;
-            const double2 ph = sh[d];
-            v0 = cfma(make_double2(cf, 0.0), cmul(ph, Ac[2 * d]), v0);
-            v1 = cfma(make_double2(cf, 0.0), cmul(ph, Ac[2 * d + 1]), v1);
+            const C ph = sh[d];
+            v0 = crfma(cf, cmul(ph, Ac[2 * d]), v0);
+            v1 = crfma(cf, cmul(ph, Ac[2 * d + 1]), v1);
         }
         sm[2 * it] = v0;
         sm[2 * it + 1] = v1;
     }
     __syncthreads();
-    double2* Ap = P.A + (static_cast<size_t>(T.par_box[par]) * P.ndir + static_cast<size_t>(r0) * nph) * 2;
+    C* Ap = P.A + (static_cast<size_t>(T.par_box[par]) * P.ndir + static_cast<size_t>(r0) * nph) * 2;
     for (int o = threadIdx.x; o < nrow * nph; o += blockDim.x) {
         const int jr = o / nph, jph = o - jr * nph;
-        double2 a0 = z0(), a1 = z0();
+        C a0 = zero<C>(), a1 = zero<C>();
         for (int c = 0; c < nch; ++c) {
-            const double2* row = sm + (static_cast<size_t>(c) * per_child + static_cast<size_t>(jr) * mph) * 2;
+            const C* row = sm + (static_cast<size_t>(c) * per_child + static_cast<size_t>(jr) * mph) * 2;
 #pragma unroll
             for (int k = 0; k < W; ++k) {
                 const int q = jph * W + k;
                 const int s = T.up_ph.src[q];
-                const double cf = T.up_ph.coef[q];
-                a0 = cadd(a0, cscale(cf, row[2 * s]));
-                a1 = cadd(a1, cscale(cf, row[2 * s + 1]));
+                const R cf = T.up_ph.coef[q];
+                a0 = crfma(cf, row[2 * s], a0);
+                a1 = crfma(cf, row[2 * s + 1], a1);
             }
         }
         Ap[2 * o] = a0;
@@ -156,31 +165,33 @@ k_m2m(const DevLevel* __restrict__ lvs, DevTrans T, int rows) {
 // ------------------------------------------------------------ M2L
 // b_B = w_theta (2 pi / nph) sum_{S in list 2} T[c_B - c_S] a_S
 // (Node::buildMpoleToLocalCoeffs, src/fmm/node.cpp:105-134).  One block per
-// (level, box, direction chunk) item, all levels in one launch; two list
+// (level, box, direction chunk) item, all levels in one launch; four list
 // entries in flight per thread.
+template <class R>
 __global__ void __launch_bounds__(128)
-k_m2l(const DevLevel* __restrict__ lvs, const int4* __restrict__ items, int zero_empty) {
+k_m2l(const DevLevelT<R>* __restrict__ lvs, const int4* __restrict__ items, int zero_empty) {
+    using C = typename Cx<R>::T;
     const int4 it = items[blockIdx.x];  // level, box, first direction, count
     if (static_cast<int>(threadIdx.x) >= it.w) return;
-    const DevLevel lv = lvs[it.x];
+    const DevLevelT<R> lv = lvs[it.x];
     const int b = it.y, d = it.z + threadIdx.x, ndir = lv.ndir;
     const int p0 = lv.m2l_ptr[b], p1 = lv.m2l_ptr[b + 1];
-    double2* Bo = lv.B + (static_cast<size_t>(b) * ndir + d) * 2;
+    C* Bo = lv.B + (static_cast<size_t>(b) * ndir + d) * 2;
     if (p0 == p1) {
-        if (zero_empty) { Bo[0] = z0(); Bo[1] = z0(); }
+        if (zero_empty) { Bo[0] = zero<C>(); Bo[1] = zero<C>(); }
         return;
     }
-    double2 a0 = z0(), a1 = z0(), c0 = z0(), c1 = z0();
+    C a0 = zero<C>(), a1 = zero<C>(), c0 = zero<C>(), c1 = zero<C>();
     int p = p0;
     for (; p + 4 <= p1; p += 4) {
         int sb[4], ob[4];
 #pragma unroll
         for (int u = 0; u < 4; ++u) { sb[u] = lv.m2l_src[p + u]; ob[u] = lv.m2l_off[p + u]; }
-        double2 t[4], xa[4], xb[4];
+        C t[4], xa[4], xb[4];
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
             t[u] = lv.transl[static_cast<size_t>(ob[u]) * ndir + d];
-            const double2* As = lv.A + (static_cast<size_t>(sb[u]) * ndir + d) * 2;
+            const C* As = lv.A + (static_cast<size_t>(sb[u]) * ndir + d) * 2;
             xa[u] = As[0];
             xb[u] = As[1];
         }
@@ -195,12 +206,12 @@ k_m2l(const DevLevel* __restrict__ lvs, const int4* __restrict__ items, int zero
     }
     for (; p < p1; ++p) {
         const int s0 = lv.m2l_src[p], o0 = lv.m2l_off[p];
-        const double2 t0 = lv.transl[static_cast<size_t>(o0) * ndir + d];
-        const double2* A0 = lv.A + (static_cast<size_t>(s0) * ndir + d) * 2;
+        const C t0 = lv.transl[static_cast<size_t>(o0) * ndir + d];
+        const C* A0 = lv.A + (static_cast<size_t>(s0) * ndir + d) * 2;
         a0 = cfma(t0, A0[0], a0);
         a1 = cfma(t0, A0[1], a1);
     }
-    const double w = lv.w[d];
+    const R w = lv.w[d];
     Bo[0] = cscale(w, cadd(a0, c0));
     Bo[1] = cscale(w, cadd(a1, c1));
 }
@@ -211,49 +222,58 @@ k_m2l(const DevLevel* __restrict__ lvs, const int4* __restrict__ items, int zero
 // reflection (Stem::getShiftedLocalCoeffs and addAnterpCoeffs,
 // src/fmm/stem.cpp:109-244).  One block per (parent, child) pair; the
 // pair list already omits parents that pass nothing down.
-template <int W>  // both transposed stencils padded to W taps per row
+template <class R, int W>  // both transposed stencils padded to W taps per row
 __global__ void __launch_bounds__(256)
-k_l2l(const DevLevel* __restrict__ lvs, DevTrans T, const int2* __restrict__ pairs) {
-    extern __shared__ double2 sm[];
+k_l2l(const DevLevelT<R>* __restrict__ lvs, DevTransT<R> T, const int2* __restrict__ pairs) {
+    using C = typename Cx<R>::T;
+    extern __shared__ unsigned char smraw[];
+    C* sm = reinterpret_cast<C*>(smraw);
     const int2 pc = pairs[blockIdx.x];  // parent index, child entry
-    const DevLevel P = lvs[T.plevel];
-    const DevLevel C = lvs[T.plevel + 1];
-    const int pth = P.nth, pph = P.nph, cth = C.nth, cph = C.nph, halfc = C.nph / 2;
-    const double2* Bp = P.B + static_cast<size_t>(T.par_box[pc.x]) * P.ndir * 2;
-    const double2* sh = P.shift_down + static_cast<size_t>(T.child_oct[pc.y]) * P.ndir;
+    const DevLevelT<R> P = lvs[T.plevel];
+    const DevLevelT<R> Cl = lvs[T.plevel + 1];
+    const int pth = P.nth, pph = P.nph, cth = Cl.nth, cph = Cl.nph, halfc = Cl.nph / 2;
+    const C* Bp = P.B + static_cast<size_t>(T.par_box[pc.x]) * P.ndir * 2;
+    const C* sh = P.shift_down + static_cast<size_t>(T.child_oct[pc.y]) * P.ndir;
     for (int e = threadIdx.x; e < pth * cph; e += blockDim.x) {
         const int ith = e / cph, jph = e - ith * cph;
-        double2 v0 = z0(), v1 = z0();
+        C v0 = zero<C>(), v1 = zero<C>();
 #pragma unroll
         for (int k = 0; k < W; ++k) {
             const int q = jph * W + k;
             const int d = ith * pph + T.dn_ph.src[q];
-            const double cf = T.dn_ph.coef[q];
-            const double2 ph = sh[d];
-            v0 = cfma(make_double2(cf, 0.0), cmul(ph, Bp[2 * d]), v0);
-            v1 = cfma(make_double2(cf, 0.0), cmul(ph, Bp[2 * d + 1]), v1);
+            const R cf = T.dn_ph.coef[q];
+            const C ph = sh[d];
+            v0 = crfma(cf, cmul(ph, Bp[2 * d]), v0);
+            v1 = crfma(cf, cmul(ph, Bp[2 * d + 1]), v1);
         }
         sm[2 * e] = v0;
         sm[2 * e + 1] = v1;
     }
     __syncthreads();
-    double2* Bc = C.B + static_cast<size_t>(T.child_box[pc.y]) * C.ndir * 2;
+    C* Bc = Cl.B + static_cast<size_t>(T.child_box[pc.y]) * Cl.ndir * 2;
     for (int e = threadIdx.x; e < cth * cph; e += blockDim.x) {
         const int jth = e / cph, jph = e - jth * cph;
-        double2 v0 = z0(), v1 = z0();
+        C v0 = zero<C>(), v1 = zero<C>();
 #pragma unroll
         for (int k = 0; k < W; ++k) {
             const int q = jth * W + k;
             const bool rf = T.dn_th.refl[q];
             const int sp = rf ? (jph < halfc ? jph + halfc : jph - halfc) : jph;
-            const double cf = T.dn_th.coef[q];
-            const double2* row = sm + (static_cast<size_t>(T.dn_th.src[q]) * cph + sp) * 2;
-            v0 = cadd(v0, cscale(cf, row[0]));
-            v1 = cadd(v1, cscale(cf, row[1]));
+            const R cf = T.dn_th.coef[q];
+            const C* row = sm + (static_cast<size_t>(T.dn_th.src[q]) * cph + sp) * 2;
+            v0 = crfma(cf, row[0], v0);
+            v1 = crfma(cf, row[1], v1);
         }
         Bc[2 * e] = cadd(Bc[2 * e], v0);
         Bc[2 * e + 1] = cadd(Bc[2 * e + 1], v1);
     }
+}
+
+// Complex double -> far-field type (patterns, tables at setup).
+template <class C>
+__global__ void k_narrow(const double2* __restrict__ src, C* __restrict__ dst, long long n) {
+    const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = from_d2<C>(src[i]);
 }
 
 }  // namespace

@@ -51,18 +51,6 @@ k_near_rows(const DevNearRow* __restrict__ rows, const int4* __restrict__ items,
 }
 
 // ------------------------------------------------------------ setup kernels
-struct DevSources {
-    int kind;
-    double k;
-    const double* pos;      // dipole positions (tree order)
-    const double* phat;     // dipole unit moments
-    const RwgGeom* rwg;     // RWG geometry (tree order)
-    const TriGeom* tris;
-    const double* tri_quad; // [tri][nq][3]
-    const double* quad_w;   // [nq]
-    int nq;
-};
-
 struct DevFarLeafGeom {
     double c[3];
 };
@@ -71,10 +59,10 @@ struct DevFarLeafGeom {
 // src/fmm/leaf.cpp:185-207) with e_n = e^{ik khat.(c - r_n)} phat_n for a
 // dipole (Dipole::getRadAlongDir, src/sources/dipole.h:47-51) and
 // e^{ik khat.c} conj(I_n(k khat)) for an RWG (src/sources/rwg.h:23-25).
-__global__ void k_patterns(const DevLevel* __restrict__ lvs, const DevFarLeaf* __restrict__ leaves,
+__global__ void k_patterns(const DevGeomLevel* __restrict__ lvs, const DevFarLeaf* __restrict__ leaves,
                            const DevFarLeafGeom* __restrict__ geo, DevSources S, double2* __restrict__ pat) {
     const DevFarLeaf lf = leaves[blockIdx.x];
-    const DevLevel lv = lvs[lf.level];
+    const DevGeomLevel lv = lvs[lf.level];
     const double* c = geo[blockIdx.x].c;
     const int ndir = lv.ndir;
     for (int e = threadIdx.x; e < lf.nsrc * ndir; e += blockDim.x) {
@@ -138,6 +126,52 @@ __device__ zd near_entry(const DevSources& S, int m, int n) {
         }
     }
     return (go.leng * gs.leng) * acc;
+}
+
+// Far field of currents I (caller order) along unit directions khat:
+// F = C k (I - khat khat^T) sum_n I_n f_n(k khat), with f_n = e^{-i r_n . k khat}
+// phat_n for a dipole (Dipole::getFarAlongDir, src/sources/dipole.h:53-57)
+// and conj(I_n(k khat)) for an RWG (RWG::getFarAlongDir, src/sources/rwg.h:27-29);
+// the sum and projection are those of Node::printFarSols
+// (src/fmm/node.cpp:155-164).  One block per direction.
+constexpr int kFarThreads = 256;
+
+__global__ void __launch_bounds__(kFarThreads)
+k_farfield(DevSources S, const int* __restrict__ perm, const double2* __restrict__ cur, int n,
+           const double* __restrict__ khat, double2 ck, double2* __restrict__ out) {
+    __shared__ double2 red[3][kFarThreads];
+    const int d = blockIdx.x;
+    const double kh[3] = {khat[3 * d], khat[3 * d + 1], khat[3 * d + 2]};
+    const double kr[3] = {kh[0] * S.k, kh[1] * S.k, kh[2] * S.k};
+    zd acc[3] = {mkz(0), mkz(0), mkz(0)};
+    for (int t = threadIdx.x; t < n; t += blockDim.x) {
+        const double2 cv = cur[perm[t]];
+        const zd c = zd{cv.x, cv.y};
+        if (S.kind == kDipole) {
+            const zd ph = c * expi(-dot3(S.pos + 3 * t, kr));
+            for (int a = 0; a < 3; ++a) acc[a] += ph * S.phat[3 * t + a];
+        } else {
+            zd I[3];
+            rwg_plane_wave_integral(S.rwg[t], S.tris, kr, I);
+            for (int a = 0; a < 3; ++a) acc[a] += c * conj(I[a]);
+        }
+    }
+    for (int a = 0; a < 3; ++a) red[a][threadIdx.x] = make_double2(acc[a].x, acc[a].y);
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (static_cast<int>(threadIdx.x) < s)
+            for (int a = 0; a < 3; ++a) red[a][threadIdx.x] = cadd(red[a][threadIdx.x], red[a][threadIdx.x + s]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const double2 v[3] = {red[0][0], red[1][0], red[2][0]};
+        const double proj = kh[0] * v[0].x + kh[1] * v[1].x + kh[2] * v[2].x;
+        const double proji = kh[0] * v[0].y + kh[1] * v[1].y + kh[2] * v[2].y;
+        for (int a = 0; a < 3; ++a) {
+            const double2 t = make_double2(v[a].x - kh[a] * proj, v[a].y - kh[a] * proji);
+            out[3 * d + a] = cmul(ck, t);
+        }
+    }
 }
 
 // Entries of the block rows: thread per entry.

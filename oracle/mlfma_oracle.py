@@ -695,6 +695,23 @@ class Oracle:
         return PHYS_C * self.k * self.srcs.block(idx, idx, self.k)
 
 
+def farfield(srcs, currents, khat, k):
+    """C k (I - khat khat^T) sum_n I_n f_n(k khat) along unit directions khat [d, 3]
+    (Node::printFarSols, src/fmm/node.cpp:155-164).  f_n = e^{-i k khat . r_n} phat_n
+    for a dipole (dipole.h:53-57), conj(I_n(k khat)) for an RWG (rwg.h:27-29).
+    Returns [d, 3] complex."""
+    kh = np.asarray(khat, dtype=float).reshape(-1, 3)
+    cur = np.asarray(currents, dtype=complex)
+    if srcs.kind == "dipole":
+        ph = np.exp(-1j * k * (srcs.pos @ kh.T))                 # [s, d]
+        v = np.einsum("s,sd,sc->dc", cur, ph, srcs.phat)
+    else:
+        I = srcs.integral(np.arange(srcs.n), k * kh)             # [s, d, 3]
+        v = np.einsum("s,sdc->dc", cur, np.conj(I))
+    v = v - kh * np.einsum("dc,dc->d", kh, v)[:, None]
+    return PHYS_C * k * v
+
+
 def gmres_reference(matvec, b, max_iter=500, eps=1e-6):
     """Unrestarted GMRES of the reference: MGS Arnoldi with the Hermitian dot,
     complex-symmetric Givens t = sqrt(z^2 + w^2), stop on |g_{k+1}|/g0, then an

@@ -314,6 +314,27 @@ int ref_radpat(int i, int s, int d, double* out) {
     return 0;
 }
 
+// Far field of the given currents along unit directions khat (ndir x 3):
+// the loop body of Node::printFarSols (src/fmm/node.cpp:155-164) for an
+// arbitrary direction list; out is ndir x 3 complex.
+int ref_farfield(const double* cur, int ndir, const double* khat, double* out) {
+    if (!g.ready) return 1;
+    const double k = g.einc->wavenum;
+    for (int d = 0; d < ndir; ++d) {
+        const vec3d kh(khat[3 * d], khat[3 * d + 1], khat[3 * d + 2]);
+        const auto& krhat = kh * k;
+        vec3cd dirFar = vec3cd::Zero();
+        for (const auto& src : g.srcs)
+            dirFar += cmplx(cur[2 * src->getIdx()], cur[2 * src->getIdx() + 1]) * src->getFarAlongDir(krhat);
+        const vec3cd& far = Phys::C * k * Math::ImRR(kh) * dirFar;
+        for (int c = 0; c < 3; ++c) {
+            out[6 * d + 2 * c] = far[c].real();
+            out[6 * d + 2 * c + 1] = far[c].imag();
+        }
+    }
+    return 0;
+}
+
 // List sizes summed over the tree: [list2 pairs, list4 pairs, near leaf pairs,
 // self entries, near entries stored, non-near entries stored].
 void ref_list_stats(long long* out) {

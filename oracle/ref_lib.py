@@ -155,6 +155,17 @@ class RefProblem:
         keys = ["list2", "list4", "near_pairs", "self_entries", "near_entries", "nonnear_entries"]
         return dict(zip(keys, (int(v) for v in out)))
 
+    def farfield(self, currents, khat):
+        """Far field (ndir x 3 complex) of `currents` along unit directions khat."""
+        L = lib()
+        L.ref_farfield.argtypes = [_dp, ctypes.c_int, _dp, _dp]
+        cur = np.ascontiguousarray(np.asarray(currents, dtype=np.complex128)).view(np.float64)
+        kh = np.ascontiguousarray(np.asarray(khat, dtype=np.float64).reshape(-1, 3))
+        out = np.zeros(kh.shape[0] * 6)
+        if L.ref_farfield(_d(cur), kh.shape[0], _d(kh), _d(out)) != 0:
+            raise RuntimeError("reference far field failed")
+        return out.view(np.complex128).reshape(-1, 3)
+
     def entry(self, m, n):
         out = np.zeros(2)
         lib().ref_entry(m, n, _d(out))

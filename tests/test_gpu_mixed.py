@@ -1,0 +1,61 @@
+"""Mixed precision (complex float far field, float accumulation; complex double
+near field): its product must stay within float rounding of the FP64 product,
+far below the MLFMA approximation error (3 digits here), and the solver must
+still converge on it."""
+import numpy as np
+import pytest
+
+from mlfma_b200 import MLFMA, inputs
+from oracle import mlfma_oracle as O
+
+pytestmark = pytest.mark.gpu
+PW = inputs.PlaneWave()
+
+
+def rel(a, b):
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+def cvec(n, seed):
+    r = np.random.default_rng(seed)
+    return r.standard_normal(n) + 1j * r.standard_normal(n)
+
+
+@pytest.mark.parametrize("kind", ["dipole", "rwg"])
+def test_mixed_close_to_fp64(cuda_device, kind):
+    if kind == "dipole":
+        g = inputs.make_dipoles(6000, seed=4)
+        mk = lambda p: MLFMA.dipoles(g, PW, max_node_srcs=24, precision=p).setup()
+    else:
+        g = inputs.make_icosphere(5, radius=2.0)
+        mk = lambda p: MLFMA.rwg(g, PW, max_node_srcs=54, precision=p).setup()
+    a, b = mk(0), mk(1)
+    x = cvec(a.n, 1)
+    e = rel(b.matvec(x), a.matvec(x))
+    assert e < 1e-5, e  # float rounding through five stages
+    a.close()
+    b.close()
+
+
+def test_mixed_error_vs_dense_matches_fp64(cuda_device):
+    d = inputs.make_dipoles(1500, seed=9)
+    orc = O.Oracle(O.DipoleSources(d.pos, d.mom, PW), max_node_srcs=24)
+    A = orc.dense()
+    x = cvec(d.n, 2)
+    yd = A @ x
+    e64 = rel(MLFMA.dipoles(d, PW, max_node_srcs=24, precision=0).setup().matvec(x), yd)
+    e32 = rel(MLFMA.dipoles(d, PW, max_node_srcs=24, precision=1).setup().matvec(x), yd)
+    assert e64 < 1e-2 and abs(e32 - e64) < 1e-4 * max(1.0, e64 / 1e-3)
+
+
+def test_mixed_gmres_tracks_fp64(cuda_device):
+    # The reference's RWG operator has no self terms and converges slowly; the
+    # check is that the mixed solve follows the FP64 solve iteration for
+    # iteration (same residual, same iterate) rather than a target residual.
+    m = inputs.make_icosphere(3, radius=1.0)
+    ops = [MLFMA.rwg(m, PW, max_node_srcs=16, ref_compat=0, precision=p).setup() for p in (0, 1)]
+    b = ops[0].rhs()
+    (x64, i64), (x32, i32) = [op.solve(b, max_iter=60, tol=1e-3, restart=30, ref_givens=False) for op in ops]
+    assert i32.iterations == i64.iterations
+    assert abs(i32.true_residual - i64.true_residual) <= 1e-3 * i64.true_residual + 1e-6
+    assert rel(x32, x64) < 1e-4
