@@ -39,6 +39,7 @@ UNIT = "matvecs/s"
 WORKLOAD = dict(name="rwg_sphere_r2lambda_ico5", kind="rwg", level=5, radius=2.0, root_leng=4.0,
                 max_node_srcs=54, quad_prec=2, digits=3, interp_order=3, over_interp=2.0)
 HERE = os.path.dirname(os.path.abspath(__file__))
+SOLVE = dict(restart=50, tol=1e-4, max_iter=3000)
 
 
 def make_problem():
@@ -209,13 +210,45 @@ def measure(torch, dev, rank, world, args, precision: int, clocks=None) -> dict:
     stages = [op.stage_times() for _ in range(max(5, min(args.steps, 50)))]
     avg = {k: float(np.mean([s[k] for s in stages])) for k in stages[0]}
     traffic = op.traffic()
+
     op.close()
+
+    # GMRES(50) solve of the plane-wave right-hand side to a 1e-4 relative
+    # residual (FP64 residual; the mixed operator refines on it).  The solve
+    # runs on the EFIE with its self terms (coincident and touching triangle
+    # pairs in mixed-potential form, 1/R extracted): the reference's operator
+    # leaves them out and GMRES then needs thousands of iterations.
+    solve = None
+    if not args.no_solve:
+        scfg = default_config(quad_prec=WORKLOAD["quad_prec"], digits=WORKLOAD["digits"],
+                              interp_order=WORKLOAD["interp_order"], over_interp=WORKLOAD["over_interp"],
+                              root_leng=WORKLOAD["root_leng"], max_node_srcs=WORKLOAD["max_node_srcs"],
+                              device=dev.index, precision=precision, self_terms=1, ref_compat=0)
+        op = MLFMA.rwg(mesh, pw, config=scfg).setup()
+        b = op.rhs()
+        op.solve(b, max_iter=5, tol=1e-12, restart=SOLVE["restart"], ref_givens=False,
+                 refine=precision == 1)  # warm-up: workspace and graphs
+        t0 = time.perf_counter()
+        xs, info = op.solve(b, max_iter=SOLVE["max_iter"], tol=SOLVE["tol"], restart=SOLVE["restart"],
+                            ref_givens=False, refine=precision == 1)
+        wall = time.perf_counter() - t0
+        far = op.farfield(xs, op.phi_cut(360))
+        solve = dict(seconds=wall, iterations=info.iterations, true_residual=info.true_residual,
+                     converged=info.converged, refinements=info.refinements, far=far, x=xs)
+        op.close()
     if world > 1:
         t = torch.tensor([ms, e2e_ms], device=dev, dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms, e2e_ms = float(t[0]), float(t[1])
     return dict(ms=ms, e2e_ms=e2e_ms, stages=avg, traffic=traffic, stats=st, setup_s=setup_s, n=n, y=y_dev,
-                clocks=clk)
+                clocks=clk, solve=solve)
+
+
+def solve_summary(sv):
+    return {"seconds": sv["seconds"], "iterations": sv["iterations"], "true_residual_fp64": sv["true_residual"],
+            "converged": sv["converged"], "refinements": sv["refinements"],
+            "method": f"GMRES({SOLVE['restart']}) to {SOLVE['tol']:g} relative residual, x0 = 0, plane-wave rhs",
+            "operator": "EFIE with self terms (self_terms=1, ref_compat=0)"}
 
 
 def roofline(avg, traffic, precision_name):
@@ -249,6 +282,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--no-solve", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=3)
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
@@ -320,6 +354,8 @@ def main():
             "clocks": r64["clocks"],
             "cpu_baseline": cpu,
         }
+        if r64["solve"] is not None:
+            line["solve_fp64"] = solve_summary(r64["solve"])
         if rmx is not None:
             err = float(np.linalg.norm(rmx["y"] - r64["y"]) / np.linalg.norm(r64["y"]))
             line["mixed"] = {"value": world * 1000.0 / rmx["ms"], "ms_per_step": rmx["ms"],
@@ -327,6 +363,12 @@ def main():
                              "rel_diff_vs_fp64": err, "dtype": "c64 far field, c128 near field",
                              "stage_ms": rmx["stages"], "roofline": roofline(rmx["stages"], rmx["traffic"], "_mixed"),
                              "matvec_alg_bytes": rmx["traffic"]["total"]}
+            if rmx["solve"] is not None and r64["solve"] is not None:
+                sm, s64 = rmx["solve"], r64["solve"]
+                line["mixed"]["solve"] = solve_summary(sm)
+                line["mixed"]["solve"]["speedup_vs_fp64"] = s64["seconds"] / sm["seconds"]
+                line["mixed"]["solve"]["farfield_rel_err_vs_fp64"] = float(
+                    np.linalg.norm(sm["far"] - s64["far"]) / np.linalg.norm(s64["far"]))
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()

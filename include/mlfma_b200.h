@@ -53,6 +53,13 @@ typedef struct {
     int precision;       /* MLFMA_FP64 (default) or MLFMA_MIXED: far field in complex
                             float with float accumulation, near field and vectors in
                             complex double */
+    int self_terms;      /* 0: the reference's operator (zero diagonal, coincident
+                            triangles skipped, src/sources/dipole.h:65,
+                            src/sources/rwg.cpp:97,113-116).  1: dipoles get a unit
+                            diagonal; RWG pairs whose triangles share a vertex are
+                            integrated in mixed-potential form with the 1/R
+                            singularity of the source triangle in closed form
+                            (symmetrised, FP64) */
 } mlfma_config;
 
 enum { MLFMA_FP64 = 0, MLFMA_MIXED = 1 };
@@ -88,6 +95,11 @@ typedef struct {
     double tol;          /* relative residual target (reference: 1e-6, src/mlfma.cpp:70) */
     int restart;         /* 0 = no restart (reference), else GMRES(restart) */
     int ref_givens;      /* 1: complex-symmetric Givens of the reference (src/math.h:168-172) */
+    int refine;          /* MLFMA_MIXED operators: 1 = iterative refinement (inner GMRES on the
+                            mixed operator, outer residual r = b - A x in FP64, x += correction;
+                            stops on the FP64 residual); 0 = GMRES on the mixed operator alone.
+                            Ignored by MLFMA_FP64 operators. */
+    double inner_tol;    /* refinement: inner relative residual target (0 = automatic) */
 } mlfma_solver_opts;
 
 typedef struct {
@@ -95,6 +107,7 @@ typedef struct {
     double residual;       /* final |g_{k+1}| / g0 estimate */
     double true_residual;  /* ||b - A x|| / ||b||, recomputed */
     double seconds;
+    int refinements;       /* FP64 residual evaluations of iterative refinement (0 otherwise) */
 } mlfma_solve_info;
 
 /* Fill *cfg with the defaults (digits 3, order 3, overInterp 2, rootLeng 4, 64 per box). */
@@ -139,7 +152,8 @@ int mlfma_matvec(mlfma_handle h, const double* x, double* y, int accumulate);
 int mlfma_matvec_device(mlfma_handle h, const void* d_x, void* d_y, int accumulate, void* stream);
 
 /* Solve A x = b with GMRES on the device; b and x host buffers (Solver::solve,
- * src/solver.cpp:116-146).  x is overwritten (initial guess 0). */
+ * src/solver.cpp:116-146).  x is overwritten (initial guess 0).  On a mixed
+ * operator with opts->refine = 1 the answer meets tol on the FP64 residual. */
 int mlfma_gmres(mlfma_handle h, const double* b, double* x, const mlfma_solver_opts* opts,
                 mlfma_solve_info* info);
 
@@ -160,7 +174,8 @@ int mlfma_farfield(mlfma_handle h, const double* x, int ndir, const double* khat
  * The workspace is one fixed array in device memory that is part of the
  * library (32 MiB, held on every GPU that loads the library until exit): n *
  * (restart + 5) must not exceed 2,097,152 complex values (restart = max_iter
- * when restart is 0), otherwise MLFMA_ERR_ARG.  All calls share that array and
+ * when restart is 0; restart + 7 with refinement on a mixed operator),
+ * otherwise MLFMA_ERR_ARG.  All calls share that array and
  * it keeps the last call's contents, so calls that overlap on the GPU race.
  * The first call on a device looks up the array's device address; make that
  * first call before any stream capture. */

@@ -61,6 +61,7 @@ class SolveResult:
     true_residual: float
     seconds: float
     converged: bool
+    refinements: int = 0
 
 
 class MLFMA:
@@ -184,17 +185,22 @@ class MLFMA:
                                         int(accumulate), ctypes.c_void_p(stream)))
 
     def solve(self, b=None, max_iter: int = 500, tol: float = 1e-6, restart: int = 0,
-              ref_givens: bool = True, raise_on_fail: bool = False):
+              ref_givens: bool = True, raise_on_fail: bool = False, refine: bool = False, inner_tol: float = 0.0):
+        """GMRES (Solver::solve).  On a mixed operator, refine=True runs
+        iterative refinement: inner GMRES on the mixed operator, outer FP64
+        residual; tol then holds for the FP64 residual."""
         bv = self.rhs() if b is None else _cvec(b, self.n)
         x = np.zeros(self.n, dtype=np.complex128)
-        o = SolverOpts(max_iter=max_iter, tol=tol, restart=restart, ref_givens=int(ref_givens))
+        o = SolverOpts(max_iter=max_iter, tol=tol, restart=restart, ref_givens=int(ref_givens),
+                       refine=int(refine), inner_tol=inner_tol)
         info = SolveInfo()
         code = lib().mlfma_gmres(self._h, bv.view(np.float64).ctypes.data_as(_dp),
                                  x.view(np.float64).ctypes.data_as(_dp), ctypes.byref(o), ctypes.byref(info))
         converged = code == 0
         if code not in (0, 4) or (raise_on_fail and code != 0):
             check(code)
-        return x, SolveResult(info.iterations, info.residual, info.true_residual, info.seconds, converged)
+        return x, SolveResult(info.iterations, info.residual, info.true_residual, info.seconds, converged,
+                              info.refinements)
 
     def farfield(self, currents, khat) -> np.ndarray:
         """Far field (ndir x 3 complex) of `currents` along unit directions `khat` (ndir x 3)."""

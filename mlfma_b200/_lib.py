@@ -27,7 +27,8 @@ class Config(ctypes.Structure):
     _fields_ = [("quad_prec", ctypes.c_int), ("digits", ctypes.c_int), ("interp_order", ctypes.c_int),
                 ("over_interp", ctypes.c_double), ("root_leng", ctypes.c_double),
                 ("max_node_srcs", ctypes.c_int), ("max_level", ctypes.c_int),
-                ("ref_compat", ctypes.c_int), ("device", ctypes.c_int), ("precision", ctypes.c_int)]
+                ("ref_compat", ctypes.c_int), ("device", ctypes.c_int), ("precision", ctypes.c_int),
+                ("self_terms", ctypes.c_int)]
 
 
 class PlaneWaveC(ctypes.Structure):
@@ -54,12 +55,13 @@ class Traffic(ctypes.Structure):
 
 class SolverOpts(ctypes.Structure):
     _fields_ = [("max_iter", ctypes.c_int), ("tol", ctypes.c_double), ("restart", ctypes.c_int),
-                ("ref_givens", ctypes.c_int)]
+                ("ref_givens", ctypes.c_int), ("refine", ctypes.c_int), ("inner_tol", ctypes.c_double)]
 
 
 class SolveInfo(ctypes.Structure):
     _fields_ = [("iterations", ctypes.c_int), ("residual", ctypes.c_double),
-                ("true_residual", ctypes.c_double), ("seconds", ctypes.c_double)]
+                ("true_residual", ctypes.c_double), ("seconds", ctypes.c_double),
+                ("refinements", ctypes.c_int)]
 
 
 # name -> (restype, argtypes); every symbol the header declares.

@@ -54,6 +54,7 @@ mlfma::Config to_cfg(const mlfma_config* c) {
     o.max_node_srcs = c->max_node_srcs;
     o.max_level = c->max_level;
     o.ref_compat = c->ref_compat;
+    o.self_terms = c->self_terms;
     return o;
 }
 
@@ -88,6 +89,7 @@ int mlfma_config_default(mlfma_config* cfg) {
     cfg->ref_compat = 1;
     cfg->device = 0;
     cfg->precision = MLFMA_FP64;
+    cfg->self_terms = 0;
     return MLFMA_OK;
 }
 
@@ -209,6 +211,8 @@ int mlfma_gmres(mlfma_handle h, const double* b, double* x, const mlfma_solver_o
         o.tol = opts->tol;
         o.restart = opts->restart;
         o.ref_givens = opts->ref_givens;
+        o.refine = opts->refine;
+        o.inner_tol = opts->inner_tol;
     }
     const size_t bytes = sizeof(double2) * h->plan.n;
     cudaStream_t s = h->dev->stream();
@@ -226,6 +230,7 @@ int mlfma_gmres(mlfma_handle h, const double* b, double* x, const mlfma_solver_o
         info->residual = r.residual;
         info->true_residual = r.true_residual;
         info->seconds = r.seconds;
+        info->refinements = r.refinements;
     }
     if (!r.converged) return fail(MLFMA_ERR_NOT_CONVERGED, "iteration limit reached");
     return MLFMA_OK;
@@ -270,12 +275,15 @@ int mlfma_gmres_noalloc(mlfma_handle h, const void* d_b, void* d_x, const mlfma_
         o.tol = opts->tol;
         o.restart = opts->restart;
         o.ref_givens = opts->ref_givens;
+        o.refine = opts->refine;
+        o.inner_tol = opts->inner_tol;
     }
     if (o.max_iter < 1 || o.restart < 0) return fail(MLFMA_ERR_ARG, "max_iter and restart must be positive");
     if (cudaSetDevice(h->device) != cudaSuccess) return fail(MLFMA_ERR_CUDA, "cudaSetDevice failed");
     if (!h->gmres_fixed) h->gmres_fixed = std::make_unique<mlfma::Gmres>();
     const int m = o.restart > 0 ? o.restart : o.max_iter;
-    std::string e = h->gmres_fixed->use_static_workspace(h->plan.n, m + 1);
+    std::string e = h->gmres_fixed->use_static_workspace(
+        h->plan.n, m + 1, (o.refine && h->precision != MLFMA_FP64) ? 2 : 0);
     if (!e.empty()) return fail(e.rfind("size:", 0) == 0 ? MLFMA_ERR_ARG : MLFMA_ERR_CUDA, e);
     mlfma::SolveResult r;
     e = h->gmres_fixed->solve(*h->dev, static_cast<const double2*>(d_b), static_cast<double2*>(d_x), o, &r);
@@ -285,6 +293,7 @@ int mlfma_gmres_noalloc(mlfma_handle h, const void* d_b, void* d_x, const mlfma_
         info->residual = r.residual;
         info->true_residual = r.true_residual;
         info->seconds = r.seconds;
+        info->refinements = r.refinements;
     }
     if (!r.converged) return fail(MLFMA_ERR_NOT_CONVERGED, "iteration limit reached");
     return MLFMA_OK;

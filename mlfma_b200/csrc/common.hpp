@@ -135,6 +135,124 @@ MLFMA_HD void rwg_plane_wave_integral(const RwgGeom& g, const TriGeom* tris, con
     for (int c = 0; c < 3; ++c) out[c] = g.leng * rad[c];
 }
 
+// ---------------------------------------------------------------- self terms
+// No reference counterpart (the reference skips coincident triangles and the
+// diagonal, src/sources/rwg.cpp:97,113-116): used when Config::self_terms = 1.
+
+MLFMA_HD void cross3(const double* a, const double* b, double* o) {
+    o[0] = a[1] * b[2] - a[2] * b[1];
+    o[1] = a[2] * b[0] - a[0] * b[2];
+    o[2] = a[0] * b[1] - a[1] * b[0];
+}
+
+// Closed-form potential integrals of the flat triangle P (3 vertices) seen
+// from r:  I0 = int_T 1/|r - r'| dS',  I1 = int_T (rho' - rho)/|r - r'| dS',
+// rho = r projected onto the plane (also returned).  Edge-by-edge formulas of
+// Wilton et al., IEEE Trans. Antennas Propag. 32(3), 1984, and Graglia, IEEE
+// Trans. Antennas Propag. 41(10), 1993; the logarithm is taken in the form
+// that avoids cancellation for each sign pattern of the edge coordinates.
+MLFMA_HD void tri_potentials(const double* P, const double* r, double* I0, double* I1, double* rho) {
+    const double e1[3] = {P[3] - P[0], P[4] - P[1], P[5] - P[2]};
+    const double e2[3] = {P[6] - P[0], P[7] - P[1], P[8] - P[2]};
+    double nv[3];
+    cross3(e1, e2, nv);
+    const double nn = sqrt(dot3(nv, nv));
+    for (int c = 0; c < 3; ++c) nv[c] /= nn;
+    const double d0[3] = {r[0] - P[0], r[1] - P[1], r[2] - P[2]};
+    const double h = dot3(nv, d0), ah = fabs(h);
+    for (int c = 0; c < 3; ++c) rho[c] = r[c] - h * nv[c];
+    double s0 = 0.0, s1[3] = {0.0, 0.0, 0.0};
+    for (int i = 0; i < 3; ++i) {
+        const double* p = P + 3 * i;
+        const double* q = P + 3 * ((i + 1) % 3);
+        const double L[3] = {q[0] - p[0], q[1] - p[1], q[2] - p[2]};
+        const double ll = sqrt(dot3(L, L));
+        const double lh[3] = {L[0] / ll, L[1] / ll, L[2] / ll};
+        double u[3];
+        cross3(lh, nv, u);
+        const double pr[3] = {p[0] - rho[0], p[1] - rho[1], p[2] - rho[2]};
+        const double qr[3] = {q[0] - rho[0], q[1] - rho[1], q[2] - rho[2]};
+        const double t0 = dot3(pr, u), lm = dot3(pr, lh), lp = dot3(qr, lh);
+        const double r0sq = t0 * t0 + h * h;
+        const double rm = sqrt(r0sq + lm * lm), rp = sqrt(r0sq + lp * lp);
+        double f = 0.0;
+        if (r0sq > (1e-12 * ll) * (1e-12 * ll)) {
+            if (lm >= 0.0) f = log((rp + lp) / (rm + lm));
+            else if (lp <= 0.0) f = log((rm - lm) / (rp - lp));
+            else f = log((rp + lp) * (rm - lm) / r0sq);
+        }
+        s0 += t0 * f - ah * (atan2(t0 * lp, r0sq + ah * rp) - atan2(t0 * lm, r0sq + ah * rm));
+        const double g = 0.5 * (r0sq * f + lp * rp - lm * rm);
+        for (int c = 0; c < 3; ++c) s1[c] += g * u[c];
+    }
+    *I0 = s0;
+    for (int c = 0; c < 3; ++c) I1[c] = s1[c];
+}
+
+// (e^{ikR} - 1)/R without cancellation (1 - cos = 2 sin^2 of the half angle);
+// ik at R = 0.
+MLFMA_HD zd smooth_green(double R, double k) {
+    if (!(R > 0.0)) return zd{0.0, k};
+    const double sh = sin(0.5 * k * R);
+    return zd{-2.0 * sh * sh / R, sin(k * R) / R};
+}
+
+MLFMA_HD double tri_area(const double* P) {
+    const double e1[3] = {P[3] - P[0], P[4] - P[1], P[5] - P[2]};
+    const double e2[3] = {P[6] - P[0], P[7] - P[1], P[8] - P[2]};
+    double c[3];
+    cross3(e1, e2, c);
+    return 0.5 * sqrt(dot3(c, c));
+}
+
+// Z_mn (operator C k Z) of RWG m (observation) and n (source) in mixed-potential form:
+//   int int [f_m . f_n - (div f_m)(div f_n)/k^2] e^{ikR}/R dS' dS,
+// f = s l/(2A) (r - X) on a triangle of area A with free vertex X (s = +1 on
+// T+, -1 on T-), div f = s l/A.  This equals the dyadic-Green form of the
+// other entries (src/sources/rwg.cpp:92-140) after integrating the grad-grad
+// term by parts over each RWG's two triangles.  On the source triangle 1/R
+// is integrated in closed form (tri_potentials) and (e^{ikR} - 1)/R by the
+// triangle rule; the observation triangle by the triangle rule.  quad_w sums
+// to 1/2 per triangle (Triangle::buildQuads, src/sources/triangle.cpp:45-130).
+MLFMA_HD zd rwg_mpie(const RwgGeom& go, const RwgGeom& gs, const double* tri_p, const double* tri_quad,
+                     const double* quad_w, int nq, double k) {
+    zd acc = mkz(0);
+    for (int ot = 0; ot < 2; ++ot) {
+        const double* P = tri_p + 9 * go.tri[ot];
+        const double A = tri_area(P);
+        const double* X = go.xpm[ot];
+        const double* qo = tri_quad + static_cast<size_t>(go.tri[ot]) * nq * 3;
+        for (int st = 0; st < 2; ++st) {
+            const double* Pp = tri_p + 9 * gs.tri[st];
+            const double Ap = tri_area(Pp);
+            const double* Xp = gs.xpm[st];
+            const double* qs = tri_quad + static_cast<size_t>(gs.tri[st]) * nq * 3;
+            zd tri_acc = mkz(0);
+            for (int p = 0; p < nq; ++p) {
+                const double* ro = qo + 3 * p;
+                double I0, I1[3], rho[3];
+                tri_potentials(Pp, ro, &I0, I1, rho);
+                zd J0 = mkz(I0);
+                zd J1[3];
+                for (int c = 0; c < 3; ++c) J1[c] = mkz(I1[c] + (rho[c] - Xp[c]) * I0);
+                for (int q = 0; q < nq; ++q) {
+                    const double* rs = qs + 3 * q;
+                    const double d[3] = {ro[0] - rs[0], ro[1] - rs[1], ro[2] - rs[2]};
+                    const zd g = smooth_green(sqrt(dot3(d, d)), k) * (2.0 * quad_w[q] * Ap);
+                    J0 += g;
+                    for (int c = 0; c < 3; ++c) J1[c] += g * (rs[c] - Xp[c]);
+                }
+                const double u[3] = {ro[0] - X[0], ro[1] - X[1], ro[2] - X[2]};
+                const zd vec = u[0] * J1[0] + u[1] * J1[1] + u[2] * J1[2];
+                const zd inner = vec / (4.0 * A * Ap) - J0 / (k * k * A * Ap);
+                tri_acc += (2.0 * quad_w[p]) * inner;
+            }
+            acc += ((ot ^ st) ? -A : A) * tri_acc;
+        }
+    }
+    return (go.leng * gs.leng) * acc;
+}
+
 // 2x3 projection onto (theta-hat, phi-hat) (Math::toThPh, src/math.h:90-95),
 // stored row-major: [cth cph, cth sph, -sth; -sph, cph, 0].
 MLFMA_HD void thph_apply(const double* T, const zd* v, zd* out) {

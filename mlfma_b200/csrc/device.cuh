@@ -5,7 +5,9 @@
 //   * FP64: complex double everywhere (the reference's arithmetic);
 //   * mixed: outgoing/local patterns, radiation patterns, transfer functions,
 //     shifts and interpolation weights in complex float, accumulated in float;
-//     the near field, x, y and the combination stay complex double.
+//     the near field, x, y and the combination stay complex double.  A mixed
+//     operator also keeps the FP64 far field, which iterative refinement uses
+//     for its FP64 residuals.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -83,6 +85,9 @@ struct DevSources {
     const double* tri_quad; // [tri][nq][3]
     const double* quad_w;   // [nq]
     int nq;
+    int self_terms;         // see Config::self_terms
+    const int* tri_v;       // [tri][3] vertex indices
+    const double* tri_p;    // [tri][3][3] vertices
 };
 
 // Geometry the setup kernels need (patterns, near-field entries).
@@ -118,12 +123,14 @@ public:
 
     // y (user order) = (accumulate ? y : 0) + A x, device pointers, on `stream`
     // (0 = the operator's own stream).  Interleaved complex FP64.
-    std::string matvec_device(const double2* x, double2* y, bool accumulate, cudaStream_t stream);
+    // prec: far-field precision (-1 = the operator's own; a mixed operator
+    // also carries the FP64 far field).
+    std::string matvec_device(const double2* x, double2* y, bool accumulate, cudaStream_t stream, int prec = -1);
 
     // Operator on tree-ordered device vectors (used by the solver).
-    void apply_tree(const double2* xt, double2* yt, cudaStream_t s);
+    void apply_tree(const double2* xt, double2* yt, cudaStream_t s, int prec = -1);
     // Same, never capturing a graph (launches the captured one if it exists).
-    void apply_tree_direct(const double2* xt, double2* yt, cudaStream_t s);
+    void apply_tree_direct(const double2* xt, double2* yt, cudaStream_t s, int prec = -1);
 
     // Per-stage CUDA-event timing of one matvec on the operator's stream.
     std::string time_stages(StageTimes* out);
@@ -153,10 +160,10 @@ private:
     template <class T> T* upload(const std::vector<T>& v);
     template <class R> std::string setup_far(const Plan& plan, FarField<R>& F, const double2* pat64);
     template <class R> void run_far_t(FarField<R>& F, const double2* xt, cudaStream_t s, int stage);
-    void run_far(const double2* xt, cudaStream_t s, int stage = -1);
+    void run_far(const double2* xt, cudaStream_t s, int stage = -1, int prec = -1);
     void run_near(const double2* xt, cudaStream_t s);
-    void enqueue_core(cudaStream_t s);   // xt_ -> yfar_, ynear_
-    std::string ensure_graph();
+    void enqueue_core(cudaStream_t s, int prec);   // xt_ -> yfar_, ynear_
+    std::string ensure_graph(int prec);
     static int m2m_rows(int nth, int nph);
 
     int device_ = 0;
@@ -167,8 +174,8 @@ private:
     cudaEvent_t ev_fork_ = nullptr, ev_join_ = nullptr;
     std::vector<void*> allocs_;
     long long bytes_ = 0;
-    cudaGraph_t graph_ = nullptr;
-    cudaGraphExec_t graph_exec_ = nullptr;
+    cudaGraph_t graph_[2] = {nullptr, nullptr};          // per far-field precision
+    cudaGraphExec_t graph_exec_[2] = {nullptr, nullptr};
     bool use_graph_ = true;
 
     // Shared by both precisions.

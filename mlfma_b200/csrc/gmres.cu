@@ -109,6 +109,20 @@ __global__ void k_scale(const double2* __restrict__ x, double2 a, double2* __res
     out[i] = make_double2(a.x * v.x - a.y * v.y, a.x * v.y + a.y * v.x);
 }
 
+// out->x = sum of partial[0..n) in a fixed order (one thread)
+__global__ void k_sum_into(const double* __restrict__ partial, int n, double2* __restrict__ out) {
+    double acc = 0.0;
+    for (int c = 0; c < n; ++c) acc += partial[c];
+    *out = make_double2(acc, 0.0);
+}
+
+// y += x
+__global__ void k_axpy1(const double2* __restrict__ x, double2* __restrict__ y, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    y[i] = make_double2(y[i].x + x[i].x, y[i].y + x[i].y);
+}
+
 // out = b - y
 __global__ void k_sub(const double2* __restrict__ b, const double2* __restrict__ y, double2* __restrict__ out, int n) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -135,13 +149,16 @@ inline int nblk(long long n, int bs) { return static_cast<int>((n + bs - 1) / bs
         if (e_ != cudaSuccess) return std::string(#call) + ": " + cudaGetErrorString(e_); \
     } while (0)
 
-std::string Gmres::ensure(int n, int ncols) {
+// extra = 2: also the two vectors of iterative refinement.
+std::string Gmres::ensure(int n, int ncols, int extra) {
     if (external_)
-        return (n == n_ && ncols <= cap_) ? std::string() : std::string("fixed workspace set up for another size");
-    if (n == n_ && ncols <= cap_) return {};
+        return (n == n_ && ncols <= cap_ && extra <= extra_) ? std::string()
+                                                             : std::string("fixed workspace set up for another size");
+    if (n == n_ && ncols <= cap_ && extra <= extra_) return {};
     release();
     n_ = n;
     cap_ = ncols;
+    extra_ = extra;
     nchunks_ = (n + kDotChunk - 1) / kDotChunk;
     GM_CK(cudaMalloc(&Q_, sizeof(double2) * static_cast<size_t>(n) * ncols));
     GM_CK(cudaMalloc(&w_, sizeof(double2) * n));
@@ -152,23 +169,27 @@ std::string Gmres::ensure(int n, int ncols) {
     GM_CK(cudaMalloc(&y_, sizeof(double2) * (ncols + 1)));
     GM_CK(cudaMalloc(&partial_, sizeof(double2) * static_cast<size_t>(nchunks_) * (ncols + 1)));
     GM_CK(cudaMalloc(&npartial_, sizeof(double) * nchunks_));
+    if (extra >= 2) {
+        GM_CK(cudaMalloc(&xo_, sizeof(double2) * n));
+        GM_CK(cudaMalloc(&bo_, sizeof(double2) * n));
+    }
     return {};
 }
 
 void Gmres::release() {
     if (!external_)
         for (void* p : {(void*)Q_, (void*)w_, (void*)b_, (void*)x_, (void*)r_, (void*)h_, (void*)y_,
-                        (void*)partial_, (void*)npartial_})
+                        (void*)partial_, (void*)npartial_, (void*)xo_, (void*)bo_})
             if (p) cudaFree(p);
-    Q_ = w_ = b_ = x_ = r_ = h_ = y_ = partial_ = nullptr;
+    Q_ = w_ = b_ = x_ = r_ = h_ = y_ = partial_ = xo_ = bo_ = nullptr;
     npartial_ = nullptr;
-    n_ = cap_ = 0;
+    n_ = cap_ = extra_ = 0;
 }
 
 Gmres::~Gmres() { release(); }
 
-void Gmres::apply(DeviceOp& op, const double2* x, double2* y, cudaStream_t s) {
-    if (external_) op.apply_tree_direct(x, y, s); else op.apply_tree(x, y, s);
+void Gmres::apply(DeviceOp& op, const double2* x, double2* y, cudaStream_t s, int prec) {
+    if (external_) op.apply_tree_direct(x, y, s, prec); else op.apply_tree(x, y, s, prec);
 }
 
 // ------------------------------------------------------------ fixed workspace
@@ -186,7 +207,7 @@ constexpr int kNoAllocNorm = 4096;
 static __device__ __align__(256) double2 g_noalloc_ws[kNoAllocWorkspace];
 static __device__ __align__(256) double g_noalloc_norm[kNoAllocNorm];
 
-std::string Gmres::use_static_workspace(int n, int ncols) {
+std::string Gmres::use_static_workspace(int n, int ncols, int extra) {
     // Device addresses of the arrays, looked up once per device (with that
     // device current); host code only sees host-side stand-ins for them.
     static std::mutex mu;
@@ -208,14 +229,16 @@ std::string Gmres::use_static_workspace(int n, int ncols) {
         }
     }
     const int nchunks = (n + kDotChunk - 1) / kDotChunk;
-    const size_t need = static_cast<size_t>(n) * ncols + 4 * static_cast<size_t>(n) +
+    const size_t need = static_cast<size_t>(n) * ncols + (4 + extra) * static_cast<size_t>(n) +
                         2 * static_cast<size_t>(ncols + 1) + static_cast<size_t>(nchunks) * (ncols + 1);
     if (need > kNoAllocWorkspace || nchunks > kNoAllocNorm)
-        return "size:N x (restart + 5) exceeds the fixed workspace of 2097152 complex values";
+        return extra ? "size:N x (restart + 7) exceeds the fixed workspace of 2097152 complex values"
+                     : "size:N x (restart + 5) exceeds the fixed workspace of 2097152 complex values";
     if (!external_) release();
     external_ = true;
     n_ = n;
     cap_ = ncols;
+    extra_ = extra;
     nchunks_ = nchunks;
     double2* p = ws;
     Q_ = p; p += static_cast<size_t>(n) * ncols;
@@ -225,6 +248,12 @@ std::string Gmres::use_static_workspace(int n, int ncols) {
     r_ = p; p += n;
     h_ = p; p += ncols + 1;
     y_ = p; p += ncols + 1;
+    if (extra >= 2) {
+        xo_ = p; p += n;
+        bo_ = p; p += n;
+    } else {
+        xo_ = bo_ = nullptr;
+    }
     partial_ = p;
     npartial_ = nws;
     return {};
@@ -257,66 +286,54 @@ std::string Gmres::cgs_pass(int ncols, cudaStream_t s, bool add) {
     return {};
 }
 
-std::string Gmres::solve(DeviceOp& op, const double2* d_b_user, double2* d_x_user, const SolveOpts& o,
-                         SolveResult* res) {
+// Restarted GMRES(m) on A(prec) x_ = b_ with x_ = 0 on entry (Solver::solve,
+// src/solver.cpp:116-146, when restart = 0).  One host synchronisation per
+// Arnoldi step: the new Hessenberg column and the norm of the orthogonalised
+// vector come back in one copy.
+std::string Gmres::cycles(DeviceOp& op, int prec, const SolveOpts& o, double bnorm, double tol_abs, int max_iter,
+                          bool refg, int* iters, double* resid, bool* conv) {
     using cd = std::complex<double>;
-    const auto t_start = std::chrono::steady_clock::now();
-    const int n = op.n();
-    const int m = o.restart > 0 ? o.restart : o.max_iter;
-    if (m < 1 || o.max_iter < 1) return "max_iter and restart must be positive";
-    std::string err = ensure(n, m + 1);
-    if (!err.empty()) return err;
+    const int n = n_;
+    const int m = o.restart > 0 ? o.restart : max_iter;
     cudaStream_t s = op.stream();
-    const int* perm = op.perm();
-    k_gather_perm<<<nblk(n, 256), 256, 0, s>>>(d_b_user, perm, b_, n);
-    GM_CK(cudaMemsetAsync(x_, 0, sizeof(double2) * n, s));
-    double bnorm = 0;
-    err = norm(b_, s, &bnorm);
-    if (!err.empty()) return err;
-    if (!std::isfinite(bnorm)) return "nonfinite:right-hand side";
-    res->iterations = 0;
-    res->residual = 0;
-    if (bnorm == 0.0) {
-        k_scatter_perm<<<nblk(n, 256), 256, 0, s>>>(x_, perm, d_x_user, n);
-        GM_CK(cudaStreamSynchronize(s));
-        res->true_residual = 0;
-        return {};
-    }
-    const bool refg = o.ref_givens != 0;
+    std::string err;
     int total = 0;
     bool converged = false;
+    double last = 0;
     std::vector<cd> H(static_cast<size_t>(m + 1) * m), cs(m), sn(m), g(m + 1);
     std::vector<double2> hcol(m + 2);
-    while (total < o.max_iter && !converged) {
+    GM_CK(cudaMemsetAsync(x_, 0, sizeof(double2) * n, s));
+    while (total < max_iter && !converged) {
         // r = b - A x  (x = 0 on the first cycle: r = b, as the reference)
         double beta;
         if (total == 0) {
             GM_CK(cudaMemcpyAsync(r_, b_, sizeof(double2) * n, cudaMemcpyDeviceToDevice, s));
+            beta = bnorm;
         } else {
-            apply(op, x_, w_, s);
+            apply(op, x_, w_, s, prec);
             k_sub<<<nblk(n, 256), 256, 0, s>>>(b_, w_, r_, n);
+            err = norm(r_, s, &beta);
+            if (!err.empty()) return err;
+            if (!std::isfinite(beta)) return "nonfinite:residual";
+            if (beta <= tol_abs) { converged = true; last = beta / bnorm; break; }
         }
-        err = norm(r_, s, &beta);
-        if (!err.empty()) return err;
-        if (!std::isfinite(beta)) return "nonfinite:residual";
-        if (beta / bnorm <= o.tol && total > 0) { converged = true; res->residual = beta / bnorm; break; }
-        const double g0 = (total == 0) ? bnorm : beta;
         k_scale<<<nblk(n, 256), 256, 0, s>>>(r_, make_double2(1.0 / beta, 0.0), Q_, n);
         std::fill(g.begin(), g.end(), cd(0));
         g[0] = beta;
         int k = 0;
-        for (; k < m && total < o.max_iter; ++k) {
+        for (; k < m && total < max_iter; ++k) {
             double2* qk = Q_ + static_cast<long long>(k) * n;
-            apply(op, qk, w_, s);  // w = A q_k
+            apply(op, qk, w_, s, prec);  // w = A q_k
             err = cgs_pass(k + 1, s, false);
             if (!err.empty()) return err;
             err = cgs_pass(k + 1, s, true);
             if (!err.empty()) return err;
-            double hn;
-            err = norm(w_, s, &hn);
-            if (!err.empty()) return err;
-            GM_CK(cudaMemcpyAsync(hcol.data(), h_, sizeof(double2) * (k + 1), cudaMemcpyDeviceToHost, s));
+            // ||w||^2 into h_[k+1].x, then h_[0..k+1] to the host in one copy.
+            k_norm2<<<nchunks_, kDotThreads, 0, s>>>(w_, n, npartial_);
+            k_sum_into<<<1, 1, 0, s>>>(npartial_, nchunks_, h_ + k + 1);
+            GM_CK(cudaMemcpyAsync(hcol.data(), h_, sizeof(double2) * (k + 2), cudaMemcpyDeviceToHost, s));
             GM_CK(cudaStreamSynchronize(s));
+            const double hn = std::sqrt(hcol[k + 1].x);
             if (!std::isfinite(hn)) return "nonfinite:Arnoldi";
             std::vector<cd> hc(k + 2);
             for (int i = 0; i <= k; ++i) hc[i] = cd(hcol[i].x, hcol[i].y);
@@ -363,9 +380,8 @@ std::string Gmres::solve(DeviceOp& op, const double2* d_b_user, double2* d_x_use
             sn[k] = sgn;
             for (int i = 0; i <= k; ++i) H[static_cast<size_t>(k) * (m + 1) + i] = hc[i];
             ++total;
-            const double rel = std::abs(g[k + 1]) / (refg ? bnorm : bnorm);
-            res->residual = rel;
-            if (!(rel > o.tol) || hn == 0.0) { ++k; converged = true; break; }
+            last = std::abs(g[k + 1]) / bnorm;
+            if (!(std::abs(g[k + 1]) > tol_abs) || hn == 0.0) { ++k; converged = true; break; }
         }
         // Solve the k x k upper-triangular system R y = g (solver.cpp:143-145).
         std::vector<cd> yv(k);
@@ -380,10 +396,43 @@ std::string Gmres::solve(DeviceOp& op, const double2* d_b_user, double2* d_x_use
         // x -= Q (-y)  ==  x += Q y
         k_sub_qh<<<nblk(n, 256), 256, 0, s>>>(Q_, n, k, y_, x_, n);
         GM_CK(cudaStreamSynchronize(s));
-        (void)g0;
         if (o.restart <= 0) break;  // unrestarted: one cycle (the reference)
     }
-    res->iterations = total;
+    *iters = total;
+    *resid = last;
+    *conv = converged;
+    return {};
+}
+
+std::string Gmres::solve(DeviceOp& op, const double2* d_b_user, double2* d_x_user, const SolveOpts& o,
+                         SolveResult* res) {
+    if (o.refine && op.precision() != kFp64) return solve_refined(op, d_b_user, d_x_user, o, res);
+    const auto t_start = std::chrono::steady_clock::now();
+    const int n = op.n();
+    const int m = o.restart > 0 ? o.restart : o.max_iter;
+    if (m < 1 || o.max_iter < 1) return "max_iter and restart must be positive";
+    std::string err = ensure(n, m + 1, 0);
+    if (!err.empty()) return err;
+    cudaStream_t s = op.stream();
+    const int* perm = op.perm();
+    k_gather_perm<<<nblk(n, 256), 256, 0, s>>>(d_b_user, perm, b_, n);
+    double bnorm = 0;
+    err = norm(b_, s, &bnorm);
+    if (!err.empty()) return err;
+    if (!std::isfinite(bnorm)) return "nonfinite:right-hand side";
+    res->iterations = 0;
+    res->residual = 0;
+    if (bnorm == 0.0) {
+        GM_CK(cudaMemsetAsync(d_x_user, 0, sizeof(double2) * n, s));
+        GM_CK(cudaStreamSynchronize(s));
+        res->true_residual = 0;
+        res->converged = true;
+        return {};
+    }
+    bool converged = false;
+    err = cycles(op, -1, o, bnorm, o.tol * bnorm, o.max_iter, o.ref_givens != 0, &res->iterations, &res->residual,
+                 &converged);
+    if (!err.empty()) return err;
     // True residual.
     apply(op, x_, w_, s);
     k_sub<<<nblk(n, 256), 256, 0, s>>>(b_, w_, r_, n);
@@ -392,6 +441,72 @@ std::string Gmres::solve(DeviceOp& op, const double2* d_b_user, double2* d_x_use
     if (!err.empty()) return err;
     res->true_residual = rn / bnorm;
     k_scatter_perm<<<nblk(n, 256), 256, 0, s>>>(x_, perm, d_x_user, n);
+    GM_CK(cudaStreamSynchronize(s));
+    res->converged = converged;
+    res->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
+    return {};
+}
+
+// Mixed-precision iterative refinement: the outer loop keeps the solution and
+// its residual r = b - A x in FP64 (FP64 far field); each inner solve runs
+// GMRES on the mixed operator for the correction d in A d = r, to a residual
+// target of 0.9 of the remaining gap, and x += d.  The mixed far field differs
+// from the FP64 one by float rounding (about 1e-8 relative on the product),
+// so one inner solve normally reaches the target and the FP64 residual only
+// confirms it.
+std::string Gmres::solve_refined(DeviceOp& op, const double2* d_b_user, double2* d_x_user, const SolveOpts& o,
+                                 SolveResult* res) {
+    const auto t_start = std::chrono::steady_clock::now();
+    const int n = op.n();
+    const int m = o.restart > 0 ? o.restart : o.max_iter;
+    if (m < 1 || o.max_iter < 1) return "max_iter and restart must be positive";
+    std::string err = ensure(n, m + 1, 2);
+    if (!err.empty()) return err;
+    cudaStream_t s = op.stream();
+    const int* perm = op.perm();
+    k_gather_perm<<<nblk(n, 256), 256, 0, s>>>(d_b_user, perm, bo_, n);
+    GM_CK(cudaMemsetAsync(xo_, 0, sizeof(double2) * n, s));
+    double bnorm = 0;
+    err = norm(bo_, s, &bnorm);
+    if (!err.empty()) return err;
+    if (!std::isfinite(bnorm)) return "nonfinite:right-hand side";
+    *res = SolveResult{};
+    if (bnorm == 0.0) {
+        GM_CK(cudaMemsetAsync(d_x_user, 0, sizeof(double2) * n, s));
+        GM_CK(cudaStreamSynchronize(s));
+        res->converged = true;
+        return {};
+    }
+    GM_CK(cudaMemcpyAsync(b_, bo_, sizeof(double2) * n, cudaMemcpyDeviceToDevice, s));
+    double rn = bnorm;
+    bool converged = false;
+    const int kMaxOuter = 20;
+    while (res->iterations < o.max_iter && res->refinements < kMaxOuter) {
+        // Inner target: residual of the correction system at most eta * ||r||;
+        // the mixed product is within about 1e-8 of the FP64 one, so aiming at
+        // 0.9 of the gap normally lands under tol on the FP64 residual.
+        double eta = o.inner_tol > 0 ? o.inner_tol : 0.9 * o.tol * bnorm / rn;
+        eta = std::min(eta, 0.5);
+        int it = 0;
+        double est = 0;
+        bool c = false;
+        err = cycles(op, kMixed, o, rn, eta * rn, o.max_iter - res->iterations, false, &it, &est, &c);
+        if (!err.empty()) return err;
+        res->iterations += it;
+        // x += d ; r = b - A64 x  (FP64)
+        k_axpy1<<<nblk(n, 256), 256, 0, s>>>(x_, xo_, n);
+        apply(op, xo_, w_, s, kFp64);
+        k_sub<<<nblk(n, 256), 256, 0, s>>>(bo_, w_, b_, n);
+        ++res->refinements;
+        err = norm(b_, s, &rn);
+        if (!err.empty()) return err;
+        if (!std::isfinite(rn)) return "nonfinite:residual";
+        res->residual = rn / bnorm;
+        if (rn <= o.tol * bnorm) { converged = true; break; }
+        if (it == 0) break;  // no progress possible
+    }
+    res->true_residual = rn / bnorm;
+    k_scatter_perm<<<nblk(n, 256), 256, 0, s>>>(xo_, perm, d_x_user, n);
     GM_CK(cudaStreamSynchronize(s));
     res->converged = converged;
     res->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();

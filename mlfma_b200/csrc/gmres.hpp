@@ -14,6 +14,9 @@ struct SolveOpts {
     double tol = 1e-6;
     int restart = 0;     // 0: no restart (reference)
     int ref_givens = 1;  // complex-symmetric rotations of the reference
+    int refine = 0;      // mixed operator: inner GMRES on the mixed far field,
+                         // outer loop on the FP64 residual
+    double inner_tol = 0;  // refinement: inner relative target (0 = automatic)
 };
 
 struct SolveResult {
@@ -22,6 +25,7 @@ struct SolveResult {
     double true_residual = 0;
     double seconds = 0;
     bool converged = false;
+    int refinements = 0;   // outer FP64 residual evaluations (refinement only)
 };
 
 class Gmres {
@@ -38,17 +42,24 @@ public:
     // Point this solver at the library's fixed device workspace instead of
     // allocating (see mlfma_gmres_noalloc); products then run without graph
     // capture.  Fails if n and ncols do not fit.
-    std::string use_static_workspace(int n, int ncols);
+    // extra = 2 reserves the two vectors of iterative refinement.
+    std::string use_static_workspace(int n, int ncols, int extra = 0);
 
 private:
-    void apply(DeviceOp& op, const double2* x, double2* y, cudaStream_t s);
+    void apply(DeviceOp& op, const double2* x, double2* y, cudaStream_t s, int prec = -1);
+    // Restarted GMRES on A(prec) x_ = b_ from x_ = 0 until the estimated
+    // residual norm is at most tol_abs or max_iter iterations have run.
+    std::string cycles(DeviceOp& op, int prec, const SolveOpts& o, double bnorm, double tol_abs, int max_iter,
+                       bool refg, int* iters, double* resid, bool* conv);
+    std::string solve_refined(DeviceOp& op, const double2* d_b_user, double2* d_x_user, const SolveOpts& o,
+                              SolveResult* res);
     bool external_ = false;   // workspace not owned (static device array)
-    std::string ensure(int n, int ncols);
+    std::string ensure(int n, int ncols, int extra);
     void release();
     std::string norm(const double2* v, cudaStream_t s, double* out);
     std::string cgs_pass(int ncols, cudaStream_t s, bool add);
 
-    int n_ = 0, cap_ = 0, nchunks_ = 0;
+    int n_ = 0, cap_ = 0, extra_ = 0, nchunks_ = 0;
     double2* Q_ = nullptr;
     double2* w_ = nullptr;
     double2* b_ = nullptr;
@@ -58,6 +69,8 @@ private:
     double2* y_ = nullptr;
     double2* partial_ = nullptr;
     double* npartial_ = nullptr;
+    double2* xo_ = nullptr;   // refinement: accumulated solution
+    double2* bo_ = nullptr;   // refinement: right-hand side
 };
 
 }  // namespace mlfma

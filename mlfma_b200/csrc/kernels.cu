@@ -85,8 +85,10 @@ constexpr int kDnWidths[] = {8, 12, 16, 24, 32};
 
 DeviceOp::~DeviceOp() {
     if (device_ >= 0) cudaSetDevice(device_);
-    if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
-    if (graph_) cudaGraphDestroy(graph_);
+    for (int p = 0; p < 2; ++p) {
+        if (graph_exec_[p]) cudaGraphExecDestroy(graph_exec_[p]);
+        if (graph_[p]) cudaGraphDestroy(graph_[p]);
+    }
     for (void* p : allocs_) cudaFree(p);
     if (ev_fork_) cudaEventDestroy(ev_fork_);
     if (ev_join_) cudaEventDestroy(ev_join_);
@@ -332,14 +334,15 @@ std::string DeviceOp::setup(const Plan& plan, int device, int precision) {
             S.tri_quad = upload(plan.tri_quad);
             S.quad_w = upload(plan.quad_w);
             S.nq = plan.nq;
+            S.tri_v = upload(plan.tri_v);
+            S.tri_p = upload(plan.tri_p);
         }
+        S.self_terms = plan.cfg.self_terms;
         src_ = S;
-        double2* pat64 = nullptr;
-        if (precision == kFp64) {
-            pat64 = alloc<double2>(static_cast<size_t>(plan.pat_elems) * 2);
-        } else {
-            MLFMA_CK(cudaMalloc(&pat64, sizeof(double2) * std::max<long long>(1, plan.pat_elems * 2)));
-        }
+        // Complex double patterns: the FP64 far field reads them; the mixed far
+        // field reads a complex float copy.  A mixed operator keeps the FP64
+        // far field too, for the FP64 residual of iterative refinement.
+        double2* pat64 = alloc<double2>(static_cast<size_t>(plan.pat_elems) * 2);
         if (n_leaves_ > 0 && plan.kind == kRwg && plan.cfg.ref_compat) {
             // Reference-compatible RWG patterns: the closed-form integral is
             // ill-conditioned near alpha, beta, gamma = 0, so it is evaluated on
@@ -358,12 +361,11 @@ std::string DeviceOp::setup(const Plan& plan, int device, int precision) {
         }
 
         // ---- far field in the chosen precision
-        std::string err = precision == kFp64 ? setup_far<double>(plan, f64_, pat64)
-                                             : setup_far<float>(plan, f32_, pat64);
+        std::string err = setup_far<double>(plan, f64_, pat64);
         if (!err.empty()) return err;
         if (precision != kFp64) {
-            MLFMA_CK(cudaStreamSynchronize(stream_));
-            cudaFree(pat64);
+            err = setup_far<float>(plan, f32_, pat64);
+            if (!err.empty()) return err;
         }
 
         // ---- near field: block rows (both orientations), gather-only application
@@ -455,8 +457,9 @@ void DeviceOp::run_far_t(FarField<R>& F, const double2* xt, cudaStream_t s, int 
         k_l2t<R><<<n_l2t_items_, kL2TThreads, 0, s>>>(F.lv_dev, l2t_items_, leaves_, F.pat, yfar_);
 }
 
-void DeviceOp::run_far(const double2* xt, cudaStream_t s, int stage) {
-    if (precision_ == kFp64) run_far_t(f64_, xt, s, stage); else run_far_t(f32_, xt, s, stage);
+void DeviceOp::run_far(const double2* xt, cudaStream_t s, int stage, int prec) {
+    if (prec < 0) prec = precision_;
+    if (prec == kFp64) run_far_t(f64_, xt, s, stage); else run_far_t(f32_, xt, s, stage);
 }
 
 void DeviceOp::run_near(const double2* xt, cudaStream_t s) {
@@ -465,48 +468,53 @@ void DeviceOp::run_near(const double2* xt, cudaStream_t s) {
 }
 
 // The tree-ordered product xt_ -> (yfar_, ynear_): near field on the side
-// stream, far-field chain on s.  Captured once into a CUDA graph.
-void DeviceOp::enqueue_core(cudaStream_t s) {
+// stream, far-field chain on s in precision prec.  Captured once per
+// precision into a CUDA graph.
+void DeviceOp::enqueue_core(cudaStream_t s, int prec) {
     cudaMemsetAsync(yfar_, 0, sizeof(double2) * n_, s);
     cudaMemsetAsync(ynear_, 0, sizeof(double2) * n_, s);
     cudaEventRecord(ev_fork_, s);
     cudaStreamWaitEvent(side_, ev_fork_, 0);
     run_near(xt_, side_);
     cudaEventRecord(ev_join_, side_);
-    run_far(xt_, s);
+    run_far(xt_, s, -1, prec);
     cudaStreamWaitEvent(s, ev_join_, 0);
 }
 
-std::string DeviceOp::ensure_graph() {
-    if (graph_exec_ || !use_graph_) return {};
+std::string DeviceOp::ensure_graph(int prec) {
+    if (graph_exec_[prec] || !use_graph_) return {};
     MLFMA_CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
-    enqueue_core(stream_);
-    MLFMA_CK(cudaStreamEndCapture(stream_, &graph_));
-    MLFMA_CK(cudaGraphInstantiate(&graph_exec_, graph_, 0));
+    enqueue_core(stream_, prec);
+    MLFMA_CK(cudaStreamEndCapture(stream_, &graph_[prec]));
+    MLFMA_CK(cudaGraphInstantiate(&graph_exec_[prec], graph_[prec], 0));
     return {};
 }
 
-void DeviceOp::apply_tree(const double2* xt, double2* yt, cudaStream_t s) {
-    if (!ensure_graph().empty()) use_graph_ = false;
+void DeviceOp::apply_tree(const double2* xt, double2* yt, cudaStream_t s, int prec) {
+    if (prec < 0) prec = precision_;
+    if (!ensure_graph(prec).empty()) use_graph_ = false;
     if (xt != xt_) cudaMemcpyAsync(xt_, xt, sizeof(double2) * n_, cudaMemcpyDeviceToDevice, s);
-    if (graph_exec_) cudaGraphLaunch(graph_exec_, s); else enqueue_core(s);
+    if (graph_exec_[prec]) cudaGraphLaunch(graph_exec_[prec], s); else enqueue_core(s, prec);
     k_finish<<<blocks_for(n_, 256), 256, 0, s>>>(yfar_, ynear_, nullptr, yt, n_, ck_, 0);
 }
 
-void DeviceOp::apply_tree_direct(const double2* xt, double2* yt, cudaStream_t s) {
+void DeviceOp::apply_tree_direct(const double2* xt, double2* yt, cudaStream_t s, int prec) {
+    if (prec < 0) prec = precision_;
     if (xt != xt_) cudaMemcpyAsync(xt_, xt, sizeof(double2) * n_, cudaMemcpyDeviceToDevice, s);
-    if (graph_exec_) cudaGraphLaunch(graph_exec_, s); else enqueue_core(s);
+    if (graph_exec_[prec]) cudaGraphLaunch(graph_exec_[prec], s); else enqueue_core(s, prec);
     k_finish<<<blocks_for(n_, 256), 256, 0, s>>>(yfar_, ynear_, nullptr, yt, n_, ck_, 0);
 }
 
-std::string DeviceOp::matvec_device(const double2* x, double2* y, bool accumulate, cudaStream_t stream) {
+std::string DeviceOp::matvec_device(const double2* x, double2* y, bool accumulate, cudaStream_t stream, int prec) {
     if (!ready_) return "operator not set up";
+    if (prec < 0) prec = precision_;
+    if (prec != kFp64 && precision_ == kFp64) return "the FP64 operator has no mixed far field";
     cudaStream_t s = stream ? stream : stream_;
     MLFMA_CK(cudaSetDevice(device_));
-    std::string e = ensure_graph();
+    std::string e = ensure_graph(prec);
     if (!e.empty()) return e;
     k_gather<<<blocks_for(n_, 256), 256, 0, s>>>(x, perm_, xt_, n_);
-    if (graph_exec_) cudaGraphLaunch(graph_exec_, s); else enqueue_core(s);
+    if (graph_exec_[prec]) cudaGraphLaunch(graph_exec_[prec], s); else enqueue_core(s, prec);
     k_finish<<<blocks_for(n_, 256), 256, 0, s>>>(yfar_, ynear_, perm_, y, n_, ck_, accumulate ? 1 : 0);
     MLFMA_CK(cudaGetLastError());
     return {};

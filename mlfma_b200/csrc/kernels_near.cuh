@@ -89,19 +89,36 @@ __global__ void k_patterns(const DevGeomLevel* __restrict__ lvs, const DevFarLea
     }
 }
 
-// Z_mn / (C k) for obs m, src n (Dipole/RWG::getIntegratedRad,
+// True when some triangle of RWG a shares a vertex with some triangle of b.
+__device__ bool rwg_touching(const DevSources& S, const RwgGeom& a, const RwgGeom& b) {
+    for (int i = 0; i < 2; ++i)
+        for (int j = 0; j < 2; ++j)
+            for (int u = 0; u < 3; ++u)
+                for (int v = 0; v < 3; ++v)
+                    if (S.tri_v[3 * a.tri[i] + u] == S.tri_v[3 * b.tri[j] + v]) return true;
+    return false;
+}
+
+// Z_mn (the operator is A = C k Z) for obs m, src n (Dipole/RWG::getIntegratedRad,
 // src/sources/dipole.h:62-70, src/sources/rwg.cpp:92-140).  Coincident
-// sources and coincident triangles contribute nothing.
+// sources and coincident triangles contribute nothing, unless self_terms is
+// set: then a dipole's diagonal is Z_mm = 1, and RWG pairs whose triangles
+// touch take the symmetrised mixed-potential value (rwg_mpie).
 __device__ zd near_entry(const DevSources& S, int m, int n) {
     if (S.kind == kDipole) {
         const double* a = S.pos + 3 * m;
         const double* b = S.pos + 3 * n;
-        if (a[0] == b[0] && a[1] == b[1] && a[2] == b[2]) return mkz(0);
+        if (a[0] == b[0] && a[1] == b[1] && a[2] == b[2]) {
+            return mkz(S.self_terms ? 1.0 : 0.0);
+        }
         const double X[3] = {a[0] - b[0], a[1] - b[1], a[2] - b[2]};
         return dyadic_uv(X, S.k, S.phat + 3 * m, S.phat + 3 * n);
     }
     const RwgGeom& go = S.rwg[m];
     const RwgGeom& gs = S.rwg[n];
+    if (S.self_terms && rwg_touching(S, go, gs))
+        return 0.5 * (rwg_mpie(go, gs, S.tri_p, S.tri_quad, S.quad_w, S.nq, S.k) +
+                      rwg_mpie(gs, go, S.tri_p, S.tri_quad, S.quad_w, S.nq, S.k));
     if (go.center[0] == gs.center[0] && go.center[1] == gs.center[1] && go.center[2] == gs.center[2])
         return mkz(0);
     zd acc = mkz(0);

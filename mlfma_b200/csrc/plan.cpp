@@ -333,12 +333,16 @@ std::string Plan::build_rwg(const Config& c, const PlaneWave& p, int nv, const d
     // Triangles (Triangle ctor, src/sources/triangle.cpp:5-21).
     tris.resize(nf);
     tri_quad.resize(static_cast<size_t>(nf) * nq * 3);
+    tri_v.resize(static_cast<size_t>(nf) * 3);
+    tri_p.resize(static_cast<size_t>(nf) * 9);
     for (int f = 0; f < nf; ++f) {
         const double* X[3];
         for (int v = 0; v < 3; ++v) {
             const int vi = faces[3 * f + v];
             if (vi < 0 || vi >= nv) return "face vertex index out of range";
             X[v] = verts + 3 * vi;
+            tri_v[3 * f + v] = vi;
+            for (int k = 0; k < 3; ++k) tri_p[9 * f + 3 * v + k] = X[v][k];
         }
         TriGeom& T = tris[f];
         double cen[3];
@@ -888,7 +892,9 @@ void Plan::build_near_plan() {
     auto add = [&](int r0, int nr, int c0, int nc, int self) {
         if (nr <= 0 || nc <= 0) return;
         NearBlock b{r0, nr, c0, nc, near_entries, self};
-        const long long cnt = self ? static_cast<long long>(nr) * (nr - 1) / 2
+        // a self block is strict-lower in the reference; with self terms it
+        // also holds the diagonal
+        const long long cnt = self ? static_cast<long long>(nr) * (nr - 1) / 2 + (cfg.self_terms ? nr : 0)
                                    : static_cast<long long>(nr) * nc;
         if (cnt == 0) return;
         near_entries += cnt;

@@ -29,6 +29,8 @@ struct Config {
     // Extensions.
     int max_level = 0;        // >0: never split below this level
     int ref_compat = 1;       // 1: reproduce the reference's stale-local rule
+    int self_terms = 0;       // 1: unit dipole diagonal; touching RWG pairs in
+                              //    mixed-potential form, 1/R extracted
 };
 
 struct PlaneWave {
@@ -125,6 +127,8 @@ struct Plan {
     std::vector<RwgGeom> rwg;
     std::vector<TriGeom> tris;
     std::vector<double> tri_quad;    // nq x 3 per triangle
+    std::vector<int> tri_v;          // 3 vertex indices per triangle
+    std::vector<double> tri_p;       // 3 vertices x 3 coordinates per triangle
     std::vector<double> quad_w;      // nq weights (same rule for all triangles)
     int nq = 0;
     // Tree

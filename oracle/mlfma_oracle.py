@@ -194,10 +194,62 @@ QUAD_RULES = {  # Triangle::buildQuads (src/sources/triangle.cpp:45-130): (bary 
 }
 
 
+# ------------------------------------------------------------------ self terms
+# No reference counterpart: the reference leaves out coincident triangles and
+# the diagonal (rwg.cpp:97,113-116, dipole.h:65).  With self_terms the dipole
+# operator gets a unit diagonal and RWG pairs whose triangles touch are
+# integrated in mixed-potential form with the 1/R singularity extracted.
+
+def tri_potentials(P, r):
+    """Closed-form potential integrals of the flat triangle with vertices
+    P[..., 3, 3] seen from r[..., 3]:
+        I0 = int_T 1/|r - r'| dS',   I1 = int_T (rho' - rho)/|r - r'| dS',
+    rho being r projected onto the triangle's plane (returned as well).
+    Edge-by-edge formulas of Wilton et al., IEEE Trans. Antennas Propag. 32(3),
+    1984, and Graglia, IEEE Trans. Antennas Propag. 41(10), 1993."""
+    P = np.asarray(P, dtype=float)
+    r = np.asarray(r, dtype=float)
+    nrm = np.cross(P[..., 1, :] - P[..., 0, :], P[..., 2, :] - P[..., 0, :])
+    nrm = nrm / np.linalg.norm(nrm, axis=-1, keepdims=True)
+    h = np.sum(nrm * (r - P[..., 0, :]), axis=-1)
+    rho = r - h[..., None] * nrm
+    ah = np.abs(h)
+    I0 = np.zeros(np.broadcast(h, h).shape)
+    I1 = np.zeros(rho.shape)
+    for i in range(3):
+        p, q = P[..., i, :], P[..., (i + 1) % 3, :]
+        L = q - p
+        ll = np.linalg.norm(L, axis=-1, keepdims=True)
+        lh = L / ll
+        u = np.cross(lh, nrm)
+        t0 = np.sum((p - rho) * u, axis=-1)
+        lm = np.sum((p - rho) * lh, axis=-1)
+        lp = np.sum((q - rho) * lh, axis=-1)
+        r0sq = t0 * t0 + h * h
+        rm = np.sqrt(r0sq + lm * lm)
+        rp = np.sqrt(r0sq + lp * lp)
+        tiny = r0sq <= (1e-12 * ll[..., 0]) ** 2
+        with np.errstate(divide="ignore", invalid="ignore"):
+            f = np.where(lm >= 0, np.log((rp + lp) / (rm + lm)),
+                         np.where(lp <= 0, np.log((rm - lm) / (rp - lp)), np.log((rp + lp) * (rm - lm) / r0sq)))
+        f = np.where(tiny, 0.0, f)
+        I0 = I0 + t0 * f - ah * (np.arctan2(t0 * lp, r0sq + ah * rp) - np.arctan2(t0 * lm, r0sq + ah * rm))
+        I1 = I1 + u * (0.5 * (r0sq * f + lp * rp - lm * rm))[..., None]
+    return I0, I1, rho
+
+
+def smooth_green(R, k):
+    """(e^{ikR} - 1)/R without cancellation; ik at R = 0."""
+    with np.errstate(divide="ignore", invalid="ignore"):
+        v = (-2.0 * np.sin(0.5 * k * R) ** 2 + 1j * np.sin(k * R)) / R
+    return np.where(R > 0, v, 1j * k)
+
+
 class DipoleSources:
     """Dipole (src/sources/dipole.h)."""
 
     kind = "dipole"
+    self_terms = False
 
     def __init__(self, pos, mom, pw):
         self.pos = np.asarray(pos, dtype=float)
@@ -223,18 +275,20 @@ class DipoleSources:
         return np.einsum("drc,sdc->sdr", thph, v)
 
     def block(self, rows, cols, k):
-        """Z[rows, cols]/(C k) (Dipole::getIntegratedRad, dipole.h:62-70)."""
+        """Z[rows, cols], the operator being C k Z (Dipole::getIntegratedRad, dipole.h:62-70)."""
         X = self.pos[rows][:, None, :] - self.pos[cols][None, :, :]
         same = np.all(X == 0.0, axis=-1)
         Xs = np.where(same[..., None], 1.0, X)
         z = dyadic_uv(Xs, k, self.phat[rows][:, None, :], self.phat[cols][None, :, :])
-        return np.where(same, 0.0, z)
+        # self_terms: unit diagonal Z_mm = 1 (the operator is C k Z)
+        return np.where(same, 1.0 if self.self_terms else 0.0, z)
 
 
 class RWGSources:
     """RWG on a triangle mesh (src/sources/rwg.*, triangle.*)."""
 
     kind = "rwg"
+    self_terms = False
 
     def __init__(self, verts, faces, rwgs, pw, quad_prec=2):
         V = np.asarray(verts, dtype=float)
@@ -243,6 +297,9 @@ class RWGSources:
         self.pw = pw
         self.n = E.shape[0]
         X = V[F]                                   # [f, 3 verts, 3]
+        self.F = F
+        self.P = X
+        self.area = 0.5 * np.linalg.norm(np.cross(X[:, 1] - X[:, 0], X[:, 2] - X[:, 0]), axis=1)
         self.X0 = X[:, 0]
         self.D0 = X[:, 1] - X[:, 0]
         self.D2 = X[:, 0] - X[:, 2]
@@ -307,7 +364,7 @@ class RWGSources:
         return np.einsum("drc,sdc->sdr", thph, v)
 
     def block(self, rows, cols, k):
-        """Z[rows, cols]/(C k) by double quadrature over the four triangle pairs,
+        """Z[rows, cols] (operator C k Z) by double quadrature over the four triangle pairs,
         skipping coincident triangles and coincident RWGs (RWG::getIntegratedRad,
         rwg.cpp:92-140)."""
         rows, cols = np.asarray(rows), np.asarray(cols)
@@ -329,7 +386,51 @@ class RWGSources:
                 out += np.where(mask, sgn * acc, 0.0)
         same = np.all(self.centers[rows][:, None, :] == self.centers[cols][None, :, :], axis=-1)
         out = out * (self.leng[rows][:, None] * self.leng[cols][None, :])
-        return np.where(same, 0.0, out)
+        out = np.where(same, 0.0, out)
+        if self.self_terms:
+            ti, tj = np.nonzero(self.touching(rows, cols))
+            m, n = rows[ti], cols[tj]
+            out[ti, tj] = 0.5 * (self.mpie(m, n, k) + self.mpie(n, m, k))
+        return out
+
+    def touching(self, rows, cols):
+        """[r, c]: some triangle of RWG r shares a vertex with some triangle of RWG c."""
+        vr = self.F[self.tri[rows]].reshape(len(rows), 6)
+        vc = self.F[self.tri[cols]].reshape(len(cols), 6)
+        return np.any(vr[:, None, :, None] == vc[None, :, None, :], axis=(2, 3))
+
+    def mpie(self, m, n, k):
+        """Z_mn (operator C k Z) for RWG pairs (m[i], n[i]) in mixed-potential form,
+        int int [f_m.f_n - (div f_m)(div f_n)/k^2] e^{ikR}/R, with f = s l/(2A) (r - X)
+        on triangle T of area A (s = +1 on T+, -1 on T-; div f = s l/A).  The
+        source triangle's integral of 1/R is closed form (tri_potentials), the
+        rest (e^{ikR} - 1)/R by the triangle rule; the observation triangle by
+        the triangle rule."""
+        m, n = np.asarray(m), np.asarray(n)
+        w2 = 2.0 * self.qw                       # weights summing to 1
+        out = np.zeros(m.size, dtype=complex)
+        for ot in range(2):
+            T = self.tri[m, ot]
+            A = self.area[T]
+            X = self.xpm[m, ot]
+            ro = self.qpts[T]                    # [i, p, 3]
+            for st in range(2):
+                Tp = self.tri[n, st]
+                Ap = self.area[Tp]
+                Xp = self.xpm[n, st]
+                rs = self.qpts[Tp]               # [i, q, 3]
+                I0, I1, rho = tri_potentials(self.P[Tp][:, None, :, :], ro)      # [i, p], [i, p, 3]
+                J0 = I0.astype(complex)
+                J1 = (I1 + (rho - Xp[:, None, :]) * I0[..., None]).astype(complex)
+                R = np.linalg.norm(ro[:, :, None, :] - rs[:, None, :, :], axis=-1)  # [i, p, q]
+                gs = smooth_green(R, k) * (Ap[:, None, None] * w2[None, None, :])
+                J0 = J0 + gs.sum(axis=-1)
+                J1 = J1 + np.einsum("ipq,iqc->ipc", gs, rs - Xp[:, None, :])
+                AAp = (A * Ap)[:, None]
+                inner = np.einsum("ipc,ipc->ip", ro - X[:, None, :], J1) / (4.0 * AAp) - J0 / (k * k * AAp)
+                sgn = -1.0 if (ot ^ st) else 1.0
+                out += sgn * A * (inner @ w2)
+        return out * self.leng[m] * self.leng[n]
 
 
 # ------------------------------------------------------------------ tree
@@ -602,10 +703,12 @@ class Oracle:
                 if len(nd.srcs):
                     self.near.append((lf.srcs, nd.srcs, srcs.block(lf.srcs, nd.srcs, self.k)))
         self.self_blocks = []
+        self.diag = np.zeros(srcs.n, dtype=complex)
         for a in self.leaves:
-            if len(a.srcs) > 1:
+            if len(a.srcs) > 1 or (srcs.self_terms and len(a.srcs)):
                 Z = srcs.block(a.srcs, a.srcs, self.k)
                 self.self_blocks.append((a.srcs, np.tril(Z, -1)))
+                self.diag[a.srcs] = np.diag(Z)  # zero unless self_terms
         for nd in self.nodes:
             if nd.level >= 2 and len(nd.srcs):
                 lv = self.levels[nd.level]
@@ -683,13 +786,14 @@ class Oracle:
             y[c] += Z.T @ x[r]
         for s, Z in self.self_blocks:  # evalSelfSols (leaf.cpp:361-383)
             y[s] += Z @ x[s] + Z.T @ x[s]
+        y += self.diag * x
         return PHYS_C * self.k * y
 
     def rhs(self):
         return -self.srcs.voltage()
 
     def dense(self):
-        """The exact operator C k Z (zero diagonal), for small N."""
+        """The exact operator C k Z (zero diagonal unless self_terms), for small N."""
         n = self.srcs.n
         idx = np.arange(n)
         return PHYS_C * self.k * self.srcs.block(idx, idx, self.k)

@@ -59,3 +59,24 @@ def test_mixed_gmres_tracks_fp64(cuda_device):
     assert i32.iterations == i64.iterations
     assert abs(i32.true_residual - i64.true_residual) <= 1e-3 * i64.true_residual + 1e-6
     assert rel(x32, x64) < 1e-4
+
+
+def test_refined_mixed_solve_meets_fp64_residual(cuda_device):
+    # Iterative refinement: inner GMRES on the mixed operator, outer residual in
+    # FP64.  The returned solution must meet the tolerance on the FP64 operator
+    # (checked here with a separate FP64 operator) and agree with the FP64 solve.
+    m = inputs.make_icosphere(3, radius=1.0)
+    op64 = MLFMA.rwg(m, PW, max_node_srcs=16, ref_compat=0, precision=0, self_terms=1).setup()
+    opmx = MLFMA.rwg(m, PW, max_node_srcs=16, ref_compat=0, precision=1, self_terms=1).setup()
+    b = op64.rhs()
+    tol = 1e-4
+    x64, i64 = op64.solve(b, max_iter=400, tol=tol, restart=50, ref_givens=False)
+    xmx, imx = opmx.solve(b, max_iter=400, tol=tol, restart=50, ref_givens=False, refine=True)
+    assert i64.converged and imx.converged
+    assert imx.refinements >= 1
+    r = rel(op64.matvec(xmx), b)
+    assert r <= tol * 1.0001, r
+    assert abs(r - imx.true_residual) <= 1e-3 * r
+    assert rel(xmx, x64) < 10 * tol
+    op64.close()
+    opmx.close()
