@@ -60,6 +60,8 @@ typedef struct {
                             integrated in mixed-potential form with the 1/R
                             singularity of the source triangle in closed form
                             (symmetrised, FP64) */
+    int max_rhs;         /* most right-hand sides of one product (1..64; mlfma_matvec_multi,
+                            mlfma_gmres_multi); > 1 reserves their device work space */
 } mlfma_config;
 
 enum { MLFMA_FP64 = 0, MLFMA_MIXED = 1 };
@@ -181,6 +183,32 @@ int mlfma_farfield(mlfma_handle h, const double* x, int ndir, const double* khat
  * first call before any stream capture. */
 int mlfma_gmres_noalloc(mlfma_handle h, const void* d_b, void* d_x, const mlfma_solver_opts* opts,
                         mlfma_solve_info* info);
+
+/* b = -V for another incident plane wave of the operator's wavenumber (the
+ * Solver ctor's right-hand side, src/solver.cpp:31-32, with
+ * Source::buildVoltage, src/sources/dipole.h:29-32, src/sources/rwg.h:18-21,
+ * evaluated for pw).  Many incident directions give the right-hand sides of
+ * mlfma_gmres_multi. */
+int mlfma_rhs_planewave(mlfma_handle h, const mlfma_planewave* pw, double* b);
+
+/* Y = A X (accumulate = 0) or Y += A X for nrhs vectors at once (1 <= nrhs <=
+ * max_rhs): Solver::evalRvec, src/solver.cpp:41-57, applied to many lvec.
+ * x and y hold the nrhs vectors one after another (nrhs x n complex, caller
+ * order).  Every coefficient of the operator is read once per call, and the
+ * per-leaf products become small complex GEMMs.  Host buffers. */
+int mlfma_matvec_multi(mlfma_handle h, int nrhs, const double* x, double* y, int accumulate);
+/* Same on device buffers (stream as in mlfma_matvec_device). */
+int mlfma_matvec_multi_device(mlfma_handle h, int nrhs, const void* d_x, void* d_y, int accumulate, void* stream);
+
+/* GMRES on nrhs right-hand sides sharing every product (Solver::solve,
+ * src/solver.cpp:116-146, for many b): each system has its own Krylov basis
+ * and Givens rotations (unitary; ref_givens is ignored) and stops on its own
+ * tolerance.  b and x: nrhs x n complex host buffers, caller order; info:
+ * nrhs records (may be NULL).  refine as in mlfma_gmres. */
+int mlfma_gmres_multi(mlfma_handle h, int nrhs, const double* b, double* x, const mlfma_solver_opts* opts,
+                      mlfma_solve_info* info);
+/* Per-stage CUDA-event time of one product on nrhs right-hand sides. */
+int mlfma_time_stages_multi(mlfma_handle h, int nrhs, mlfma_stage_times* t);
 
 /* The handle's own CUDA stream (cudaStream_t as void*), on which mlfma_matvec
  * and mlfma_gmres run; callers may record events on it. */

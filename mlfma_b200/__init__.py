@@ -202,6 +202,55 @@ class MLFMA:
         return x, SolveResult(info.iterations, info.residual, info.true_residual, info.seconds, converged,
                               info.refinements)
 
+    # ---------------------------------------------------------------- many right-hand sides
+    def rhs_planewave(self, pw: inputs.PlaneWave) -> np.ndarray:
+        """-V for another incident plane wave (same wavenumber)."""
+        b = np.zeros(self.n, dtype=np.complex128)
+        p = _pw(pw)
+        check(lib().mlfma_rhs_planewave(self._h, ctypes.byref(p), b.view(np.float64).ctypes.data_as(_dp)))
+        return b
+
+    def _cmat(self, X):
+        a = np.ascontiguousarray(np.asarray(X, dtype=np.complex128))
+        if a.ndim != 2 or a.shape[1] != self.n:
+            raise ValueError(f"expected (nrhs, {self.n}) array")
+        return a
+
+    def matvec_multi(self, X, accumulate: bool = False, out: np.ndarray | None = None) -> np.ndarray:
+        """Y = A X for the rows of X (nrhs x n), one batched product."""
+        xv = self._cmat(X)
+        y = out if out is not None else np.zeros_like(xv)
+        check(lib().mlfma_matvec_multi(self._h, xv.shape[0], xv.view(np.float64).ctypes.data_as(_dp),
+                                       y.view(np.float64).ctypes.data_as(_dp), int(accumulate)))
+        return y
+
+    def matvec_multi_device(self, nrhs: int, x_ptr: int, y_ptr: int, accumulate: bool = False,
+                            stream: int = 0) -> None:
+        check(lib().mlfma_matvec_multi_device(self._h, nrhs, ctypes.c_void_p(x_ptr), ctypes.c_void_p(y_ptr),
+                                              int(accumulate), ctypes.c_void_p(stream)))
+
+    def solve_multi(self, B, max_iter: int = 500, tol: float = 1e-6, restart: int = 0, refine: bool = False,
+                    inner_tol: float = 0.0, raise_on_fail: bool = False):
+        """GMRES on the rows of B (nrhs x n) at once; returns (X, [SolveResult])."""
+        bv = self._cmat(B)
+        nr = bv.shape[0]
+        x = np.zeros_like(bv)
+        o = SolverOpts(max_iter=max_iter, tol=tol, restart=restart, ref_givens=0, refine=int(refine),
+                       inner_tol=inner_tol)
+        infos = (SolveInfo * nr)()
+        code = lib().mlfma_gmres_multi(self._h, nr, bv.view(np.float64).ctypes.data_as(_dp),
+                                       x.view(np.float64).ctypes.data_as(_dp), ctypes.byref(o), infos)
+        if code not in (0, 4) or (raise_on_fail and code != 0):
+            check(code)
+        tol_ok = [i.true_residual <= tol * (1 + 1e-12) for i in infos]
+        return x, [SolveResult(i.iterations, i.residual, i.true_residual, i.seconds, ok, i.refinements)
+                   for i, ok in zip(infos, tol_ok)]
+
+    def stage_times_multi(self, nrhs: int) -> dict:
+        t = StageTimes()
+        check(lib().mlfma_time_stages_multi(self._h, nrhs, ctypes.byref(t)))
+        return {k: float(getattr(t, k)) for k, _ in StageTimes._fields_}
+
     def farfield(self, currents, khat) -> np.ndarray:
         """Far field (ndir x 3 complex) of `currents` along unit directions `khat` (ndir x 3)."""
         cur = _cvec(currents, self.n)

@@ -28,7 +28,7 @@ class Config(ctypes.Structure):
                 ("over_interp", ctypes.c_double), ("root_leng", ctypes.c_double),
                 ("max_node_srcs", ctypes.c_int), ("max_level", ctypes.c_int),
                 ("ref_compat", ctypes.c_int), ("device", ctypes.c_int), ("precision", ctypes.c_int),
-                ("self_terms", ctypes.c_int)]
+                ("self_terms", ctypes.c_int), ("max_rhs", ctypes.c_int)]
 
 
 class PlaneWaveC(ctypes.Structure):
@@ -83,6 +83,13 @@ SIGNATURES = {
     "mlfma_farfield": (ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_int, _dp, _dp]),
     "mlfma_gmres_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                            ctypes.POINTER(SolverOpts), ctypes.POINTER(SolveInfo)]),
+    "mlfma_rhs_planewave": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(PlaneWaveC), _dp]),
+    "mlfma_matvec_multi": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _dp, _dp, ctypes.c_int]),
+    "mlfma_matvec_multi_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                                 ctypes.c_int, ctypes.c_void_p]),
+    "mlfma_gmres_multi": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _dp, _dp, ctypes.POINTER(SolverOpts),
+                                         ctypes.POINTER(SolveInfo)]),
+    "mlfma_time_stages_multi": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(StageTimes)]),
     "mlfma_get_stream": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]),
     "mlfma_time_stages": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(StageTimes)]),
     "mlfma_get_traffic": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Traffic)]),

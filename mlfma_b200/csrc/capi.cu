@@ -5,6 +5,7 @@
 #include <exception>
 #include <memory>
 #include <string>
+#include <vector>
 
 #include "../../include/mlfma_b200.h"
 #include "device.cuh"
@@ -18,13 +19,19 @@ struct mlfma_op_s {
     std::unique_ptr<mlfma::DeviceOp> dev;
     std::unique_ptr<mlfma::Gmres> gmres;
     std::unique_ptr<mlfma::Gmres> gmres_fixed;  // runs on the library's fixed workspace
+    std::unique_ptr<mlfma::GmresMulti> gmres_multi;
+    int max_rhs = 1;
+    double2* d_xm = nullptr;  // staging for host-buffer calls on many right-hand sides
+    double2* d_ym = nullptr;
     double2* d_x = nullptr;  // staging for host-buffer calls
     double2* d_y = nullptr;
     ~mlfma_op_s() {
-        if (d_x || d_y) {
+        if (d_x || d_y || d_xm || d_ym) {
             cudaSetDevice(device);
             if (d_x) cudaFree(d_x);
             if (d_y) cudaFree(d_y);
+            if (d_xm) cudaFree(d_xm);
+            if (d_ym) cudaFree(d_ym);
         }
     }
 };
@@ -41,6 +48,7 @@ int fail(int code, const std::string& msg) {
 int from_msg(const std::string& msg) {
     if (msg.empty()) return MLFMA_OK;
     if (msg.rfind("nonfinite", 0) == 0) return fail(MLFMA_ERR_NONFINITE, msg);
+    if (msg.rfind("arg:", 0) == 0) return fail(MLFMA_ERR_ARG, msg);
     return fail(MLFMA_ERR_CUDA, msg);
 }
 
@@ -90,6 +98,7 @@ int mlfma_config_default(mlfma_config* cfg) {
     cfg->device = 0;
     cfg->precision = MLFMA_FP64;
     cfg->self_terms = 0;
+    cfg->max_rhs = 1;
     return MLFMA_OK;
 }
 
@@ -100,6 +109,8 @@ int mlfma_create_dipoles(const mlfma_config* cfg, const mlfma_planewave* pw, int
         auto h = std::make_unique<mlfma_op_s>();
         h->device = cfg->device;
         h->precision = cfg->precision;
+        h->max_rhs = cfg->max_rhs < 1 ? 1 : cfg->max_rhs;
+        if (h->max_rhs > 64) return fail(MLFMA_ERR_ARG, "max_rhs must be at most 64");
         const std::string e = h->plan.build_dipoles(to_cfg(cfg), to_pw(pw), n, pos, mom);
         if (!e.empty()) return fail(MLFMA_ERR_ARG, e);
         *out = h.release();
@@ -116,6 +127,8 @@ int mlfma_create_rwg(const mlfma_config* cfg, const mlfma_planewave* pw, int nv,
         auto h = std::make_unique<mlfma_op_s>();
         h->device = cfg->device;
         h->precision = cfg->precision;
+        h->max_rhs = cfg->max_rhs < 1 ? 1 : cfg->max_rhs;
+        if (h->max_rhs > 64) return fail(MLFMA_ERR_ARG, "max_rhs must be at most 64");
         const std::string e = h->plan.build_rwg(to_cfg(cfg), to_pw(pw), nv, verts, nf, faces, ne, rwgs);
         if (!e.empty()) return fail(MLFMA_ERR_ARG, e);
         *out = h.release();
@@ -130,7 +143,7 @@ int mlfma_setup(mlfma_handle h) {
     if (h->dev) return fail(MLFMA_ERR_STATE, "already set up");
     try {
         auto dev = std::make_unique<mlfma::DeviceOp>();
-        std::string e = dev->setup(h->plan, h->device, h->precision);
+        std::string e = dev->setup(h->plan, h->device, h->precision, h->max_rhs);
         if (!e.empty()) return fail(MLFMA_ERR_CUDA, e);
         if (cudaMalloc(&h->d_x, sizeof(double2) * h->plan.n) != cudaSuccess ||
             cudaMalloc(&h->d_y, sizeof(double2) * h->plan.n) != cudaSuccess)
@@ -296,6 +309,113 @@ int mlfma_gmres_noalloc(mlfma_handle h, const void* d_b, void* d_x, const mlfma_
         info->refinements = r.refinements;
     }
     if (!r.converged) return fail(MLFMA_ERR_NOT_CONVERGED, "iteration limit reached");
+    return MLFMA_OK;
+}
+
+int mlfma_rhs_planewave(mlfma_handle h, const mlfma_planewave* pw, double* b) {
+    if (!h || !pw || !b) return fail(MLFMA_ERR_ARG, "null argument");
+    if (pw->wavenum != h->plan.pw.wavenum) return fail(MLFMA_ERR_ARG, "wavenumber differs from the operator's");
+    h->plan.rhs_for(to_pw(pw), reinterpret_cast<mlfma::cplx*>(b));
+    return MLFMA_OK;
+}
+
+int mlfma_matvec_multi_device(mlfma_handle h, int nrhs, const void* d_x, void* d_y, int accumulate, void* stream) {
+    if (!h || !d_x || !d_y) return fail(MLFMA_ERR_ARG, "null argument");
+    if (!ready(h)) return fail(MLFMA_ERR_STATE, "mlfma_setup has not run");
+    std::string e = h->dev->matvec_multi_device(static_cast<const double2*>(d_x), static_cast<double2*>(d_y), nrhs,
+                                                accumulate != 0, static_cast<cudaStream_t>(stream));
+    if (!e.empty()) return from_msg(e);
+    return MLFMA_OK;
+}
+
+static int ensure_multi_staging(mlfma_handle h) {
+    if (h->d_xm) return MLFMA_OK;
+    const size_t bytes = sizeof(double2) * static_cast<size_t>(h->plan.n) * h->max_rhs;
+    if (cudaMalloc(&h->d_xm, bytes) != cudaSuccess || cudaMalloc(&h->d_ym, bytes) != cudaSuccess)
+        return fail(MLFMA_ERR_CUDA, "cudaMalloc failed");
+    return MLFMA_OK;
+}
+
+int mlfma_matvec_multi(mlfma_handle h, int nrhs, const double* x, double* y, int accumulate) {
+    if (!h || !x || !y) return fail(MLFMA_ERR_ARG, "null argument");
+    if (!ready(h)) return fail(MLFMA_ERR_STATE, "mlfma_setup has not run");
+    if (nrhs < 1 || nrhs > h->max_rhs) return fail(MLFMA_ERR_ARG, "nrhs must be between 1 and max_rhs");
+    if (cudaSetDevice(h->device) != cudaSuccess) return fail(MLFMA_ERR_CUDA, "cudaSetDevice failed");
+    int code = ensure_multi_staging(h);
+    if (code != MLFMA_OK) return code;
+    const size_t bytes = sizeof(double2) * static_cast<size_t>(h->plan.n) * nrhs;
+    cudaStream_t s = h->dev->stream();
+    if (cudaMemcpyAsync(h->d_xm, x, bytes, cudaMemcpyHostToDevice, s) != cudaSuccess)
+        return fail(MLFMA_ERR_CUDA, "copy of x failed");
+    if (accumulate && cudaMemcpyAsync(h->d_ym, y, bytes, cudaMemcpyHostToDevice, s) != cudaSuccess)
+        return fail(MLFMA_ERR_CUDA, "copy of y failed");
+    std::string e = h->dev->matvec_multi_device(h->d_xm, h->d_ym, nrhs, accumulate != 0, s);
+    if (!e.empty()) return from_msg(e);
+    if (cudaMemcpyAsync(y, h->d_ym, bytes, cudaMemcpyDeviceToHost, s) != cudaSuccess)
+        return fail(MLFMA_ERR_CUDA, "copy of y failed");
+    const cudaError_t ce = cudaStreamSynchronize(s);
+    if (ce != cudaSuccess) return fail(MLFMA_ERR_CUDA, cudaGetErrorString(ce));
+    return MLFMA_OK;
+}
+
+int mlfma_gmres_multi(mlfma_handle h, int nrhs, const double* b, double* x, const mlfma_solver_opts* opts,
+                      mlfma_solve_info* info) {
+    if (!h || !b || !x) return fail(MLFMA_ERR_ARG, "null argument");
+    if (!ready(h)) return fail(MLFMA_ERR_STATE, "mlfma_setup has not run");
+    if (nrhs < 1 || nrhs > h->max_rhs) return fail(MLFMA_ERR_ARG, "nrhs must be between 1 and max_rhs");
+    mlfma::SolveOpts o;
+    if (opts) {
+        o.max_iter = opts->max_iter;
+        o.tol = opts->tol;
+        o.restart = opts->restart;
+        o.ref_givens = opts->ref_givens;
+        o.refine = opts->refine;
+        o.inner_tol = opts->inner_tol;
+    }
+    if (cudaSetDevice(h->device) != cudaSuccess) return fail(MLFMA_ERR_CUDA, "cudaSetDevice failed");
+    int code = ensure_multi_staging(h);
+    if (code != MLFMA_OK) return code;
+    if (!h->gmres_multi) h->gmres_multi = std::make_unique<mlfma::GmresMulti>();
+    const size_t bytes = sizeof(double2) * static_cast<size_t>(h->plan.n) * nrhs;
+    cudaStream_t s = h->dev->stream();
+    if (cudaMemcpyAsync(h->d_xm, b, bytes, cudaMemcpyHostToDevice, s) != cudaSuccess)
+        return fail(MLFMA_ERR_CUDA, "copy of b failed");
+    std::vector<mlfma::SolveResult> r;
+    std::string e = h->gmres_multi->solve(*h->dev, nrhs, h->d_xm, h->d_ym, o, r);
+    if (!e.empty()) return from_msg(e);
+    if (cudaMemcpyAsync(x, h->d_ym, bytes, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+        return fail(MLFMA_ERR_CUDA, "copy of x failed");
+    bool all = true;
+    for (int i = 0; i < nrhs; ++i) {
+        if (info) {
+            info[i].iterations = r[i].iterations;
+            info[i].residual = r[i].residual;
+            info[i].true_residual = r[i].true_residual;
+            info[i].seconds = r[i].seconds;
+            info[i].refinements = r[i].refinements;
+        }
+        all = all && r[i].converged;
+    }
+    if (!all) return fail(MLFMA_ERR_NOT_CONVERGED, "iteration limit reached for some right-hand side");
+    return MLFMA_OK;
+}
+
+int mlfma_time_stages_multi(mlfma_handle h, int nrhs, mlfma_stage_times* t) {
+    if (!h || !t) return fail(MLFMA_ERR_ARG, "null argument");
+    if (!ready(h)) return fail(MLFMA_ERR_STATE, "mlfma_setup has not run");
+    mlfma::StageTimes st{};
+    std::string e = h->dev->time_stages_multi(nrhs, &st);
+    if (!e.empty()) return from_msg(e);
+    t->gather = st.gather;
+    t->s2m = st.s2m;
+    t->m2m = st.m2m;
+    t->m2l = st.m2l;
+    t->l2l = st.l2l;
+    t->l2t = st.l2t;
+    t->near_field = st.near;
+    t->finish = st.finish;
+    t->total = st.total;
     return MLFMA_OK;
 }
 

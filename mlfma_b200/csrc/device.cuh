@@ -33,6 +33,8 @@ struct DevLevelT {
     int nth, nph, ndir, nbox;
     C* A;                        // outgoing patterns [nbox][ndir][2]
     C* B;                        // local (incoming) patterns [nbox][ndir][2]
+    C* Am;                       // many right-hand sides: [nbox][ndir][2][max_rhs]
+    C* Bm;
     const C* transl;             // [316][ndir]
     const R* w;                  // [ndir] quadrature weight applied after M2L
     const C* shift_up;           // [8][ndir]
@@ -67,6 +69,20 @@ struct DevTransT {
 struct DevFarLeaf {
     int level, box, src0, nsrc;
     long long pat_off;
+};
+
+// M2L on many right-hand sides: the boxes of one level that share a parent
+// (at most 8) and the union of their list-2 sources; for each candidate source
+// the offset id towards every target (-1: not in that target's list 2).
+constexpr int kMaxGroup = 8;
+constexpr int kMaxRhs = 64;  // right-hand sides of one product
+
+struct DevM2LGroup {
+    int level, ntgt;
+    int tgt[kMaxGroup];       // target boxes (this level)
+    int empty_mask;           // bit t: target t has an empty list 2
+    int cand0, ncand;         // candidate range
+    long long t8_off;         // this group's transfer values: [ndir][ncand][kMaxGroup]
 };
 
 struct DevNearRow {
@@ -109,6 +125,7 @@ struct FarField {
     DevLevelT<R>* lv_dev = nullptr;
     std::vector<DevTransT<R>> trans;  // index = parent level
     C* pat = nullptr;                 // radiation patterns [pat_elems][2]
+    C* m2l_t8 = nullptr;              // many-rhs M2L: pre-gathered weighted transfer values
 };
 
 class DeviceOp {
@@ -119,7 +136,9 @@ public:
     DeviceOp& operator=(const DeviceOp&) = delete;
 
     // Uploads the plan and assembles radiation patterns and near-field blocks.
-    std::string setup(const Plan& plan, int device, int precision);
+    // max_rhs > 1 also allocates the work space of products on up to max_rhs
+    // right-hand sides at once.
+    std::string setup(const Plan& plan, int device, int precision, int max_rhs = 1);
 
     // y (user order) = (accumulate ? y : 0) + A x, device pointers, on `stream`
     // (0 = the operator's own stream).  Interleaved complex FP64.
@@ -132,8 +151,18 @@ public:
     // Same, never capturing a graph (launches the captured one if it exists).
     void apply_tree_direct(const double2* xt, double2* yt, cudaStream_t s, int prec = -1);
 
+    // Products on nr right-hand sides at once (1 <= nr <= max_rhs).  x and y are
+    // nr vectors one after another in the caller's order ([nr][n]).
+    std::string matvec_multi_device(const double2* x, double2* y, int nr, bool accumulate, cudaStream_t stream,
+                                    int prec = -1);
+    // Tree order, right-hand side innermost ([n][nr]), for the solver.
+    void apply_tree_multi(const double2* xt, double2* yt, int nr, cudaStream_t s, int prec = -1);
+    int max_rhs() const { return max_rhs_; }
+
     // Per-stage CUDA-event timing of one matvec on the operator's stream.
     std::string time_stages(StageTimes* out);
+    // Same for a product on nr right-hand sides.
+    std::string time_stages_multi(int nr, StageTimes* out);
 
     // Far field of currents (caller order, device) along ndir unit directions
     // (device, ndir x 3); out: ndir x 3 complex (device).
@@ -163,6 +192,11 @@ private:
     void run_far(const double2* xt, cudaStream_t s, int stage = -1, int prec = -1);
     void run_near(const double2* xt, cudaStream_t s);
     void enqueue_core(cudaStream_t s, int prec);   // xt_ -> yfar_, ynear_
+    template <class R> void run_far_multi_t(FarField<R>& F, int nr, cudaStream_t s, int stage);
+    void run_far_multi(int nr, cudaStream_t s, int stage, int prec);
+    void run_near_multi(int nr, cudaStream_t s);
+    void enqueue_multi(int nr, cudaStream_t s, int prec);  // xtm_ -> yfarm_, ynearm_
+    std::string setup_multi(const Plan& plan);
     std::string ensure_graph(int prec);
     static int m2m_rows(int nth, int nph);
 
@@ -209,6 +243,22 @@ private:
     double2* yfar_ = nullptr;  // tree-ordered far result (before C k)
     double2* ynear_ = nullptr; // tree-ordered near result (before C k)
     double2* yt_ = nullptr;    // tree-ordered total (stage timing)
+    // Many right-hand sides ([n][max_rhs], tree order) and their work items.
+    int max_rhs_ = 1;
+    double2* xtm_ = nullptr;
+    double2* yfarm_ = nullptr;
+    double2* ynearm_ = nullptr;
+    double2* ytm_ = nullptr;
+    int2* s2m_items_m_ = nullptr;
+    int n_s2m_items_m_ = 0;
+    int2* l2t_items_m_ = nullptr;
+    int n_l2t_items_m_ = 0;
+    int2* near_items_m_ = nullptr;
+    int n_near_items_m_ = 0;
+    DevM2LGroup* m2l_groups_ = nullptr;
+    int* m2l_cand_src_ = nullptr;
+    int2* m2l_items_m_ = nullptr;
+    int n_m2l_items_m_ = 0;
     double2 ck_{};             // Phys::C * k
     Traffic traffic_{};
 };

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <string>
+#include <vector>
 
 #include "device.cuh"
 
@@ -71,6 +72,35 @@ private:
     double* npartial_ = nullptr;
     double2* xo_ = nullptr;   // refinement: accumulated solution
     double2* bo_ = nullptr;   // refinement: right-hand side
+};
+
+// GMRES on nr right-hand sides sharing every product (gmres_multi.cu).
+class GmresMulti {
+public:
+    GmresMulti() = default;
+    ~GmresMulti();
+    GmresMulti(const GmresMulti&) = delete;
+    GmresMulti& operator=(const GmresMulti&) = delete;
+
+    // b and x: nr device vectors one after another, caller order ([nr][n]).
+    // Unitary Givens rotations (ref_givens is ignored); restart as in Gmres;
+    // refine on a mixed operator: FP64 outer residual, mixed inner solves.
+    std::string solve(DeviceOp& op, int nr, const double2* d_b_user, double2* d_x_user, const SolveOpts& o,
+                      std::vector<SolveResult>& res);
+
+private:
+    std::string ensure(int n, int nr, int ncols);
+    void release();
+    std::string norms(const double2* v, cudaStream_t s, std::vector<double>& out);
+    void cgs_pass(int ncols, cudaStream_t s, bool add);
+    std::string cycles(DeviceOp& op, int prec, int restart, int max_iter, const std::vector<double>& bnorm,
+                       const std::vector<double>& tol_abs, std::vector<char>& done, std::vector<int>& iters,
+                       std::vector<double>& est);
+
+    int n_ = 0, nr_ = 0, cap_ = 0, nchunks_ = 0;
+    double2 *Q_ = nullptr, *w_ = nullptr, *b_ = nullptr, *x_ = nullptr, *r_ = nullptr;
+    double2 *h_ = nullptr, *y_ = nullptr, *partial_ = nullptr, *xo_ = nullptr, *bo_ = nullptr;
+    double *npartial_ = nullptr, *scale_ = nullptr;
 };
 
 }  // namespace mlfma

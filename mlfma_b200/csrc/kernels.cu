@@ -20,6 +20,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cstdio>
 #include <cstring>
 #include <stdexcept>
@@ -28,6 +29,7 @@
 
 #include "device.cuh"
 #include "kernels_far.cuh"
+#include "kernels_multi.cuh"
 #include "kernels_near.cuh"
 #include "zmath.cuh"
 
@@ -135,6 +137,13 @@ std::string DeviceOp::setup_far(const Plan& plan, FarField<R>& F, const double2*
         d.B = alloc<C>(cnt);
         MLFMA_CK(cudaMemset(d.A, 0, cnt * sizeof(C)));
         MLFMA_CK(cudaMemset(d.B, 0, cnt * sizeof(C)));
+        d.Am = d.Bm = nullptr;
+        if (max_rhs_ > 1) {
+            d.Am = alloc<C>(cnt * max_rhs_);
+            d.Bm = alloc<C>(cnt * max_rhs_);
+            MLFMA_CK(cudaMemset(d.Am, 0, cnt * max_rhs_ * sizeof(C)));
+            MLFMA_CK(cudaMemset(d.Bm, 0, cnt * max_rhs_ * sizeof(C)));
+        }
         d.transl = upload(conv_c<C>(L.transl));
         d.w = upload(conv_r<R>(L.m2l_w));
         d.shift_up = upload(conv_c<C>(L.shift_up));
@@ -206,14 +215,46 @@ std::string DeviceOp::setup_far(const Plan& plan, FarField<R>& F, const double2*
     MLFMA_CK(cudaFuncSetAttribute(k_l2l<R, 24>, attr, static_cast<int>(l2l_smem)));
     MLFMA_CK(cudaFuncSetAttribute(k_l2l<R, 32>, attr, static_cast<int>(l2l_smem)));
     MLFMA_CK(cudaFuncSetAttribute(k_s2m<R>, attr, static_cast<int>(s2m_smem)));
+    if (max_rhs_ > 1) {
+        // dynamic shared memory up to the opt-in limit less the kernel's static part
+        auto dyn = [&](const void* fn) -> cudaError_t {
+            cudaFuncAttributes fa{};
+            cudaError_t e = cudaFuncGetAttributes(&fa, fn);
+            if (e != cudaSuccess) return e;
+            return cudaFuncSetAttribute(fn, attr, dev_smem - static_cast<int>(fa.sharedSizeBytes));
+        };
+        MLFMA_CK(dyn(reinterpret_cast<const void*>(k_m2m_m<R, 2>)));
+        MLFMA_CK(dyn(reinterpret_cast<const void*>(k_m2m_m<R, 4>)));
+        MLFMA_CK(dyn(reinterpret_cast<const void*>(k_m2m_m<R, 6>)));
+        MLFMA_CK(dyn(reinterpret_cast<const void*>(k_m2m_m<R, 8>)));
+        MLFMA_CK(dyn(reinterpret_cast<const void*>(k_m2m_m<R, 10>)));
+        MLFMA_CK(dyn(reinterpret_cast<const void*>(k_l2l_m<R, 8>)));
+        MLFMA_CK(dyn(reinterpret_cast<const void*>(k_l2l_m<R, 12>)));
+        MLFMA_CK(dyn(reinterpret_cast<const void*>(k_l2l_m<R, 16>)));
+        MLFMA_CK(dyn(reinterpret_cast<const void*>(k_l2l_m<R, 24>)));
+        MLFMA_CK(dyn(reinterpret_cast<const void*>(k_l2l_m<R, 32>)));
+        for (int p = lmin_; p < lmax_; ++p) {
+            const size_t m2m1 = static_cast<size_t>(nph_[p + 1]) * 32 * sizeof(C);
+            const size_t l2l1 = static_cast<size_t>(nth_[p]) * 2 * 32 * sizeof(C) +
+                                static_cast<size_t>(nth_[p + 1]) * dn_w_[p] * (sizeof(R) + 2 * sizeof(int));
+            // (the static stencil staging takes at most 11 KB)
+            if (m2m1 + 11264 > static_cast<size_t>(dev_smem) || l2l1 + 1024 > static_cast<size_t>(dev_smem) ||
+                nph_[p] > kM2MOut * kInterpWarps)
+                return "angular grid too large for the many-right-hand-side interpolation kernels";
+        }
+    }
     return {};
 }
 
-std::string DeviceOp::setup(const Plan& plan, int device, int precision) {
+
+
+std::string DeviceOp::setup(const Plan& plan, int device, int precision, int max_rhs) {
     try {
         device_ = device;
         precision_ = precision;
         if (precision != kFp64 && precision != kMixed) return "precision must be 0 (FP64) or 1 (mixed)";
+        if (max_rhs < 1 || max_rhs > kMaxRhs) return "max_rhs must be 1..64";
+        max_rhs_ = max_rhs;
         MLFMA_CK(cudaSetDevice(device));
         MLFMA_CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
         MLFMA_CK(cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking));
@@ -391,6 +432,10 @@ std::string DeviceOp::setup(const Plan& plan, int device, int precision) {
         }
         traffic_.near = near_entries_ * 16.0 + n_ * 16.0 * 2.0;
         traffic_.total = traffic_.s2m + traffic_.m2m + traffic_.m2l + traffic_.l2l + traffic_.l2t + traffic_.near;
+        if (max_rhs_ > 1) {
+            err = setup_multi(plan);
+            if (!err.empty()) return err;
+        }
         MLFMA_CK(cudaStreamSynchronize(stream_));
         MLFMA_CK(cudaGetLastError());
         ready_ = true;
@@ -591,6 +636,231 @@ std::string DeviceOp::copy_level(int level, int which, double2* host, long long 
         MLFMA_CK(cudaMemcpyAsync(host + o, tmp, m * sizeof(double2), cudaMemcpyDeviceToHost, stream_));
         MLFMA_CK(cudaStreamSynchronize(stream_));
     }
+    return {};
+}
+
+// ================================================================= many right-hand sides
+
+// Work items of the many-rhs kernels and the M2L sibling groups.
+std::string DeviceOp::setup_multi(const Plan& plan) {
+    const size_t nm = static_cast<size_t>(n_) * max_rhs_;
+    xtm_ = alloc<double2>(nm);
+    yfarm_ = alloc<double2>(nm);
+    ynearm_ = alloc<double2>(nm);
+    ytm_ = alloc<double2>(nm);
+    MLFMA_CK(cudaMemset(xtm_, 0, nm * sizeof(double2)));
+    MLFMA_CK(cudaMemset(yfarm_, 0, nm * sizeof(double2)));
+    MLFMA_CK(cudaMemset(ynearm_, 0, nm * sizeof(double2)));
+    // S2M and L2T: tiles of kBM pattern rows / sources per leaf.
+    std::vector<int2> s2m, l2t;
+    for (size_t i = 0; i < plan.far_leaves.size(); ++i) {
+        const FarLeaf& f = plan.far_leaves[i];
+        const int ne = 2 * plan.levels[f.level].ndir;
+        for (int e0 = 0; e0 < ne; e0 += kBM) s2m.push_back(make_int2(static_cast<int>(i), e0));
+        for (int s0 = 0; s0 < f.nsrc; s0 += kBM) l2t.push_back(make_int2(static_cast<int>(i), s0));
+    }
+    n_s2m_items_m_ = static_cast<int>(s2m.size());
+    s2m_items_m_ = upload(s2m);
+    n_l2t_items_m_ = static_cast<int>(l2t.size());
+    l2t_items_m_ = upload(l2t);
+    // Near field: tiles of kBM rows per block row.
+    std::vector<int2> nit;
+    for (size_t i = 0; i < plan.near_rows.size(); ++i)
+        for (int r0 = 0; r0 < plan.near_rows[i].nrow; r0 += kBM) nit.push_back(make_int2(static_cast<int>(i), r0));
+    n_near_items_m_ = static_cast<int>(nit.size());
+    near_items_m_ = upload(nit);
+    // M2L sibling groups: boxes of a level grouped by parent node.
+    std::vector<DevM2LGroup> groups;
+    std::vector<int> cand_src;
+    std::vector<cplx> t8;  // [group][direction][candidate][kMaxGroup], weights folded in
+    std::vector<int2> items;
+    for (int l = lmin_; l <= lmax_; ++l) {
+        const Level& L = plan.levels[l];
+        std::vector<int> order(L.boxes.size());
+        for (size_t b = 0; b < order.size(); ++b) order[b] = static_cast<int>(b);
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+            return plan.nodes[L.boxes[a]].parent < plan.nodes[L.boxes[b]].parent;
+        });
+        for (size_t i = 0; i < order.size();) {
+            const int par = plan.nodes[L.boxes[order[i]]].parent;
+            size_t j = i;
+            while (j < order.size() && plan.nodes[L.boxes[order[j]]].parent == par) ++j;
+            if (j - i > static_cast<size_t>(kMaxGroup)) return "internal: sibling group larger than 8";
+            DevM2LGroup g{};
+            g.level = l;
+            g.ntgt = static_cast<int>(j - i);
+            g.cand0 = static_cast<int>(cand_src.size());
+            std::vector<int> cands;
+            std::vector<std::array<short, kMaxGroup>> offs;
+            for (int t = 0; t < g.ntgt; ++t) {
+                const int b = order[i + t];
+                g.tgt[t] = b;
+                if (L.m2l_ptr[b + 1] == L.m2l_ptr[b]) g.empty_mask |= 1 << t;
+                for (int q = L.m2l_ptr[b]; q < L.m2l_ptr[b + 1]; ++q) {
+                    const int src = L.m2l_src[q];
+                    size_t c = 0;
+                    while (c < cands.size() && cands[c] != src) ++c;
+                    if (c == cands.size()) {
+                        cands.push_back(src);
+                        std::array<short, kMaxGroup> o;
+                        o.fill(-1);
+                        offs.push_back(o);
+                    }
+                    offs[c][t] = static_cast<short>(L.m2l_off[q]);
+                }
+            }
+            g.ncand = static_cast<int>(cands.size());
+            for (size_t c = 0; c < cands.size(); ++c) cand_src.push_back(cands[c]);
+            g.t8_off = static_cast<long long>(t8.size());
+            t8.resize(t8.size() + static_cast<size_t>(L.ndir) * g.ncand * kMaxGroup, cplx(0));
+            for (int d = 0; d < L.ndir; ++d)
+                for (int c = 0; c < g.ncand; ++c)
+                    for (int t = 0; t < kMaxGroup; ++t) {
+                        const int o = offs[c][t];
+                        if (o >= 0)
+                            t8[g.t8_off + (static_cast<size_t>(d) * g.ncand + c) * kMaxGroup + t] =
+                                L.transl[static_cast<size_t>(o) * L.ndir + d] * L.m2l_w[d];
+                    }
+            const bool all_empty = g.empty_mask == (1 << g.ntgt) - 1;
+            if (!(all_empty && ref_compat_)) {
+                const int gi = static_cast<int>(groups.size());
+                for (int d = 0; d < L.ndir; ++d) items.push_back(make_int2(gi, d));
+                groups.push_back(g);
+            }
+            i = j;
+        }
+    }
+    m2l_groups_ = upload(groups);
+    m2l_cand_src_ = upload(cand_src);
+    f64_.m2l_t8 = upload(conv_c<double2>(t8));
+    if (precision_ != kFp64) f32_.m2l_t8 = upload(conv_c<float2>(t8));
+    n_m2l_items_m_ = static_cast<int>(items.size());
+    m2l_items_m_ = upload(items);
+    return {};
+}
+
+// stage: -1 all, 0 S2M, 1 M2M, 2 M2L, 3 L2L, 4 L2T.
+template <class R>
+void DeviceOp::run_far_multi_t(FarField<R>& F, int nr, cudaStream_t s, int stage) {
+    using C = typename Cx<R>::T;
+    if (n_leaves_ == 0) return;
+    if ((stage < 0 || stage == 0) && n_s2m_items_m_)
+        k_s2m_m<R><<<n_s2m_items_m_, kGemmThreads, 0, s>>>(F.lv_dev, s2m_items_m_, leaves_, F.pat, xtm_, nr);
+    if (stage < 0 || stage == 1)
+        for (int p = lmax_ - 1; p >= lmin_; --p) {
+            if (npar_[p] == 0) continue;
+            const dim3 grid(npar_[p], nth_[p], (nr + kRc - 1) / kRc);
+            const size_t smem = static_cast<size_t>(nph_[p + 1]) * 32 * sizeof(C);
+            const DevTransT<R>& T = F.trans[p];
+            switch (up_w_[p]) {
+                case 2: k_m2m_m<R, 2><<<grid, kInterpThreads, smem, s>>>(F.lv_dev, T, nr); break;
+                case 4: k_m2m_m<R, 4><<<grid, kInterpThreads, smem, s>>>(F.lv_dev, T, nr); break;
+                case 6: k_m2m_m<R, 6><<<grid, kInterpThreads, smem, s>>>(F.lv_dev, T, nr); break;
+                case 8: k_m2m_m<R, 8><<<grid, kInterpThreads, smem, s>>>(F.lv_dev, T, nr); break;
+                default: k_m2m_m<R, 10><<<grid, kInterpThreads, smem, s>>>(F.lv_dev, T, nr); break;
+            }
+        }
+    if ((stage < 0 || stage == 2) && n_m2l_items_m_) {
+        const int threads = std::min(kM2LmThreads, ((2 * nr + 31) / 32) * 32);
+        k_m2l_m<R><<<n_m2l_items_m_, threads, 0, s>>>(F.lv_dev, m2l_items_m_, m2l_groups_, m2l_cand_src_,
+                                                      F.m2l_t8, nr, ref_compat_ ? 0 : 1);
+    }
+    if (stage < 0 || stage == 3)
+        for (int p = lmin_; p < lmax_; ++p) {
+            const int g = n_l2l_pairs_[p];
+            if (!g) continue;
+            const dim3 grid(g, nph_[p + 1] / 2, (nr + kRc - 1) / kRc);
+            const size_t smem = static_cast<size_t>(nth_[p]) * 2 * 32 * sizeof(C) +
+                                static_cast<size_t>(nth_[p + 1]) * dn_w_[p] * (sizeof(R) + 2 * sizeof(int));
+            const DevTransT<R>& T = F.trans[p];
+            switch (dn_w_[p]) {
+                case 8: k_l2l_m<R, 8><<<grid, kInterpThreads, smem, s>>>(F.lv_dev, T, l2l_pairs_[p], nr); break;
+                case 12: k_l2l_m<R, 12><<<grid, kInterpThreads, smem, s>>>(F.lv_dev, T, l2l_pairs_[p], nr); break;
+                case 16: k_l2l_m<R, 16><<<grid, kInterpThreads, smem, s>>>(F.lv_dev, T, l2l_pairs_[p], nr); break;
+                case 24: k_l2l_m<R, 24><<<grid, kInterpThreads, smem, s>>>(F.lv_dev, T, l2l_pairs_[p], nr); break;
+                default: k_l2l_m<R, 32><<<grid, kInterpThreads, smem, s>>>(F.lv_dev, T, l2l_pairs_[p], nr); break;
+            }
+        }
+    if ((stage < 0 || stage == 4) && n_l2t_items_m_)
+        k_l2t_m<R><<<n_l2t_items_m_, kGemmThreads, 0, s>>>(F.lv_dev, l2t_items_m_, leaves_, F.pat, yfarm_, nr);
+}
+
+void DeviceOp::run_far_multi(int nr, cudaStream_t s, int stage, int prec) {
+    if (prec < 0) prec = precision_;
+    if (prec == kFp64) run_far_multi_t(f64_, nr, s, stage); else run_far_multi_t(f32_, nr, s, stage);
+}
+
+void DeviceOp::run_near_multi(int nr, cudaStream_t s) {
+    if (n_near_items_m_ == 0) return;
+    k_near_m<<<n_near_items_m_, kGemmThreads, 0, s>>>(near_rows_, near_items_m_, near_z_, near_cols_, xtm_, ynearm_,
+                                                       nr);
+}
+
+// xtm_ -> (yfarm_, ynearm_): near field on the side stream, far field on s.
+void DeviceOp::enqueue_multi(int nr, cudaStream_t s, int prec) {
+    const size_t bytes = sizeof(double2) * static_cast<size_t>(n_) * nr;
+    cudaMemsetAsync(yfarm_, 0, bytes, s);
+    cudaMemsetAsync(ynearm_, 0, bytes, s);
+    cudaEventRecord(ev_fork_, s);
+    cudaStreamWaitEvent(side_, ev_fork_, 0);
+    run_near_multi(nr, side_);
+    cudaEventRecord(ev_join_, side_);
+    run_far_multi(nr, s, -1, prec);
+    cudaStreamWaitEvent(s, ev_join_, 0);
+}
+
+std::string DeviceOp::matvec_multi_device(const double2* x, double2* y, int nr, bool accumulate, cudaStream_t stream,
+                                          int prec) {
+    if (!ready_) return "operator not set up";
+    if (nr < 1 || nr > max_rhs_) return "arg:nrhs must be between 1 and the operator's max_rhs";
+    if (prec < 0) prec = precision_;
+    if (prec != kFp64 && precision_ == kFp64) return "the FP64 operator has no mixed far field";
+    cudaStream_t s = stream ? stream : stream_;
+    MLFMA_CK(cudaSetDevice(device_));
+    const long long tot = static_cast<long long>(n_) * nr;
+    k_gather_m<<<blocks_for(tot, 256), 256, 0, s>>>(x, perm_, xtm_, n_, nr);
+    enqueue_multi(nr, s, prec);
+    k_finish_m<<<blocks_for(tot, 256), 256, 0, s>>>(yfarm_, ynearm_, perm_, y, n_, nr, ck_, accumulate ? 1 : 0);
+    MLFMA_CK(cudaGetLastError());
+    return {};
+}
+
+void DeviceOp::apply_tree_multi(const double2* xt, double2* yt, int nr, cudaStream_t s, int prec) {
+    if (prec < 0) prec = precision_;
+    const long long tot = static_cast<long long>(n_) * nr;
+    if (xt != xtm_) cudaMemcpyAsync(xtm_, xt, sizeof(double2) * tot, cudaMemcpyDeviceToDevice, s);
+    enqueue_multi(nr, s, prec);
+    k_finish_m<<<blocks_for(tot, 256), 256, 0, s>>>(yfarm_, ynearm_, nullptr, yt, n_, nr, ck_, 0);
+}
+
+std::string DeviceOp::time_stages_multi(int nr, StageTimes* out) {
+    if (!ready_) return "operator not set up";
+    if (nr < 1 || nr > max_rhs_) return "arg:nrhs must be between 1 and the operator's max_rhs";
+    MLFMA_CK(cudaSetDevice(device_));
+    cudaEvent_t ev[9];
+    for (auto& e : ev) MLFMA_CK(cudaEventCreate(&e));
+    cudaStream_t s = stream_;
+    const size_t bytes = sizeof(double2) * static_cast<size_t>(n_) * nr;
+    cudaEventRecord(ev[0], s);
+    cudaMemsetAsync(yfarm_, 0, bytes, s);
+    cudaMemsetAsync(ynearm_, 0, bytes, s);
+    cudaEventRecord(ev[1], s);
+    for (int st = 0; st < 5; ++st) {
+        run_far_multi(nr, s, st, precision_);
+        cudaEventRecord(ev[2 + st], s);
+    }
+    run_near_multi(nr, s);
+    cudaEventRecord(ev[7], s);
+    const long long tot = static_cast<long long>(n_) * nr;
+    k_finish_m<<<blocks_for(tot, 256), 256, 0, s>>>(yfarm_, ynearm_, nullptr, ytm_, n_, nr, ck_, 0);
+    cudaEventRecord(ev[8], s);
+    MLFMA_CK(cudaEventSynchronize(ev[8]));
+    float t[8];
+    for (int i = 0; i < 8; ++i) cudaEventElapsedTime(&t[i], ev[i], ev[i + 1]);
+    *out = StageTimes{t[0], t[1], t[2], t[3], t[4], t[5], t[6], t[7], 0.f};
+    cudaEventElapsedTime(&out->total, ev[0], ev[8]);
+    for (auto& e : ev) cudaEventDestroy(e);
+    MLFMA_CK(cudaGetLastError());
     return {};
 }
 

@@ -402,7 +402,9 @@ std::string Plan::build_rwg(const Config& c, const PlaneWave& p, int nv, const d
     return {};
 }
 
-void Plan::rhs(cplx* b) const {
+void Plan::rhs(cplx* b) const { rhs_for(pw, b); }
+
+void Plan::rhs_for(const PlaneWave& pw, cplx* b) const {
     const cplx iu(0, 1);
     const double* kin = pw.khat;
     double kvec[3] = {pw.wavenum * kin[0], pw.wavenum * kin[1], pw.wavenum * kin[2]};

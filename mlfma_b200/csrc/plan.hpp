@@ -157,6 +157,8 @@ struct Plan {
 
     // b = -V in original source order (Solver ctor, src/solver.cpp:31-32).
     void rhs(cplx* b) const;
+    // Same for another incident plane wave of the same wavenumber.
+    void rhs_for(const PlaneWave& p, cplx* b) const;
 
     // RWG radiation patterns evaluated on the host exactly as the reference
     // rounds them (layout of the device pattern array).

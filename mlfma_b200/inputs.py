@@ -162,3 +162,20 @@ def read_planewave(path: str) -> PlaneWave:
         raise RuntimeError("Unable to parse line")
     v = [float(x) for x in vals]
     return PlaneWave(amplitude=v[0], pol=tuple(v[1:4]), khat=tuple(v[4:7]), wavenum=v[7])
+
+
+def fibonacci_planewaves(n: int, wavenum: float = 2.0 * np.pi, amplitude: float = 1.0) -> list[PlaneWave]:
+    """n incident plane waves with directions on a Fibonacci sphere, each
+    polarised along theta-hat of its direction (the many-right-hand-side
+    benchmark excitation)."""
+    golden = np.pi * (3.0 - np.sqrt(5.0))
+    out = []
+    for i in range(n):
+        z = 1.0 - 2.0 * (i + 0.5) / n
+        rho = np.sqrt(max(0.0, 1.0 - z * z))
+        phi = golden * i
+        k = np.array([rho * np.cos(phi), rho * np.sin(phi), z])
+        th = np.arccos(np.clip(z, -1.0, 1.0))
+        pol = np.array([np.cos(th) * np.cos(phi), np.cos(th) * np.sin(phi), -np.sin(th)])
+        out.append(PlaneWave(amplitude=amplitude, pol=tuple(pol), khat=tuple(k), wavenum=wavenum))
+    return out

@@ -1,0 +1,110 @@
+"""Products and solves on many right-hand sides at once (mlfma_matvec_multi,
+mlfma_gmres_multi) against the one-vector path, column by column.
+
+The batched kernels sum in a different order (GEMM tiles, sibling-group M2L),
+so FP64 columns agree to rounding (1e-12 relative); mixed columns to float
+rounding (1e-5)."""
+import numpy as np
+import pytest
+
+from mlfma_b200 import MLFMA, MlfmaError, inputs
+from mlfma_b200 import _lib
+
+pytestmark = pytest.mark.gpu
+PW = inputs.PlaneWave()
+
+
+def rel(a, b):
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+def cmat(nr, n, seed):
+    r = np.random.default_rng(seed)
+    return r.standard_normal((nr, n)) + 1j * r.standard_normal((nr, n))
+
+
+def make(kind, **kw):
+    if kind == "dipole":
+        return MLFMA.dipoles(inputs.make_dipoles(3000, seed=31), PW, max_node_srcs=16, **kw).setup()
+    return MLFMA.rwg(inputs.make_icosphere(4, radius=1.5), PW, max_node_srcs=24, **kw).setup()
+
+
+@pytest.mark.parametrize("kind", ["dipole", "rwg"])
+@pytest.mark.parametrize("nr", [1, 5, 64])
+def test_matvec_multi_matches_single(cuda_device, kind, nr):
+    op = make(kind, ref_compat=0, max_rhs=64)
+    X = cmat(nr, op.n, 7)
+    Y = op.matvec_multi(X)
+    for r in range(nr):
+        assert rel(Y[r], op.matvec(X[r])) <= 1e-12
+    # accumulate: Y += A X
+    Y2 = op.matvec_multi(X, accumulate=True, out=Y.copy())
+    assert rel(Y2, 2 * Y) <= 1e-14
+    op.close()
+
+
+def test_matvec_multi_reference_state_matches_single(cuda_device):
+    # ref_compat = 1: boxes with an empty list 2 keep their local patterns from
+    # the previous product; the batched path keeps its own copy of that state
+    # and must follow the same sequence.
+    single = make("rwg", max_rhs=1)
+    multi = make("rwg", max_rhs=8)
+    X = cmat(2, single.n, 9)
+    for r in range(2):
+        assert rel(multi.matvec_multi(X[r:r + 1])[0], single.matvec(X[r])) <= 1e-12
+    single.close()
+    multi.close()
+
+
+@pytest.mark.parametrize("kind", ["dipole", "rwg"])
+def test_matvec_multi_mixed(cuda_device, kind):
+    op = make(kind, ref_compat=0, max_rhs=16, precision=1)
+    X = cmat(16, op.n, 3)
+    Y = op.matvec_multi(X)
+    for r in (0, 7, 15):
+        assert rel(Y[r], op.matvec(X[r])) <= 1e-5
+    op.close()
+
+
+def test_matvec_multi_rejects_too_many(cuda_device):
+    op = make("dipole", max_rhs=4)
+    with pytest.raises(MlfmaError) as e:
+        op.matvec_multi(cmat(5, op.n, 1))
+    assert e.value.code == _lib.MLFMA_ERR_ARG
+    op.close()
+
+
+def test_gmres_multi_matches_single(cuda_device):
+    m = inputs.make_icosphere(3, radius=1.0)
+    op = MLFMA.rwg(m, PW, max_node_srcs=16, ref_compat=0, self_terms=1, max_rhs=8).setup()
+    B = np.stack([op.rhs_planewave(p) for p in inputs.fibonacci_planewaves(8)])
+    tol = 1e-6
+    X, infos = op.solve_multi(B, max_iter=400, tol=tol, restart=40)
+    for r in range(8):
+        assert infos[r].converged
+        assert rel(op.matvec(X[r]), B[r]) <= tol * 1.0001
+        x1, i1 = op.solve(B[r], max_iter=400, tol=tol, restart=40, ref_givens=False)
+        assert i1.converged
+        assert abs(infos[r].iterations - i1.iterations) <= 2
+        assert rel(X[r], x1) <= 1e-4
+    op.close()
+
+
+def test_gmres_multi_refined_mixed(cuda_device):
+    m = inputs.make_icosphere(3, radius=1.0)
+    op64 = MLFMA.rwg(m, PW, max_node_srcs=16, ref_compat=0, self_terms=1).setup()
+    opmx = MLFMA.rwg(m, PW, max_node_srcs=16, ref_compat=0, self_terms=1, max_rhs=6, precision=1).setup()
+    B = np.stack([opmx.rhs_planewave(p) for p in inputs.fibonacci_planewaves(6)])
+    tol = 1e-4
+    X, infos = opmx.solve_multi(B, max_iter=400, tol=tol, restart=50, refine=True)
+    for r in range(6):
+        assert infos[r].converged and infos[r].refinements >= 1
+        assert rel(op64.matvec(X[r]), B[r]) <= tol * 1.0001
+    op64.close()
+    opmx.close()
+
+
+def test_rhs_planewave_matches_handle_rhs(cuda_device):
+    op = make("rwg", max_rhs=1)
+    assert np.array_equal(op.rhs_planewave(PW), op.rhs())
+    op.close()
