@@ -40,6 +40,7 @@ WORKLOAD = dict(name="rwg_sphere_r2lambda_ico5", kind="rwg", level=5, radius=2.0
                 max_node_srcs=54, quad_prec=2, digits=3, interp_order=3, over_interp=2.0)
 HERE = os.path.dirname(os.path.abspath(__file__))
 SOLVE = dict(restart=50, tol=1e-4, max_iter=3000)
+NRHS = 64
 
 
 def make_problem():
@@ -244,6 +245,76 @@ def measure(torch, dev, rank, world, args, precision: int, clocks=None) -> dict:
                 clocks=clk, solve=solve)
 
 
+def measure_batched(torch, dev, args, precision: int) -> dict:
+    """Products and the GMRES solve on NRHS incident plane waves at once
+    (Fibonacci-sphere directions, theta polarisation) on the EFIE with self
+    terms: device-resident matvecs/s over all right-hand sides, per-stage times,
+    and the batched solve to the same 1e-4 FP64 residual."""
+    from mlfma_b200 import MLFMA, default_config, inputs
+    mesh, pw = make_problem()
+    cfg = default_config(quad_prec=WORKLOAD["quad_prec"], digits=WORKLOAD["digits"],
+                         interp_order=WORKLOAD["interp_order"], over_interp=WORKLOAD["over_interp"],
+                         root_leng=WORKLOAD["root_leng"], max_node_srcs=WORKLOAD["max_node_srcs"],
+                         device=dev.index, precision=precision, self_terms=1, ref_compat=0, max_rhs=NRHS)
+    op = MLFMA.rwg(mesh, pw, config=cfg).setup()
+    n = op.n
+    pws = inputs.fibonacci_planewaves(NRHS, wavenum=pw.wavenum)
+    B = np.stack([op.rhs_planewave(p) for p in pws])
+    X = torch.from_numpy(B).to(dev)
+    Y = torch.zeros_like(X)
+    stream = torch.cuda.ExternalStream(op.stream(), device=dev)
+    for _ in range(args.warmup):
+        op.matvec_multi_device(NRHS, X.data_ptr(), Y.data_ptr(), False, stream.cuda_stream)
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    steps = max(3, args.steps // 10)
+    e0.record(stream)
+    for _ in range(steps):
+        op.matvec_multi_device(NRHS, X.data_ptr(), Y.data_ptr(), False, stream.cuda_stream)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1) / steps
+    st = op.stage_times_multi(NRHS)
+    out = {"nrhs": NRHS, "ms_per_product": ms, "matvecs_per_s": NRHS * 1000.0 / ms,
+           "us_per_rhs": ms * 1000.0 / NRHS, "stage_ms": st}
+    if not args.no_solve:
+        op.solve_multi(B, max_iter=3, tol=1e-12, restart=SOLVE["restart"], refine=precision == 1)  # warm-up
+        t0 = time.perf_counter()
+        Xs, infos = op.solve_multi(B, max_iter=SOLVE["max_iter"], tol=SOLVE["tol"], restart=SOLVE["restart"],
+                                   refine=precision == 1)
+        wall = time.perf_counter() - t0
+        out["solve"] = {"seconds": wall, "seconds_per_rhs": wall / NRHS,
+                        "iterations_max": max(i.iterations for i in infos),
+                        "iterations_mean": float(np.mean([i.iterations for i in infos])),
+                        "true_residual_fp64_max": max(i.true_residual for i in infos),
+                        "converged": all(i.converged for i in infos),
+                        "method": f"{NRHS} simultaneous GMRES({SOLVE['restart']}) to {SOLVE['tol']:g}, x0 = 0"}
+        out["_x0"] = Xs[0]
+        out["_far0"] = op.farfield(Xs[0], op.phi_cut(360))
+    op.close()
+    return out
+
+
+def batched_summary(bat, r64):
+    """The many-right-hand-side block of the JSON line: per precision the
+    product throughput and the solve, compared per right-hand side with the
+    one-at-a-time FP64 path (matvec and solve of the benchmark's own plane wave)."""
+    out = {"workload": f"{NRHS} plane waves, Fibonacci-sphere directions, theta polarisation, EFIE with self terms"}
+    fp64_ms = r64["ms"]
+    fp64_solve = r64["solve"]["seconds"] if r64["solve"] else None
+    for p, b in bat.items():
+        key = "fp64" if p == 0 else "mixed"
+        d = {k: v for k, v in b.items() if not k.startswith("_")}
+        d["matvec_speedup_per_rhs_vs_fp64_single"] = fp64_ms * 1000.0 / b["us_per_rhs"]
+        if "solve" in b and fp64_solve:
+            d["solve"]["speedup_per_rhs_vs_fp64_single_solve"] = fp64_solve / b["solve"]["seconds_per_rhs"]
+        out[key] = d
+    if 0 in bat and 1 in bat and "_far0" in bat[0] and "_far0" in bat[1]:
+        f64, fmx = bat[0]["_far0"], bat[1]["_far0"]
+        out["mixed"]["farfield_rel_err_vs_fp64_rhs0"] = float(np.linalg.norm(fmx - f64) / np.linalg.norm(f64))
+    return out
+
+
 def solve_summary(sv):
     return {"seconds": sv["seconds"], "iterations": sv["iterations"], "true_residual_fp64": sv["true_residual"],
             "converged": sv["converged"], "refinements": sv["refinements"],
@@ -283,6 +354,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-solve", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=3)
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
@@ -325,6 +397,9 @@ def main():
 
     r64 = measure(torch, dev, rank, world, args, precision=0, clocks=ClockSampler(local_rank))
     rmx = None if args.no_mixed else measure(torch, dev, rank, world, args, precision=1)
+    bat = None
+    if not args.no_batched:
+        bat = {p: measure_batched(torch, dev, args, p) for p in ((0, 1) if not args.no_mixed else (0,))}
 
     if rank == 0:
         cpu = None
@@ -369,6 +444,8 @@ def main():
                 line["mixed"]["solve"]["speedup_vs_fp64"] = s64["seconds"] / sm["seconds"]
                 line["mixed"]["solve"]["farfield_rel_err_vs_fp64"] = float(
                     np.linalg.norm(sm["far"] - s64["far"]) / np.linalg.norm(s64["far"]))
+        if bat is not None:
+            line["batched"] = batched_summary(bat, r64)
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()

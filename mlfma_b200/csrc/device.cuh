@@ -64,6 +64,13 @@ struct DevTransT {
     const int* child_ptr;
     const int* child_box;
     const int* child_oct;
+    // Many right-hand sides: stencil weights with the octant shift folded in,
+    //   fold_up[oct][jth][iph][k] = up_th weight (sign included) x shift_up of the
+    //                                child direction that tap reads,
+    //   fold_dn[oct][ith][jph][k] = dn_ph weight x shift_down of the parent
+    //                                direction that tap reads.
+    const typename Cx<R>::T* fold_up;
+    const typename Cx<R>::T* fold_dn;
 };
 
 struct DevFarLeaf {

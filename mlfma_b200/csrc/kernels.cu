@@ -177,6 +177,39 @@ std::string DeviceOp::setup_far(const Plan& plan, FarField<R>& F, const double2*
         d.dn_th = st(T.dn_th, dn_w_[p]);
         d.plevel = p;
         d.npar = static_cast<int>(T.par_box.size());
+        d.fold_up = d.fold_dn = nullptr;
+        if (max_rhs_ > 1) {
+            const Level& PL = plan.levels[p];
+            const Level& CL = plan.levels[p + 1];
+            const int wu = up_w_[p], wd = dn_w_[p];
+            const int mph = CL.nph, halfm = CL.nph / 2;
+            std::vector<cplx> fu(static_cast<size_t>(8) * PL.nth * mph * wu, cplx(0));
+            for (int oct = 0; oct < 8; ++oct)
+                for (int jth = 0; jth < PL.nth; ++jth)
+                    for (int q = T.up_th.ptr[jth]; q < T.up_th.ptr[jth + 1]; ++q) {
+                        const int k = q - T.up_th.ptr[jth];
+                        const double cf = T.up_th.refl[q] ? -T.up_th.coef[q] : T.up_th.coef[q];
+                        for (int iph = 0; iph < mph; ++iph) {
+                            const int sp = T.up_th.refl[q] ? (iph < halfm ? iph + halfm : iph - halfm) : iph;
+                            const int dd = T.up_th.src[q] * mph + sp;
+                            fu[((static_cast<size_t>(oct) * PL.nth + jth) * mph + iph) * wu + k] =
+                                cf * CL.shift_up[static_cast<size_t>(oct) * CL.ndir + dd];
+                        }
+                    }
+            std::vector<cplx> fd(static_cast<size_t>(8) * PL.nth * CL.nph * wd, cplx(0));
+            for (int oct = 0; oct < 8; ++oct)
+                for (int ith = 0; ith < PL.nth; ++ith)
+                    for (int jph = 0; jph < CL.nph; ++jph)
+                        for (int q = T.dn_ph.ptr[jph]; q < T.dn_ph.ptr[jph + 1]; ++q) {
+                            const int k = q - T.dn_ph.ptr[jph];
+                            const double cf = T.dn_ph.refl[q] ? -T.dn_ph.coef[q] : T.dn_ph.coef[q];
+                            const int dd = ith * PL.nph + T.dn_ph.src[q];
+                            fd[((static_cast<size_t>(oct) * PL.nth + ith) * CL.nph + jph) * wd + k] =
+                                cf * PL.shift_down[static_cast<size_t>(oct) * PL.ndir + dd];
+                        }
+            d.fold_up = upload(conv_c<C>(fu));
+            d.fold_dn = upload(conv_c<C>(fd));
+        }
         d.par_box = upload(T.par_box);
         d.par_ilist = upload(T.par_ilist);
         d.child_ptr = upload(T.child_ptr);
@@ -223,11 +256,16 @@ std::string DeviceOp::setup_far(const Plan& plan, FarField<R>& F, const double2*
             if (e != cudaSuccess) return e;
             return cudaFuncSetAttribute(fn, attr, dev_smem - static_cast<int>(fa.sharedSizeBytes));
         };
-        MLFMA_CK(dyn(reinterpret_cast<const void*>(k_m2m_m<R, 2>)));
-        MLFMA_CK(dyn(reinterpret_cast<const void*>(k_m2m_m<R, 4>)));
-        MLFMA_CK(dyn(reinterpret_cast<const void*>(k_m2m_m<R, 6>)));
-        MLFMA_CK(dyn(reinterpret_cast<const void*>(k_m2m_m<R, 8>)));
-        MLFMA_CK(dyn(reinterpret_cast<const void*>(k_m2m_m<R, 10>)));
+        MLFMA_CK(dyn(reinterpret_cast<const void*>(k_m2m_m<R, 2, 8>)));
+        MLFMA_CK(dyn(reinterpret_cast<const void*>(k_m2m_m<R, 4, 8>)));
+        MLFMA_CK(dyn(reinterpret_cast<const void*>(k_m2m_m<R, 6, 8>)));
+        MLFMA_CK(dyn(reinterpret_cast<const void*>(k_m2m_m<R, 8, 8>)));
+        MLFMA_CK(dyn(reinterpret_cast<const void*>(k_m2m_m<R, 10, 8>)));
+        MLFMA_CK(dyn(reinterpret_cast<const void*>(k_m2m_m<R, 2, kM2MOut>)));
+        MLFMA_CK(dyn(reinterpret_cast<const void*>(k_m2m_m<R, 4, kM2MOut>)));
+        MLFMA_CK(dyn(reinterpret_cast<const void*>(k_m2m_m<R, 6, kM2MOut>)));
+        MLFMA_CK(dyn(reinterpret_cast<const void*>(k_m2m_m<R, 8, kM2MOut>)));
+        MLFMA_CK(dyn(reinterpret_cast<const void*>(k_m2m_m<R, 10, kM2MOut>)));
         MLFMA_CK(dyn(reinterpret_cast<const void*>(k_l2l_m<R, 8>)));
         MLFMA_CK(dyn(reinterpret_cast<const void*>(k_l2l_m<R, 12>)));
         MLFMA_CK(dyn(reinterpret_cast<const void*>(k_l2l_m<R, 16>)));
@@ -235,7 +273,7 @@ std::string DeviceOp::setup_far(const Plan& plan, FarField<R>& F, const double2*
         MLFMA_CK(dyn(reinterpret_cast<const void*>(k_l2l_m<R, 32>)));
         for (int p = lmin_; p < lmax_; ++p) {
             const size_t m2m1 = static_cast<size_t>(nph_[p + 1]) * 32 * sizeof(C);
-            const size_t l2l1 = static_cast<size_t>(nth_[p]) * 2 * 32 * sizeof(C) +
+            const size_t l2l1 = static_cast<size_t>(nth_[p]) * 2 * l2l_pairs<R>() * 32 * sizeof(C) +
                                 static_cast<size_t>(nth_[p + 1]) * dn_w_[p] * (sizeof(R) + 2 * sizeof(int));
             // (the static stencil staging takes at most 11 KB)
             if (m2m1 + 11264 > static_cast<size_t>(dev_smem) || l2l1 + 1024 > static_cast<size_t>(dev_smem) ||
@@ -752,13 +790,18 @@ void DeviceOp::run_far_multi_t(FarField<R>& F, int nr, cudaStream_t s, int stage
             const dim3 grid(npar_[p], nth_[p], (nr + kRc - 1) / kRc);
             const size_t smem = static_cast<size_t>(nph_[p + 1]) * 32 * sizeof(C);
             const DevTransT<R>& T = F.trans[p];
+            const bool small = nph_[p] <= 8 * kInterpWarps;
+#define MLFMA_M2M_M(WW)                                                                        \
+    (small ? k_m2m_m<R, WW, 8><<<grid, kInterpThreads, smem, s>>>(F.lv_dev, T, nr)            \
+           : k_m2m_m<R, WW, kM2MOut><<<grid, kInterpThreads, smem, s>>>(F.lv_dev, T, nr))
             switch (up_w_[p]) {
-                case 2: k_m2m_m<R, 2><<<grid, kInterpThreads, smem, s>>>(F.lv_dev, T, nr); break;
-                case 4: k_m2m_m<R, 4><<<grid, kInterpThreads, smem, s>>>(F.lv_dev, T, nr); break;
-                case 6: k_m2m_m<R, 6><<<grid, kInterpThreads, smem, s>>>(F.lv_dev, T, nr); break;
-                case 8: k_m2m_m<R, 8><<<grid, kInterpThreads, smem, s>>>(F.lv_dev, T, nr); break;
-                default: k_m2m_m<R, 10><<<grid, kInterpThreads, smem, s>>>(F.lv_dev, T, nr); break;
+                case 2: MLFMA_M2M_M(2); break;
+                case 4: MLFMA_M2M_M(4); break;
+                case 6: MLFMA_M2M_M(6); break;
+                case 8: MLFMA_M2M_M(8); break;
+                default: MLFMA_M2M_M(10); break;
             }
+#undef MLFMA_M2M_M
         }
     if ((stage < 0 || stage == 2) && n_m2l_items_m_) {
         const int threads = std::min(kM2LmThreads, ((2 * nr + 31) / 32) * 32);
@@ -769,8 +812,9 @@ void DeviceOp::run_far_multi_t(FarField<R>& F, int nr, cudaStream_t s, int stage
         for (int p = lmin_; p < lmax_; ++p) {
             const int g = n_l2l_pairs_[p];
             if (!g) continue;
-            const dim3 grid(g, nph_[p + 1] / 2, (nr + kRc - 1) / kRc);
-            const size_t smem = static_cast<size_t>(nth_[p]) * 2 * 32 * sizeof(C) +
+            constexpr int kL2LPairs = l2l_pairs<R>();
+            const dim3 grid(g, (nph_[p + 1] / 2 + kL2LPairs - 1) / kL2LPairs, (nr + kRc - 1) / kRc);
+            const size_t smem = static_cast<size_t>(nth_[p]) * 2 * kL2LPairs * 32 * sizeof(C) +
                                 static_cast<size_t>(nth_[p + 1]) * dn_w_[p] * (sizeof(R) + 2 * sizeof(int));
             const DevTransT<R>& T = F.trans[p];
             switch (dn_w_[p]) {

@@ -29,9 +29,12 @@ namespace {
 // with opA(m, k) = A[m * sam + k * sak] (conjugated when CONJ_A), B row k at
 // B + (bidx ? bidx[k] : k) * ldb (entries n contiguous), output element (m, n)
 // at out + m * ldc + n, converted to the output type.  K is walked in chunks of
-// BK through shared memory; each thread keeps a 2 x 4 register tile.
-constexpr int kGemmThreads = 256;
-constexpr int kBM = 32, kBN = 64, kBK = 16;
+// BK through shared memory; each of the 128 threads keeps a 4 x 4 register
+// tile (16 complex products per 8 shared-memory loads).
+constexpr int kGemmThreads = 128;
+constexpr int kBM = 32, kBN = 64, kBK = 8;
+constexpr int kLdA = kBM * kBK / kGemmThreads;  // A entries loaded per thread (2)
+constexpr int kLdB = kBK * kBN / kGemmThreads;  // B entries loaded per thread (4)
 
 template <class C> __device__ __forceinline__ C conj_c(C a) { a.y = -a.y; return a; }
 template <class C, class S> __device__ __forceinline__ C to_c(S v);
@@ -46,20 +49,20 @@ template <class C, class TA, class TB, class TO, bool CONJ_A, bool A_KMAJOR>
 __device__ __forceinline__ void cgemm_tile(int M, int N, int K, int m0, int n0, const TA* __restrict__ A,
                                            long long sam, long long sak, const TB* __restrict__ B,
                                            const int* __restrict__ bidx, long long ldb, TO* __restrict__ out,
-                                           long long ldc, C (*As)[kBM], C (*Bs)[kBN]) {
+                                           long long ldc, C (*As)[kBM + 1], C (*Bs)[kBN]) {
     const int tid = threadIdx.x;
-    const int ty = tid >> 4, tx = tid & 15;
-    C acc[2][4];
+    const int ty = tid >> 4, tx = tid & 15;  // rows 4 ty .. 4 ty + 3, columns tx + 16 j
+    C acc[4][4];
 #pragma unroll
-    for (int i = 0; i < 2; ++i)
+    for (int i = 0; i < 4; ++i)
 #pragma unroll
         for (int j = 0; j < 4; ++j) acc[i][j] = zero<C>();
     // Registers of the next tile: its global loads are in flight while the
     // current tile is multiplied out of shared memory.
-    C ra[2], rb[4];
+    C ra[kLdA], rb[kLdB];
     auto load = [&](int k0) {
 #pragma unroll
-        for (int u = 0; u < 2; ++u) {  // A tile: BM x BK, two entries per thread
+        for (int u = 0; u < kLdA; ++u) {  // A tile: BM x BK
             const int idx = tid + u * kGemmThreads;
             int mm, kk;
             if (A_KMAJOR) { mm = idx / kBK; kk = idx % kBK; } else { kk = idx / kBM; mm = idx % kBM; }
@@ -72,7 +75,7 @@ __device__ __forceinline__ void cgemm_tile(int M, int N, int K, int m0, int n0, 
             ra[u] = v;
         }
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {  // B tile: BK x BN, four entries per thread
+        for (int u = 0; u < kLdB; ++u) {  // B tile: BK x BN
             const int idx = tid + u * kGemmThreads;
             const int kk = idx / kBN, nn = idx % kBN;
             const int k = k0 + kk, n = n0 + nn;
@@ -87,12 +90,12 @@ __device__ __forceinline__ void cgemm_tile(int M, int N, int K, int m0, int n0, 
     load(0);
     for (int k0 = 0; k0 < K; k0 += kBK) {
 #pragma unroll
-        for (int u = 0; u < 2; ++u) {
+        for (int u = 0; u < kLdA; ++u) {
             const int idx = tid + u * kGemmThreads;
             if (A_KMAJOR) As[idx % kBK][idx / kBK] = ra[u]; else As[idx / kBM][idx % kBM] = ra[u];
         }
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
+        for (int u = 0; u < kLdB; ++u) {
             const int idx = tid + u * kGemmThreads;
             Bs[idx / kBN][idx % kBN] = rb[u];
         }
@@ -100,19 +103,21 @@ __device__ __forceinline__ void cgemm_tile(int M, int N, int K, int m0, int n0, 
         if (k0 + kBK < K) load(k0 + kBK);
 #pragma unroll
         for (int kk = 0; kk < kBK; ++kk) {
-            const C a0 = As[kk][2 * ty], a1 = As[kk][2 * ty + 1];
+            C a[4], b[4];
 #pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const C b = Bs[kk][tx + 16 * j];
-                acc[0][j] = cfma(a0, b, acc[0][j]);
-                acc[1][j] = cfma(a1, b, acc[1][j]);
-            }
+            for (int i = 0; i < 4; ++i) a[i] = As[kk][4 * ty + i];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) b[j] = Bs[kk][tx + 16 * j];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) acc[i][j] = cfma(a[i], b[j], acc[i][j]);
         }
         __syncthreads();
     }
 #pragma unroll
-    for (int i = 0; i < 2; ++i) {
-        const int m = m0 + 2 * ty + i;
+    for (int i = 0; i < 4; ++i) {
+        const int m = m0 + 4 * ty + i;
         if (m >= M) continue;
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
@@ -130,7 +135,7 @@ __global__ void __launch_bounds__(kGemmThreads)
 k_s2m_m(const DevLevelT<R>* __restrict__ lvs, const int2* __restrict__ items, const DevFarLeaf* __restrict__ leaves,
         const typename Cx<R>::T* __restrict__ pat, const double2* __restrict__ x, int nr) {
     using C = typename Cx<R>::T;
-    __shared__ C As[kBK][kBM];
+    __shared__ C As[kBK][kBM + 1];
     __shared__ C Bs[kBK][kBN];
     const int2 it = items[blockIdx.x];
     const DevFarLeaf lf = leaves[it.x];
@@ -150,7 +155,7 @@ __global__ void __launch_bounds__(kGemmThreads)
 k_l2t_m(const DevLevelT<R>* __restrict__ lvs, const int2* __restrict__ items, const DevFarLeaf* __restrict__ leaves,
         const typename Cx<R>::T* __restrict__ pat, double2* __restrict__ yfar, int nr) {
     using C = typename Cx<R>::T;
-    __shared__ C As[kBK][kBM];
+    __shared__ C As[kBK][kBM + 1];
     __shared__ C Bs[kBK][kBN];
     const int2 it = items[blockIdx.x];
     const DevFarLeaf lf = leaves[it.x];
@@ -167,7 +172,7 @@ k_l2t_m(const DevLevelT<R>* __restrict__ lvs, const int2* __restrict__ items, co
 __global__ void __launch_bounds__(kGemmThreads)
 k_near_m(const DevNearRow* __restrict__ rows, const int2* __restrict__ items, const double2* __restrict__ Z,
          const int* __restrict__ cols, const double2* __restrict__ x, double2* __restrict__ y, int nr) {
-    __shared__ double2 As[kBK][kBM];
+    __shared__ double2 As[kBK][kBM + 1];
     __shared__ double2 Bs[kBK][kBN];
     const int2 it = items[blockIdx.x];
     const DevNearRow Rw = rows[it.x];
@@ -256,14 +261,14 @@ k_m2l_m(const DevLevelT<R>* __restrict__ lvs, const int2* __restrict__ items, co
 constexpr int kRc = 16;
 constexpr int kInterpThreads = 256;
 constexpr int kInterpWarps = kInterpThreads / 32;
-constexpr int kM2MOut = 16;  // parent positions per warp held in registers
+constexpr int kM2MOut = 16;  // most parent phi columns per warp held in registers
 
 // Parent outgoing patterns = sum over children of Interp[shift(child)]
 // (Stem::buildMpoleCoeffs and addInterpCoeffs, src/fmm/stem.cpp:72-184).
 // Block = (parent, parent theta row, rhs chunk).  Children one at a time:
 // theta pass of the child into shared memory (one row of child phi columns),
 // then the phi pass accumulated in registers over the children.
-template <class R, int W>
+template <class R, int W, int OUT>  // OUT: parent phi columns per warp (nph <= OUT * 8)
 __global__ void __launch_bounds__(kInterpThreads)
 k_m2m_m(const DevLevelT<R>* __restrict__ lvs, DevTransT<R> T, int nr) {
     using C = typename Cx<R>::T;
@@ -278,40 +283,49 @@ k_m2m_m(const DevLevelT<R>* __restrict__ lvs, DevTransT<R> T, int nr) {
     const DevLevelT<R> Cl = lvs[T.plevel + 1];
     const int nph = P.nph, mph = Cl.nph, halfm = Cl.nph / 2;
     const int c0 = T.child_ptr[par], nch = T.child_ptr[par + 1] - c0;
-    // Stencils in shared memory: this row's theta taps, every column's phi taps.
+    // Stencils in shared memory: this row's theta taps (sources; the weights
+    // come with the shift from fold_up), every column's phi taps.
     __shared__ int th_src[W], th_refl[W];
-    __shared__ R th_cf[W];
-    __shared__ int ph_src[kM2MOut * kInterpWarps * W];
-    __shared__ R ph_cf[kM2MOut * kInterpWarps * W];
+    __shared__ int ph_src[OUT * kInterpWarps * W];
+    __shared__ R ph_cf[OUT * kInterpWarps * W];
     if (threadIdx.x < W) {
         th_src[threadIdx.x] = T.up_th.src[jth * W + threadIdx.x];
         th_refl[threadIdx.x] = T.up_th.refl[jth * W + threadIdx.x];
-        th_cf[threadIdx.x] = T.up_th.coef[jth * W + threadIdx.x];
     }
     for (int i = threadIdx.x; i < nph * W; i += blockDim.x) {
         ph_src[i] = T.up_ph.src[i];
         ph_cf[i] = T.up_ph.coef[i];
     }
     __syncthreads();
-    C acc[kM2MOut];
+    C acc[OUT];
 #pragma unroll
-    for (int u = 0; u < kM2MOut; ++u) acc[u] = zero<C>();
+    for (int u = 0; u < OUT; ++u) acc[u] = zero<C>();
     for (int c = 0; c < nch; ++c) {
-        const C* Ac = Cl.Am + static_cast<size_t>(T.child_box[c0 + c]) * Cl.ndir * 2 * nr;
-        const C* sh = Cl.shift_up + static_cast<size_t>(T.child_oct[c0 + c]) * Cl.ndir;
-        for (int iph = warp; iph < mph; iph += kInterpWarps) {
-            C v = zero<C>();
-            const int iref = iph < halfm ? iph + halfm : iph - halfm;
+        const C* Ac = Cl.Am + static_cast<size_t>(T.child_box[c0 + c]) * Cl.ndir * 2 * nr + col;
+        // weights of this row with the child's octant shift folded in: [iph][k]
+        const C* fu = T.fold_up + (static_cast<size_t>(T.child_oct[c0 + c]) * P.nth + jth) * mph * W;
+        // two child columns per step: twice the loads in flight
+        for (int i0 = warp; i0 < mph; i0 += 2 * kInterpWarps) {
+            const int i1 = i0 + kInterpWarps;
+            const bool two = i1 < mph;
+            const int r0 = i0 < halfm ? i0 + halfm : i0 - halfm;
+            const int r1 = i1 < halfm ? i1 + halfm : i1 - halfm;
+            C v0 = zero<C>(), v1 = zero<C>();
 #pragma unroll
             for (int k = 0; k < W; ++k) {
-                const int dd = th_src[k] * mph + (th_refl[k] ? iref : iph);
-                if (live) v = crfma(th_cf[k], cmul(sh[dd], Ac[static_cast<size_t>(dd) * 2 * nr + col]), v);
+                const int d0 = th_src[k] * mph + (th_refl[k] ? r0 : i0);
+                const int d1 = th_src[k] * mph + (th_refl[k] ? r1 : i1);
+                if (live) {
+                    v0 = cfma(fu[i0 * W + k], Ac[static_cast<size_t>(d0) * 2 * nr], v0);
+                    if (two) v1 = cfma(fu[i1 * W + k], Ac[static_cast<size_t>(d1) * 2 * nr], v1);
+                }
             }
-            sm[iph * 32 + lane] = v;
+            sm[i0 * 32 + lane] = v0;
+            if (two) sm[i1 * 32 + lane] = v1;
         }
         __syncthreads();
 #pragma unroll
-        for (int u = 0; u < kM2MOut; ++u) {
+        for (int u = 0; u < OUT; ++u) {
             const int jph = warp + u * kInterpWarps;
             if (jph >= nph) break;
 #pragma unroll
@@ -322,7 +336,7 @@ k_m2m_m(const DevLevelT<R>* __restrict__ lvs, DevTransT<R> T, int nr) {
     if (!live) return;
     C* Ap = P.Am + (static_cast<size_t>(T.par_box[par]) * P.ndir + static_cast<size_t>(jth) * nph) * 2 * nr + col;
 #pragma unroll
-    for (int u = 0; u < kM2MOut; ++u) {
+    for (int u = 0; u < OUT; ++u) {
         const int jph = warp + u * kInterpWarps;
         if (jph >= nph) break;
         Ap[static_cast<size_t>(jph) * 2 * nr] = acc[u];
@@ -332,18 +346,25 @@ k_m2m_m(const DevLevelT<R>* __restrict__ lvs, DevTransT<R> T, int nr) {
 // ------------------------------------------------------------ L2L (many)
 // child local += Anterp[shift(parent local)] (Stem::getShiftedLocalCoeffs and
 // addAnterpCoeffs, src/fmm/stem.cpp:109-244).  Block = ((parent, child) pair,
-// child phi column pair {j, j + cph/2}, rhs chunk): the transposed phi pass
-// for those two columns over all parent theta rows into shared memory, then
-// the transposed theta pass, whose pole reflection only moves between the two
-// columns of the pair.
+// l2l_pairs child phi column pairs {j, j + cph/2}, rhs chunk): the transposed
+// phi pass for those columns over all parent theta rows into shared memory
+// (neighbouring columns share most of their parent taps, which then hit L1),
+// then the transposed theta pass, whose pole reflection only moves between
+// the two columns of a pair.
+// (4 column pairs for complex float; 1 for complex double, whose tile would
+// otherwise hold occupancy to two blocks per SM)
+template <class R> constexpr int l2l_pairs() { return sizeof(R) == 4 ? 4 : 1; }
+
 template <class R, int W>
 __global__ void __launch_bounds__(kInterpThreads)
 k_l2l_m(const DevLevelT<R>* __restrict__ lvs, DevTransT<R> T, const int2* __restrict__ pairs, int nr) {
     using C = typename Cx<R>::T;
+    constexpr int kL2LPairs = l2l_pairs<R>();
+    constexpr int NC = 2 * kL2LPairs;  // columns of the block
     extern __shared__ unsigned char smraw[];
-    C* sm = reinterpret_cast<C*>(smraw);  // [pth][2][32], then the theta taps
+    C* sm = reinterpret_cast<C*>(smraw);  // [pth][NC][32], then the theta taps
     const int2 pc = pairs[blockIdx.x];
-    const int j0 = blockIdx.y, r0 = blockIdx.z * kRc;
+    const int r0 = blockIdx.z * kRc;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int comp = lane >> 4, r = lane & 15;
     const bool live = r0 + r < nr;
@@ -351,19 +372,21 @@ k_l2l_m(const DevLevelT<R>* __restrict__ lvs, DevTransT<R> T, const int2* __rest
     const DevLevelT<R> P = lvs[T.plevel];
     const DevLevelT<R> Cl = lvs[T.plevel + 1];
     const int pth = P.nth, pph = P.nph, cth = Cl.nth, cph = Cl.nph, halfc = Cl.nph / 2;
-    const C* Bp = P.Bm + static_cast<size_t>(T.par_box[pc.x]) * P.ndir * 2 * nr;
-    const C* sh = P.shift_down + static_cast<size_t>(T.child_oct[pc.y]) * P.ndir;
-    // Stencils in shared memory: the phi taps of the two columns, every row's theta taps.
-    __shared__ int ph_src[2 * W];
-    __shared__ R ph_cf[2 * W];
+    const int j0 = blockIdx.y * kL2LPairs, npair = min(kL2LPairs, halfc - j0);
+    const C* Bp = P.Bm + static_cast<size_t>(T.par_box[pc.x]) * P.ndir * 2 * nr + col;
+    // weights with the child's octant shift folded in: [ith][jph][k]
+    const C* fd = T.fold_dn + static_cast<size_t>(T.child_oct[pc.y]) * pth * cph * W;
+    // column c of the block: pair c % kL2LPairs, side c / kL2LPairs
+    __shared__ int ph_src[NC * W];
     // dynamic shared memory: the tile, then cth x W theta taps (weight, source, reflection)
-    R* th_cf = reinterpret_cast<R*>(sm + static_cast<size_t>(pth) * 2 * 32);
+    R* th_cf = reinterpret_cast<R*>(sm + static_cast<size_t>(pth) * NC * 32);
     int* th_src = reinterpret_cast<int*>(th_cf + cth * W);
     int* th_refl = th_src + cth * W;
-    if (threadIdx.x < 2 * W) {
-        const int q = (j0 + (threadIdx.x / W) * halfc) * W + threadIdx.x % W;
-        ph_src[threadIdx.x] = T.dn_ph.src[q];
-        ph_cf[threadIdx.x] = T.dn_ph.coef[q];
+    for (int i = threadIdx.x; i < NC * W; i += blockDim.x) {
+        const int c = i / W, k = i - c * W;
+        const int pr = c % kL2LPairs;
+        const int jph = j0 + min(pr, npair - 1) + (c / kL2LPairs) * halfc;
+        ph_src[i] = T.dn_ph.src[jph * W + k];
     }
     for (int i = threadIdx.x; i < cth * W; i += blockDim.x) {
         th_src[i] = T.dn_th.src[i];
@@ -371,29 +394,33 @@ k_l2l_m(const DevLevelT<R>* __restrict__ lvs, DevTransT<R> T, const int2* __rest
         th_cf[i] = T.dn_th.coef[i];
     }
     __syncthreads();
-    for (int pos = warp; pos < 2 * pth; pos += kInterpWarps) {
-        const int ith = pos >> 1, side = pos & 1;
+    for (int pos = warp; pos < pth * NC; pos += kInterpWarps) {
+        const int ith = pos / NC, c = pos - ith * NC;
+        const int jph = j0 + min(c % kL2LPairs, npair - 1) + (c / kL2LPairs) * halfc;
+        const C* f = fd + (static_cast<size_t>(ith) * cph + jph) * W;
         C v = zero<C>();
 #pragma unroll
         for (int k = 0; k < W; ++k) {
-            const int dd = ith * pph + ph_src[side * W + k];
-            if (live) v = crfma(ph_cf[side * W + k], cmul(sh[dd], Bp[static_cast<size_t>(dd) * 2 * nr + col]), v);
+            const int dd = ith * pph + ph_src[c * W + k];
+            if (live) v = cfma(f[k], Bp[static_cast<size_t>(dd) * 2 * nr], v);
         }
         sm[pos * 32 + lane] = v;
     }
     __syncthreads();
     if (!live) return;
     C* Bc = Cl.Bm + static_cast<size_t>(T.child_box[pc.y]) * Cl.ndir * 2 * nr + col;
-    for (int pos = warp; pos < 2 * cth; pos += kInterpWarps) {
-        const int jth = pos >> 1, side = pos & 1, jph = j0 + side * halfc;
+    for (int pos = warp; pos < cth * NC; pos += kInterpWarps) {
+        const int jth = pos / NC, c = pos - jth * NC;
+        const int pr = c % kL2LPairs, side = c / kL2LPairs;
+        if (pr >= npair) continue;
         C v = zero<C>();
 #pragma unroll
         for (int k = 0; k < W; ++k) {
             const int q = jth * W + k;
-            const int s2 = th_refl[q] ? 1 - side : side;
-            v = crfma(th_cf[q], sm[(th_src[q] * 2 + s2) * 32 + lane], v);
+            const int c2 = th_refl[q] ? pr + (1 - side) * kL2LPairs : c;
+            v = crfma(th_cf[q], sm[(th_src[q] * NC + c2) * 32 + lane], v);
         }
-        C* o = Bc + static_cast<size_t>(jth * cph + jph) * 2 * nr;
+        C* o = Bc + static_cast<size_t>(jth * cph + j0 + pr + side * halfc) * 2 * nr;
         *o = cadd(*o, v);
     }
 }
