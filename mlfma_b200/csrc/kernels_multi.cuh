@@ -353,7 +353,7 @@ k_m2m_m(const DevLevelT<R>* __restrict__ lvs, DevTransT<R> T, int nr) {
 // the two columns of a pair.
 // (4 column pairs for complex float; 1 for complex double, whose tile would
 // otherwise hold occupancy to two blocks per SM)
-template <class R> constexpr int l2l_pairs() { return sizeof(R) == 4 ? 4 : 1; }
+template <class R> __host__ __device__ constexpr int l2l_pairs() { return sizeof(R) == 4 ? 4 : 1; }
 
 template <class R, int W>
 __global__ void __launch_bounds__(kInterpThreads)
