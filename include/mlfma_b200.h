@@ -210,6 +210,43 @@ int mlfma_gmres_multi(mlfma_handle h, int nrhs, const double* b, double* x, cons
 /* Per-stage CUDA-event time of one product on nrhs right-hand sides. */
 int mlfma_time_stages_multi(mlfma_handle h, int nrhs, mlfma_stage_times* t);
 
+/* ---- Adjoint and gradients (no counterpart in the reference).  The
+ * operator must be set up with ref_compat = 0: the reference's stale-local
+ * rule makes the product depend on earlier products, and such a map has no
+ * adjoint.  The transposed product is the exact transpose of the discrete
+ * MLFMA pipeline (conjugated and plain patterns swap ends, interpolation and
+ * anterpolation swap with the octant shifts moved to the other grid,
+ * translations use the negated offsets); the stored near field is symmetric
+ * to rounding and is reused. */
+
+/* Diagonal loads added to the operator: A x + z .* x (surface-impedance loads
+ * per unknown, in ohms, like the entries of A = C k Z).  z: n complex, caller
+ * order; NULL removes them.  Applies to every later product and solve. */
+int mlfma_set_loads(mlfma_handle h, const double* z);
+
+/* y = A^H x (accumulate = 0) or y += A^H x, host buffers. */
+int mlfma_matvec_adjoint(mlfma_handle h, const double* x, double* y, int accumulate);
+
+/* Solve A^H x = b with GMRES (unitary Givens rotations); as mlfma_gmres. */
+int mlfma_gmres_adjoint(mlfma_handle h, const double* b, double* x, const mlfma_solver_opts* opts,
+                        mlfma_solve_info* info);
+
+/* g = M^H F: the adjoint of mlfma_farfield (M: currents -> far field along
+ * khat), for F (ndir x 3 complex); g: n complex, caller order. */
+int mlfma_farfield_adjoint(mlfma_handle h, int ndir, const double* khat, const double* F, double* g);
+
+/* Far-field power objective and its gradient by one forward and one adjoint
+ * solve.  Excitation b = sum_j w_j b_j over nexc incident plane waves (b_j as
+ * mlfma_rhs_planewave; w: nexc complex weights); currents I solve
+ * (A + diag(z)) I = b with the loads z of mlfma_set_loads; J = sum over the
+ * ndir directions khat of |F|^2, F = mlfma_farfield(I).  Outputs: *J;
+ * grad_loads[n] = dJ/dRe z_n + i dJ/dIm z_n; grad_w[nexc] likewise for the
+ * weights; currents[n] = I (each may be NULL); info[2] = forward and adjoint
+ * solve records (may be NULL). */
+int mlfma_vjp_farfield_power(mlfma_handle h, int nexc, const mlfma_planewave* pws, const double* w, int ndir,
+                             const double* khat, const mlfma_solver_opts* opts, double* J, double* grad_loads,
+                             double* grad_w, double* currents, mlfma_solve_info* info);
+
 /* The handle's own CUDA stream (cudaStream_t as void*), on which mlfma_matvec
  * and mlfma_gmres run; callers may record events on it. */
 int mlfma_get_stream(mlfma_handle h, void** stream);

@@ -251,6 +251,67 @@ class MLFMA:
         check(lib().mlfma_time_stages_multi(self._h, nrhs, ctypes.byref(t)))
         return {k: float(getattr(t, k)) for k, _ in StageTimes._fields_}
 
+    # ---------------------------------------------------------------- adjoint and gradients
+    def set_loads(self, z=None) -> None:
+        """Diagonal loads z (n complex, caller order) added to the operator; None removes them."""
+        if z is None:
+            check(lib().mlfma_set_loads(self._h, None))
+            return
+        zv = _cvec(z, self.n)
+        check(lib().mlfma_set_loads(self._h, zv.view(np.float64).ctypes.data_as(_dp)))
+
+    def matvec_adjoint(self, x, accumulate: bool = False, out: np.ndarray | None = None) -> np.ndarray:
+        """y = A^H x (loads included)."""
+        xv = _cvec(x, self.n)
+        y = out if out is not None else np.zeros(self.n, dtype=np.complex128)
+        check(lib().mlfma_matvec_adjoint(self._h, xv.view(np.float64).ctypes.data_as(_dp),
+                                         y.view(np.float64).ctypes.data_as(_dp), int(accumulate)))
+        return y
+
+    def solve_adjoint(self, b, max_iter: int = 500, tol: float = 1e-6, restart: int = 0, raise_on_fail: bool = False):
+        """GMRES on A^H x = b."""
+        bv = _cvec(b, self.n)
+        x = np.zeros(self.n, dtype=np.complex128)
+        o = SolverOpts(max_iter=max_iter, tol=tol, restart=restart, ref_givens=0)
+        info = SolveInfo()
+        code = lib().mlfma_gmres_adjoint(self._h, bv.view(np.float64).ctypes.data_as(_dp),
+                                         x.view(np.float64).ctypes.data_as(_dp), ctypes.byref(o), ctypes.byref(info))
+        if code not in (0, 4) or (raise_on_fail and code != 0):
+            check(code)
+        return x, SolveResult(info.iterations, info.residual, info.true_residual, info.seconds, code == 0,
+                              info.refinements)
+
+    def farfield_adjoint(self, F, khat) -> np.ndarray:
+        """g = M^H F, the adjoint of farfield (F: ndir x 3 complex)."""
+        kh = np.ascontiguousarray(np.asarray(khat, dtype=np.float64).reshape(-1, 3))
+        Fv = np.ascontiguousarray(np.asarray(F, dtype=np.complex128).reshape(kh.shape[0], 3))
+        g = np.zeros(self.n, dtype=np.complex128)
+        check(lib().mlfma_farfield_adjoint(self._h, kh.shape[0], kh.ctypes.data_as(_dp),
+                                           Fv.view(np.float64).ctypes.data_as(_dp),
+                                           g.view(np.float64).ctypes.data_as(_dp)))
+        return g
+
+    def vjp_farfield_power(self, pws, weights, khat, max_iter: int = 500, tol: float = 1e-10, restart: int = 0):
+        """J = sum |F(khat)|^2 for currents solving (A + diag(loads)) I = sum_j w_j b_j, and
+        its gradient: returns (J, grad_loads, grad_w, I, (forward info, adjoint info)),
+        gradients packed as dJ/dRe + i dJ/dIm."""
+        pws = list(pws)
+        w = np.ascontiguousarray(np.asarray(weights, dtype=np.complex128).reshape(len(pws)))
+        kh = np.ascontiguousarray(np.asarray(khat, dtype=np.float64).reshape(-1, 3))
+        parr = (PlaneWaveC * len(pws))(*[_pw(p) for p in pws])
+        o = SolverOpts(max_iter=max_iter, tol=tol, restart=restart, ref_givens=0)
+        J = ctypes.c_double()
+        gz = np.zeros(self.n, dtype=np.complex128)
+        gw = np.zeros(len(pws), dtype=np.complex128)
+        cur = np.zeros(self.n, dtype=np.complex128)
+        infos = (SolveInfo * 2)()
+        check(lib().mlfma_vjp_farfield_power(self._h, len(pws), parr, w.view(np.float64).ctypes.data_as(_dp),
+                                             kh.shape[0], kh.ctypes.data_as(_dp), ctypes.byref(o), ctypes.byref(J),
+                                             gz.view(np.float64).ctypes.data_as(_dp),
+                                             gw.view(np.float64).ctypes.data_as(_dp),
+                                             cur.view(np.float64).ctypes.data_as(_dp), infos))
+        return J.value, gz, gw, cur, tuple(infos)
+
     def farfield(self, currents, khat) -> np.ndarray:
         """Far field (ndir x 3 complex) of `currents` along unit directions `khat` (ndir x 3)."""
         cur = _cvec(currents, self.n)

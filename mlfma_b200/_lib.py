@@ -90,6 +90,14 @@ SIGNATURES = {
     "mlfma_gmres_multi": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _dp, _dp, ctypes.POINTER(SolverOpts),
                                          ctypes.POINTER(SolveInfo)]),
     "mlfma_time_stages_multi": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(StageTimes)]),
+    "mlfma_set_loads": (ctypes.c_int, [ctypes.c_void_p, _dp]),
+    "mlfma_matvec_adjoint": (ctypes.c_int, [ctypes.c_void_p, _dp, _dp, ctypes.c_int]),
+    "mlfma_gmres_adjoint": (ctypes.c_int, [ctypes.c_void_p, _dp, _dp, ctypes.POINTER(SolverOpts),
+                                           ctypes.POINTER(SolveInfo)]),
+    "mlfma_farfield_adjoint": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _dp, _dp, _dp]),
+    "mlfma_vjp_farfield_power": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(PlaneWaveC), _dp,
+                                                ctypes.c_int, _dp, ctypes.POINTER(SolverOpts), _dp, _dp, _dp, _dp,
+                                                ctypes.POINTER(SolveInfo)]),
     "mlfma_get_stream": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]),
     "mlfma_time_stages": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(StageTimes)]),
     "mlfma_get_traffic": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Traffic)]),

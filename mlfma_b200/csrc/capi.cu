@@ -2,6 +2,8 @@
 #include <cuda_runtime.h>
 
 #include <cstring>
+#include <complex>
+#include <cmath>
 #include <exception>
 #include <memory>
 #include <string>
@@ -416,6 +418,179 @@ int mlfma_time_stages_multi(mlfma_handle h, int nrhs, mlfma_stage_times* t) {
     t->near_field = st.near;
     t->finish = st.finish;
     t->total = st.total;
+    return MLFMA_OK;
+}
+
+// ---------------------------------------------------------------- adjoint
+// No counterpart in the reference: loads, the adjoint product and solve, and
+// the far-field power gradient built on them.
+
+int mlfma_set_loads(mlfma_handle h, const double* z) {
+    if (!h) return fail(MLFMA_ERR_ARG, "null handle");
+    if (!ready(h)) return fail(MLFMA_ERR_STATE, "mlfma_setup has not run");
+    if (z)
+        for (int i = 0; i < 2 * h->plan.n; ++i)
+            if (!std::isfinite(z[i])) return fail(MLFMA_ERR_NONFINITE, "nonfinite load");
+    std::string e = h->dev->set_loads(reinterpret_cast<const double2*>(z));
+    if (!e.empty()) return from_msg(e);
+    return MLFMA_OK;
+}
+
+int mlfma_matvec_adjoint(mlfma_handle h, const double* x, double* y, int accumulate) {
+    if (!h || !x || !y) return fail(MLFMA_ERR_ARG, "null argument");
+    if (!ready(h)) return fail(MLFMA_ERR_STATE, "mlfma_setup has not run");
+    const size_t bytes = sizeof(double2) * h->plan.n;
+    cudaStream_t s = h->dev->stream();
+    if (cudaSetDevice(h->device) != cudaSuccess) return fail(MLFMA_ERR_CUDA, "cudaSetDevice failed");
+    if (cudaMemcpyAsync(h->d_x, x, bytes, cudaMemcpyHostToDevice, s) != cudaSuccess)
+        return fail(MLFMA_ERR_CUDA, "copy of x failed");
+    if (accumulate && cudaMemcpyAsync(h->d_y, y, bytes, cudaMemcpyHostToDevice, s) != cudaSuccess)
+        return fail(MLFMA_ERR_CUDA, "copy of y failed");
+    std::string e = h->dev->matvec_device(h->d_x, h->d_y, accumulate != 0, s, -1, true);
+    if (!e.empty()) return from_msg(e);
+    if (cudaMemcpyAsync(y, h->d_y, bytes, cudaMemcpyDeviceToHost, s) != cudaSuccess)
+        return fail(MLFMA_ERR_CUDA, "copy of y failed");
+    const cudaError_t ce = cudaStreamSynchronize(s);
+    if (ce != cudaSuccess) return fail(MLFMA_ERR_CUDA, cudaGetErrorString(ce));
+    return MLFMA_OK;
+}
+
+static mlfma::SolveOpts to_opts(const mlfma_solver_opts* opts) {
+    mlfma::SolveOpts o;
+    if (opts) {
+        o.max_iter = opts->max_iter;
+        o.tol = opts->tol;
+        o.restart = opts->restart;
+        o.ref_givens = opts->ref_givens;
+        o.refine = opts->refine;
+        o.inner_tol = opts->inner_tol;
+    }
+    return o;
+}
+
+static void to_info(const mlfma::SolveResult& r, mlfma_solve_info* info) {
+    if (!info) return;
+    info->iterations = r.iterations;
+    info->residual = r.residual;
+    info->true_residual = r.true_residual;
+    info->seconds = r.seconds;
+    info->refinements = r.refinements;
+}
+
+// Host b -> host x through the handle's GMRES (adjoint when adj).
+static int solve_host(mlfma_handle h, const double* b, double* x, mlfma::SolveOpts o, bool adj,
+                      mlfma_solve_info* info) {
+    o.adjoint = adj ? 1 : 0;
+    if (adj) o.ref_givens = 0;
+    const size_t bytes = sizeof(double2) * h->plan.n;
+    cudaStream_t s = h->dev->stream();
+    if (cudaSetDevice(h->device) != cudaSuccess) return fail(MLFMA_ERR_CUDA, "cudaSetDevice failed");
+    if (cudaMemcpyAsync(h->d_x, b, bytes, cudaMemcpyHostToDevice, s) != cudaSuccess)
+        return fail(MLFMA_ERR_CUDA, "copy of b failed");
+    mlfma::SolveResult r;
+    std::string e = h->gmres->solve(*h->dev, h->d_x, h->d_y, o, &r);
+    if (!e.empty()) return from_msg(e);
+    if (cudaMemcpyAsync(x, h->d_y, bytes, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+        return fail(MLFMA_ERR_CUDA, "copy of x failed");
+    to_info(r, info);
+    if (!r.converged) return fail(MLFMA_ERR_NOT_CONVERGED, "iteration limit reached");
+    return MLFMA_OK;
+}
+
+int mlfma_gmres_adjoint(mlfma_handle h, const double* b, double* x, const mlfma_solver_opts* opts,
+                        mlfma_solve_info* info) {
+    if (!h || !b || !x) return fail(MLFMA_ERR_ARG, "null argument");
+    if (!ready(h)) return fail(MLFMA_ERR_STATE, "mlfma_setup has not run");
+    return solve_host(h, b, x, to_opts(opts), true, info);
+}
+
+int mlfma_farfield_adjoint(mlfma_handle h, int ndir, const double* khat, const double* F, double* g) {
+    if (!h || ndir < 0 || (ndir > 0 && (!khat || !F)) || !g) return fail(MLFMA_ERR_ARG, "null argument");
+    if (!ready(h)) return fail(MLFMA_ERR_STATE, "mlfma_setup has not run");
+    if (cudaSetDevice(h->device) != cudaSuccess) return fail(MLFMA_ERR_CUDA, "cudaSetDevice failed");
+    cudaStream_t s = h->dev->stream();
+    double* d_k = nullptr;
+    double2* d_F = nullptr;
+    const int nd = ndir > 0 ? ndir : 1;
+    if (cudaMalloc(&d_k, sizeof(double) * 3 * nd) != cudaSuccess ||
+        cudaMalloc(&d_F, sizeof(double2) * 3 * nd) != cudaSuccess) {
+        cudaFree(d_k);
+        return fail(MLFMA_ERR_CUDA, "cudaMalloc failed");
+    }
+    std::string e;
+    if (ndir > 0 && (cudaMemcpyAsync(d_k, khat, sizeof(double) * 3 * ndir, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+                     cudaMemcpyAsync(d_F, F, sizeof(double2) * 3 * ndir, cudaMemcpyHostToDevice, s) != cudaSuccess))
+        e = "copy failed";
+    if (e.empty()) e = h->dev->farfield_adjoint(d_F, ndir, d_k, h->d_y, s);
+    if (e.empty() && (cudaMemcpyAsync(g, h->d_y, sizeof(double2) * h->plan.n, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+                      cudaStreamSynchronize(s) != cudaSuccess))
+        e = "copy of g failed";
+    cudaFree(d_k);
+    cudaFree(d_F);
+    if (!e.empty()) return fail(MLFMA_ERR_CUDA, e);
+    return MLFMA_OK;
+}
+
+int mlfma_vjp_farfield_power(mlfma_handle h, int nexc, const mlfma_planewave* pws, const double* w, int ndir,
+                             const double* khat, const mlfma_solver_opts* opts, double* J, double* grad_loads,
+                             double* grad_w, double* currents, mlfma_solve_info* info) {
+    if (!h || nexc < 1 || !pws || !w || ndir < 1 || !khat || !J) return fail(MLFMA_ERR_ARG, "null argument");
+    if (!ready(h)) return fail(MLFMA_ERR_STATE, "mlfma_setup has not run");
+    if (h->dev->ref_compat()) return fail(MLFMA_ERR_ARG, "the adjoint needs ref_compat = 0");
+    using cd = std::complex<double>;
+    const int n = h->plan.n;
+    try {
+        // b = sum_j w_j b_j
+        std::vector<std::vector<cd>> bj(nexc, std::vector<cd>(n));
+        std::vector<cd> b(n, cd(0));
+        for (int j = 0; j < nexc; ++j) {
+            if (pws[j].wavenum != h->plan.pw.wavenum) return fail(MLFMA_ERR_ARG, "wavenumber differs from the operator's");
+            h->plan.rhs_for(to_pw(&pws[j]), bj[j].data());
+            const cd wj(w[2 * j], w[2 * j + 1]);
+            for (int i = 0; i < n; ++i) b[i] += wj * bj[j][i];
+        }
+        const mlfma::SolveOpts o = to_opts(opts);
+        // forward solve A I = b
+        std::vector<cd> I(n);
+        int code = solve_host(h, reinterpret_cast<const double*>(b.data()), reinterpret_cast<double*>(I.data()), o,
+                              false, info);
+        if (code != MLFMA_OK) return code;
+        // F = M I, J = |F|^2
+        std::vector<cd> F(3 * static_cast<size_t>(ndir));
+        code = mlfma_farfield(h, reinterpret_cast<const double*>(I.data()), ndir, khat, reinterpret_cast<double*>(F.data()));
+        if (code != MLFMA_OK) return code;
+        double Jv = 0;
+        for (const cd& f : F) Jv += std::norm(f);
+        *J = Jv;
+        // g = M^H F ; adjoint solve A^H lambda = g
+        std::vector<cd> g(n), lam(n);
+        code = mlfma_farfield_adjoint(h, ndir, khat, reinterpret_cast<const double*>(F.data()),
+                                      reinterpret_cast<double*>(g.data()));
+        if (code != MLFMA_OK) return code;
+        code = solve_host(h, reinterpret_cast<const double*>(g.data()), reinterpret_cast<double*>(lam.data()), o, true,
+                          info ? info + 1 : nullptr);
+        if (code != MLFMA_OK) return code;
+        // dJ = 2 Re(lambda^H (db - dZ I)):  dJ/dRe z + i dJ/dIm z = -2 lambda conj(I);
+        // dJ/dRe w_j + i dJ/dIm w_j = 2 conj(lambda^H b_j)
+        if (grad_loads)
+            for (int i = 0; i < n; ++i) {
+                const cd v = -2.0 * lam[i] * std::conj(I[i]);
+                grad_loads[2 * i] = v.real();
+                grad_loads[2 * i + 1] = v.imag();
+            }
+        if (grad_w)
+            for (int j = 0; j < nexc; ++j) {
+                cd d(0);
+                for (int i = 0; i < n; ++i) d += std::conj(lam[i]) * bj[j][i];
+                const cd v = 2.0 * std::conj(d);
+                grad_w[2 * j] = v.real();
+                grad_w[2 * j + 1] = v.imag();
+            }
+        if (currents) std::memcpy(currents, I.data(), sizeof(cd) * n);
+    } catch (const std::exception& e) {
+        return fail(MLFMA_ERR_INTERNAL, e.what());
+    }
     return MLFMA_OK;
 }
 

@@ -151,12 +151,21 @@ public:
     // (0 = the operator's own stream).  Interleaved complex FP64.
     // prec: far-field precision (-1 = the operator's own; a mixed operator
     // also carries the FP64 far field).
-    std::string matvec_device(const double2* x, double2* y, bool accumulate, cudaStream_t stream, int prec = -1);
+    // adj: y = A^H x (needs ref_compat = 0).
+    std::string matvec_device(const double2* x, double2* y, bool accumulate, cudaStream_t stream, int prec = -1,
+                              bool adj = false);
 
     // Operator on tree-ordered device vectors (used by the solver).
-    void apply_tree(const double2* xt, double2* yt, cudaStream_t s, int prec = -1);
+    void apply_tree(const double2* xt, double2* yt, cudaStream_t s, int prec = -1, bool adj = false);
     // Same, never capturing a graph (launches the captured one if it exists).
-    void apply_tree_direct(const double2* xt, double2* yt, cudaStream_t s, int prec = -1);
+    void apply_tree_direct(const double2* xt, double2* yt, cudaStream_t s, int prec = -1, bool adj = false);
+
+    // Diagonal loads z (host, caller order, n complex) added to the operator:
+    // A x + z .* x (A^H x + conj(z) .* x for the adjoint).  nullptr removes them.
+    std::string set_loads(const double2* z_user);
+    bool ref_compat() const { return ref_compat_ != 0; }
+    const DevSources& sources() const { return src_; }
+    double2 ck() const { return ck_; }
 
     // Products on nr right-hand sides at once (1 <= nr <= max_rhs).  x and y are
     // nr vectors one after another in the caller's order ([nr][n]).
@@ -174,6 +183,8 @@ public:
     // Far field of currents (caller order, device) along ndir unit directions
     // (device, ndir x 3); out: ndir x 3 complex (device).
     std::string farfield(const double2* cur, int ndir, const double* khat, double2* out, cudaStream_t s);
+    // Its adjoint: g (caller order, device, n) = M^H F for F (device, ndir x 3).
+    std::string farfield_adjoint(const double2* F, int ndir, const double* khat, double2* g, cudaStream_t s);
 
     int n() const { return n_; }
     int precision() const { return precision_; }
@@ -195,16 +206,17 @@ private:
     template <class T> T* alloc(size_t count);
     template <class T> T* upload(const std::vector<T>& v);
     template <class R> std::string setup_far(const Plan& plan, FarField<R>& F, const double2* pat64);
-    template <class R> void run_far_t(FarField<R>& F, const double2* xt, cudaStream_t s, int stage);
-    void run_far(const double2* xt, cudaStream_t s, int stage = -1, int prec = -1);
+    template <class R, bool TR> void run_far_t(FarField<R>& F, const double2* xt, cudaStream_t s, int stage);
+    void run_far(const double2* xt, cudaStream_t s, int stage = -1, int prec = -1, bool tr = false);
     void run_near(const double2* xt, cudaStream_t s);
-    void enqueue_core(cudaStream_t s, int prec);   // xt_ -> yfar_, ynear_
+    void enqueue_core(cudaStream_t s, int prec, bool tr);   // xt_ -> yfar_, ynear_
+    void launch_core(cudaStream_t s, int prec, bool tr);
     template <class R> void run_far_multi_t(FarField<R>& F, int nr, cudaStream_t s, int stage);
     void run_far_multi(int nr, cudaStream_t s, int stage, int prec);
     void run_near_multi(int nr, cudaStream_t s);
     void enqueue_multi(int nr, cudaStream_t s, int prec);  // xtm_ -> yfarm_, ynearm_
     std::string setup_multi(const Plan& plan);
-    std::string ensure_graph(int prec);
+    std::string ensure_graph(int prec, bool tr);
     static int m2m_rows(int nth, int nph);
 
     int device_ = 0;
@@ -215,8 +227,8 @@ private:
     cudaEvent_t ev_fork_ = nullptr, ev_join_ = nullptr;
     std::vector<void*> allocs_;
     long long bytes_ = 0;
-    cudaGraph_t graph_[2] = {nullptr, nullptr};          // per far-field precision
-    cudaGraphExec_t graph_exec_[2] = {nullptr, nullptr};
+    cudaGraph_t graph_[2][2] = {};          // per far-field precision, forward / transposed
+    cudaGraphExec_t graph_exec_[2][2] = {};
     bool use_graph_ = true;
 
     // Shared by both precisions.
@@ -267,6 +279,8 @@ private:
     int2* m2l_items_m_ = nullptr;
     int n_m2l_items_m_ = 0;
     double2 ck_{};             // Phys::C * k
+    double2* loads_ = nullptr; // diagonal loads, tree order
+    bool has_loads_ = false;
     Traffic traffic_{};
 };
 

@@ -189,7 +189,7 @@ void Gmres::release() {
 Gmres::~Gmres() { release(); }
 
 void Gmres::apply(DeviceOp& op, const double2* x, double2* y, cudaStream_t s, int prec) {
-    if (external_) op.apply_tree_direct(x, y, s, prec); else op.apply_tree(x, y, s, prec);
+    if (external_) op.apply_tree_direct(x, y, s, prec, adj_); else op.apply_tree(x, y, s, prec, adj_);
 }
 
 // ------------------------------------------------------------ fixed workspace
@@ -406,6 +406,8 @@ std::string Gmres::cycles(DeviceOp& op, int prec, const SolveOpts& o, double bno
 
 std::string Gmres::solve(DeviceOp& op, const double2* d_b_user, double2* d_x_user, const SolveOpts& o,
                          SolveResult* res) {
+    if (o.adjoint && op.ref_compat()) return "arg:the adjoint needs ref_compat = 0";
+    adj_ = o.adjoint != 0;
     if (o.refine && op.precision() != kFp64) return solve_refined(op, d_b_user, d_x_user, o, res);
     const auto t_start = std::chrono::steady_clock::now();
     const int n = op.n();

@@ -18,6 +18,7 @@ struct SolveOpts {
     int refine = 0;      // mixed operator: inner GMRES on the mixed far field,
                          // outer loop on the FP64 residual
     double inner_tol = 0;  // refinement: inner relative target (0 = automatic)
+    int adjoint = 0;       // solve A^H x = b (operator set up with ref_compat = 0)
 };
 
 struct SolveResult {
@@ -55,6 +56,7 @@ private:
     std::string solve_refined(DeviceOp& op, const double2* d_b_user, double2* d_x_user, const SolveOpts& o,
                               SolveResult* res);
     bool external_ = false;   // workspace not owned (static device array)
+    bool adj_ = false;        // products with A^H (SolveOpts::adjoint)
     std::string ensure(int n, int ncols, int extra);
     void release();
     std::string norm(const double2* v, cudaStream_t s, double* out);

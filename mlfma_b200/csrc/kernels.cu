@@ -44,19 +44,32 @@ namespace mlfma {
 
 namespace {
 
+// xt[t] = x[perm[t]] (conjugated when cj)
 __global__ void k_gather(const double2* __restrict__ x, const int* __restrict__ perm,
-                         double2* __restrict__ xt, int n) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t < n) xt[t] = x[perm[t]];
-}
-
-// y[perm[t]] (+)= ck * (yfar[t] + ynear[t]); perm == nullptr keeps tree order.
-__global__ void k_finish(const double2* __restrict__ yfar, const double2* __restrict__ ynear,
-                         const int* __restrict__ perm, double2* __restrict__ y, int n, double2 ck,
-                         int accumulate) {
+                         double2* __restrict__ xt, int n, int cj) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n) return;
-    const double2 v = cmul(ck, cadd(yfar[t], ynear[t]));
+    double2 v = x[perm[t]];
+    if (cj) v.y = -v.y;
+    xt[t] = v;
+}
+
+__global__ void k_conj_copy(const double2* __restrict__ x, double2* __restrict__ out, int n) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) out[t] = make_double2(x[t].x, -x[t].y);
+}
+
+// v = ck (yfar[t] + ynear[t]) + loads[t] xt[t] (loads: a diagonal added to the
+// operator, may be null), conjugated when cj (the adjoint, xt then holding
+// conj(x)); y[perm[t]] (+)= v, perm == nullptr keeps tree order.
+__global__ void k_finish(const double2* __restrict__ yfar, const double2* __restrict__ ynear,
+                         const int* __restrict__ perm, double2* __restrict__ y, int n, double2 ck,
+                         int accumulate, const double2* __restrict__ xt, const double2* __restrict__ loads, int cj) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    double2 v = cmul(ck, cadd(yfar[t], ynear[t]));
+    if (loads) v = cfma(loads[t], xt[t], v);
+    if (cj) v.y = -v.y;
     const int o = perm ? perm[t] : t;
     y[o] = accumulate ? cadd(y[o], v) : v;
 }
@@ -87,10 +100,11 @@ constexpr int kDnWidths[] = {8, 12, 16, 24, 32};
 
 DeviceOp::~DeviceOp() {
     if (device_ >= 0) cudaSetDevice(device_);
-    for (int p = 0; p < 2; ++p) {
-        if (graph_exec_[p]) cudaGraphExecDestroy(graph_exec_[p]);
-        if (graph_[p]) cudaGraphDestroy(graph_[p]);
-    }
+    for (int p = 0; p < 2; ++p)
+        for (int t = 0; t < 2; ++t) {
+            if (graph_exec_[p][t]) cudaGraphExecDestroy(graph_exec_[p][t]);
+            if (graph_[p][t]) cudaGraphDestroy(graph_[p][t]);
+        }
     for (void* p : allocs_) cudaFree(p);
     if (ev_fork_) cudaEventDestroy(ev_fork_);
     if (ev_join_) cudaEventDestroy(ev_join_);
@@ -237,17 +251,20 @@ std::string DeviceOp::setup_far(const Plan& plan, FarField<R>& F, const double2*
         s2m_smem > static_cast<size_t>(dev_smem))
         return "angular grid or leaf too large for the kernels' shared memory";
     const auto attr = cudaFuncAttributeMaxDynamicSharedMemorySize;
-    MLFMA_CK(cudaFuncSetAttribute(k_m2m<R, 2>, attr, static_cast<int>(m2m_smem)));
-    MLFMA_CK(cudaFuncSetAttribute(k_m2m<R, 4>, attr, static_cast<int>(m2m_smem)));
-    MLFMA_CK(cudaFuncSetAttribute(k_m2m<R, 6>, attr, static_cast<int>(m2m_smem)));
-    MLFMA_CK(cudaFuncSetAttribute(k_m2m<R, 8>, attr, static_cast<int>(m2m_smem)));
-    MLFMA_CK(cudaFuncSetAttribute(k_m2m<R, 10>, attr, static_cast<int>(m2m_smem)));
-    MLFMA_CK(cudaFuncSetAttribute(k_l2l<R, 8>, attr, static_cast<int>(l2l_smem)));
-    MLFMA_CK(cudaFuncSetAttribute(k_l2l<R, 12>, attr, static_cast<int>(l2l_smem)));
-    MLFMA_CK(cudaFuncSetAttribute(k_l2l<R, 16>, attr, static_cast<int>(l2l_smem)));
-    MLFMA_CK(cudaFuncSetAttribute(k_l2l<R, 24>, attr, static_cast<int>(l2l_smem)));
-    MLFMA_CK(cudaFuncSetAttribute(k_l2l<R, 32>, attr, static_cast<int>(l2l_smem)));
-    MLFMA_CK(cudaFuncSetAttribute(k_s2m<R>, attr, static_cast<int>(s2m_smem)));
+    for (int tr = 0; tr < 2; ++tr) {  // forward and transposed variants
+        const bool t = tr != 0;
+        MLFMA_CK(cudaFuncSetAttribute(t ? k_m2m<R, 2, true> : k_m2m<R, 2, false>, attr, static_cast<int>(m2m_smem)));
+        MLFMA_CK(cudaFuncSetAttribute(t ? k_m2m<R, 4, true> : k_m2m<R, 4, false>, attr, static_cast<int>(m2m_smem)));
+        MLFMA_CK(cudaFuncSetAttribute(t ? k_m2m<R, 6, true> : k_m2m<R, 6, false>, attr, static_cast<int>(m2m_smem)));
+        MLFMA_CK(cudaFuncSetAttribute(t ? k_m2m<R, 8, true> : k_m2m<R, 8, false>, attr, static_cast<int>(m2m_smem)));
+        MLFMA_CK(cudaFuncSetAttribute(t ? k_m2m<R, 10, true> : k_m2m<R, 10, false>, attr, static_cast<int>(m2m_smem)));
+        MLFMA_CK(cudaFuncSetAttribute(t ? k_l2l<R, 8, true> : k_l2l<R, 8, false>, attr, static_cast<int>(l2l_smem)));
+        MLFMA_CK(cudaFuncSetAttribute(t ? k_l2l<R, 12, true> : k_l2l<R, 12, false>, attr, static_cast<int>(l2l_smem)));
+        MLFMA_CK(cudaFuncSetAttribute(t ? k_l2l<R, 16, true> : k_l2l<R, 16, false>, attr, static_cast<int>(l2l_smem)));
+        MLFMA_CK(cudaFuncSetAttribute(t ? k_l2l<R, 24, true> : k_l2l<R, 24, false>, attr, static_cast<int>(l2l_smem)));
+        MLFMA_CK(cudaFuncSetAttribute(t ? k_l2l<R, 32, true> : k_l2l<R, 32, false>, attr, static_cast<int>(l2l_smem)));
+        MLFMA_CK(cudaFuncSetAttribute(t ? k_s2m<R, true> : k_s2m<R, false>, attr, static_cast<int>(s2m_smem)));
+    }
     if (max_rhs_ > 1) {
         // dynamic shared memory up to the opt-in limit less the kernel's static part
         auto dyn = [&](const void* fn) -> cudaError_t {
@@ -498,13 +515,17 @@ int DeviceOp::launches_per_matvec() const {
 }
 
 // stage: -1 all, 0 S2M, 1 M2M, 2 M2L, 3 L2L, 4 L2T.
-template <class R>
+// TR: the transposed far field, Far^T = S2M^T L2L^T M2L^T M2M^T L2T^T, run in
+// the same order with the mirrored kernels: conjugated patterns going up,
+// interpolation with the shift after it (L2L^T), negated translation offsets,
+// anterpolation with the shift after it (M2M^T), plain patterns coming down.
+template <class R, bool TR>
 void DeviceOp::run_far_t(FarField<R>& F, const double2* xt, cudaStream_t s, int stage) {
     using C = typename Cx<R>::T;
     if (n_leaves_ == 0) return;
     if ((stage < 0 || stage == 0) && n_s2m_items_)
-        k_s2m<R><<<n_s2m_items_, kS2MThreads, sizeof(C) * std::max(1, max_src_), s>>>(F.lv_dev, s2m_items_, leaves_,
-                                                                                        F.pat, xt);
+        k_s2m<R, TR><<<n_s2m_items_, kS2MThreads, sizeof(C) * std::max(1, max_src_), s>>>(F.lv_dev, s2m_items_,
+                                                                                            leaves_, F.pat, xt);
     if (stage < 0 || stage == 1)
         for (int p = lmax_ - 1; p >= lmin_; --p) {
             if (npar_[p] == 0) continue;
@@ -513,15 +534,15 @@ void DeviceOp::run_far_t(FarField<R>& F, const double2* xt, cudaStream_t s, int 
             const size_t smem = static_cast<size_t>(8) * rows * nph_[p + 1] * 2 * sizeof(C);
             const DevTransT<R>& T = F.trans[p];
             switch (up_w_[p]) {
-                case 2: k_m2m<R, 2><<<grid, 128, smem, s>>>(F.lv_dev, T, rows); break;
-                case 4: k_m2m<R, 4><<<grid, 128, smem, s>>>(F.lv_dev, T, rows); break;
-                case 6: k_m2m<R, 6><<<grid, 128, smem, s>>>(F.lv_dev, T, rows); break;
-                case 8: k_m2m<R, 8><<<grid, 128, smem, s>>>(F.lv_dev, T, rows); break;
-                default: k_m2m<R, 10><<<grid, 128, smem, s>>>(F.lv_dev, T, rows); break;
+                case 2: k_m2m<R, 2, TR><<<grid, 128, smem, s>>>(F.lv_dev, T, rows); break;
+                case 4: k_m2m<R, 4, TR><<<grid, 128, smem, s>>>(F.lv_dev, T, rows); break;
+                case 6: k_m2m<R, 6, TR><<<grid, 128, smem, s>>>(F.lv_dev, T, rows); break;
+                case 8: k_m2m<R, 8, TR><<<grid, 128, smem, s>>>(F.lv_dev, T, rows); break;
+                default: k_m2m<R, 10, TR><<<grid, 128, smem, s>>>(F.lv_dev, T, rows); break;
             }
         }
     if ((stage < 0 || stage == 2) && n_m2l_items_)
-        k_m2l<R><<<n_m2l_items_, 128, 0, s>>>(F.lv_dev, m2l_items_, ref_compat_ ? 0 : 1);
+        k_m2l<R, TR><<<n_m2l_items_, 128, 0, s>>>(F.lv_dev, m2l_items_, ref_compat_ ? 0 : 1);
     if (stage < 0 || stage == 3)
         for (int p = lmin_; p < lmax_; ++p) {
             const int g = n_l2l_pairs_[p];
@@ -529,20 +550,24 @@ void DeviceOp::run_far_t(FarField<R>& F, const double2* xt, cudaStream_t s, int 
             const size_t smem = static_cast<size_t>(nth_[p]) * nph_[p + 1] * 2 * sizeof(C);
             const DevTransT<R>& T = F.trans[p];
             switch (dn_w_[p]) {
-                case 8: k_l2l<R, 8><<<g, 256, smem, s>>>(F.lv_dev, T, l2l_pairs_[p]); break;
-                case 12: k_l2l<R, 12><<<g, 256, smem, s>>>(F.lv_dev, T, l2l_pairs_[p]); break;
-                case 16: k_l2l<R, 16><<<g, 256, smem, s>>>(F.lv_dev, T, l2l_pairs_[p]); break;
-                case 24: k_l2l<R, 24><<<g, 256, smem, s>>>(F.lv_dev, T, l2l_pairs_[p]); break;
-                default: k_l2l<R, 32><<<g, 256, smem, s>>>(F.lv_dev, T, l2l_pairs_[p]); break;
+                case 8: k_l2l<R, 8, TR><<<g, 256, smem, s>>>(F.lv_dev, T, l2l_pairs_[p]); break;
+                case 12: k_l2l<R, 12, TR><<<g, 256, smem, s>>>(F.lv_dev, T, l2l_pairs_[p]); break;
+                case 16: k_l2l<R, 16, TR><<<g, 256, smem, s>>>(F.lv_dev, T, l2l_pairs_[p]); break;
+                case 24: k_l2l<R, 24, TR><<<g, 256, smem, s>>>(F.lv_dev, T, l2l_pairs_[p]); break;
+                default: k_l2l<R, 32, TR><<<g, 256, smem, s>>>(F.lv_dev, T, l2l_pairs_[p]); break;
             }
         }
     if ((stage < 0 || stage == 4) && n_l2t_items_)
-        k_l2t<R><<<n_l2t_items_, kL2TThreads, 0, s>>>(F.lv_dev, l2t_items_, leaves_, F.pat, yfar_);
+        k_l2t<R, !TR><<<n_l2t_items_, kL2TThreads, 0, s>>>(F.lv_dev, l2t_items_, leaves_, F.pat, yfar_);
 }
 
-void DeviceOp::run_far(const double2* xt, cudaStream_t s, int stage, int prec) {
+void DeviceOp::run_far(const double2* xt, cudaStream_t s, int stage, int prec, bool tr) {
     if (prec < 0) prec = precision_;
-    if (prec == kFp64) run_far_t(f64_, xt, s, stage); else run_far_t(f32_, xt, s, stage);
+    if (prec == kFp64) {
+        if (tr) run_far_t<double, true>(f64_, xt, s, stage); else run_far_t<double, false>(f64_, xt, s, stage);
+    } else {
+        if (tr) run_far_t<float, true>(f32_, xt, s, stage); else run_far_t<float, false>(f32_, xt, s, stage);
+    }
 }
 
 void DeviceOp::run_near(const double2* xt, cudaStream_t s) {
@@ -551,54 +576,85 @@ void DeviceOp::run_near(const double2* xt, cudaStream_t s) {
 }
 
 // The tree-ordered product xt_ -> (yfar_, ynear_): near field on the side
-// stream, far-field chain on s in precision prec.  Captured once per
-// precision into a CUDA graph.
-void DeviceOp::enqueue_core(cudaStream_t s, int prec) {
+// stream, far-field chain on s in precision prec (transposed when tr).
+// Captured once per (precision, direction) into a CUDA graph.  The stored near
+// field is symmetric to rounding (both orientations are assembled from the
+// same symmetric kernel), so the transposed product reuses it.
+void DeviceOp::enqueue_core(cudaStream_t s, int prec, bool tr) {
     cudaMemsetAsync(yfar_, 0, sizeof(double2) * n_, s);
     cudaMemsetAsync(ynear_, 0, sizeof(double2) * n_, s);
     cudaEventRecord(ev_fork_, s);
     cudaStreamWaitEvent(side_, ev_fork_, 0);
     run_near(xt_, side_);
     cudaEventRecord(ev_join_, side_);
-    run_far(xt_, s, -1, prec);
+    run_far(xt_, s, -1, prec, tr);
     cudaStreamWaitEvent(s, ev_join_, 0);
 }
 
-std::string DeviceOp::ensure_graph(int prec) {
-    if (graph_exec_[prec] || !use_graph_) return {};
+std::string DeviceOp::ensure_graph(int prec, bool tr) {
+    const int t = tr ? 1 : 0;
+    if (graph_exec_[prec][t] || !use_graph_) return {};
     MLFMA_CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
-    enqueue_core(stream_, prec);
-    MLFMA_CK(cudaStreamEndCapture(stream_, &graph_[prec]));
-    MLFMA_CK(cudaGraphInstantiate(&graph_exec_[prec], graph_[prec], 0));
+    enqueue_core(stream_, prec, tr);
+    MLFMA_CK(cudaStreamEndCapture(stream_, &graph_[prec][t]));
+    MLFMA_CK(cudaGraphInstantiate(&graph_exec_[prec][t], graph_[prec][t], 0));
     return {};
 }
 
-void DeviceOp::apply_tree(const double2* xt, double2* yt, cudaStream_t s, int prec) {
-    if (prec < 0) prec = precision_;
-    if (!ensure_graph(prec).empty()) use_graph_ = false;
-    if (xt != xt_) cudaMemcpyAsync(xt_, xt, sizeof(double2) * n_, cudaMemcpyDeviceToDevice, s);
-    if (graph_exec_[prec]) cudaGraphLaunch(graph_exec_[prec], s); else enqueue_core(s, prec);
-    k_finish<<<blocks_for(n_, 256), 256, 0, s>>>(yfar_, ynear_, nullptr, yt, n_, ck_, 0);
+void DeviceOp::launch_core(cudaStream_t s, int prec, bool tr) {
+    const int t = tr ? 1 : 0;
+    if (graph_exec_[prec][t]) cudaGraphLaunch(graph_exec_[prec][t], s); else enqueue_core(s, prec, tr);
 }
 
-void DeviceOp::apply_tree_direct(const double2* xt, double2* yt, cudaStream_t s, int prec) {
-    if (prec < 0) prec = precision_;
-    if (xt != xt_) cudaMemcpyAsync(xt_, xt, sizeof(double2) * n_, cudaMemcpyDeviceToDevice, s);
-    if (graph_exec_[prec]) cudaGraphLaunch(graph_exec_[prec], s); else enqueue_core(s, prec);
-    k_finish<<<blocks_for(n_, 256), 256, 0, s>>>(yfar_, ynear_, nullptr, yt, n_, ck_, 0);
+std::string DeviceOp::set_loads(const double2* z_user) {
+    if (!ready_) return "operator not set up";
+    MLFMA_CK(cudaSetDevice(device_));
+    if (!z_user) {
+        has_loads_ = false;
+        return {};
+    }
+    if (!loads_) loads_ = alloc<double2>(n_);
+    MLFMA_CK(cudaMemcpy(yt_, z_user, sizeof(double2) * n_, cudaMemcpyHostToDevice));
+    k_gather<<<blocks_for(n_, 256), 256, 0, stream_>>>(yt_, perm_, loads_, n_, 0);
+    MLFMA_CK(cudaStreamSynchronize(stream_));
+    has_loads_ = true;
+    return {};
 }
 
-std::string DeviceOp::matvec_device(const double2* x, double2* y, bool accumulate, cudaStream_t stream, int prec) {
+// Tree-ordered y = A x (adj: y = A^H x = conj(A^T conj(x))), loads included.
+void DeviceOp::apply_tree(const double2* xt, double2* yt, cudaStream_t s, int prec, bool adj) {
+    if (prec < 0) prec = precision_;
+    if (!ensure_graph(prec, adj).empty()) use_graph_ = false;
+    if (adj) k_conj_copy<<<blocks_for(n_, 256), 256, 0, s>>>(xt, xt_, n_);
+    else if (xt != xt_) cudaMemcpyAsync(xt_, xt, sizeof(double2) * n_, cudaMemcpyDeviceToDevice, s);
+    launch_core(s, prec, adj);
+    k_finish<<<blocks_for(n_, 256), 256, 0, s>>>(yfar_, ynear_, nullptr, yt, n_, ck_, 0, xt_,
+                                                 has_loads_ ? loads_ : nullptr, adj ? 1 : 0);
+}
+
+void DeviceOp::apply_tree_direct(const double2* xt, double2* yt, cudaStream_t s, int prec, bool adj) {
+    if (prec < 0) prec = precision_;
+    if (adj) k_conj_copy<<<blocks_for(n_, 256), 256, 0, s>>>(xt, xt_, n_);
+    else if (xt != xt_) cudaMemcpyAsync(xt_, xt, sizeof(double2) * n_, cudaMemcpyDeviceToDevice, s);
+    launch_core(s, prec, adj);
+    k_finish<<<blocks_for(n_, 256), 256, 0, s>>>(yfar_, ynear_, nullptr, yt, n_, ck_, 0, xt_,
+                                                 has_loads_ ? loads_ : nullptr, adj ? 1 : 0);
+}
+
+std::string DeviceOp::matvec_device(const double2* x, double2* y, bool accumulate, cudaStream_t stream, int prec,
+                                    bool adj) {
     if (!ready_) return "operator not set up";
     if (prec < 0) prec = precision_;
     if (prec != kFp64 && precision_ == kFp64) return "the FP64 operator has no mixed far field";
+    if (adj && ref_compat_) return "arg:the adjoint needs ref_compat = 0 (the reference's rule keeps state between products)";
     cudaStream_t s = stream ? stream : stream_;
     MLFMA_CK(cudaSetDevice(device_));
-    std::string e = ensure_graph(prec);
+    std::string e = ensure_graph(prec, adj);
     if (!e.empty()) return e;
-    k_gather<<<blocks_for(n_, 256), 256, 0, s>>>(x, perm_, xt_, n_);
-    if (graph_exec_[prec]) cudaGraphLaunch(graph_exec_[prec], s); else enqueue_core(s, prec);
-    k_finish<<<blocks_for(n_, 256), 256, 0, s>>>(yfar_, ynear_, perm_, y, n_, ck_, accumulate ? 1 : 0);
+    k_gather<<<blocks_for(n_, 256), 256, 0, s>>>(x, perm_, xt_, n_, adj ? 1 : 0);
+    launch_core(s, prec, adj);
+    k_finish<<<blocks_for(n_, 256), 256, 0, s>>>(yfar_, ynear_, perm_, y, n_, ck_, accumulate ? 1 : 0, xt_,
+                                                 has_loads_ ? loads_ : nullptr, adj ? 1 : 0);
     MLFMA_CK(cudaGetLastError());
     return {};
 }
@@ -619,7 +675,7 @@ std::string DeviceOp::time_stages(StageTimes* out) {
     }
     run_near(xt_, s);
     cudaEventRecord(ev[7], s);
-    k_finish<<<blocks_for(n_, 256), 256, 0, s>>>(yfar_, ynear_, nullptr, yt_, n_, ck_, 0);
+    k_finish<<<blocks_for(n_, 256), 256, 0, s>>>(yfar_, ynear_, nullptr, yt_, n_, ck_, 0, xt_, nullptr, 0);
     cudaEventRecord(ev[8], s);
     MLFMA_CK(cudaEventSynchronize(ev[8]));
     float t[8];
@@ -643,6 +699,22 @@ std::string DeviceOp::farfield(const double2* cur, int ndir, const double* khat,
     if (ndir <= 0) return {};
     MLFMA_CK(cudaSetDevice(device_));
     k_farfield<<<ndir, kFarThreads, 0, s>>>(src_, perm_, cur, n_, khat, ck_, out);
+    MLFMA_CK(cudaGetLastError());
+    return {};
+}
+
+std::string DeviceOp::farfield_adjoint(const double2* F, int ndir, const double* khat, double2* g, cudaStream_t s) {
+    if (!ready_) return "operator not set up";
+    MLFMA_CK(cudaSetDevice(device_));
+    if (ndir <= 0) {
+        MLFMA_CK(cudaMemsetAsync(g, 0, sizeof(double2) * n_, s));
+        return {};
+    }
+    double2* PF = nullptr;
+    MLFMA_CK(cudaMallocAsync(&PF, sizeof(double2) * 3 * ndir, s));
+    k_project<<<blocks_for(ndir, 128), 128, 0, s>>>(khat, F, ndir, PF);
+    k_farfield_adj<<<blocks_for(n_, 128), 128, 0, s>>>(src_, perm_, n_, khat, PF, ndir, ck_, g);
+    MLFMA_CK(cudaFreeAsync(PF, s));
     MLFMA_CK(cudaGetLastError());
     return {};
 }
@@ -864,7 +936,8 @@ std::string DeviceOp::matvec_multi_device(const double2* x, double2* y, int nr, 
     const long long tot = static_cast<long long>(n_) * nr;
     k_gather_m<<<blocks_for(tot, 256), 256, 0, s>>>(x, perm_, xtm_, n_, nr);
     enqueue_multi(nr, s, prec);
-    k_finish_m<<<blocks_for(tot, 256), 256, 0, s>>>(yfarm_, ynearm_, perm_, y, n_, nr, ck_, accumulate ? 1 : 0);
+    k_finish_m<<<blocks_for(tot, 256), 256, 0, s>>>(yfarm_, ynearm_, perm_, y, n_, nr, ck_, accumulate ? 1 : 0, xtm_,
+                                                     has_loads_ ? loads_ : nullptr);
     MLFMA_CK(cudaGetLastError());
     return {};
 }
@@ -874,7 +947,8 @@ void DeviceOp::apply_tree_multi(const double2* xt, double2* yt, int nr, cudaStre
     const long long tot = static_cast<long long>(n_) * nr;
     if (xt != xtm_) cudaMemcpyAsync(xtm_, xt, sizeof(double2) * tot, cudaMemcpyDeviceToDevice, s);
     enqueue_multi(nr, s, prec);
-    k_finish_m<<<blocks_for(tot, 256), 256, 0, s>>>(yfarm_, ynearm_, nullptr, yt, n_, nr, ck_, 0);
+    k_finish_m<<<blocks_for(tot, 256), 256, 0, s>>>(yfarm_, ynearm_, nullptr, yt, n_, nr, ck_, 0, xtm_,
+                                                     has_loads_ ? loads_ : nullptr);
 }
 
 std::string DeviceOp::time_stages_multi(int nr, StageTimes* out) {
@@ -896,7 +970,7 @@ std::string DeviceOp::time_stages_multi(int nr, StageTimes* out) {
     run_near_multi(nr, s);
     cudaEventRecord(ev[7], s);
     const long long tot = static_cast<long long>(n_) * nr;
-    k_finish_m<<<blocks_for(tot, 256), 256, 0, s>>>(yfarm_, ynearm_, nullptr, ytm_, n_, nr, ck_, 0);
+    k_finish_m<<<blocks_for(tot, 256), 256, 0, s>>>(yfarm_, ynearm_, nullptr, ytm_, n_, nr, ck_, 0, xtm_, nullptr);
     cudaEventRecord(ev[8], s);
     MLFMA_CK(cudaEventSynchronize(ev[8]));
     float t[8];

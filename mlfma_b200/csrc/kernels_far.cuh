@@ -25,7 +25,9 @@ constexpr int kS2MThreads = 352;
 constexpr int kL2TThreads = 256;
 constexpr int kL2TSrcPerBlock = kL2TThreads / 32;
 
-template <class R>
+// CJ: conjugated patterns, a_B[e] = sum_n x_n conj(R_n[e]) -- the transpose of
+// L2T, first stage of the transposed product.
+template <class R, bool CJ>
 __global__ void __launch_bounds__(kS2MThreads)
 k_s2m(const DevLevelT<R>* __restrict__ lvs, const int4* __restrict__ items, const DevFarLeaf* __restrict__ leaves,
       const typename Cx<R>::T* __restrict__ pat, const double2* __restrict__ x) {
@@ -47,16 +49,30 @@ k_s2m(const DevLevelT<R>* __restrict__ lvs, const int4* __restrict__ items, cons
         C v[8];
 #pragma unroll
         for (int u = 0; u < 8; ++u) v[u] = ldg_stream(r + static_cast<size_t>(s + u) * ne);
-        a0 = cfma(xs[s], v[0], a0);
-        a1 = cfma(xs[s + 1], v[1], a1);
-        a2 = cfma(xs[s + 2], v[2], a2);
-        a3 = cfma(xs[s + 3], v[3], a3);
-        a0 = cfma(xs[s + 4], v[4], a0);
-        a1 = cfma(xs[s + 5], v[5], a1);
-        a2 = cfma(xs[s + 6], v[6], a2);
-        a3 = cfma(xs[s + 7], v[7], a3);
+        if (CJ) {
+            a0 = cjfma(v[0], xs[s], a0);
+            a1 = cjfma(v[1], xs[s + 1], a1);
+            a2 = cjfma(v[2], xs[s + 2], a2);
+            a3 = cjfma(v[3], xs[s + 3], a3);
+            a0 = cjfma(v[4], xs[s + 4], a0);
+            a1 = cjfma(v[5], xs[s + 5], a1);
+            a2 = cjfma(v[6], xs[s + 6], a2);
+            a3 = cjfma(v[7], xs[s + 7], a3);
+        } else {
+            a0 = cfma(xs[s], v[0], a0);
+            a1 = cfma(xs[s + 1], v[1], a1);
+            a2 = cfma(xs[s + 2], v[2], a2);
+            a3 = cfma(xs[s + 3], v[3], a3);
+            a0 = cfma(xs[s + 4], v[4], a0);
+            a1 = cfma(xs[s + 5], v[5], a1);
+            a2 = cfma(xs[s + 6], v[6], a2);
+            a3 = cfma(xs[s + 7], v[7], a3);
+        }
     }
-    for (; s < lf.nsrc; ++s) a0 = cfma(xs[s], ldg_stream(r + static_cast<size_t>(s) * ne), a0);
+    for (; s < lf.nsrc; ++s) {
+        const C v = ldg_stream(r + static_cast<size_t>(s) * ne);
+        a0 = CJ ? cjfma(v, xs[s], a0) : cfma(xs[s], v, a0);
+    }
     A[e] = cadd(cadd(a0, a1), cadd(a2, a3));
 }
 
@@ -65,7 +81,9 @@ k_s2m(const DevLevelT<R>* __restrict__ lvs, const int4* __restrict__ items, cons
 // C k is applied when the result is written out).  One block per work item
 // (leaf, run of up to eight sources), one warp per source, eight loads in
 // flight per lane; the sum is widened to complex double on output.
-template <class R>
+// CJ = false: plain patterns, y_m = sum_e R_m[e] b_B[e] -- the transpose of S2M,
+// last stage of the transposed product.
+template <class R, bool CJ>
 __global__ void __launch_bounds__(kL2TThreads)
 k_l2t(const DevLevelT<R>* __restrict__ lvs, const int4* __restrict__ items, const DevFarLeaf* __restrict__ leaves,
       const typename Cx<R>::T* __restrict__ pat, double2* __restrict__ yfar) {
@@ -84,16 +102,27 @@ k_l2t(const DevLevelT<R>* __restrict__ lvs, const int4* __restrict__ items, cons
         C v[8];
 #pragma unroll
         for (int u = 0; u < 8; ++u) v[u] = ldg_stream(r + e + 32 * u);
-        a0 = cjfma(v[0], Bb[e], a0);
-        a1 = cjfma(v[1], Bb[e + 32], a1);
-        a2 = cjfma(v[2], Bb[e + 64], a2);
-        a3 = cjfma(v[3], Bb[e + 96], a3);
-        a0 = cjfma(v[4], Bb[e + 128], a0);
-        a1 = cjfma(v[5], Bb[e + 160], a1);
-        a2 = cjfma(v[6], Bb[e + 192], a2);
-        a3 = cjfma(v[7], Bb[e + 224], a3);
+        if (CJ) {
+            a0 = cjfma(v[0], Bb[e], a0);
+            a1 = cjfma(v[1], Bb[e + 32], a1);
+            a2 = cjfma(v[2], Bb[e + 64], a2);
+            a3 = cjfma(v[3], Bb[e + 96], a3);
+            a0 = cjfma(v[4], Bb[e + 128], a0);
+            a1 = cjfma(v[5], Bb[e + 160], a1);
+            a2 = cjfma(v[6], Bb[e + 192], a2);
+            a3 = cjfma(v[7], Bb[e + 224], a3);
+        } else {
+            a0 = cfma(v[0], Bb[e], a0);
+            a1 = cfma(v[1], Bb[e + 32], a1);
+            a2 = cfma(v[2], Bb[e + 64], a2);
+            a3 = cfma(v[3], Bb[e + 96], a3);
+            a0 = cfma(v[4], Bb[e + 128], a0);
+            a1 = cfma(v[5], Bb[e + 160], a1);
+            a2 = cfma(v[6], Bb[e + 192], a2);
+            a3 = cfma(v[7], Bb[e + 224], a3);
+        }
     }
-    for (; e < ne; e += 32) a0 = cjfma(ldg_stream(r + e), Bb[e], a0);
+    for (; e < ne; e += 32) a0 = CJ ? cjfma(ldg_stream(r + e), Bb[e], a0) : cfma(ldg_stream(r + e), Bb[e], a0);
     const C acc = warp_sum(cadd(cadd(a0, a1), cadd(a2, a3)));
     if (lane == 0) yfar[lf.src0 + s] = to_d2(acc);
 }
@@ -105,7 +134,10 @@ k_l2t(const DevLevelT<R>* __restrict__ lvs, const int4* __restrict__ items, cons
 // Block = (parent, tile of `rows` parent theta rows).  Phase 1 computes the
 // theta pass of every child into shared memory at once (all loads
 // independent); phase 2 forms each parent output from the children's rows.
-template <class R, int W>  // taps per row: 2 * interp_order (both passes)
+// POST: the transposed L2L -- no shift before the theta pass; each child's
+// interpolated pattern is multiplied by the parent-grid shift of its octant
+// (shift_down of the parent level) before the sum over children.
+template <class R, int W, bool POST>  // taps per row: 2 * interp_order (both passes)
 __global__ void __launch_bounds__(128)
 k_m2m(const DevLevelT<R>* __restrict__ lvs, DevTransT<R> T, int rows) {
     using C = typename Cx<R>::T;
@@ -134,9 +166,14 @@ k_m2m(const DevLevelT<R>* __restrict__ lvs, DevTransT<R> T, int rows) {
             const int sp = rf ? (iph < halfm ? iph + halfm : iph - halfm) : iph;
             const R cf = T.up_th.coef[q];
             const int d = T.up_th.src[q] * mph + sp;
-            const C ph = sh[d];
-            v0 = crfma(cf, cmul(ph, Ac[2 * d]), v0);
-            v1 = crfma(cf, cmul(ph, Ac[2 * d + 1]), v1);
+            if (POST) {
+                v0 = crfma(cf, Ac[2 * d], v0);
+                v1 = crfma(cf, Ac[2 * d + 1], v1);
+            } else {
+                const C ph = sh[d];
+                v0 = crfma(cf, cmul(ph, Ac[2 * d]), v0);
+                v1 = crfma(cf, cmul(ph, Ac[2 * d + 1]), v1);
+            }
         }
         sm[2 * it] = v0;
         sm[2 * it + 1] = v1;
@@ -148,13 +185,28 @@ k_m2m(const DevLevelT<R>* __restrict__ lvs, DevTransT<R> T, int rows) {
         C a0 = zero<C>(), a1 = zero<C>();
         for (int c = 0; c < nch; ++c) {
             const C* row = sm + (static_cast<size_t>(c) * per_child + static_cast<size_t>(jr) * mph) * 2;
+            if (POST) {
+                C t0 = zero<C>(), t1 = zero<C>();
 #pragma unroll
-            for (int k = 0; k < W; ++k) {
-                const int q = jph * W + k;
-                const int s = T.up_ph.src[q];
-                const R cf = T.up_ph.coef[q];
-                a0 = crfma(cf, row[2 * s], a0);
-                a1 = crfma(cf, row[2 * s + 1], a1);
+                for (int k = 0; k < W; ++k) {
+                    const int q = jph * W + k;
+                    const int s = T.up_ph.src[q];
+                    const R cf = T.up_ph.coef[q];
+                    t0 = crfma(cf, row[2 * s], t0);
+                    t1 = crfma(cf, row[2 * s + 1], t1);
+                }
+                const C ph = P.shift_down[static_cast<size_t>(T.child_oct[c0 + c]) * P.ndir + (r0 + jr) * nph + jph];
+                a0 = cfma(ph, t0, a0);
+                a1 = cfma(ph, t1, a1);
+            } else {
+#pragma unroll
+                for (int k = 0; k < W; ++k) {
+                    const int q = jph * W + k;
+                    const int s = T.up_ph.src[q];
+                    const R cf = T.up_ph.coef[q];
+                    a0 = crfma(cf, row[2 * s], a0);
+                    a1 = crfma(cf, row[2 * s + 1], a1);
+                }
             }
         }
         Ap[2 * o] = a0;
@@ -167,7 +219,11 @@ k_m2m(const DevLevelT<R>* __restrict__ lvs, DevTransT<R> T, int rows) {
 // (Node::buildMpoleToLocalCoeffs, src/fmm/node.cpp:105-134).  One block per
 // (level, box, direction chunk) item, all levels in one launch; four list
 // entries in flight per thread.
-template <class R>
+// TR: the transposed translation, T(c_S - c_B) in place of T(c_B - c_S): the
+// negated offset, id 315 - id in the order of Math::getINodeDistVecs (the
+// offset set is symmetric and listed lexicographically).  Lists 2 are
+// symmetric, so the same lists serve.
+template <class R, bool TR>
 __global__ void __launch_bounds__(128)
 k_m2l(const DevLevelT<R>* __restrict__ lvs, const int4* __restrict__ items, int zero_empty) {
     using C = typename Cx<R>::T;
@@ -186,7 +242,10 @@ k_m2l(const DevLevelT<R>* __restrict__ lvs, const int4* __restrict__ items, int 
     for (; p + 4 <= p1; p += 4) {
         int sb[4], ob[4];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) { sb[u] = lv.m2l_src[p + u]; ob[u] = lv.m2l_off[p + u]; }
+        for (int u = 0; u < 4; ++u) {
+            sb[u] = lv.m2l_src[p + u];
+            ob[u] = TR ? 315 - lv.m2l_off[p + u] : lv.m2l_off[p + u];
+        }
         C t[4], xa[4], xb[4];
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
@@ -205,7 +264,7 @@ k_m2l(const DevLevelT<R>* __restrict__ lvs, const int4* __restrict__ items, int 
         c1 = cfma(t[3], xb[3], c1);
     }
     for (; p < p1; ++p) {
-        const int s0 = lv.m2l_src[p], o0 = lv.m2l_off[p];
+        const int s0 = lv.m2l_src[p], o0 = TR ? 315 - lv.m2l_off[p] : lv.m2l_off[p];
         const C t0 = lv.transl[static_cast<size_t>(o0) * ndir + d];
         const C* A0 = lv.A + (static_cast<size_t>(s0) * ndir + d) * 2;
         a0 = cfma(t0, A0[0], a0);
@@ -222,7 +281,10 @@ k_m2l(const DevLevelT<R>* __restrict__ lvs, const int4* __restrict__ items, int 
 // reflection (Stem::getShiftedLocalCoeffs and addAnterpCoeffs,
 // src/fmm/stem.cpp:109-244).  One block per (parent, child) pair; the
 // pair list already omits parents that pass nothing down.
-template <class R, int W>  // both transposed stencils padded to W taps per row
+// POST: the transposed M2M -- no shift before the phi pass; the anterpolated
+// pattern is multiplied by the child-grid shift of the child's octant
+// (shift_up of the child level) as it is added to the child.
+template <class R, int W, bool POST>  // both transposed stencils padded to W taps per row
 __global__ void __launch_bounds__(256)
 k_l2l(const DevLevelT<R>* __restrict__ lvs, DevTransT<R> T, const int2* __restrict__ pairs) {
     using C = typename Cx<R>::T;
@@ -242,9 +304,14 @@ k_l2l(const DevLevelT<R>* __restrict__ lvs, DevTransT<R> T, const int2* __restri
             const int q = jph * W + k;
             const int d = ith * pph + T.dn_ph.src[q];
             const R cf = T.dn_ph.coef[q];
-            const C ph = sh[d];
-            v0 = crfma(cf, cmul(ph, Bp[2 * d]), v0);
-            v1 = crfma(cf, cmul(ph, Bp[2 * d + 1]), v1);
+            if (POST) {
+                v0 = crfma(cf, Bp[2 * d], v0);
+                v1 = crfma(cf, Bp[2 * d + 1], v1);
+            } else {
+                const C ph = sh[d];
+                v0 = crfma(cf, cmul(ph, Bp[2 * d]), v0);
+                v1 = crfma(cf, cmul(ph, Bp[2 * d + 1]), v1);
+            }
         }
         sm[2 * e] = v0;
         sm[2 * e + 1] = v1;
@@ -263,6 +330,11 @@ k_l2l(const DevLevelT<R>* __restrict__ lvs, DevTransT<R> T, const int2* __restri
             const C* row = sm + (static_cast<size_t>(T.dn_th.src[q]) * cph + sp) * 2;
             v0 = crfma(cf, row[0], v0);
             v1 = crfma(cf, row[1], v1);
+        }
+        if (POST) {
+            const C ph = Cl.shift_up[static_cast<size_t>(T.child_oct[pc.y]) * Cl.ndir + e];
+            v0 = cmul(ph, v0);
+            v1 = cmul(ph, v1);
         }
         Bc[2 * e] = cadd(Bc[2 * e], v0);
         Bc[2 * e + 1] = cadd(Bc[2 * e + 1], v1);

@@ -436,14 +436,16 @@ __global__ void k_gather_m(const double2* __restrict__ x, const int* __restrict_
     xt[i] = x[static_cast<size_t>(r) * n + perm[t]];
 }
 
-// y[r][perm[t]] (+)= ck (yfar[t][r] + ynear[t][r]); perm == nullptr: tree order, rhs innermost.
+// y[r][perm[t]] (+)= ck (yfar[t][r] + ynear[t][r]) + loads[t] xt[t][r] (loads may
+// be null); perm == nullptr: tree order, rhs innermost.
 __global__ void k_finish_m(const double2* __restrict__ yfar, const double2* __restrict__ ynear,
                            const int* __restrict__ perm, double2* __restrict__ y, int n, int nr, double2 ck,
-                           int accumulate) {
+                           int accumulate, const double2* __restrict__ xt, const double2* __restrict__ loads) {
     const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= static_cast<long long>(n) * nr) return;
     const int t = static_cast<int>(i / nr), r = static_cast<int>(i - static_cast<long long>(t) * nr);
-    const double2 v = cmul(ck, cadd(yfar[i], ynear[i]));
+    double2 v = cmul(ck, cadd(yfar[i], ynear[i]));
+    if (loads) v = cfma(loads[t], xt[i], v);
     const size_t o = perm ? static_cast<size_t>(r) * n + perm[t] : static_cast<size_t>(i);
     y[o] = accumulate ? cadd(y[o], v) : v;
 }

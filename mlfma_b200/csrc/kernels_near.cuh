@@ -191,6 +191,46 @@ k_farfield(DevSources S, const int* __restrict__ perm, const double2* __restrict
     }
 }
 
+// Adjoint of the far-field map: g = M^H F for F (ndir x 3) along unit
+// directions khat, M the linear map of k_farfield (currents -> far field):
+//   g_n = conj(C k) sum_d conj(f_n(k khat_d)) . (I - khat_d khat_d^T) F_d,
+// written in caller order.  PF holds the projected F_d (ndir x 3), formed
+// first by k_project.  One thread per unknown.  No counterpart in the
+// reference (the far-field power gradient uses it).
+__global__ void k_project(const double* __restrict__ khat, const double2* __restrict__ F, int ndir,
+                          double2* __restrict__ PF) {
+    const int d = blockIdx.x * blockDim.x + threadIdx.x;
+    if (d >= ndir) return;
+    const double* kh = khat + 3 * d;
+    const double2* v = F + 3 * d;
+    const double pr = kh[0] * v[0].x + kh[1] * v[1].x + kh[2] * v[2].x;
+    const double pi = kh[0] * v[0].y + kh[1] * v[1].y + kh[2] * v[2].y;
+    for (int a = 0; a < 3; ++a) PF[3 * d + a] = make_double2(v[a].x - kh[a] * pr, v[a].y - kh[a] * pi);
+}
+
+__global__ void k_farfield_adj(DevSources S, const int* __restrict__ perm, int n, const double* __restrict__ khat,
+                               const double2* __restrict__ PF, int ndir, double2 ck, double2* __restrict__ g) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    zd acc = mkz(0);
+    for (int d = 0; d < ndir; ++d) {
+        const double kr[3] = {khat[3 * d] * S.k, khat[3 * d + 1] * S.k, khat[3 * d + 2] * S.k};
+        zd cf[3];  // conj(f_t(k khat_d))
+        if (S.kind == kDipole) {
+            const zd ph = expi(dot3(S.pos + 3 * t, kr));
+            for (int a = 0; a < 3; ++a) cf[a] = ph * S.phat[3 * t + a];
+        } else {
+            rwg_plane_wave_integral(S.rwg[t], S.tris, kr, cf);  // f = conj(I)
+        }
+        for (int a = 0; a < 3; ++a) {
+            const double2 p = PF[3 * d + a];
+            acc += cf[a] * zd{p.x, p.y};
+        }
+    }
+    const zd r = zd{ck.x, -ck.y} * acc;
+    g[perm[t]] = make_double2(r.x, r.y);
+}
+
 // Entries of the block rows: thread per entry.
 __global__ void k_near_rows_assemble(const DevNearRow* __restrict__ rows, int nrows, long long total,
                                      const int* __restrict__ cols, DevSources S, double2* __restrict__ Z) {
