@@ -786,6 +786,7 @@ std::string DeviceOp::setup_multi(const Plan& plan) {
     std::vector<int2> items;
     for (int l = lmin_; l <= lmax_; ++l) {
         const Level& L = plan.levels[l];
+        const int level_first = static_cast<int>(groups.size());
         std::vector<int> order(L.boxes.size());
         for (size_t b = 0; b < order.size(); ++b) order[b] = static_cast<int>(b);
         std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
@@ -832,13 +833,14 @@ std::string DeviceOp::setup_multi(const Plan& plan) {
                                 L.transl[static_cast<size_t>(o) * L.ndir + d] * L.m2l_w[d];
                     }
             const bool all_empty = g.empty_mask == (1 << g.ntgt) - 1;
-            if (!(all_empty && ref_compat_)) {
-                const int gi = static_cast<int>(groups.size());
-                for (int d = 0; d < L.ndir; ++d) items.push_back(make_int2(gi, d));
-                groups.push_back(g);
-            }
+            if (!(all_empty && ref_compat_)) groups.push_back(g);
             i = j;
         }
+        // Items direction-major: the blocks in flight together all read the
+        // patterns of one direction (2 KB per box at 64 rhs), which stay in
+        // L2 for every group that needs them.
+        for (int d = 0; d < L.ndir; ++d)
+            for (int gi = level_first; gi < static_cast<int>(groups.size()); ++gi) items.push_back(make_int2(gi, d));
     }
     m2l_groups_ = upload(groups);
     m2l_cand_src_ = upload(cand_src);
