@@ -216,6 +216,7 @@ private:
     void run_near_multi(int nr, cudaStream_t s);
     void enqueue_multi(int nr, cudaStream_t s, int prec);  // xtm_ -> yfarm_, ynearm_
     std::string setup_multi(const Plan& plan);
+    std::string build_m2l_groups(const Plan& plan);
     std::string ensure_graph(int prec, bool tr);
     static int m2m_rows(int nth, int nph);
 
@@ -274,7 +275,9 @@ private:
     int n_l2t_items_m_ = 0;
     int2* near_items_m_ = nullptr;
     int n_near_items_m_ = 0;
-    DevM2LGroup* m2l_groups_ = nullptr;
+    DevM2LGroup* m2l_groups_ = nullptr;   // M2L sibling groups (many-rhs path)
+    std::vector<DevM2LGroup> h_groups_;
+    std::vector<short> h_cand_off_;        // [candidate][kMaxGroup] offset ids (-1: none)
     int* m2l_cand_src_ = nullptr;
     int2* m2l_items_m_ = nullptr;
     int n_m2l_items_m_ = 0;

@@ -488,6 +488,8 @@ std::string DeviceOp::setup(const Plan& plan, int device, int precision, int max
         traffic_.near = near_entries_ * 16.0 + n_ * 16.0 * 2.0;
         traffic_.total = traffic_.s2m + traffic_.m2m + traffic_.m2l + traffic_.l2l + traffic_.l2t + traffic_.near;
         if (max_rhs_ > 1) {
+            err = build_m2l_groups(plan);
+            if (!err.empty()) return err;
             err = setup_multi(plan);
             if (!err.empty()) return err;
         }
@@ -779,14 +781,53 @@ std::string DeviceOp::setup_multi(const Plan& plan) {
         for (int r0 = 0; r0 < plan.near_rows[i].nrow; r0 += kBM) nit.push_back(make_int2(static_cast<int>(i), r0));
     n_near_items_m_ = static_cast<int>(nit.size());
     near_items_m_ = upload(nit);
-    // M2L sibling groups: boxes of a level grouped by parent node.
-    std::vector<DevM2LGroup> groups;
-    std::vector<int> cand_src;
-    std::vector<cplx> t8;  // [group][direction][candidate][kMaxGroup], weights folded in
+    // Many-rhs M2L: weighted transfer values per (group, direction, candidate,
+    // target), and direction-major items (the blocks in flight together all
+    // read the patterns of one direction, 2 KB per box at 64 rhs, which stay
+    // in L2 for every group that needs them).
+    std::vector<cplx> t8;
     std::vector<int2> items;
     for (int l = lmin_; l <= lmax_; ++l) {
         const Level& L = plan.levels[l];
-        const int level_first = static_cast<int>(groups.size());
+        std::vector<int> gl;
+        for (size_t gi = 0; gi < h_groups_.size(); ++gi)
+            if (h_groups_[gi].level == l) gl.push_back(static_cast<int>(gi));
+        for (int gi : gl) {
+            DevM2LGroup& g = h_groups_[gi];
+            g.t8_off = static_cast<long long>(t8.size());
+            t8.resize(t8.size() + static_cast<size_t>(L.ndir) * g.ncand * kMaxGroup, cplx(0));
+            for (int d = 0; d < L.ndir; ++d)
+                for (int c = 0; c < g.ncand; ++c)
+                    for (int t = 0; t < kMaxGroup; ++t) {
+                        const int o = h_cand_off_[(static_cast<size_t>(g.cand0) + c) * kMaxGroup + t];
+                        if (o >= 0)
+                            t8[g.t8_off + (static_cast<size_t>(d) * g.ncand + c) * kMaxGroup + t] =
+                                L.transl[static_cast<size_t>(o) * L.ndir + d] * L.m2l_w[d];
+                    }
+        }
+        for (int d = 0; d < L.ndir; ++d)
+            for (int gi : gl) items.push_back(make_int2(gi, d));
+    }
+    MLFMA_CK(cudaMemcpy(m2l_groups_, h_groups_.data(), sizeof(DevM2LGroup) * h_groups_.size(), cudaMemcpyHostToDevice));
+    f64_.m2l_t8 = upload(conv_c<double2>(t8));
+    if (precision_ != kFp64) f32_.m2l_t8 = upload(conv_c<float2>(t8));
+    n_m2l_items_m_ = static_cast<int>(items.size());
+    m2l_items_m_ = upload(items);
+    return {};
+}
+
+// M2L sibling groups of the many-rhs path: the boxes of a level that share a
+// parent node (at most 8) and the union of their list-2 sources, with each
+// candidate's offset id towards every target (-1: not in that target's list 2).
+// (A one-vector M2L over the same groups measured slower than the per-box
+// kernel k_m2l: 59 against 58 us in FP64, 55 against 37 us mixed, on the
+// r = 2 lambda sphere; its few, register-heavy blocks do not hide latency.)
+std::string DeviceOp::build_m2l_groups(const Plan& plan) {
+    h_groups_.clear();
+    h_cand_off_.clear();
+    std::vector<int> cand_src;
+    for (int l = lmin_; l <= lmax_; ++l) {
+        const Level& L = plan.levels[l];
         std::vector<int> order(L.boxes.size());
         for (size_t b = 0; b < order.size(); ++b) order[b] = static_cast<int>(b);
         std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
@@ -820,34 +861,19 @@ std::string DeviceOp::setup_multi(const Plan& plan) {
                     offs[c][t] = static_cast<short>(L.m2l_off[q]);
                 }
             }
-            g.ncand = static_cast<int>(cands.size());
-            for (size_t c = 0; c < cands.size(); ++c) cand_src.push_back(cands[c]);
-            g.t8_off = static_cast<long long>(t8.size());
-            t8.resize(t8.size() + static_cast<size_t>(L.ndir) * g.ncand * kMaxGroup, cplx(0));
-            for (int d = 0; d < L.ndir; ++d)
-                for (int c = 0; c < g.ncand; ++c)
-                    for (int t = 0; t < kMaxGroup; ++t) {
-                        const int o = offs[c][t];
-                        if (o >= 0)
-                            t8[g.t8_off + (static_cast<size_t>(d) * g.ncand + c) * kMaxGroup + t] =
-                                L.transl[static_cast<size_t>(o) * L.ndir + d] * L.m2l_w[d];
-                    }
-            const bool all_empty = g.empty_mask == (1 << g.ntgt) - 1;
-            if (!(all_empty && ref_compat_)) groups.push_back(g);
             i = j;
+            const bool all_empty = g.empty_mask == (1 << g.ntgt) - 1;
+            if (all_empty && ref_compat_) continue;  // nothing written (node.cpp:106-108)
+            g.ncand = static_cast<int>(cands.size());
+            for (size_t c = 0; c < cands.size(); ++c) {
+                cand_src.push_back(cands[c]);
+                h_cand_off_.insert(h_cand_off_.end(), offs[c].begin(), offs[c].end());
+            }
+            h_groups_.push_back(g);
         }
-        // Items direction-major: the blocks in flight together all read the
-        // patterns of one direction (2 KB per box at 64 rhs), which stay in
-        // L2 for every group that needs them.
-        for (int d = 0; d < L.ndir; ++d)
-            for (int gi = level_first; gi < static_cast<int>(groups.size()); ++gi) items.push_back(make_int2(gi, d));
     }
-    m2l_groups_ = upload(groups);
+    m2l_groups_ = upload(h_groups_);
     m2l_cand_src_ = upload(cand_src);
-    f64_.m2l_t8 = upload(conv_c<double2>(t8));
-    if (precision_ != kFp64) f32_.m2l_t8 = upload(conv_c<float2>(t8));
-    n_m2l_items_m_ = static_cast<int>(items.size());
-    m2l_items_m_ = upload(items);
     return {};
 }
 
