@@ -289,8 +289,8 @@ std::string DeviceOp::setup_far(const Plan& plan, FarField<R>& F, const double2*
         MLFMA_CK(dyn(reinterpret_cast<const void*>(k_l2l_m<R, 24>)));
         MLFMA_CK(dyn(reinterpret_cast<const void*>(k_l2l_m<R, 32>)));
         for (int p = lmin_; p < lmax_; ++p) {
-            const size_t m2m1 = static_cast<size_t>(nph_[p + 1]) * 32 * sizeof(C);
-            const size_t l2l1 = static_cast<size_t>(nth_[p]) * 2 * l2l_pairs<R>() * 32 * sizeof(C) +
+            const size_t m2m1 = static_cast<size_t>(nph_[p + 1]) * 32 * m2m_rpl<R>() * sizeof(C);
+            const size_t l2l1 = static_cast<size_t>(nth_[p]) * 2 * l2l_pairs<R>() * 64 * sizeof(C) +
                                 static_cast<size_t>(nth_[p + 1]) * dn_w_[p] * (sizeof(R) + 2 * sizeof(int));
             // (the static stencil staging takes at most 11 KB)
             if (m2m1 + 11264 > static_cast<size_t>(dev_smem) || l2l1 + 1024 > static_cast<size_t>(dev_smem) ||
@@ -887,8 +887,9 @@ void DeviceOp::run_far_multi_t(FarField<R>& F, int nr, cudaStream_t s, int stage
     if (stage < 0 || stage == 1)
         for (int p = lmax_ - 1; p >= lmin_; --p) {
             if (npar_[p] == 0) continue;
-            const dim3 grid(npar_[p], nth_[p], (nr + kRc - 1) / kRc);
-            const size_t smem = static_cast<size_t>(nph_[p + 1]) * 32 * sizeof(C);
+            constexpr int rc = 16 * m2m_rpl<R>();
+            const dim3 grid(npar_[p], nth_[p], (nr + rc - 1) / rc);
+            const size_t smem = static_cast<size_t>(nph_[p + 1]) * 32 * m2m_rpl<R>() * sizeof(C);
             const DevTransT<R>& T = F.trans[p];
             const bool small = nph_[p] <= 8 * kInterpWarps;
 #define MLFMA_M2M_M(WW)                                                                        \
@@ -914,7 +915,7 @@ void DeviceOp::run_far_multi_t(FarField<R>& F, int nr, cudaStream_t s, int stage
             if (!g) continue;
             constexpr int kL2LPairs = l2l_pairs<R>();
             const dim3 grid(g, (nph_[p + 1] / 2 + kL2LPairs - 1) / kL2LPairs, (nr + kRc - 1) / kRc);
-            const size_t smem = static_cast<size_t>(nth_[p]) * 2 * kL2LPairs * 32 * sizeof(C) +
+            const size_t smem = static_cast<size_t>(nth_[p]) * 2 * kL2LPairs * 64 * sizeof(C) +
                                 static_cast<size_t>(nth_[p + 1]) * dn_w_[p] * (sizeof(R) + 2 * sizeof(int));
             const DevTransT<R>& T = F.trans[p];
             switch (dn_w_[p]) {

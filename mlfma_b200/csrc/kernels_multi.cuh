@@ -254,30 +254,39 @@ k_m2l_m(const DevLevelT<R>* __restrict__ lvs, const int2* __restrict__ items, co
 
 // ------------------------------------------------------------ M2M (many)
 // Interpolation and anterpolation on many right-hand sides work on chunks of
-// kRc = 16 right-hand sides: lane = component * 16 + rhs, so the 32 lanes of a
-// warp read one pattern entry for 16 right-hand sides and both components
-// (two 256-byte runs), while every stencil index, weight and shift is the same
-// for the whole warp; warps stride over grid positions.
-constexpr int kRc = 16;
+// 16 x RPL right-hand sides: lane = component * 16 + r, and each lane carries
+// right-hand sides r, r + 16, ... of the chunk, so the 32 lanes of a warp read
+// one pattern entry for the whole chunk and both components, while every
+// stencil index, weight and shift is the same for the whole warp and is paid
+// once per RPL values; warps stride over grid positions.  (kRc: the chunk of
+// the anterpolation kernel, RPL = 2.)
+constexpr int kRc = 32;
 constexpr int kInterpThreads = 256;
 constexpr int kInterpWarps = kInterpThreads / 32;
 constexpr int kM2MOut = 16;  // most parent phi columns per warp held in registers
 
 // Parent outgoing patterns = sum over children of Interp[shift(child)]
 // (Stem::buildMpoleCoeffs and addInterpCoeffs, src/fmm/stem.cpp:72-184).
-// Block = (parent, parent theta row, rhs chunk).  Children one at a time:
-// theta pass of the child into shared memory (one row of child phi columns),
-// then the phi pass accumulated in registers over the children.
+// Block = (parent, parent theta row, rhs chunk of 16 m2m_rpl right-hand
+// sides).  Children one at a time: theta pass of the child into shared memory
+// (one row of child phi columns), then the phi pass accumulated in registers
+// over the children.  Complex double carries two right-hand sides per lane;
+// complex float one (two measured slower: register pressure).
+template <class R> __host__ __device__ constexpr int m2m_rpl() { return sizeof(R) == 4 ? 1 : 2; }
+
 template <class R, int W, int OUT>  // OUT: parent phi columns per warp (nph <= OUT * 8)
 __global__ void __launch_bounds__(kInterpThreads)
 k_m2m_m(const DevLevelT<R>* __restrict__ lvs, DevTransT<R> T, int nr) {
     using C = typename Cx<R>::T;
+    constexpr int RPL = m2m_rpl<R>();
     extern __shared__ unsigned char smraw[];
-    C* sm = reinterpret_cast<C*>(smraw);  // [mph][32]
-    const int par = blockIdx.x, jth = blockIdx.y, r0 = blockIdx.z * kRc;
+    C* sm = reinterpret_cast<C*>(smraw);  // [mph][32 lanes][RPL]
+    const int par = blockIdx.x, jth = blockIdx.y, r0 = blockIdx.z * 16 * RPL;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int comp = lane >> 4, r = lane & 15;
-    const bool live = r0 + r < nr;
+    bool live[RPL];
+#pragma unroll
+    for (int j = 0; j < RPL; ++j) live[j] = r0 + r + 16 * j < nr;
     const int col = comp * nr + r0 + r;  // offset of (component, rhs) inside a direction
     const DevLevelT<R> P = lvs[T.plevel];
     const DevLevelT<R> Cl = lvs[T.plevel + 1];
@@ -297,31 +306,30 @@ k_m2m_m(const DevLevelT<R>* __restrict__ lvs, DevTransT<R> T, int nr) {
         ph_cf[i] = T.up_ph.coef[i];
     }
     __syncthreads();
-    C acc[OUT];
+    C acc[OUT][RPL];
 #pragma unroll
-    for (int u = 0; u < OUT; ++u) acc[u] = zero<C>();
+    for (int u = 0; u < OUT; ++u)
+#pragma unroll
+        for (int j = 0; j < RPL; ++j) acc[u][j] = zero<C>();
     for (int c = 0; c < nch; ++c) {
         const C* Ac = Cl.Am + static_cast<size_t>(T.child_box[c0 + c]) * Cl.ndir * 2 * nr + col;
         // weights of this row with the child's octant shift folded in: [iph][k]
         const C* fu = T.fold_up + (static_cast<size_t>(T.child_oct[c0 + c]) * P.nth + jth) * mph * W;
-        // two child columns per step: twice the loads in flight
-        for (int i0 = warp; i0 < mph; i0 += 2 * kInterpWarps) {
-            const int i1 = i0 + kInterpWarps;
-            const bool two = i1 < mph;
-            const int r0 = i0 < halfm ? i0 + halfm : i0 - halfm;
-            const int r1 = i1 < halfm ? i1 + halfm : i1 - halfm;
-            C v0 = zero<C>(), v1 = zero<C>();
+        for (int iph = warp; iph < mph; iph += kInterpWarps) {
+            const int iref = iph < halfm ? iph + halfm : iph - halfm;
+            C v[RPL];
+#pragma unroll
+            for (int j = 0; j < RPL; ++j) v[j] = zero<C>();
 #pragma unroll
             for (int k = 0; k < W; ++k) {
-                const int d0 = th_src[k] * mph + (th_refl[k] ? r0 : i0);
-                const int d1 = th_src[k] * mph + (th_refl[k] ? r1 : i1);
-                if (live) {
-                    v0 = cfma(fu[i0 * W + k], Ac[static_cast<size_t>(d0) * 2 * nr], v0);
-                    if (two) v1 = cfma(fu[i1 * W + k], Ac[static_cast<size_t>(d1) * 2 * nr], v1);
-                }
+                const C* a = Ac + static_cast<size_t>(th_src[k] * mph + (th_refl[k] ? iref : iph)) * 2 * nr;
+                const C f = fu[iph * W + k];
+#pragma unroll
+                for (int j = 0; j < RPL; ++j)
+                    if (live[j]) v[j] = cfma(f, a[16 * j], v[j]);
             }
-            sm[i0 * 32 + lane] = v0;
-            if (two) sm[i1 * 32 + lane] = v1;
+#pragma unroll
+            for (int j = 0; j < RPL; ++j) sm[(iph * 32 + lane) * RPL + j] = v[j];
         }
         __syncthreads();
 #pragma unroll
@@ -329,17 +337,23 @@ k_m2m_m(const DevLevelT<R>* __restrict__ lvs, DevTransT<R> T, int nr) {
             const int jph = warp + u * kInterpWarps;
             if (jph >= nph) break;
 #pragma unroll
-            for (int k = 0; k < W; ++k) acc[u] = crfma(ph_cf[jph * W + k], sm[ph_src[jph * W + k] * 32 + lane], acc[u]);
+            for (int k = 0; k < W; ++k) {
+                const R cf = ph_cf[jph * W + k];
+                const C* v = sm + (ph_src[jph * W + k] * 32 + lane) * RPL;
+#pragma unroll
+                for (int j = 0; j < RPL; ++j) acc[u][j] = crfma(cf, v[j], acc[u][j]);
+            }
         }
         __syncthreads();
     }
-    if (!live) return;
     C* Ap = P.Am + (static_cast<size_t>(T.par_box[par]) * P.ndir + static_cast<size_t>(jth) * nph) * 2 * nr + col;
 #pragma unroll
     for (int u = 0; u < OUT; ++u) {
         const int jph = warp + u * kInterpWarps;
         if (jph >= nph) break;
-        Ap[static_cast<size_t>(jph) * 2 * nr] = acc[u];
+#pragma unroll
+        for (int j = 0; j < RPL; ++j)
+            if (live[j]) Ap[static_cast<size_t>(jph) * 2 * nr + 16 * j] = acc[u][j];
     }
 }
 
@@ -351,9 +365,9 @@ k_m2m_m(const DevLevelT<R>* __restrict__ lvs, DevTransT<R> T, int nr) {
 // (neighbouring columns share most of their parent taps, which then hit L1),
 // then the transposed theta pass, whose pole reflection only moves between
 // the two columns of a pair.
-// (4 column pairs for complex float; 1 for complex double, whose tile would
+// (2 column pairs for complex float; 1 for complex double, whose tile would
 // otherwise hold occupancy to two blocks per SM)
-template <class R> __host__ __device__ constexpr int l2l_pairs() { return sizeof(R) == 4 ? 4 : 1; }
+template <class R> __host__ __device__ constexpr int l2l_pairs() { return sizeof(R) == 4 ? 2 : 1; }
 
 template <class R, int W>
 __global__ void __launch_bounds__(kInterpThreads)
@@ -362,12 +376,12 @@ k_l2l_m(const DevLevelT<R>* __restrict__ lvs, DevTransT<R> T, const int2* __rest
     constexpr int kL2LPairs = l2l_pairs<R>();
     constexpr int NC = 2 * kL2LPairs;  // columns of the block
     extern __shared__ unsigned char smraw[];
-    C* sm = reinterpret_cast<C*>(smraw);  // [pth][NC][32], then the theta taps
+    C* sm = reinterpret_cast<C*>(smraw);  // [pth][NC][32 lanes][2], then the theta taps
     const int2 pc = pairs[blockIdx.x];
     const int r0 = blockIdx.z * kRc;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int comp = lane >> 4, r = lane & 15;
-    const bool live = r0 + r < nr;
+    const bool live0 = r0 + r < nr, live1 = r0 + r + 16 < nr;
     const int col = comp * nr + r0 + r;
     const DevLevelT<R> P = lvs[T.plevel];
     const DevLevelT<R> Cl = lvs[T.plevel + 1];
@@ -379,7 +393,7 @@ k_l2l_m(const DevLevelT<R>* __restrict__ lvs, DevTransT<R> T, const int2* __rest
     // column c of the block: pair c % kL2LPairs, side c / kL2LPairs
     __shared__ int ph_src[NC * W];
     // dynamic shared memory: the tile, then cth x W theta taps (weight, source, reflection)
-    R* th_cf = reinterpret_cast<R*>(sm + static_cast<size_t>(pth) * NC * 32);
+    R* th_cf = reinterpret_cast<R*>(sm + static_cast<size_t>(pth) * NC * 64);
     int* th_src = reinterpret_cast<int*>(th_cf + cth * W);
     int* th_refl = th_src + cth * W;
     for (int i = threadIdx.x; i < NC * W; i += blockDim.x) {
@@ -398,30 +412,35 @@ k_l2l_m(const DevLevelT<R>* __restrict__ lvs, DevTransT<R> T, const int2* __rest
         const int ith = pos / NC, c = pos - ith * NC;
         const int jph = j0 + min(c % kL2LPairs, npair - 1) + (c / kL2LPairs) * halfc;
         const C* f = fd + (static_cast<size_t>(ith) * cph + jph) * W;
-        C v = zero<C>();
+        C v0 = zero<C>(), v1 = zero<C>();
 #pragma unroll
         for (int k = 0; k < W; ++k) {
-            const int dd = ith * pph + ph_src[c * W + k];
-            if (live) v = cfma(f[k], Bp[static_cast<size_t>(dd) * 2 * nr], v);
+            const C* b = Bp + static_cast<size_t>(ith * pph + ph_src[c * W + k]) * 2 * nr;
+            const C fk = f[k];
+            if (live0) v0 = cfma(fk, b[0], v0);
+            if (live1) v1 = cfma(fk, b[16], v1);
         }
-        sm[pos * 32 + lane] = v;
+        sm[(pos * 32 + lane) * 2] = v0;
+        sm[(pos * 32 + lane) * 2 + 1] = v1;
     }
     __syncthreads();
-    if (!live) return;
     C* Bc = Cl.Bm + static_cast<size_t>(T.child_box[pc.y]) * Cl.ndir * 2 * nr + col;
     for (int pos = warp; pos < cth * NC; pos += kInterpWarps) {
         const int jth = pos / NC, c = pos - jth * NC;
         const int pr = c % kL2LPairs, side = c / kL2LPairs;
         if (pr >= npair) continue;
-        C v = zero<C>();
+        C v0 = zero<C>(), v1 = zero<C>();
 #pragma unroll
         for (int k = 0; k < W; ++k) {
             const int q = jth * W + k;
             const int c2 = th_refl[q] ? pr + (1 - side) * kL2LPairs : c;
-            v = crfma(th_cf[q], sm[(th_src[q] * NC + c2) * 32 + lane], v);
+            const C* v = sm + ((th_src[q] * NC + c2) * 32 + lane) * 2;
+            v0 = crfma(th_cf[q], v[0], v0);
+            v1 = crfma(th_cf[q], v[1], v1);
         }
         C* o = Bc + static_cast<size_t>(jth * cph + j0 + pr + side * halfc) * 2 * nr;
-        *o = cadd(*o, v);
+        if (live0) o[0] = cadd(o[0], v0);
+        if (live1) o[16] = cadd(o[16], v1);
     }
 }
 
