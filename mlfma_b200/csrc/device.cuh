@@ -207,6 +207,14 @@ private:
     template <class T> T* upload(const std::vector<T>& v);
     template <class R> std::string setup_far(const Plan& plan, FarField<R>& F, const double2* pat64);
     template <class R, bool TR> void run_far_t(FarField<R>& F, const double2* xt, cudaStream_t s, int stage);
+    template <class R, bool TR> void run_far_overlap_t(FarField<R>& F, const double2* xt, cudaStream_t s,
+                                                       cudaStream_t s2);
+    void run_far_overlap(const double2* xt, cudaStream_t s, cudaStream_t s2, int prec, bool tr);
+    template <class R, bool TR> void far_s2m(FarField<R>& F, const double2* xt, cudaStream_t s);
+    template <class R, bool TR> void far_m2m(FarField<R>& F, int p, cudaStream_t s);
+    template <class R, bool TR> void far_m2l(FarField<R>& F, int lo, int hi, cudaStream_t s);
+    template <class R, bool TR> void far_l2l(FarField<R>& F, int p, cudaStream_t s);
+    template <class R, bool TR> void far_l2t(FarField<R>& F, cudaStream_t s);
     void run_far(const double2* xt, cudaStream_t s, int stage = -1, int prec = -1, bool tr = false);
     void run_near(const double2* xt, cudaStream_t s);
     void enqueue_core(cudaStream_t s, int prec, bool tr);   // xt_ -> yfar_, ynear_
@@ -224,8 +232,9 @@ private:
     int n_ = 0;
     int precision_ = kFp64;
     bool ready_ = false;
-    cudaStream_t stream_ = nullptr, side_ = nullptr;
-    cudaEvent_t ev_fork_ = nullptr, ev_join_ = nullptr;
+    cudaStream_t stream_ = nullptr, side_ = nullptr, side2_ = nullptr;
+    cudaEvent_t ev_fork_ = nullptr, ev_join_ = nullptr, ev_m2l_done_ = nullptr;
+    cudaEvent_t ev_level_[kMaxLevels] = {};  // outgoing patterns of a level final
     std::vector<void*> allocs_;
     long long bytes_ = 0;
     cudaGraph_t graph_[2][2] = {};          // per far-field precision, forward / transposed
@@ -237,6 +246,7 @@ private:
     int nbox_[kMaxLevels] = {}, ndir_[kMaxLevels] = {}, nth_[kMaxLevels] = {}, nph_[kMaxLevels] = {};
     int4* m2l_items_ = nullptr;          // (level, box, first direction, count)
     int n_m2l_items_ = 0;
+    int m2l_first_[kMaxLevels] = {}, m2l_count_[kMaxLevels] = {};  // items of each level
     std::vector<int2*> l2l_pairs_;       // per parent level: (parent, child entry)
     std::vector<int> n_l2l_pairs_, npar_, up_w_, dn_w_;
     int4* s2m_items_ = nullptr;          // (leaf, first element, element count)

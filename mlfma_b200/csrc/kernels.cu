@@ -108,6 +108,10 @@ DeviceOp::~DeviceOp() {
     for (void* p : allocs_) cudaFree(p);
     if (ev_fork_) cudaEventDestroy(ev_fork_);
     if (ev_join_) cudaEventDestroy(ev_join_);
+    if (ev_m2l_done_) cudaEventDestroy(ev_m2l_done_);
+    for (auto& e : ev_level_)
+        if (e) cudaEventDestroy(e);
+    if (side2_) cudaStreamDestroy(side2_);
     if (stream_) cudaStreamDestroy(stream_);
     if (side_) cudaStreamDestroy(side_);
 }
@@ -313,8 +317,11 @@ std::string DeviceOp::setup(const Plan& plan, int device, int precision, int max
         MLFMA_CK(cudaSetDevice(device));
         MLFMA_CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
         MLFMA_CK(cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking));
+        MLFMA_CK(cudaStreamCreateWithFlags(&side2_, cudaStreamNonBlocking));
         MLFMA_CK(cudaEventCreateWithFlags(&ev_fork_, cudaEventDisableTiming));
         MLFMA_CK(cudaEventCreateWithFlags(&ev_join_, cudaEventDisableTiming));
+        MLFMA_CK(cudaEventCreateWithFlags(&ev_m2l_done_, cudaEventDisableTiming));
+        for (auto& e : ev_level_) MLFMA_CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         n_ = plan.n;
         if (plan.max_level >= kMaxLevels) return "tree deeper than supported";
         const cplx ck = cplx(0, -kC0 * kMu0 / (4.0 * kPi)) * plan.pw.wavenum;
@@ -344,11 +351,13 @@ std::string DeviceOp::setup(const Plan& plan, int device, int precision, int max
             traffic_.m2l += cnt * cbytes * 2.0 + 316.0 * L.ndir * cbytes;
             const int nchunk = (L.ndir + 127) / 128;
             const int chunk = (L.ndir + nchunk - 1) / nchunk;
+            m2l_first_[l] = static_cast<int>(items.size());
             for (int b = 0; b < nbox_[l]; ++b) {
                 if (ref_compat_ && L.m2l_ptr[b + 1] == L.m2l_ptr[b]) continue;
                 for (int d0 = 0; d0 < L.ndir; d0 += chunk)
                     items.push_back(make_int4(l, b, d0, std::min(chunk, L.ndir - d0)));
             }
+            m2l_count_[l] = static_cast<int>(items.size()) - m2l_first_[l];
         }
         n_m2l_items_ = static_cast<int>(items.size());
         m2l_items_ = upload(items);
@@ -522,45 +531,105 @@ int DeviceOp::launches_per_matvec() const {
 // interpolation with the shift after it (L2L^T), negated translation offsets,
 // anterpolation with the shift after it (M2M^T), plain patterns coming down.
 template <class R, bool TR>
-void DeviceOp::run_far_t(FarField<R>& F, const double2* xt, cudaStream_t s, int stage) {
+void DeviceOp::far_s2m(FarField<R>& F, const double2* xt, cudaStream_t s) {
     using C = typename Cx<R>::T;
-    if (n_leaves_ == 0) return;
-    if ((stage < 0 || stage == 0) && n_s2m_items_)
+    if (n_s2m_items_)
         k_s2m<R, TR><<<n_s2m_items_, kS2MThreads, sizeof(C) * std::max(1, max_src_), s>>>(F.lv_dev, s2m_items_,
                                                                                             leaves_, F.pat, xt);
-    if (stage < 0 || stage == 1)
-        for (int p = lmax_ - 1; p >= lmin_; --p) {
-            if (npar_[p] == 0) continue;
-            const int rows = m2m_rows(nth_[p], nph_[p]);
-            const dim3 grid(npar_[p], (nth_[p] + rows - 1) / rows);
-            const size_t smem = static_cast<size_t>(8) * rows * nph_[p + 1] * 2 * sizeof(C);
-            const DevTransT<R>& T = F.trans[p];
-            switch (up_w_[p]) {
-                case 2: k_m2m<R, 2, TR><<<grid, 128, smem, s>>>(F.lv_dev, T, rows); break;
-                case 4: k_m2m<R, 4, TR><<<grid, 128, smem, s>>>(F.lv_dev, T, rows); break;
-                case 6: k_m2m<R, 6, TR><<<grid, 128, smem, s>>>(F.lv_dev, T, rows); break;
-                case 8: k_m2m<R, 8, TR><<<grid, 128, smem, s>>>(F.lv_dev, T, rows); break;
-                default: k_m2m<R, 10, TR><<<grid, 128, smem, s>>>(F.lv_dev, T, rows); break;
-            }
-        }
-    if ((stage < 0 || stage == 2) && n_m2l_items_)
-        k_m2l<R, TR><<<n_m2l_items_, 128, 0, s>>>(F.lv_dev, m2l_items_, ref_compat_ ? 0 : 1);
-    if (stage < 0 || stage == 3)
-        for (int p = lmin_; p < lmax_; ++p) {
-            const int g = n_l2l_pairs_[p];
-            if (!g) continue;
-            const size_t smem = static_cast<size_t>(nth_[p]) * nph_[p + 1] * 2 * sizeof(C);
-            const DevTransT<R>& T = F.trans[p];
-            switch (dn_w_[p]) {
-                case 8: k_l2l<R, 8, TR><<<g, 256, smem, s>>>(F.lv_dev, T, l2l_pairs_[p]); break;
-                case 12: k_l2l<R, 12, TR><<<g, 256, smem, s>>>(F.lv_dev, T, l2l_pairs_[p]); break;
-                case 16: k_l2l<R, 16, TR><<<g, 256, smem, s>>>(F.lv_dev, T, l2l_pairs_[p]); break;
-                case 24: k_l2l<R, 24, TR><<<g, 256, smem, s>>>(F.lv_dev, T, l2l_pairs_[p]); break;
-                default: k_l2l<R, 32, TR><<<g, 256, smem, s>>>(F.lv_dev, T, l2l_pairs_[p]); break;
-            }
-        }
-    if ((stage < 0 || stage == 4) && n_l2t_items_)
+}
+
+template <class R, bool TR>
+void DeviceOp::far_m2m(FarField<R>& F, int p, cudaStream_t s) {
+    using C = typename Cx<R>::T;
+    if (npar_[p] == 0) return;
+    const int rows = m2m_rows(nth_[p], nph_[p]);
+    const dim3 grid(npar_[p], (nth_[p] + rows - 1) / rows);
+    const size_t smem = static_cast<size_t>(8) * rows * nph_[p + 1] * 2 * sizeof(C);
+    const DevTransT<R>& T = F.trans[p];
+    switch (up_w_[p]) {
+        case 2: k_m2m<R, 2, TR><<<grid, 128, smem, s>>>(F.lv_dev, T, rows); break;
+        case 4: k_m2m<R, 4, TR><<<grid, 128, smem, s>>>(F.lv_dev, T, rows); break;
+        case 6: k_m2m<R, 6, TR><<<grid, 128, smem, s>>>(F.lv_dev, T, rows); break;
+        case 8: k_m2m<R, 8, TR><<<grid, 128, smem, s>>>(F.lv_dev, T, rows); break;
+        default: k_m2m<R, 10, TR><<<grid, 128, smem, s>>>(F.lv_dev, T, rows); break;
+    }
+}
+
+// M2L of levels lo..hi (their items are contiguous, level by level).
+template <class R, bool TR>
+void DeviceOp::far_m2l(FarField<R>& F, int lo, int hi, cudaStream_t s) {
+    if (lo > hi) return;
+    const int first = m2l_first_[lo];
+    const int count = m2l_first_[hi] + m2l_count_[hi] - first;
+    if (count > 0) k_m2l<R, TR><<<count, 128, 0, s>>>(F.lv_dev, m2l_items_ + first, ref_compat_ ? 0 : 1);
+}
+
+template <class R, bool TR>
+void DeviceOp::far_l2l(FarField<R>& F, int p, cudaStream_t s) {
+    using C = typename Cx<R>::T;
+    const int g = n_l2l_pairs_[p];
+    if (!g) return;
+    const size_t smem = static_cast<size_t>(nth_[p]) * nph_[p + 1] * 2 * sizeof(C);
+    const DevTransT<R>& T = F.trans[p];
+    switch (dn_w_[p]) {
+        case 8: k_l2l<R, 8, TR><<<g, 256, smem, s>>>(F.lv_dev, T, l2l_pairs_[p]); break;
+        case 12: k_l2l<R, 12, TR><<<g, 256, smem, s>>>(F.lv_dev, T, l2l_pairs_[p]); break;
+        case 16: k_l2l<R, 16, TR><<<g, 256, smem, s>>>(F.lv_dev, T, l2l_pairs_[p]); break;
+        case 24: k_l2l<R, 24, TR><<<g, 256, smem, s>>>(F.lv_dev, T, l2l_pairs_[p]); break;
+        default: k_l2l<R, 32, TR><<<g, 256, smem, s>>>(F.lv_dev, T, l2l_pairs_[p]); break;
+    }
+}
+
+template <class R, bool TR>
+void DeviceOp::far_l2t(FarField<R>& F, cudaStream_t s) {
+    if (n_l2t_items_)
         k_l2t<R, !TR><<<n_l2t_items_, kL2TThreads, 0, s>>>(F.lv_dev, l2t_items_, leaves_, F.pat, yfar_);
+}
+
+// stage: -1 all, 0 S2M, 1 M2M, 2 M2L, 3 L2L, 4 L2T, in sequence on s.
+// TR: the transposed far field, Far^T = S2M^T L2L^T M2L^T M2M^T L2T^T, run in
+// the same order with the mirrored kernels: conjugated patterns going up,
+// interpolation with the shift after it (L2L^T), negated translation offsets,
+// anterpolation with the shift after it (M2M^T), plain patterns coming down.
+template <class R, bool TR>
+void DeviceOp::run_far_t(FarField<R>& F, const double2* xt, cudaStream_t s, int stage) {
+    if (n_leaves_ == 0) return;
+    if (stage < 0 || stage == 0) far_s2m<R, TR>(F, xt, s);
+    if (stage < 0 || stage == 1)
+        for (int p = lmax_ - 1; p >= lmin_; --p) far_m2m<R, TR>(F, p, s);
+    if (stage < 0 || stage == 2) far_m2l<R, TR>(F, lmin_, lmax_, s);
+    if (stage < 0 || stage == 3)
+        for (int p = lmin_; p < lmax_; ++p) far_l2l<R, TR>(F, p, s);
+    if (stage < 0 || stage == 4) far_l2t<R, TR>(F, s);
+}
+
+// The same chain with the translations of the finer levels taken off the
+// critical path: M2L at level l needs only the outgoing patterns of level l,
+// final once S2M (l = max level) or M2M(l+1 -> l) has run, so levels
+// lmax..lmin+1 translate on s2 while the interpolations climb to the coarsest
+// level on s; the anterpolations wait for both.
+template <class R, bool TR>
+void DeviceOp::run_far_overlap_t(FarField<R>& F, const double2* xt, cudaStream_t s, cudaStream_t s2) {
+    if (n_leaves_ == 0) return;
+    if (lmax_ <= lmin_) {  // one far level: nothing to overlap
+        run_far_t<R, TR>(F, xt, s, -1);
+        return;
+    }
+    far_s2m<R, TR>(F, xt, s);
+    cudaEventRecord(ev_level_[lmax_], s);
+    for (int p = lmax_ - 1; p >= lmin_; --p) {
+        far_m2m<R, TR>(F, p, s);
+        cudaEventRecord(ev_level_[p], s);
+    }
+    for (int l = lmax_; l > lmin_; --l) {
+        cudaStreamWaitEvent(s2, ev_level_[l], 0);
+        far_m2l<R, TR>(F, l, l, s2);
+    }
+    cudaEventRecord(ev_m2l_done_, s2);
+    far_m2l<R, TR>(F, lmin_, lmin_, s);
+    cudaStreamWaitEvent(s, ev_m2l_done_, 0);
+    for (int p = lmin_; p < lmax_; ++p) far_l2l<R, TR>(F, p, s);
+    far_l2t<R, TR>(F, s);
 }
 
 void DeviceOp::run_far(const double2* xt, cudaStream_t s, int stage, int prec, bool tr) {
@@ -569,6 +638,15 @@ void DeviceOp::run_far(const double2* xt, cudaStream_t s, int stage, int prec, b
         if (tr) run_far_t<double, true>(f64_, xt, s, stage); else run_far_t<double, false>(f64_, xt, s, stage);
     } else {
         if (tr) run_far_t<float, true>(f32_, xt, s, stage); else run_far_t<float, false>(f32_, xt, s, stage);
+    }
+}
+
+void DeviceOp::run_far_overlap(const double2* xt, cudaStream_t s, cudaStream_t s2, int prec, bool tr) {
+    if (prec < 0) prec = precision_;
+    if (prec == kFp64) {
+        if (tr) run_far_overlap_t<double, true>(f64_, xt, s, s2); else run_far_overlap_t<double, false>(f64_, xt, s, s2);
+    } else {
+        if (tr) run_far_overlap_t<float, true>(f32_, xt, s, s2); else run_far_overlap_t<float, false>(f32_, xt, s, s2);
     }
 }
 
@@ -589,7 +667,7 @@ void DeviceOp::enqueue_core(cudaStream_t s, int prec, bool tr) {
     cudaStreamWaitEvent(side_, ev_fork_, 0);
     run_near(xt_, side_);
     cudaEventRecord(ev_join_, side_);
-    run_far(xt_, s, -1, prec, tr);
+    run_far_overlap(xt_, s, side2_, prec, tr);
     cudaStreamWaitEvent(s, ev_join_, 0);
 }
 
