@@ -519,7 +519,8 @@ int DeviceOp::launches_per_matvec() const {
             if (npar_[p]) n += 1;           // M2M
             if (n_l2l_pairs_[p]) n += 1;    // L2L
         }
-        if (n_m2l_items_) n += 1;
+        for (int l = lmin_; l <= lmax_; ++l)
+            if (m2l_count_[l]) n += 1;  // one M2L launch per level
     }
     if (n_near_items_) n += 1;
     return n;
@@ -966,7 +967,8 @@ void DeviceOp::run_far_multi_t(FarField<R>& F, int nr, cudaStream_t s, int stage
         for (int p = lmax_ - 1; p >= lmin_; --p) {
             if (npar_[p] == 0) continue;
             constexpr int rc = 16 * m2m_rpl<R>();
-            const dim3 grid(npar_[p], nth_[p], (nr + rc - 1) / rc);
+            const dim3 grid = m2m_rows_fast<R>() ? dim3(nth_[p], (nr + rc - 1) / rc, npar_[p])
+                                                 : dim3(npar_[p], nth_[p], (nr + rc - 1) / rc);
             const size_t smem = static_cast<size_t>(nph_[p + 1]) * 32 * m2m_rpl<R>() * sizeof(C);
             const DevTransT<R>& T = F.trans[p];
             const bool small = nph_[p] <= 8 * kInterpWarps;

@@ -273,6 +273,7 @@ constexpr int kM2MOut = 16;  // most parent phi columns per warp held in registe
 // over the children.  Complex double carries two right-hand sides per lane;
 // complex float one (two measured slower: register pressure).
 template <class R> __host__ __device__ constexpr int m2m_rpl() { return sizeof(R) == 4 ? 1 : 2; }
+template <class R> __host__ __device__ constexpr bool m2m_rows_fast() { return sizeof(R) == 8; }
 
 template <class R, int W, int OUT>  // OUT: parent phi columns per warp (nph <= OUT * 8)
 __global__ void __launch_bounds__(kInterpThreads)
@@ -281,7 +282,12 @@ k_m2m_m(const DevLevelT<R>* __restrict__ lvs, DevTransT<R> T, int nr) {
     constexpr int RPL = m2m_rpl<R>();
     extern __shared__ unsigned char smraw[];
     C* sm = reinterpret_cast<C*>(smraw);  // [mph][32 lanes][RPL]
-    const int par = blockIdx.x, jth = blockIdx.y, r0 = blockIdx.z * 16 * RPL;
+    // grid order (m2m_rows_fast): FP64 rows fastest (the blocks of one parent
+    // together, its children read from DRAM about once); FP32 parents fastest
+    // (measured faster there)
+    const int jth = m2m_rows_fast<R>() ? blockIdx.x : blockIdx.y;
+    const int par = m2m_rows_fast<R>() ? blockIdx.z : blockIdx.x;
+    const int r0 = (m2m_rows_fast<R>() ? blockIdx.y : blockIdx.z) * 16 * RPL;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int comp = lane >> 4, r = lane & 15;
     bool live[RPL];
