@@ -157,6 +157,7 @@ def measure(torch, dev, rank, world, args, precision: int, clocks=None) -> dict:
     op = MLFMA.rwg(mesh, pw, config=cfg)
     op.setup()
     setup_s = time.perf_counter() - t0
+    tuning = op.autotune(1, reps=5)  # launch shapes timed on this operator (mlfma_autotune)
     st = op.stats()
     n = op.n
     g = torch.Generator(device="cpu").manual_seed(1234 + rank)
@@ -226,6 +227,7 @@ def measure(torch, dev, rank, world, args, precision: int, clocks=None) -> dict:
                               root_leng=WORKLOAD["root_leng"], max_node_srcs=WORKLOAD["max_node_srcs"],
                               device=dev.index, precision=precision, self_terms=1, ref_compat=0)
         op = MLFMA.rwg(mesh, pw, config=scfg).setup()
+        op.autotune(1, reps=5)
         b = op.rhs()
         op.solve(b, max_iter=5, tol=1e-12, restart=SOLVE["restart"], ref_givens=False,
                  refine=precision == 1)  # warm-up: workspace and graphs
@@ -242,7 +244,7 @@ def measure(torch, dev, rank, world, args, precision: int, clocks=None) -> dict:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms, e2e_ms = float(t[0]), float(t[1])
     return dict(ms=ms, e2e_ms=e2e_ms, stages=avg, traffic=traffic, stats=st, setup_s=setup_s, n=n, y=y_dev,
-                clocks=clk, solve=solve)
+                clocks=clk, solve=solve, tuning=tuning)
 
 
 def measure_batched(torch, dev, args, precision: int) -> dict:
@@ -257,6 +259,8 @@ def measure_batched(torch, dev, args, precision: int) -> dict:
                          root_leng=WORKLOAD["root_leng"], max_node_srcs=WORKLOAD["max_node_srcs"],
                          device=dev.index, precision=precision, self_terms=1, ref_compat=0, max_rhs=NRHS)
     op = MLFMA.rwg(mesh, pw, config=cfg).setup()
+    op.autotune(1, reps=5)
+    tuning = op.autotune(NRHS, reps=3)
     n = op.n
     pws = inputs.fibonacci_planewaves(NRHS, wavenum=pw.wavenum)
     B = np.stack([op.rhs_planewave(p) for p in pws])
@@ -276,7 +280,8 @@ def measure_batched(torch, dev, args, precision: int) -> dict:
     ms = e0.elapsed_time(e1) / steps
     st = op.stage_times_multi(NRHS)
     out = {"nrhs": NRHS, "ms_per_product": ms, "matvecs_per_s": NRHS * 1000.0 / ms,
-           "us_per_rhs": ms * 1000.0 / NRHS, "stage_ms": st}
+           "us_per_rhs": ms * 1000.0 / NRHS, "stage_ms": st,
+           "tuning": {k: v for k, v in tuning.items() if k != "m2m_rows"}}
     if not args.no_solve:
         op.solve_multi(B, max_iter=3, tol=1e-12, restart=SOLVE["restart"], refine=precision == 1)  # warm-up
         t0 = time.perf_counter()
@@ -419,7 +424,9 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic (seeded icosphere mesh)",
             "config": config_dict({"parallelism": f"replicas{world}", "levels": st["max_level"],
-                                   "near_entries": st["near_entries"], "setup_s": r64["setup_s"]}),
+                                   "near_entries": st["near_entries"], "setup_s": r64["setup_s"],
+                                   "autotuned": {"m2l_chunk": r64["tuning"]["m2l_chunk"],
+                                                 "m2m_rows": [v for v in r64["tuning"]["m2m_rows"] if v]}}),
             "e2e": {"value": world * 1000.0 / e2e_ms, "unit": UNIT, "h2d_bytes_per_step": n * 16,
                     "d2h_bytes_per_step": n * 16},
             "gpu_launches": int(st.get("launches_per_matvec", 0)) * args.steps,

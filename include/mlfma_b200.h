@@ -247,6 +247,24 @@ int mlfma_vjp_farfield_power(mlfma_handle h, int nexc, const mlfma_planewave* pw
                              const double* khat, const mlfma_solver_opts* opts, double* J, double* grad_loads,
                              double* grad_w, double* currents, mlfma_solve_info* info);
 
+/* Launch shapes chosen by mlfma_autotune (no counterpart in the reference). */
+typedef struct {
+    int m2l_chunk;             /* one-vector translation: directions per thread block */
+    int m2m_rows[20];          /* one-vector interpolation: parent theta rows per block, by parent level */
+    int multi_m2m_rows_fast;   /* many-rhs interpolation grid: 1 rows fastest, 0 parents fastest */
+    int multi_l2l_pairs;       /* many-rhs anterpolation: column pairs per block */
+    float product_ms_before;   /* one product (nrhs right-hand sides) before and after, ms */
+    float product_ms_after;
+} mlfma_tuning;
+
+/* Autotuner: times the candidate launch shapes of the stages on this operator
+ * (reps timed launches each, CUDA events on the handle's stream) and keeps
+ * the fastest.  nrhs = 1 tunes the one-vector product; 2 <= nrhs <= max_rhs the
+ * many-rhs product at that width.  Results are unchanged up to rounding; the
+ * operator's state (the reference's stale locals) is preserved.  Call outside
+ * any stream capture; out may be NULL. */
+int mlfma_autotune(mlfma_handle h, int nrhs, int reps, mlfma_tuning* out);
+
 /* The handle's own CUDA stream (cudaStream_t as void*), on which mlfma_matvec
  * and mlfma_gmres run; callers may record events on it. */
 int mlfma_get_stream(mlfma_handle h, void** stream);

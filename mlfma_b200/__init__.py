@@ -19,7 +19,7 @@ import numpy as np
 
 from . import inputs
 from ._lib import (Config, MlfmaError, NotConverged, PlaneWaveC, SolveInfo, SolverOpts, StageTimes, Stats,
-                   Traffic, check, lib)
+                   Traffic, Tuning, check, lib)
 
 __all__ = ["MLFMA", "MlfmaError", "NotConverged", "inputs", "default_config"]
 
@@ -326,6 +326,14 @@ class MLFMA:
         """Unit directions of a phi cut at fixed theta (n equally spaced phi)."""
         ph = 2.0 * np.pi * np.arange(n) / n
         return np.stack([np.sin(theta) * np.cos(ph), np.sin(theta) * np.sin(ph), np.full(n, np.cos(theta))], -1)
+
+    def autotune(self, nrhs: int = 1, reps: int = 5) -> dict:
+        """Choose launch shapes by timing them on this operator (mlfma_autotune)."""
+        t = Tuning()
+        check(lib().mlfma_autotune(self._h, nrhs, reps, ctypes.byref(t)))
+        return {"m2l_chunk": t.m2l_chunk, "m2m_rows": list(t.m2m_rows), "multi_m2m_rows_fast": t.multi_m2m_rows_fast,
+                "multi_l2l_pairs": t.multi_l2l_pairs, "product_ms_before": t.product_ms_before,
+                "product_ms_after": t.product_ms_after}
 
     def stream(self) -> int:
         s = ctypes.c_void_p()

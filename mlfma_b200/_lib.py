@@ -64,6 +64,12 @@ class SolveInfo(ctypes.Structure):
                 ("refinements", ctypes.c_int)]
 
 
+class Tuning(ctypes.Structure):
+    _fields_ = [("m2l_chunk", ctypes.c_int), ("m2m_rows", ctypes.c_int * 20), ("multi_m2m_rows_fast", ctypes.c_int),
+                ("multi_l2l_pairs", ctypes.c_int), ("product_ms_before", ctypes.c_float),
+                ("product_ms_after", ctypes.c_float)]
+
+
 # name -> (restype, argtypes); every symbol the header declares.
 SIGNATURES = {
     "mlfma_config_default": (ctypes.c_int, [ctypes.POINTER(Config)]),
@@ -98,6 +104,7 @@ SIGNATURES = {
     "mlfma_vjp_farfield_power": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(PlaneWaveC), _dp,
                                                 ctypes.c_int, _dp, ctypes.POINTER(SolverOpts), _dp, _dp, _dp, _dp,
                                                 ctypes.POINTER(SolveInfo)]),
+    "mlfma_autotune": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(Tuning)]),
     "mlfma_get_stream": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]),
     "mlfma_time_stages": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(StageTimes)]),
     "mlfma_get_traffic": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Traffic)]),

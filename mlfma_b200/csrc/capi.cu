@@ -594,6 +594,24 @@ int mlfma_vjp_farfield_power(mlfma_handle h, int nexc, const mlfma_planewave* pw
     return MLFMA_OK;
 }
 
+int mlfma_autotune(mlfma_handle h, int nrhs, int reps, mlfma_tuning* out) {
+    if (!h) return fail(MLFMA_ERR_ARG, "null handle");
+    if (!ready(h)) return fail(MLFMA_ERR_STATE, "mlfma_setup has not run");
+    mlfma::TuneReport r{};
+    std::string e = h->dev->autotune(nrhs, reps, &r);
+    if (!e.empty()) return from_msg(e);
+    if (out) {
+        std::memset(out, 0, sizeof(*out));
+        out->m2l_chunk = r.m2l_chunk;
+        for (int i = 0; i < 20 && i < mlfma::kMaxLevels; ++i) out->m2m_rows[i] = r.m2m_rows[i];
+        out->multi_m2m_rows_fast = r.multi_rows_fast;
+        out->multi_l2l_pairs = r.multi_l2l_pairs;
+        out->product_ms_before = r.before_ms;
+        out->product_ms_after = r.after_ms;
+    }
+    return MLFMA_OK;
+}
+
 int mlfma_get_stream(mlfma_handle h, void** stream) {
     if (!h || !stream) return fail(MLFMA_ERR_ARG, "null argument");
     if (!ready(h)) return fail(MLFMA_ERR_STATE, "mlfma_setup has not run");

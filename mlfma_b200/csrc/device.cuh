@@ -120,6 +120,14 @@ struct DevGeomLevel {
     int ndir;
 };
 
+struct TuneReport {
+    int m2l_chunk;                 // one-vector M2L directions per block
+    int m2m_rows[kMaxLevels];      // one-vector M2M parent rows per block (index: parent level)
+    int multi_rows_fast;           // many-rhs M2M grid order (1 rows fastest, 0 parents fastest)
+    int multi_l2l_pairs;           // many-rhs L2L column pairs per block
+    float before_ms, after_ms;     // product time before and after
+};
+
 struct StageTimes {
     float gather, s2m, m2m, m2l, l2l, l2t, near, finish, total;
 };
@@ -177,6 +185,8 @@ public:
 
     // Per-stage CUDA-event timing of one matvec on the operator's stream.
     std::string time_stages(StageTimes* out);
+    // Chooses launch shapes by timing them on this operator (see kernels.cu).
+    std::string autotune(int nr, int reps, TuneReport* rep);
     // Same for a product on nr right-hand sides.
     std::string time_stages_multi(int nr, StageTimes* out);
 
@@ -225,6 +235,8 @@ private:
     void enqueue_multi(int nr, cudaStream_t s, int prec);  // xtm_ -> yfarm_, ynearm_
     std::string setup_multi(const Plan& plan);
     std::string build_m2l_groups(const Plan& plan);
+    size_t m2l_item_capacity(int min_chunk) const;
+    void build_m2l_items(int max_chunk);
     std::string ensure_graph(int prec, bool tr);
     static int m2m_rows(int nth, int nph);
 
@@ -247,6 +259,12 @@ private:
     int4* m2l_items_ = nullptr;          // (level, box, first direction, count)
     int n_m2l_items_ = 0;
     int m2l_first_[kMaxLevels] = {}, m2l_count_[kMaxLevels] = {};  // items of each level
+    std::vector<char> m2l_has_list_[kMaxLevels];  // box has a non-empty list 2
+    // Launch shapes (defaults at setup; mlfma_autotune may change them).
+    int m2l_chunk_ = 128;                 // one-vector M2L directions per block
+    std::vector<int> m2m_rows_;           // one-vector M2M parent rows per block, per transition
+    int m_m2m_rows_fast_ = -1;            // many-rhs M2M grid order (-1: precision default)
+    int m_l2l_pairs_ = 0;                 // many-rhs L2L column pairs per block (0: precision default)
     std::vector<int2*> l2l_pairs_;       // per parent level: (parent, child entry)
     std::vector<int> n_l2l_pairs_, npar_, up_w_, dn_w_;
     int4* s2m_items_ = nullptr;          // (leaf, first element, element count)

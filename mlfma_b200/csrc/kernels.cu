@@ -139,6 +139,32 @@ int DeviceOp::m2m_rows(int nth, int nph) {
     return std::max(1, std::min(nth, 128 / std::max(nph, 1)));
 }
 
+// One-vector M2L work items (level, box, first direction, count) for a
+// direction chunk of at most max_chunk, written to the device array; items of
+// each level are contiguous (m2l_first_, m2l_count_).
+size_t DeviceOp::m2l_item_capacity(int min_chunk) const {
+    size_t n = 1;
+    for (int l = lmin_; l <= lmax_; ++l) n += static_cast<size_t>(nbox_[l]) * ((ndir_[l] + min_chunk - 1) / min_chunk + 1);
+    return n;
+}
+
+void DeviceOp::build_m2l_items(int max_chunk) {
+    std::vector<int4> items;
+    for (int l = lmin_; l <= lmax_; ++l) {
+        const int nchunk = (ndir_[l] + max_chunk - 1) / max_chunk;
+        const int chunk = (ndir_[l] + nchunk - 1) / nchunk;
+        m2l_first_[l] = static_cast<int>(items.size());
+        for (int b = 0; b < nbox_[l]; ++b) {
+            if (ref_compat_ && !m2l_has_list_[l][b]) continue;
+            for (int d0 = 0; d0 < ndir_[l]; d0 += chunk) items.push_back(make_int4(l, b, d0, std::min(chunk, ndir_[l] - d0)));
+        }
+        m2l_count_[l] = static_cast<int>(items.size()) - m2l_first_[l];
+    }
+    n_m2l_items_ = static_cast<int>(items.size());
+    m2l_chunk_ = max_chunk;
+    if (!items.empty()) cudaMemcpy(m2l_items_, items.data(), sizeof(int4) * items.size(), cudaMemcpyHostToDevice);
+}
+
 // Far-field arrays in precision R (levels, transitions, patterns).
 template <class R>
 std::string DeviceOp::setup_far(const Plan& plan, FarField<R>& F, const double2* pat64) {
@@ -257,11 +283,12 @@ std::string DeviceOp::setup_far(const Plan& plan, FarField<R>& F, const double2*
     const auto attr = cudaFuncAttributeMaxDynamicSharedMemorySize;
     for (int tr = 0; tr < 2; ++tr) {  // forward and transposed variants
         const bool t = tr != 0;
-        MLFMA_CK(cudaFuncSetAttribute(t ? k_m2m<R, 2, true> : k_m2m<R, 2, false>, attr, static_cast<int>(m2m_smem)));
-        MLFMA_CK(cudaFuncSetAttribute(t ? k_m2m<R, 4, true> : k_m2m<R, 4, false>, attr, static_cast<int>(m2m_smem)));
-        MLFMA_CK(cudaFuncSetAttribute(t ? k_m2m<R, 6, true> : k_m2m<R, 6, false>, attr, static_cast<int>(m2m_smem)));
-        MLFMA_CK(cudaFuncSetAttribute(t ? k_m2m<R, 8, true> : k_m2m<R, 8, false>, attr, static_cast<int>(m2m_smem)));
-        MLFMA_CK(cudaFuncSetAttribute(t ? k_m2m<R, 10, true> : k_m2m<R, 10, false>, attr, static_cast<int>(m2m_smem)));
+        // up to the opt-in limit: the autotuner may choose more rows per block
+        MLFMA_CK(cudaFuncSetAttribute(t ? k_m2m<R, 2, true> : k_m2m<R, 2, false>, attr, dev_smem));
+        MLFMA_CK(cudaFuncSetAttribute(t ? k_m2m<R, 4, true> : k_m2m<R, 4, false>, attr, dev_smem));
+        MLFMA_CK(cudaFuncSetAttribute(t ? k_m2m<R, 6, true> : k_m2m<R, 6, false>, attr, dev_smem));
+        MLFMA_CK(cudaFuncSetAttribute(t ? k_m2m<R, 8, true> : k_m2m<R, 8, false>, attr, dev_smem));
+        MLFMA_CK(cudaFuncSetAttribute(t ? k_m2m<R, 10, true> : k_m2m<R, 10, false>, attr, dev_smem));
         MLFMA_CK(cudaFuncSetAttribute(t ? k_l2l<R, 8, true> : k_l2l<R, 8, false>, attr, static_cast<int>(l2l_smem)));
         MLFMA_CK(cudaFuncSetAttribute(t ? k_l2l<R, 12, true> : k_l2l<R, 12, false>, attr, static_cast<int>(l2l_smem)));
         MLFMA_CK(cudaFuncSetAttribute(t ? k_l2l<R, 16, true> : k_l2l<R, 16, false>, attr, static_cast<int>(l2l_smem)));
@@ -287,14 +314,19 @@ std::string DeviceOp::setup_far(const Plan& plan, FarField<R>& F, const double2*
         MLFMA_CK(dyn(reinterpret_cast<const void*>(k_m2m_m<R, 6, kM2MOut>)));
         MLFMA_CK(dyn(reinterpret_cast<const void*>(k_m2m_m<R, 8, kM2MOut>)));
         MLFMA_CK(dyn(reinterpret_cast<const void*>(k_m2m_m<R, 10, kM2MOut>)));
-        MLFMA_CK(dyn(reinterpret_cast<const void*>(k_l2l_m<R, 8>)));
-        MLFMA_CK(dyn(reinterpret_cast<const void*>(k_l2l_m<R, 12>)));
-        MLFMA_CK(dyn(reinterpret_cast<const void*>(k_l2l_m<R, 16>)));
-        MLFMA_CK(dyn(reinterpret_cast<const void*>(k_l2l_m<R, 24>)));
-        MLFMA_CK(dyn(reinterpret_cast<const void*>(k_l2l_m<R, 32>)));
+        MLFMA_CK(dyn(reinterpret_cast<const void*>(k_l2l_m<R, 8, 1>)));
+        MLFMA_CK(dyn(reinterpret_cast<const void*>(k_l2l_m<R, 12, 1>)));
+        MLFMA_CK(dyn(reinterpret_cast<const void*>(k_l2l_m<R, 16, 1>)));
+        MLFMA_CK(dyn(reinterpret_cast<const void*>(k_l2l_m<R, 24, 1>)));
+        MLFMA_CK(dyn(reinterpret_cast<const void*>(k_l2l_m<R, 32, 1>)));
+        MLFMA_CK(dyn(reinterpret_cast<const void*>(k_l2l_m<R, 8, 2>)));
+        MLFMA_CK(dyn(reinterpret_cast<const void*>(k_l2l_m<R, 12, 2>)));
+        MLFMA_CK(dyn(reinterpret_cast<const void*>(k_l2l_m<R, 16, 2>)));
+        MLFMA_CK(dyn(reinterpret_cast<const void*>(k_l2l_m<R, 24, 2>)));
+        MLFMA_CK(dyn(reinterpret_cast<const void*>(k_l2l_m<R, 32, 2>)));
         for (int p = lmin_; p < lmax_; ++p) {
             const size_t m2m1 = static_cast<size_t>(nph_[p + 1]) * 32 * m2m_rpl<R>() * sizeof(C);
-            const size_t l2l1 = static_cast<size_t>(nth_[p]) * 2 * l2l_pairs<R>() * 64 * sizeof(C) +
+            const size_t l2l1 = static_cast<size_t>(nth_[p]) * 2 * 1 * 64 * sizeof(C) +
                                 static_cast<size_t>(nth_[p + 1]) * dn_w_[p] * (sizeof(R) + 2 * sizeof(int));
             // (the static stencil staging takes at most 11 KB)
             if (m2m1 + 11264 > static_cast<size_t>(dev_smem) || l2l1 + 1024 > static_cast<size_t>(dev_smem) ||
@@ -338,7 +370,6 @@ std::string DeviceOp::setup(const Plan& plan, int device, int precision, int max
         const double cbytes = precision == kFp64 ? 16.0 : 8.0;  // one far-field complex value
 
         // ---- level sizes and M2L work items: direction chunks of at most 128
-        std::vector<int4> items;
         for (int l = lmin_; l <= lmax_; ++l) {
             const Level& L = plan.levels[l];
             nbox_[l] = static_cast<int>(L.boxes.size());
@@ -349,21 +380,15 @@ std::string DeviceOp::setup(const Plan& plan, int device, int precision, int max
             // M2L reads every source box's pattern and the transfer table once
             // (repeats hit L2) and writes every local pattern once.
             traffic_.m2l += cnt * cbytes * 2.0 + 316.0 * L.ndir * cbytes;
-            const int nchunk = (L.ndir + 127) / 128;
-            const int chunk = (L.ndir + nchunk - 1) / nchunk;
-            m2l_first_[l] = static_cast<int>(items.size());
-            for (int b = 0; b < nbox_[l]; ++b) {
-                if (ref_compat_ && L.m2l_ptr[b + 1] == L.m2l_ptr[b]) continue;
-                for (int d0 = 0; d0 < L.ndir; d0 += chunk)
-                    items.push_back(make_int4(l, b, d0, std::min(chunk, L.ndir - d0)));
-            }
-            m2l_count_[l] = static_cast<int>(items.size()) - m2l_first_[l];
+            m2l_has_list_[l].resize(nbox_[l]);
+            for (int b = 0; b < nbox_[l]; ++b) m2l_has_list_[l][b] = L.m2l_ptr[b + 1] > L.m2l_ptr[b];
         }
-        n_m2l_items_ = static_cast<int>(items.size());
-        m2l_items_ = upload(items);
+        m2l_items_ = alloc<int4>(m2l_item_capacity(8));
+        build_m2l_items(128);
 
         // ---- transitions: L2L pairs and stencil widths
         l2l_pairs_.assign(std::max(lmax_, 0) + 1, nullptr);
+        m2m_rows_.assign(std::max(lmax_, 0) + 1, 1);
         n_l2l_pairs_.assign(std::max(lmax_, 0) + 1, 0);
         npar_.assign(std::max(lmax_, 0) + 1, 0);
         up_w_.assign(std::max(lmax_, 0) + 1, 0);
@@ -386,6 +411,7 @@ std::string DeviceOp::setup(const Plan& plan, int device, int precision, int max
             if (!w_dn) return "anterpolation stencil wider than 32 taps";
             up_w_[p] = w_up;
             dn_w_[p] = w_dn;
+            m2m_rows_[p] = m2m_rows(nth_[p], nph_[p]);
             npar_[p] = static_cast<int>(T.par_box.size());
             std::vector<int2> pairs;
             for (int q = 0; q < npar_[p]; ++q) {
@@ -543,7 +569,7 @@ template <class R, bool TR>
 void DeviceOp::far_m2m(FarField<R>& F, int p, cudaStream_t s) {
     using C = typename Cx<R>::T;
     if (npar_[p] == 0) return;
-    const int rows = m2m_rows(nth_[p], nph_[p]);
+    const int rows = m2m_rows_[p];
     const dim3 grid(npar_[p], (nth_[p] + rows - 1) / rows);
     const size_t smem = static_cast<size_t>(8) * rows * nph_[p + 1] * 2 * sizeof(C);
     const DevTransT<R>& T = F.trans[p];
@@ -967,14 +993,15 @@ void DeviceOp::run_far_multi_t(FarField<R>& F, int nr, cudaStream_t s, int stage
         for (int p = lmax_ - 1; p >= lmin_; --p) {
             if (npar_[p] == 0) continue;
             constexpr int rc = 16 * m2m_rpl<R>();
-            const dim3 grid = m2m_rows_fast<R>() ? dim3(nth_[p], (nr + rc - 1) / rc, npar_[p])
-                                                 : dim3(npar_[p], nth_[p], (nr + rc - 1) / rc);
+            const int rows_fast = m_m2m_rows_fast_ < 0 ? (m2m_rows_fast<R>() ? 1 : 0) : m_m2m_rows_fast_;
+            const dim3 grid = rows_fast ? dim3(nth_[p], (nr + rc - 1) / rc, npar_[p])
+                                        : dim3(npar_[p], nth_[p], (nr + rc - 1) / rc);
             const size_t smem = static_cast<size_t>(nph_[p + 1]) * 32 * m2m_rpl<R>() * sizeof(C);
             const DevTransT<R>& T = F.trans[p];
             const bool small = nph_[p] <= 8 * kInterpWarps;
 #define MLFMA_M2M_M(WW)                                                                        \
-    (small ? k_m2m_m<R, WW, 8><<<grid, kInterpThreads, smem, s>>>(F.lv_dev, T, nr)            \
-           : k_m2m_m<R, WW, kM2MOut><<<grid, kInterpThreads, smem, s>>>(F.lv_dev, T, nr))
+    (small ? k_m2m_m<R, WW, 8><<<grid, kInterpThreads, smem, s>>>(F.lv_dev, T, nr, rows_fast)            \
+           : k_m2m_m<R, WW, kM2MOut><<<grid, kInterpThreads, smem, s>>>(F.lv_dev, T, nr, rows_fast))
             switch (up_w_[p]) {
                 case 2: MLFMA_M2M_M(2); break;
                 case 4: MLFMA_M2M_M(4); break;
@@ -993,18 +1020,22 @@ void DeviceOp::run_far_multi_t(FarField<R>& F, int nr, cudaStream_t s, int stage
         for (int p = lmin_; p < lmax_; ++p) {
             const int g = n_l2l_pairs_[p];
             if (!g) continue;
-            constexpr int kL2LPairs = l2l_pairs<R>();
-            const dim3 grid(g, (nph_[p + 1] / 2 + kL2LPairs - 1) / kL2LPairs, (nr + kRc - 1) / kRc);
-            const size_t smem = static_cast<size_t>(nth_[p]) * 2 * kL2LPairs * 64 * sizeof(C) +
+            const int pairs = m_l2l_pairs_ > 0 ? m_l2l_pairs_ : l2l_pairs<R>();
+            const dim3 grid(g, (nph_[p + 1] / 2 + pairs - 1) / pairs, (nr + kRc - 1) / kRc);
+            const size_t smem = static_cast<size_t>(nth_[p]) * 2 * pairs * 64 * sizeof(C) +
                                 static_cast<size_t>(nth_[p + 1]) * dn_w_[p] * (sizeof(R) + 2 * sizeof(int));
             const DevTransT<R>& T = F.trans[p];
+#define MLFMA_L2L_M(WW)                                                                                    \
+    (pairs == 1 ? k_l2l_m<R, WW, 1><<<grid, kInterpThreads, smem, s>>>(F.lv_dev, T, l2l_pairs_[p], nr)     \
+                : k_l2l_m<R, WW, 2><<<grid, kInterpThreads, smem, s>>>(F.lv_dev, T, l2l_pairs_[p], nr))
             switch (dn_w_[p]) {
-                case 8: k_l2l_m<R, 8><<<grid, kInterpThreads, smem, s>>>(F.lv_dev, T, l2l_pairs_[p], nr); break;
-                case 12: k_l2l_m<R, 12><<<grid, kInterpThreads, smem, s>>>(F.lv_dev, T, l2l_pairs_[p], nr); break;
-                case 16: k_l2l_m<R, 16><<<grid, kInterpThreads, smem, s>>>(F.lv_dev, T, l2l_pairs_[p], nr); break;
-                case 24: k_l2l_m<R, 24><<<grid, kInterpThreads, smem, s>>>(F.lv_dev, T, l2l_pairs_[p], nr); break;
-                default: k_l2l_m<R, 32><<<grid, kInterpThreads, smem, s>>>(F.lv_dev, T, l2l_pairs_[p], nr); break;
+                case 8: MLFMA_L2L_M(8); break;
+                case 12: MLFMA_L2L_M(12); break;
+                case 16: MLFMA_L2L_M(16); break;
+                case 24: MLFMA_L2L_M(24); break;
+                default: MLFMA_L2L_M(32); break;
             }
+#undef MLFMA_L2L_M
         }
     if ((stage < 0 || stage == 4) && n_l2t_items_m_)
         k_l2t_m<R><<<n_l2t_items_m_, kGemmThreads, 0, s>>>(F.lv_dev, l2t_items_m_, leaves_, F.pat, yfarm_, nr);
@@ -1087,6 +1118,143 @@ std::string DeviceOp::time_stages_multi(int nr, StageTimes* out) {
     *out = StageTimes{t[0], t[1], t[2], t[3], t[4], t[5], t[6], t[7], 0.f};
     cudaEventElapsedTime(&out->total, ev[0], ev[8]);
     for (auto& e : ev) cudaEventDestroy(e);
+    MLFMA_CK(cudaGetLastError());
+    return {};
+}
+
+// ================================================================= autotuner
+
+// Times the candidate launch shapes of the stages on this operator (CUDA
+// events on the operator's stream, after one untimed launch each) and keeps
+// the fastest: nr = 1 tunes the one-vector path (M2L directions per block,
+// M2M parent rows per block per level transition), nr > 1 the many-rhs path at
+// that width (interpolation grid order, anterpolation column pairs).  The
+// local patterns are saved and restored around the trial launches, so the
+// reference's stale-local rule sees no change; captured graphs are dropped
+// and recaptured with the new shapes on the next product.
+std::string DeviceOp::autotune(int nr, int reps, TuneReport* rep) {
+    if (!ready_) return "operator not set up";
+    if (nr < 1 || (nr > 1 && nr > max_rhs_)) return "arg:nrhs must be 1 or between 2 and the operator's max_rhs";
+    if (reps < 1) reps = 5;
+    MLFMA_CK(cudaSetDevice(device_));
+    cudaStream_t s = stream_;
+    int dev_smem = 0;
+    MLFMA_CK(cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, device_));
+    const size_t csize = precision_ == kFp64 ? sizeof(double2) : sizeof(float2);
+    // save the local patterns of the tuned precision
+    std::vector<std::pair<void*, size_t>> saved;
+    std::vector<void*> tmp;
+    auto save = [&](void* p, size_t bytes) -> std::string {
+        void* t = nullptr;
+        MLFMA_CK(cudaMalloc(&t, bytes));
+        MLFMA_CK(cudaMemcpyAsync(t, p, bytes, cudaMemcpyDeviceToDevice, s));
+        saved.emplace_back(p, bytes);
+        tmp.push_back(t);
+        return {};
+    };
+    for (int l = lmin_; l <= lmax_; ++l) {
+        const size_t cnt = static_cast<size_t>(nbox_[l]) * ndir_[l] * 2;
+        void* B = precision_ == kFp64 ? static_cast<void*>(f64_.lv[l].B) : static_cast<void*>(f32_.lv[l].B);
+        void* Bm = precision_ == kFp64 ? static_cast<void*>(f64_.lv[l].Bm) : static_cast<void*>(f32_.lv[l].Bm);
+        std::string e = save(B, cnt * csize);
+        if (!e.empty()) return e;
+        if (nr > 1 && Bm) {
+            e = save(Bm, cnt * max_rhs_ * csize);
+            if (!e.empty()) return e;
+        }
+    }
+    cudaEvent_t e0, e1;
+    MLFMA_CK(cudaEventCreate(&e0));
+    MLFMA_CK(cudaEventCreate(&e1));
+    auto timed = [&](const auto& launch) -> float {
+        launch();
+        cudaEventRecord(e0, s);
+        for (int i = 0; i < reps; ++i) launch();
+        cudaEventRecord(e1, s);
+        cudaEventSynchronize(e1);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        return ms / reps;
+    };
+    TuneReport r{};
+    if (nr == 1) {
+        auto product = [&] { enqueue_core(s, precision_, false); };
+        r.before_ms = timed(product);
+        // M2L: directions per block
+        float best = 1e30f;
+        int best_chunk = m2l_chunk_;
+        for (int chunk : {32, 64, 96, 128}) {  // k_m2l runs 128 threads: one direction each
+            build_m2l_items(chunk);
+            const float t = timed([&] { run_far(xt_, s, 2, precision_, false); });
+            if (t < best) { best = t; best_chunk = chunk; }
+        }
+        build_m2l_items(best_chunk);
+        r.m2l_chunk = best_chunk;
+        // M2M: parent rows per block, per transition
+        for (int p = lmin_; p < lmax_; ++p) {
+            if (!npar_[p]) continue;
+            float bt = 1e30f;
+            int brows = m2m_rows_[p];
+            for (int rows : {1, 2, 4, 8, 16}) {
+                if (rows > nth_[p] || static_cast<size_t>(8) * rows * nph_[p + 1] * 2 * csize > static_cast<size_t>(dev_smem))
+                    continue;
+                m2m_rows_[p] = rows;
+                const float t = timed([&] {
+                    if (precision_ == kFp64) far_m2m<double, false>(f64_, p, s); else far_m2m<float, false>(f32_, p, s);
+                });
+                if (t < bt) { bt = t; brows = rows; }
+            }
+            m2m_rows_[p] = brows;
+            r.m2m_rows[p] = brows;
+        }
+        r.after_ms = timed(product);
+    } else {
+        auto product = [&] { enqueue_multi(nr, s, precision_); };
+        r.before_ms = timed(product);
+        float bt = 1e30f;
+        int border = m_m2m_rows_fast_;
+        for (int o : {0, 1}) {
+            m_m2m_rows_fast_ = o;
+            const float t = timed([&] { run_far_multi(nr, s, 1, precision_); });
+            if (t < bt) { bt = t; border = o; }
+        }
+        m_m2m_rows_fast_ = border;
+        bt = 1e30f;
+        int bpairs = m_l2l_pairs_;
+        for (int q : {1, 2}) {
+            bool fits = true;
+            for (int p = lmin_; p < lmax_; ++p)
+                if (static_cast<size_t>(nth_[p]) * 2 * q * 64 * csize + static_cast<size_t>(nth_[p + 1]) * dn_w_[p] * 16 + 1024 >
+                    static_cast<size_t>(dev_smem))
+                    fits = false;
+            if (!fits) continue;
+            m_l2l_pairs_ = q;
+            const float t = timed([&] { run_far_multi(nr, s, 3, precision_); });
+            if (t < bt) { bt = t; bpairs = q; }
+        }
+        m_l2l_pairs_ = bpairs;
+        r.multi_rows_fast = border;
+        r.multi_l2l_pairs = bpairs;
+        r.after_ms = timed(product);
+    }
+    r.m2l_chunk = m2l_chunk_;
+    for (int p = lmin_; p < lmax_; ++p) r.m2m_rows[p] = m2m_rows_[p];
+    if (r.multi_rows_fast == 0 && m_m2m_rows_fast_ < 0) r.multi_rows_fast = -1;
+    // restore the local patterns, drop captured graphs
+    for (size_t i = 0; i < saved.size(); ++i)
+        MLFMA_CK(cudaMemcpyAsync(saved[i].first, tmp[i], saved[i].second, cudaMemcpyDeviceToDevice, s));
+    MLFMA_CK(cudaStreamSynchronize(s));
+    for (void* t : tmp) cudaFree(t);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    for (int p = 0; p < 2; ++p)
+        for (int t = 0; t < 2; ++t) {
+            if (graph_exec_[p][t]) cudaGraphExecDestroy(graph_exec_[p][t]);
+            if (graph_[p][t]) cudaGraphDestroy(graph_[p][t]);
+            graph_exec_[p][t] = nullptr;
+            graph_[p][t] = nullptr;
+        }
+    if (rep) *rep = r;
     MLFMA_CK(cudaGetLastError());
     return {};
 }

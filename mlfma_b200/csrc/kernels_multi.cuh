@@ -277,17 +277,17 @@ template <class R> __host__ __device__ constexpr bool m2m_rows_fast() { return s
 
 template <class R, int W, int OUT>  // OUT: parent phi columns per warp (nph <= OUT * 8)
 __global__ void __launch_bounds__(kInterpThreads)
-k_m2m_m(const DevLevelT<R>* __restrict__ lvs, DevTransT<R> T, int nr) {
+k_m2m_m(const DevLevelT<R>* __restrict__ lvs, DevTransT<R> T, int nr, int rows_fast) {
     using C = typename Cx<R>::T;
     constexpr int RPL = m2m_rpl<R>();
     extern __shared__ unsigned char smraw[];
     C* sm = reinterpret_cast<C*>(smraw);  // [mph][32 lanes][RPL]
-    // grid order (m2m_rows_fast): FP64 rows fastest (the blocks of one parent
-    // together, its children read from DRAM about once); FP32 parents fastest
-    // (measured faster there)
-    const int jth = m2m_rows_fast<R>() ? blockIdx.x : blockIdx.y;
-    const int par = m2m_rows_fast<R>() ? blockIdx.z : blockIdx.x;
-    const int r0 = (m2m_rows_fast<R>() ? blockIdx.y : blockIdx.z) * 16 * RPL;
+    // grid order: rows fastest (the blocks of one parent together, its
+    // children read from DRAM about once; the FP64 default) or parents
+    // fastest (the complex-float default); the autotuner may change it
+    const int jth = rows_fast ? blockIdx.x : blockIdx.y;
+    const int par = rows_fast ? blockIdx.z : blockIdx.x;
+    const int r0 = (rows_fast ? blockIdx.y : blockIdx.z) * 16 * RPL;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int comp = lane >> 4, r = lane & 15;
     bool live[RPL];
@@ -371,15 +371,15 @@ k_m2m_m(const DevLevelT<R>* __restrict__ lvs, DevTransT<R> T, int nr) {
 // (neighbouring columns share most of their parent taps, which then hit L1),
 // then the transposed theta pass, whose pole reflection only moves between
 // the two columns of a pair.
-// (2 column pairs for complex float; 1 for complex double, whose tile would
-// otherwise hold occupancy to two blocks per SM)
+// (default: 2 column pairs for complex float; 1 for complex double, whose tile
+// would otherwise hold occupancy to two blocks per SM; the autotuner may change
+// it)
 template <class R> __host__ __device__ constexpr int l2l_pairs() { return sizeof(R) == 4 ? 2 : 1; }
 
-template <class R, int W>
+template <class R, int W, int kL2LPairs>
 __global__ void __launch_bounds__(kInterpThreads)
 k_l2l_m(const DevLevelT<R>* __restrict__ lvs, DevTransT<R> T, const int2* __restrict__ pairs, int nr) {
     using C = typename Cx<R>::T;
-    constexpr int kL2LPairs = l2l_pairs<R>();
     constexpr int NC = 2 * kL2LPairs;  // columns of the block
     extern __shared__ unsigned char smraw[];
     C* sm = reinterpret_cast<C*>(smraw);  // [pth][NC][32 lanes][2], then the theta taps

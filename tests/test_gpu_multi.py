@@ -108,3 +108,31 @@ def test_rhs_planewave_matches_handle_rhs(cuda_device):
     op = make("rwg", max_rhs=1)
     assert np.array_equal(op.rhs_planewave(PW), op.rhs())
     op.close()
+
+
+def test_autotune_keeps_results(cuda_device):
+    # The tuner changes launch shapes only: the same call sequence on a tuned
+    # and an untuned operator gives the same products to rounding, including
+    # the reference's stale-local state (ref_compat = 1), which the tuner saves
+    # and restores around its trial launches.
+    tuned, plain = make("rwg", max_rhs=8), make("rwg", max_rhs=8)
+    x = cmat(1, tuned.n, 21)[0]
+    X = cmat(8, tuned.n, 22)
+    seq = []
+    for op, tune in ((tuned, True), (plain, False)):
+        out = [op.matvec(x)]
+        if tune:
+            t1 = op.autotune(1, reps=3)
+            assert t1["m2l_chunk"] in (32, 64, 96, 128) and t1["product_ms_after"] > 0
+        out.append(op.matvec(x))
+        out.append(op.matvec_multi(X))
+        if tune:
+            t8 = op.autotune(8, reps=3)
+            assert t8["multi_l2l_pairs"] in (1, 2) and t8["multi_m2m_rows_fast"] in (0, 1)
+        out.append(op.matvec_multi(X))
+        out.append(op.matvec(x))
+        seq.append(out)
+    for a, b in zip(*seq):
+        assert rel(a, b) <= 1e-12
+    tuned.close()
+    plain.close()
