@@ -81,6 +81,38 @@ public:
         check(mlfma_matvec(h_, reinterpret_cast<const double*>(lvec.data()), reinterpret_cast<double*>(rvec.data()), 1));
     }
 
+    // Many right-hand sides at once: Y = A X for the rows of X (nrhs x n).
+    std::vector<cplx> evalRvecMulti(int nrhs, const std::vector<cplx>& X) {
+        std::vector<cplx> Y(X.size());
+        check(mlfma_matvec_multi(h_, nrhs, reinterpret_cast<const double*>(X.data()),
+                                 reinterpret_cast<double*>(Y.data()), 0));
+        return Y;
+    }
+
+    // -V for another incident plane wave of the same wavenumber.
+    std::vector<cplx> rhs(const mlfma_planewave& pw) const {
+        std::vector<cplx> b(numSrcs());
+        check(mlfma_rhs_planewave(h_, &pw, reinterpret_cast<double*>(b.data())));
+        return b;
+    }
+
+    // y = A^H x (operators set up with ref_compat = 0).
+    std::vector<cplx> evalAdjoint(const std::vector<cplx>& x) {
+        std::vector<cplx> y(x.size());
+        check(mlfma_matvec_adjoint(h_, reinterpret_cast<const double*>(x.data()), reinterpret_cast<double*>(y.data()), 0));
+        return y;
+    }
+
+    // Diagonal impedance loads z (n complex) added to the operator.
+    void setLoads(const std::vector<cplx>& z) { check(mlfma_set_loads(h_, reinterpret_cast<const double*>(z.data()))); }
+
+    // Launch shapes timed on this operator (nrhs = 1: one-vector product).
+    mlfma_tuning autotune(int nrhs = 1, int reps = 5) {
+        mlfma_tuning t{};
+        check(mlfma_autotune(h_, nrhs, reps, &t));
+        return t;
+    }
+
     mlfma_handle handle() const { return h_; }
 
 private:

@@ -27,6 +27,8 @@ int main() {
     auto op = mlfma_b200::Operator::dipoles(cfg, pw, pos, mom);
     auto b = op.rhs();
     std::printf("%d %.17g %.17g\n", op.numSrcs(), b[0].real(), b[0].imag());
+    auto b2 = op.rhs(pw);  // mlfma_rhs_planewave with the operator's own wave
+    std::printf("%d\n", b2 == b ? 1 : 0);
     try {
         std::vector<double> bad(pos.size(), 10.0);
         mlfma_b200::Operator::dipoles(cfg, pw, bad, mom);
@@ -52,4 +54,5 @@ def test_cpp_wrapper_host_calls(tmp_path):
     assert int(n) == 500
     # reference-compatible voltage: -(-amp e^{ik.r} p0 pol_x) with p0 = 1e-8
     assert abs(complex(float(re_), float(im_))) == pytest.approx(1e-8, rel=1e-12)
-    assert out[1].startswith("caught mlfma_b200:") and "root box" in out[1]
+    assert out[1] == "1"
+    assert out[2].startswith("caught mlfma_b200:") and "root box" in out[2]

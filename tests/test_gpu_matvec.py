@@ -113,3 +113,25 @@ def test_stage_times_and_traffic(cuda_device, bench_op):
     assert t["total"] > 0 and all(t[k] >= 0 for k in t)
     tr = bench_op.traffic()
     assert tr["total"] > 4e8  # ~0.54 GB of operator data per matvec
+
+
+
+def test_single_leaf_and_single_source(cuda_device):
+    from oracle import mlfma_oracle as O
+    # one leaf holds every source: near field only
+    d = inputs.make_dipoles(50, seed=6, side=1.0)
+    op = MLFMA.dipoles(d, PW, max_node_srcs=64).setup()
+    x = cvec(op.n, 1)
+    orc = O.Oracle(O.DipoleSources(d.pos, d.mom, PW), max_node_srcs=64)
+    assert rel(op.matvec(x), orc.matvec(x)) <= 1e-12
+    op.close()
+    # one source: the reference's operator is zero (no self term); with self
+    # terms it is C k
+    d1 = inputs.make_dipoles(1, seed=7)
+    op0 = MLFMA.dipoles(d1, PW, max_node_srcs=8).setup()
+    assert np.all(op0.matvec(np.array([1.0 + 2.0j])) == 0)
+    op0.close()
+    op1 = MLFMA.dipoles(d1, PW, max_node_srcs=8, self_terms=1).setup()
+    ck = O.PHYS_C * PW.wavenum
+    assert abs(op1.matvec(np.array([1.0 + 2.0j]))[0] - ck * (1.0 + 2.0j)) <= 1e-12 * abs(ck)
+    op1.close()

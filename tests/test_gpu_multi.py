@@ -30,7 +30,7 @@ def make(kind, **kw):
 
 
 @pytest.mark.parametrize("kind", ["dipole", "rwg"])
-@pytest.mark.parametrize("nr", [1, 5, 64])
+@pytest.mark.parametrize("nr", [1, 5, 33, 64])
 def test_matvec_multi_matches_single(cuda_device, kind, nr):
     op = make(kind, ref_compat=0, max_rhs=64)
     X = cmat(nr, op.n, 7)
@@ -136,3 +136,19 @@ def test_autotune_keeps_results(cuda_device):
         assert rel(a, b) <= 1e-12
     tuned.close()
     plain.close()
+
+
+def test_multi_edge_cases(cuda_device):
+    # every source in one leaf (no far field), and a zero right-hand side
+    d = inputs.make_dipoles(40, seed=5, side=0.5)
+    op = MLFMA.dipoles(d, PW, max_node_srcs=64, ref_compat=0, self_terms=1, max_rhs=4).setup()
+    X = cmat(3, op.n, 8)
+    Y = op.matvec_multi(X)
+    for r in range(3):
+        assert rel(Y[r], op.matvec(X[r])) <= 1e-13
+    B = np.stack([op.rhs(), np.zeros(op.n, dtype=complex)])
+    Xs, infos = op.solve_multi(B, max_iter=200, tol=1e-10, restart=0)
+    assert infos[0].converged and infos[1].converged
+    assert np.all(Xs[1] == 0)
+    assert rel(op.matvec(Xs[0]), B[0]) <= 1.0001e-10
+    op.close()
