@@ -265,6 +265,32 @@ typedef struct {
  * any stream capture; out may be NULL. */
 int mlfma_autotune(mlfma_handle h, int nrhs, int reps, mlfma_tuning* out);
 
+/* ---- Many independent operators of uneven size (no counterpart in the
+ * reference, which holds one problem per process).  A batch refers to set-up
+ * operators on one device (it does not own them; destroy it first).  Vectors
+ * are packed: operator 0's n0 values, then operator 1's, ... (caller order
+ * within each). */
+typedef struct mlfma_batch_s* mlfma_batch;
+
+/* One CUDA graph holds every operator's product as a parallel branch, so one
+ * graph launch applies all of them.  The operators' own products must not
+ * overlap a batch product on the GPU (they share work buffers), and the graph
+ * keeps the launch shapes the operators had at creation: run mlfma_autotune
+ * on them first. */
+int mlfma_batch_create(int nops, const mlfma_handle* ops, mlfma_batch* out);
+/* Total length of the packed vectors. */
+int mlfma_batch_size(mlfma_batch b, long long* total);
+/* y = blockdiag(A_0, A_1, ...) x: host buffers, or device buffers on stream
+ * (NULL = the batch's own stream; asynchronous). */
+int mlfma_batch_matvec(mlfma_batch b, const double* x, double* y);
+int mlfma_batch_matvec_device(mlfma_batch b, const void* d_x, void* d_y, void* stream);
+/* Every operator's GMRES at once (one host thread each, each on its
+ * operator's streams); info: one record per operator (may be NULL).  Returns
+ * the worst status. */
+int mlfma_batch_gmres(mlfma_batch b, const double* rhs, double* x, const mlfma_solver_opts* opts,
+                      mlfma_solve_info* info);
+int mlfma_batch_destroy(mlfma_batch b);
+
 /* The handle's own CUDA stream (cudaStream_t as void*), on which mlfma_matvec
  * and mlfma_gmres run; callers may record events on it. */
 int mlfma_get_stream(mlfma_handle h, void** stream);

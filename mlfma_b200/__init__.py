@@ -21,7 +21,7 @@ from . import inputs
 from ._lib import (Config, MlfmaError, NotConverged, PlaneWaveC, SolveInfo, SolverOpts, StageTimes, Stats,
                    Traffic, Tuning, check, lib)
 
-__all__ = ["MLFMA", "MlfmaError", "NotConverged", "inputs", "default_config"]
+__all__ = ["MLFMA", "Batch", "MlfmaError", "NotConverged", "inputs", "default_config"]
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int)
@@ -358,3 +358,60 @@ class MLFMA:
         check(lib().mlfma_level_patterns(self._h, level, which, out.view(np.float64).ctypes.data_as(_dp),
                                          out.size))
         return out.reshape(nb, ndir, 2)
+
+
+class Batch:
+    """Many set-up operators applied together (mlfma_batch_*): one graph launch
+    runs every product; solve() runs every GMRES at once.  Vectors are lists
+    (one array per operator) or one packed array."""
+
+    def __init__(self, ops):
+        self.ops = list(ops)
+        arr = (ctypes.c_void_p * len(self.ops))(*[o._h.value for o in self.ops])
+        h = ctypes.c_void_p()
+        check(lib().mlfma_batch_create(len(self.ops), arr, ctypes.byref(h)))
+        self._h = h
+        self.sizes = [o.n for o in self.ops]
+        self.total = sum(self.sizes)
+
+    def _pack(self, xs):
+        if isinstance(xs, np.ndarray) and xs.ndim == 1 and xs.shape[0] == self.total:
+            return np.ascontiguousarray(xs, dtype=np.complex128)
+        return np.ascontiguousarray(np.concatenate([np.asarray(x, dtype=np.complex128) for x in xs]))
+
+    def _split(self, v):
+        return np.split(v, np.cumsum(self.sizes)[:-1])
+
+    def matvec(self, xs):
+        x = self._pack(xs)
+        y = np.zeros_like(x)
+        check(lib().mlfma_batch_matvec(self._h, x.view(np.float64).ctypes.data_as(_dp),
+                                       y.view(np.float64).ctypes.data_as(_dp)))
+        return self._split(y)
+
+    def matvec_device(self, x_ptr: int, y_ptr: int, stream: int = 0) -> None:
+        check(lib().mlfma_batch_matvec_device(self._h, ctypes.c_void_p(x_ptr), ctypes.c_void_p(y_ptr),
+                                              ctypes.c_void_p(stream)))
+
+    def solve(self, bs, max_iter: int = 500, tol: float = 1e-6, restart: int = 0, refine: bool = False):
+        b = self._pack(bs)
+        x = np.zeros_like(b)
+        o = SolverOpts(max_iter=max_iter, tol=tol, restart=restart, ref_givens=0, refine=int(refine))
+        infos = (SolveInfo * len(self.ops))()
+        code = lib().mlfma_batch_gmres(self._h, b.view(np.float64).ctypes.data_as(_dp),
+                                       x.view(np.float64).ctypes.data_as(_dp), ctypes.byref(o), infos)
+        if code not in (0, 4):
+            check(code)
+        return self._split(x), [SolveResult(i.iterations, i.residual, i.true_residual, i.seconds,
+                                            i.true_residual <= tol * (1 + 1e-12), i.refinements) for i in infos]
+
+    def close(self):
+        if self._h:
+            lib().mlfma_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -105,6 +105,14 @@ SIGNATURES = {
                                                 ctypes.c_int, _dp, ctypes.POINTER(SolverOpts), _dp, _dp, _dp, _dp,
                                                 ctypes.POINTER(SolveInfo)]),
     "mlfma_autotune": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(Tuning)]),
+    "mlfma_batch_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_void_p),
+                                          ctypes.POINTER(ctypes.c_void_p)]),
+    "mlfma_batch_size": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong)]),
+    "mlfma_batch_matvec": (ctypes.c_int, [ctypes.c_void_p, _dp, _dp]),
+    "mlfma_batch_matvec_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "mlfma_batch_gmres": (ctypes.c_int, [ctypes.c_void_p, _dp, _dp, ctypes.POINTER(SolverOpts),
+                                         ctypes.POINTER(SolveInfo)]),
+    "mlfma_batch_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "mlfma_get_stream": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]),
     "mlfma_time_stages": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(StageTimes)]),
     "mlfma_get_traffic": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Traffic)]),

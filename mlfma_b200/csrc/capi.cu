@@ -83,6 +83,11 @@ bool ready(mlfma_handle h) { return h && h->dev; }
 
 }  // namespace
 
+// Used by batch.cu.
+mlfma::DeviceOp* mlfma_internal_device(mlfma_handle h) { return h ? h->dev.get() : nullptr; }
+int mlfma_internal_fail(int code, const std::string& msg) { return fail(code, msg); }
+int mlfma_internal_device_ordinal(mlfma_handle h) { return h ? h->device : -1; }
+
 extern "C" {
 
 const char* mlfma_last_error(void) { return g_err.c_str(); }

@@ -183,6 +183,10 @@ public:
     void apply_tree_multi(const double2* xt, double2* yt, int nr, cudaStream_t s, int prec = -1);
     int max_rhs() const { return max_rhs_; }
 
+    // One product on caller-order device vectors, recorded on stream s with
+    // plain launches (for a capture that holds many operators' products).
+    void enqueue_matvec(const double2* x, double2* y, cudaStream_t s);
+
     // Per-stage CUDA-event timing of one matvec on the operator's stream.
     std::string time_stages(StageTimes* out);
     // Chooses launch shapes by timing them on this operator (see kernels.cu).

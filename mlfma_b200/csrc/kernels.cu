@@ -280,21 +280,25 @@ std::string DeviceOp::setup_far(const Plan& plan, FarField<R>& F, const double2*
     if (m2m_smem > static_cast<size_t>(dev_smem) || l2l_smem > static_cast<size_t>(dev_smem) ||
         s2m_smem > static_cast<size_t>(dev_smem))
         return "angular grid or leaf too large for the kernels' shared memory";
+    // The limit is a property of the kernel, shared by every operator in the
+    // process: set it to the device's opt-in maximum (this operator's needs
+    // were checked above), never to this operator's own size, or an operator
+    // set up later with smaller leaves or grids would make an earlier one's
+    // launches fail.
     const auto attr = cudaFuncAttributeMaxDynamicSharedMemorySize;
     for (int tr = 0; tr < 2; ++tr) {  // forward and transposed variants
         const bool t = tr != 0;
-        // up to the opt-in limit: the autotuner may choose more rows per block
         MLFMA_CK(cudaFuncSetAttribute(t ? k_m2m<R, 2, true> : k_m2m<R, 2, false>, attr, dev_smem));
         MLFMA_CK(cudaFuncSetAttribute(t ? k_m2m<R, 4, true> : k_m2m<R, 4, false>, attr, dev_smem));
         MLFMA_CK(cudaFuncSetAttribute(t ? k_m2m<R, 6, true> : k_m2m<R, 6, false>, attr, dev_smem));
         MLFMA_CK(cudaFuncSetAttribute(t ? k_m2m<R, 8, true> : k_m2m<R, 8, false>, attr, dev_smem));
         MLFMA_CK(cudaFuncSetAttribute(t ? k_m2m<R, 10, true> : k_m2m<R, 10, false>, attr, dev_smem));
-        MLFMA_CK(cudaFuncSetAttribute(t ? k_l2l<R, 8, true> : k_l2l<R, 8, false>, attr, static_cast<int>(l2l_smem)));
-        MLFMA_CK(cudaFuncSetAttribute(t ? k_l2l<R, 12, true> : k_l2l<R, 12, false>, attr, static_cast<int>(l2l_smem)));
-        MLFMA_CK(cudaFuncSetAttribute(t ? k_l2l<R, 16, true> : k_l2l<R, 16, false>, attr, static_cast<int>(l2l_smem)));
-        MLFMA_CK(cudaFuncSetAttribute(t ? k_l2l<R, 24, true> : k_l2l<R, 24, false>, attr, static_cast<int>(l2l_smem)));
-        MLFMA_CK(cudaFuncSetAttribute(t ? k_l2l<R, 32, true> : k_l2l<R, 32, false>, attr, static_cast<int>(l2l_smem)));
-        MLFMA_CK(cudaFuncSetAttribute(t ? k_s2m<R, true> : k_s2m<R, false>, attr, static_cast<int>(s2m_smem)));
+        MLFMA_CK(cudaFuncSetAttribute(t ? k_l2l<R, 8, true> : k_l2l<R, 8, false>, attr, dev_smem));
+        MLFMA_CK(cudaFuncSetAttribute(t ? k_l2l<R, 12, true> : k_l2l<R, 12, false>, attr, dev_smem));
+        MLFMA_CK(cudaFuncSetAttribute(t ? k_l2l<R, 16, true> : k_l2l<R, 16, false>, attr, dev_smem));
+        MLFMA_CK(cudaFuncSetAttribute(t ? k_l2l<R, 24, true> : k_l2l<R, 24, false>, attr, dev_smem));
+        MLFMA_CK(cudaFuncSetAttribute(t ? k_l2l<R, 32, true> : k_l2l<R, 32, false>, attr, dev_smem));
+        MLFMA_CK(cudaFuncSetAttribute(t ? k_s2m<R, true> : k_s2m<R, false>, attr, dev_smem));
     }
     if (max_rhs_ > 1) {
         // dynamic shared memory up to the opt-in limit less the kernel's static part
@@ -764,6 +768,15 @@ std::string DeviceOp::matvec_device(const double2* x, double2* y, bool accumulat
                                                  has_loads_ ? loads_ : nullptr, adj ? 1 : 0);
     MLFMA_CK(cudaGetLastError());
     return {};
+}
+
+// One product y = A x (caller order, device) on stream s, without graph
+// launches: for recording into a larger capture (many operators in one graph).
+void DeviceOp::enqueue_matvec(const double2* x, double2* y, cudaStream_t s) {
+    k_gather<<<blocks_for(n_, 256), 256, 0, s>>>(x, perm_, xt_, n_, 0);
+    enqueue_core(s, precision_, false);
+    k_finish<<<blocks_for(n_, 256), 256, 0, s>>>(yfar_, ynear_, perm_, y, n_, ck_, 0, xt_,
+                                                 has_loads_ ? loads_ : nullptr, 0);
 }
 
 std::string DeviceOp::time_stages(StageTimes* out) {

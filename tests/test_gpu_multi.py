@@ -152,3 +152,21 @@ def test_multi_edge_cases(cuda_device):
     assert np.all(Xs[1] == 0)
     assert rel(op.matvec(Xs[0]), B[0]) <= 1.0001e-10
     op.close()
+
+
+def test_operators_of_different_sizes_coexist(cuda_device):
+    # Kernel launch limits are shared by every operator in the process: an
+    # operator set up after one with larger leaves must not break the first
+    # one's products (first launched here after the second set-up).
+    from oracle import mlfma_oracle as O
+    d = inputs.make_dipoles(3000, seed=51)
+    big = MLFMA.dipoles(d, PW, max_node_srcs=64).setup()
+    small = MLFMA.dipoles(inputs.make_dipoles(500, seed=52), PW, max_node_srcs=8).setup()
+    x = cmat(1, big.n, 23)[0]
+    y = big.matvec(x)
+    ys = small.matvec(cmat(1, small.n, 24)[0])
+    assert np.all(np.isfinite(ys))
+    orc = O.Oracle(O.DipoleSources(d.pos, d.mom, PW), max_node_srcs=64)
+    assert rel(y, orc.matvec(x)) <= 1e-10
+    big.close()
+    small.close()
