@@ -41,6 +41,7 @@ WORKLOAD = dict(name="rwg_sphere_r2lambda_ico5", kind="rwg", level=5, radius=2.0
 HERE = os.path.dirname(os.path.abspath(__file__))
 SOLVE = dict(restart=50, tol=1e-4, max_iter=3000)
 NRHS = 64
+NPROB = 32
 
 
 def make_problem():
@@ -320,6 +321,71 @@ def batched_summary(bat, r64):
     return out
 
 
+def measure_problems(torch, dev, args) -> dict:
+    """Many independent dipole problems of uneven size in one graph launch
+    (mlfma_batch_*): NPROB problems, N log-uniform in [2,000, 50,000], seeded
+    uniform positions in cubes of side 2-6 wavelengths, unit diagonal,
+    complex-float far field and FP64 near field.  Device-resident batched
+    product against the same products one operator at a time."""
+    from mlfma_b200 import MLFMA, Batch, default_config, inputs
+    rng = np.random.default_rng(2024)
+    pw = inputs.PlaneWave(amplitude=1.0, pol=(1.0, 0.0, 0.0), khat=(0.0, 0.0, -1.0), wavenum=2.0 * np.pi)
+    ops = []
+    t0 = time.perf_counter()
+    for i in range(NPROB):
+        n = int(np.exp(rng.uniform(np.log(2000), np.log(50000))))
+        side = float(rng.uniform(2.0, 6.0))
+        d = inputs.make_dipoles(n, side=side, seed=100 + i)
+        cfg = default_config(max_node_srcs=64, root_leng=side, digits=3, interp_order=3, over_interp=2.0,
+                             device=dev.index, precision=1, ref_compat=0, self_terms=1)
+        op = MLFMA.dipoles(d, pw, config=cfg).setup()
+        op.autotune(1, reps=3)
+        ops.append(op)
+    setup_s = time.perf_counter() - t0
+    batch = Batch(ops)
+    sizes = [o.n for o in ops]
+    offs = np.concatenate([[0], np.cumsum(sizes)])
+    x = torch.randn(batch.total, dtype=torch.complex128, device=dev)
+    y = torch.zeros_like(x)
+    stream = torch.cuda.Stream(device=dev)
+    steps = max(3, args.steps // 5)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for _ in range(args.warmup):
+        batch.matvec_device(x.data_ptr(), y.data_ptr(), stream.cuda_stream)
+    torch.cuda.synchronize(dev)
+    e0.record(stream)
+    for _ in range(steps):
+        batch.matvec_device(x.data_ptr(), y.data_ptr(), stream.cuda_stream)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms_batch = e0.elapsed_time(e1) / steps
+    # the same products one operator at a time, on one stream
+    s0 = torch.cuda.ExternalStream(ops[0].stream(), device=dev)
+
+    def one_at_a_time():
+        for i, o in enumerate(ops):
+            o.matvec_device(x.data_ptr() + 16 * int(offs[i]), y.data_ptr() + 16 * int(offs[i]), False,
+                            s0.cuda_stream)
+
+    for _ in range(args.warmup):
+        one_at_a_time()
+    torch.cuda.synchronize(dev)
+    e0.record(s0)
+    for _ in range(steps):
+        one_at_a_time()
+    e1.record(s0)
+    torch.cuda.synchronize(dev)
+    ms_seq = e0.elapsed_time(e1) / steps
+    batch.close()
+    for o in ops:
+        o.close()
+    return {"workload": f"{NPROB} dipole problems, N log-uniform in [2000, 50000], cubes of side 2-6 wavelengths, "
+                        "unit diagonal, complex-float far field, FP64 near field",
+            "unknowns_total": int(offs[-1]), "sizes_min_max": [int(min(sizes)), int(max(sizes))],
+            "setup_s": setup_s, "ms_per_batched_product": ms_batch, "ms_one_operator_at_a_time": ms_seq,
+            "speedup": ms_seq / ms_batch, "problem_products_per_s": NPROB * 1000.0 / ms_batch}
+
+
 def solve_summary(sv):
     return {"seconds": sv["seconds"], "iterations": sv["iterations"], "true_residual_fp64": sv["true_residual"],
             "converged": sv["converged"], "refinements": sv["refinements"],
@@ -405,6 +471,7 @@ def main():
     bat = None
     if not args.no_batched:
         bat = {p: measure_batched(torch, dev, args, p) for p in ((0, 1) if not args.no_mixed else (0,))}
+    probs = None if args.no_batched else measure_problems(torch, dev, args)
 
     if rank == 0:
         cpu = None
@@ -453,6 +520,8 @@ def main():
                     np.linalg.norm(sm["far"] - s64["far"]) / np.linalg.norm(s64["far"]))
         if bat is not None:
             line["batched"] = batched_summary(bat, r64)
+        if probs is not None:
+            line["problems"] = probs
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
