@@ -209,6 +209,8 @@ int mlfma_matvec(mlfma_handle h, const double* x, double* y, int accumulate) {
         return fail(MLFMA_ERR_CUDA, "copy of y failed");
     const cudaError_t ce = cudaStreamSynchronize(s);
     if (ce != cudaSuccess) return fail(MLFMA_ERR_CUDA, cudaGetErrorString(ce));
+    e = h->dev->device_error();
+    if (!e.empty()) return fail(MLFMA_ERR_CUDA, e);
     return MLFMA_OK;
 }
 
@@ -245,6 +247,8 @@ int mlfma_gmres(mlfma_handle h, const double* b, double* x, const mlfma_solver_o
     if (cudaMemcpyAsync(x, h->d_y, bytes, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
         cudaStreamSynchronize(s) != cudaSuccess)
         return fail(MLFMA_ERR_CUDA, "copy of x failed");
+    e = h->dev->device_error();
+    if (!e.empty()) return fail(MLFMA_ERR_CUDA, e);
     if (info) {
         info->iterations = r.iterations;
         info->residual = r.residual;
@@ -498,6 +502,8 @@ static int solve_host(mlfma_handle h, const double* b, double* x, mlfma::SolveOp
     if (cudaMemcpyAsync(x, h->d_y, bytes, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
         cudaStreamSynchronize(s) != cudaSuccess)
         return fail(MLFMA_ERR_CUDA, "copy of x failed");
+    e = h->dev->device_error();
+    if (!e.empty()) return fail(MLFMA_ERR_CUDA, e);
     to_info(r, info);
     if (!r.converged) return fail(MLFMA_ERR_NOT_CONVERGED, "iteration limit reached");
     return MLFMA_OK;

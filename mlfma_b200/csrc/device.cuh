@@ -92,6 +92,19 @@ struct DevM2LGroup {
     long long t8_off;         // this group's transfer values: [ndir][ncand][kMaxGroup]
 };
 
+// A stored near-field block (the reference's storage: each interaction once)
+// and one tile of it; see NearBlock and NearTile in plan.hpp.
+struct DevNearBlock {
+    int row0, nrow, col0, ncol;
+    long long off;
+    int kind, pad;  // 0 rectangular, 1 strict-lower self, 2 lower self with diagonal
+};
+
+struct DevNearTile {
+    long long z;
+    int r0, c0, i0, ni, j0, nj, ld, kind, slot, mode;
+};
+
 struct DevNearRow {
     int row0, nrow, ncol, pad;
     long long off, col_off;
@@ -162,6 +175,10 @@ public:
     // adj: y = A^H x (needs ref_compat = 0).
     std::string matvec_device(const double2* x, double2* y, bool accumulate, cudaStream_t stream, int prec = -1,
                               bool adj = false);
+
+    // Non-empty when a kernel of this operator gave up a bounded wait (its
+    // results since then are not valid); read after the stream is synchronised.
+    std::string device_error() const;
 
     // Operator on tree-ordered device vectors (used by the solver).
     void apply_tree(const double2* xt, double2* yt, cudaStream_t s, int prec = -1, bool adj = false);
@@ -281,11 +298,22 @@ private:
     FarField<double> f64_;
     FarField<float> f32_;
 
-    DevNearRow* near_rows_ = nullptr;    // block rows (device storage of the near field)
+    // Near field, one vector: the stored blocks (each interaction once) applied
+    // as Z and Z^T tile by tile, partial sums added per target.
+    DevNearTile* near_tiles_ = nullptr;
+    int n_near_tiles_ = 0;
+    double2* near_bz_ = nullptr;          // block entries
+    long long near_block_entries_ = 0;
+    double2* near_part_ = nullptr;        // partial sums (near_parts)
+    int near_grid_ = 0;                   // persistent blocks of k_near_sym
+    int* err_host_ = nullptr;             // error word in mapped host memory
+    int* err_dev_ = nullptr;              //   and its device address
+    int* near_slot_ = nullptr;            // per tile: slots of its partials
+    int* near_red_ptr_ = nullptr;         // [n + 1]: target t's slots
+    // Near field, many right-hand sides: block rows (both orientations).
+    DevNearRow* near_rows_ = nullptr;
     int n_near_rows_ = 0;
     int* near_cols_ = nullptr;
-    int4* near_items_ = nullptr;         // (row block, first row, row count)
-    int n_near_items_ = 0;
     double2* near_z_ = nullptr;
     long long near_entries_ = 0;
 

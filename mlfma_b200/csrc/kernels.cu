@@ -9,8 +9,10 @@
 //     [box][direction][2 polarisation components];
 //   * radiation patterns as [source][direction of its leaf level][2];
 //   * transfer functions as [316 offsets][direction] per level;
-//   * the near field as block rows (both orientations of each reference
-//     block) with a shared column list per leaf.
+//   * the near field as the reference stores it, each interaction once
+//     (rectangular blocks row-major, self blocks packed lower-triangular),
+//     applied as Z and Z^T; with many right-hand sides also as block rows
+//     (both orientations) with a shared column list per leaf.
 // The far-field arrays are complex double (FP64 path) or complex float (mixed
 // path); x, y and the near field are complex double in both.
 //
@@ -114,6 +116,13 @@ DeviceOp::~DeviceOp() {
     if (side2_) cudaStreamDestroy(side2_);
     if (stream_) cudaStreamDestroy(stream_);
     if (side_) cudaStreamDestroy(side_);
+    if (err_host_) cudaFreeHost(err_host_);
+}
+
+std::string DeviceOp::device_error() const {
+    if (err_host_ && *static_cast<volatile int*>(err_host_))
+        return "near-field kernel: a bulk copy did not complete within its bounded wait";
+    return {};
 }
 
 template <class T>
@@ -503,28 +512,55 @@ std::string DeviceOp::setup(const Plan& plan, int device, int precision, int max
             if (!err.empty()) return err;
         }
 
-        // ---- near field: block rows (both orientations), gather-only application
-        std::vector<DevNearRow> nr;
-        std::vector<int4> nitems;
-        for (const NearRow& r : plan.near_rows) {
-            nr.push_back(DevNearRow{r.row0, r.nrow, r.ncol, 0, r.off, r.col_off});
-            for (int i0 = 0; i0 < r.nrow; i0 += kNearRowsPerBlock)
-                nitems.push_back(
-                    make_int4(static_cast<int>(nr.size()) - 1, i0, std::min(kNearRowsPerBlock, r.nrow - i0), 0));
+        // ---- near field: the stored blocks (each interaction once), applied
+        // as Z and Z^T tile by tile (one right-hand side)
+        {
+            std::vector<DevNearBlock> nb;
+            for (const NearBlock& b : plan.near_blocks)
+                nb.push_back(DevNearBlock{b.row0, b.nrow, b.col0, b.ncol, b.off,
+                                          b.self ? (plan.cfg.self_terms ? 2 : 1) : 0, 0});
+            std::vector<DevNearTile> nt;
+            for (const NearTile& t : plan.near_tiles)
+                nt.push_back(DevNearTile{t.z, t.r0, t.c0, t.i0, t.ni, t.j0, t.nj, t.ld, t.kind, t.slot, t.mode});
+            near_block_entries_ = plan.near_entries;
+            n_near_tiles_ = static_cast<int>(nt.size());
+            if (n_near_tiles_ > 0) {
+                near_tiles_ = upload(nt);
+                near_bz_ = alloc<double2>(static_cast<size_t>(near_block_entries_));
+                near_part_ = alloc<double2>(static_cast<size_t>(plan.near_parts));
+                near_red_ptr_ = upload(plan.near_red_ptr);
+                near_slot_ = upload(plan.near_slot);
+                MLFMA_CK(cudaHostAlloc(reinterpret_cast<void**>(&err_host_), sizeof(int), cudaHostAllocMapped));
+                *err_host_ = 0;
+                MLFMA_CK(cudaHostGetDevicePointer(reinterpret_cast<void**>(&err_dev_), err_host_, 0));
+                MLFMA_CK(cudaFuncSetAttribute(k_near_sym, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              static_cast<int>(kSymSmemBytes)));
+                int per_sm = 0, sms = 0;
+                MLFMA_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_near_sym, kSymThreads, kSymSmemBytes));
+                MLFMA_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_));
+                near_grid_ = std::max(1, std::min(n_near_tiles_, std::max(1, per_sm) * sms));
+                DevNearBlock* d_nb = upload(nb);
+                k_near_blocks_assemble<<<blocks_for(near_block_entries_, 128), 128, 0, stream_>>>(
+                    d_nb, static_cast<int>(nb.size()), near_block_entries_, S, near_bz_);
+                MLFMA_CK(cudaGetLastError());
+            }
         }
-        n_near_rows_ = static_cast<int>(nr.size());
-        near_rows_ = upload(nr);
-        near_cols_ = upload(plan.near_cols);
-        n_near_items_ = static_cast<int>(nitems.size());
-        near_items_ = upload(nitems);
-        near_entries_ = plan.near_row_entries;
-        near_z_ = alloc<double2>(static_cast<size_t>(near_entries_));
-        if (near_entries_ > 0) {
-            k_near_rows_assemble<<<blocks_for(near_entries_, 128), 128, 0, stream_>>>(
-                near_rows_, n_near_rows_, near_entries_, near_cols_, S, near_z_);
-            MLFMA_CK(cudaGetLastError());
+        // many right-hand sides: block rows (both orientations), gather-only GEMM tiles
+        if (max_rhs > 1) {
+            std::vector<DevNearRow> nr;
+            for (const NearRow& r : plan.near_rows) nr.push_back(DevNearRow{r.row0, r.nrow, r.ncol, 0, r.off, r.col_off});
+            n_near_rows_ = static_cast<int>(nr.size());
+            near_rows_ = upload(nr);
+            near_cols_ = upload(plan.near_cols);
+            near_entries_ = plan.near_row_entries;
+            near_z_ = alloc<double2>(static_cast<size_t>(near_entries_));
+            if (near_entries_ > 0) {
+                k_near_rows_assemble<<<blocks_for(near_entries_, 128), 128, 0, stream_>>>(
+                    near_rows_, n_near_rows_, near_entries_, near_cols_, S, near_z_);
+                MLFMA_CK(cudaGetLastError());
+            }
         }
-        traffic_.near = near_entries_ * 16.0 + n_ * 16.0 * 2.0;
+        traffic_.near = near_block_entries_ * 16.0 + n_ * 16.0 * 2.0;
         traffic_.total = traffic_.s2m + traffic_.m2m + traffic_.m2l + traffic_.l2l + traffic_.l2t + traffic_.near;
         if (max_rhs_ > 1) {
             err = build_m2l_groups(plan);
@@ -552,7 +588,7 @@ int DeviceOp::launches_per_matvec() const {
         for (int l = lmin_; l <= lmax_; ++l)
             if (m2l_count_[l]) n += 1;  // one M2L launch per level
     }
-    if (n_near_items_) n += 1;
+    if (n_near_tiles_) n += 2;  // tiles + per-target sums
     return n;
 }
 
@@ -682,18 +718,23 @@ void DeviceOp::run_far_overlap(const double2* xt, cudaStream_t s, cudaStream_t s
 }
 
 void DeviceOp::run_near(const double2* xt, cudaStream_t s) {
-    if (n_near_items_ == 0) return;
-    k_near_rows<<<n_near_items_, kNearRowThreads, 0, s>>>(near_rows_, near_items_, near_z_, near_cols_, xt, ynear_);
+    if (n_near_tiles_ == 0) {
+        cudaMemsetAsync(ynear_, 0, sizeof(double2) * n_, s);
+        return;
+    }
+    k_near_sym<<<near_grid_, kSymThreads, kSymSmemBytes, s>>>(near_tiles_, n_near_tiles_, near_bz_, xt, near_slot_,
+                                                             near_part_, err_dev_);
+    k_near_reduce<<<blocks_for(static_cast<long long>(n_) * kReduceLanes, 256), 256, 0, s>>>(near_red_ptr_, near_part_,
+                                                                                           n_, ynear_);
 }
 
 // The tree-ordered product xt_ -> (yfar_, ynear_): near field on the side
 // stream, far-field chain on s in precision prec (transposed when tr).
-// Captured once per (precision, direction) into a CUDA graph.  The stored near
-// field is symmetric to rounding (both orientations are assembled from the
-// same symmetric kernel), so the transposed product reuses it.
+// Captured once per (precision, direction) into a CUDA graph.  The near field
+// is symmetric (each stored block is applied as Z and Z^T), so the transposed
+// product reuses it; run_near writes every entry of ynear_.
 void DeviceOp::enqueue_core(cudaStream_t s, int prec, bool tr) {
     cudaMemsetAsync(yfar_, 0, sizeof(double2) * n_, s);
-    cudaMemsetAsync(ynear_, 0, sizeof(double2) * n_, s);
     cudaEventRecord(ev_fork_, s);
     cudaStreamWaitEvent(side_, ev_fork_, 0);
     run_near(xt_, side_);
@@ -787,7 +828,6 @@ std::string DeviceOp::time_stages(StageTimes* out) {
     cudaStream_t s = stream_;
     cudaEventRecord(ev[0], s);
     cudaMemsetAsync(yfar_, 0, sizeof(double2) * n_, s);
-    cudaMemsetAsync(ynear_, 0, sizeof(double2) * n_, s);
     cudaEventRecord(ev[1], s);
     for (int st = 0; st < 5; ++st) {
         run_far(xt_, s, st);

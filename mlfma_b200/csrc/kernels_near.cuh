@@ -15,39 +15,318 @@ namespace {
 // written out).  The reference stores each block once and applies it as Z and
 // Z^T.
 //
-// Block-row form: every leaf stores its rows against all sources it meets in
-// the near field (both orientations of each reference block, so no transposed
-// sums), sharing one column list per leaf.  A warp owns a row: coalesced
-// streaming reads of the row, gathers of x through the column list (the eight
-// warps of a thread block work on rows of the same leaf, so those gathers hit
-// L1), one shuffle reduction per row, a plain store (no atomics, fixed order).
-constexpr int kNearRowThreads = 256;
-constexpr int kNearRowsPerBlock = kNearRowThreads / 32;
+// Symmetric form (one right-hand side): every stored block is read once, in
+// tiles (NearTile in plan.hpp), and gives both its row sums (Z x, to the
+// block's rows) and its column sums (Z^T x, to its columns), as the reference
+// applies each block (Leaf::evalPairSols, src/fmm/leaf.cpp:329-354; a self
+// block strict-lower packed, Leaf::evalSelfSols, leaf.cpp:361-380).
+//
+// Persistent thread blocks, warp-specialised, a kSymStages-deep ring of
+// shared-memory stages per block.  Warp 0 (producer) fills a stage with bulk
+// asynchronous copies (cp.async.bulk on the TMA engine, no multicast): a tile
+// of whole rows is one contiguous span of the block storage and moves in one
+// copy of up to 16 KB (a tile of a wide or large self block moves row by row),
+// plus one copy each for the tile's column and row values of x and for the
+// slots of its partials, all counted on the stage's "full" mbarrier.  It reads
+// the tile headers a batch of 32 ahead, so no global load stands between two
+// tiles.  Warps 1-4 (consumers) compute from shared memory: 64 threads the row
+// sums, 64 the column sums (two threads per row or column when the tile has
+// at most 32; the diagonal of a self tile counts once, in its row), release the
+// stage on its "empty" mbarrier and write the partials to their slots.
+// k_near_reduce then adds each target's consecutive slots in a fixed order: no
+// atomics, a deterministic product.  HBM traffic: the block entries once (half
+// the block-row form), x from L2.
+//
+// Every mbarrier wait is bounded (about a second).  A consumer group that gives
+// up sets *err and returns; so does the producer, after bounded waits for the
+// copies it still has in flight.
+constexpr int kSymConsumers = 128;
+constexpr int kSymThreads = 32 + kSymConsumers;
+constexpr int kSymStages = 3;
+constexpr int kSymXc = kNearTileEntries;  // entry offsets within a stage
+constexpr int kSymXr = kSymXc + kNearTileCols;
+constexpr int kSymSlot = kSymXr + kNearTileRows;
+constexpr int kSymStageEntries = kSymSlot + (kNearTileRows + kNearTileCols) * 4 / 16;
+constexpr size_t kSymSmemBytes = sizeof(double2) * kSymStageEntries * kSymStages;
+static_assert(kNearTileCols == 64 && kNearTileRows == 64, "k_near_sym maps 64 row and 64 column threads");
+static_assert(kNearTileRowsSplit <= 32, "a mode-2 tile's rows are copied by one lane each");
+static_assert((kSymStageEntries * sizeof(double2)) % 16 == 0, "bulk copies need 16-byte aligned stages");
 
-__global__ void __launch_bounds__(kNearRowThreads)
-k_near_rows(const DevNearRow* __restrict__ rows, const int4* __restrict__ items, const double2* __restrict__ Z,
-            const int* __restrict__ cols, const double2* __restrict__ x, double2* __restrict__ y) {
-    const int4 it = items[blockIdx.x];  // row block, first row, row count
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (warp >= it.z) return;
-    const DevNearRow R = rows[it.x];
-    const int i = it.y + warp;
-    const double2* z = Z + R.off + static_cast<long long>(i) * R.ncol;
-    const int* ci = cols + R.col_off;
-    double2 a0 = z0(), a1 = z0(), a2 = z0(), a3 = z0();
-    int k = lane;
-    for (; k + 96 < R.ncol; k += 128) {
-        const double2 z0v = ldg_stream(z + k), z1v = ldg_stream(z + k + 32);
-        const double2 z2v = ldg_stream(z + k + 64), z3v = ldg_stream(z + k + 96);
-        const int c0 = ci[k], c1 = ci[k + 32], c2 = ci[k + 64], c3 = ci[k + 96];
-        a0 = cfma(z0v, x[c0], a0);
-        a1 = cfma(z1v, x[c1], a1);
-        a2 = cfma(z2v, x[c2], a2);
-        a3 = cfma(z3v, x[c3], a3);
+__device__ __forceinline__ long long packed_row(int i, int kind) {
+    return kind == 1 ? static_cast<long long>(i) * (i - 1) / 2 : static_cast<long long>(i) * (i + 1) / 2;
+}
+
+// Tile row r: its entries (from column j0 on) and where they start in the stage.
+__device__ __forceinline__ int tile_row_len(const DevNearTile& T, int r) {
+    if (T.kind == 0) return T.nj;
+    return max(0, min(T.nj, T.i0 + r + (T.kind == 2 ? 1 : 0) - T.j0));
+}
+__device__ __forceinline__ int tile_row_start(const DevNearTile& T, int r) {
+    return T.mode == 1 ? static_cast<int>(packed_row(T.i0 + r, T.kind) - packed_row(T.i0, T.kind)) : r * T.nj;
+}
+// First tile row holding an off-diagonal entry in tile column c.
+__device__ __forceinline__ int tile_col_start(const DevNearTile& T, int c) {
+    return T.kind == 0 ? 0 : max(0, T.j0 + c - T.i0 + 1);
+}
+// Entries the tile holds.
+__device__ __forceinline__ int tile_entries(const DevNearTile& T) {
+    return T.mode == 0 ? T.ni * T.nj : static_cast<int>(packed_row(T.i0 + T.ni, T.kind) - packed_row(T.i0, T.kind));
+}
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}" ::"r"(bar),
+                 "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+constexpr long long kWaitCycles = 1ll << 31;  // about a second at the B200 clock
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const long long t0 = clock64();
+    while (!mbar_try_wait(bar, parity))
+        if (clock64() - t0 > kWaitCycles) return false;
+    return true;
+}
+// Global -> this block's shared memory, completion counted on bar (bytes and
+// both addresses multiples of 16).
+__device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(src), "r"(bytes), "r"(bar)
+                 : "memory");
+}
+// OR of v over the consumer threads (named barrier 1), which all call it.
+__device__ __forceinline__ bool consumers_any(bool v) {
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\tsetp.ne.u32 p, %1, 0;\n\tbar.red.or.pred q, 1, %2, p;\n\tselp.u32 %0, 1, 0, q;\n\t}"
+        : "=r"(r)
+        : "r"(static_cast<uint32_t>(v)), "n"(kSymConsumers)
+        : "memory");
+    return r != 0;
+}
+__device__ __forceinline__ void consumers_sync() {
+    asm volatile("bar.sync 1, %0;" ::"n"(kSymConsumers) : "memory");
+}
+
+__global__ void __launch_bounds__(kSymThreads, 3)
+k_near_sym(const DevNearTile* __restrict__ tiles, int ntiles, const double2* __restrict__ Z,
+           const double2* __restrict__ x, const int* __restrict__ slots, double2* __restrict__ part,
+           int* __restrict__ err) {
+    extern __shared__ __align__(128) unsigned char sym_smem[];
+    double2* stages = reinterpret_cast<double2*>(sym_smem);
+    __shared__ __align__(8) unsigned long long full[kSymStages], empty[kSymStages];
+    __shared__ DevNearTile hdr[kSymStages];
+    __shared__ DevNearTile hbuf[32];  // producer's header batch
+    __shared__ double2 rowp[2][2][kNearTileRows], colp[2][2][kNearTileCols];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int step = gridDim.x;
+    if (tid == 0) {
+        for (int s = 0; s < kSymStages; ++s) {
+            mbar_init(smem_addr(&full[s]), 1);
+            mbar_init(smem_addr(&empty[s]), 1);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    for (; k < R.ncol; k += 32) a0 = cfma(ldg_stream(z + k), x[ci[k]], a0);
-    const double2 acc = warp_sum(cadd(cadd(a0, a1), cadd(a2, a3)));
-    if (lane == 0) y[R.row0 + i] = acc;
+    __syncthreads();
+
+    if (warp == 0) {  // ---- producer warp
+        // Lane k holds the k-th header of the next batch in registers (loaded
+        // a whole batch ahead) and parks it in hbuf when the batch starts.
+        int it = 0;
+        DevNearTile Tn{};
+        if (blockIdx.x + lane * step < ntiles) Tn = tiles[blockIdx.x + lane * step];
+        for (int t = blockIdx.x; t < ntiles; t += step, ++it) {
+            if ((it & 31) == 0) {
+                __syncwarp();
+                hbuf[lane] = Tn;
+                __syncwarp();
+                const int tb = t + (32 + lane) * step;
+                if (tb < ntiles) Tn = tiles[tb];
+            }
+            const DevNearTile T = hbuf[it & 31];
+            const int s = it % kSymStages;
+            if (it >= kSymStages && !mbar_wait_bounded(smem_addr(&empty[s]), ((it / kSymStages) - 1) & 1)) {
+                if (lane == 0) {
+                    atomicExch(err, 1);
+                    for (int k = 1; k <= kSymStages && k <= it; ++k)  // copies still in flight
+                        mbar_wait_bounded(smem_addr(&full[(it - k) % kSymStages]), ((it - k) / kSymStages) & 1);
+                }
+                return;
+            }
+            double2* st = stages + static_cast<size_t>(s) * kSymStageEntries;
+            int nv = 0, total;
+            long long off = 0;
+            if (T.mode == 2) {
+                if (lane < T.ni) {
+                    const int il = T.i0 + lane;
+                    nv = tile_row_len(T, lane);
+                    off = T.z + (T.kind == 0 ? static_cast<long long>(il) * T.ld : packed_row(il, T.kind)) + T.j0;
+                }
+                total = nv;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) total += __shfl_xor_sync(0xffffffffu, total, o);
+            } else {
+                total = tile_entries(T);
+            }
+            const int nslot = (T.ni + T.nj + 3) & ~3;
+            const uint32_t bytes = static_cast<uint32_t>((total + T.nj + T.ni) * sizeof(double2) + nslot * sizeof(int));
+            const uint32_t b = smem_addr(&full[s]);
+            if (lane == 0) {
+                hdr[s] = T;
+                mbar_arrive_expect_tx(b, bytes);
+            }
+            __syncwarp();
+            if (T.mode == 2) {
+                if (nv > 0) bulk_load(smem_addr(st + lane * T.nj), Z + off, static_cast<uint32_t>(nv * sizeof(double2)), b);
+            } else if (lane == 0) {
+                bulk_load(smem_addr(st), Z + T.z, static_cast<uint32_t>(total * sizeof(double2)), b);
+            }
+            if (lane == 31) bulk_load(smem_addr(st + kSymXc), x + T.c0 + T.j0, static_cast<uint32_t>(T.nj * sizeof(double2)), b);
+            if (lane == 30) bulk_load(smem_addr(st + kSymXr), x + T.r0 + T.i0, static_cast<uint32_t>(T.ni * sizeof(double2)), b);
+            if (lane == 29) bulk_load(smem_addr(st + kSymSlot), slots + T.slot, static_cast<uint32_t>(nslot * sizeof(int)), b);
+        }
+        return;
+    }
+
+    // ---- consumers: threads 0-63 rows, 64-127 columns
+    const int ct = tid - 32;
+    int it = 0;
+    for (int t = blockIdx.x; t < ntiles; t += step, ++it) {
+        const int s = it % kSymStages;
+        const bool ok = mbar_wait_bounded(smem_addr(&full[s]), (it / kSymStages) & 1);
+        if (consumers_any(!ok)) {
+            if (ct == 0) atomicExch(err, 1);
+            return;
+        }
+        const DevNearTile T = hdr[s];
+        const double2* zt = stages + static_cast<size_t>(s) * kSymStageEntries;
+        const double2* xc = zt + kSymXc;
+        const double2* xr = zt + kSymXr;
+        const int* sl = reinterpret_cast<const int*>(zt + kSymSlot);
+        const int b = it & 1;
+        int my_slot = -1, idx;
+        if (ct < 64) {  // row sums: two threads per row when the tile has at most 32 rows
+            const bool split = T.ni <= 32;
+            const int r = split ? (ct & 31) : ct, h = split ? (ct >> 5) : 0;
+            idx = r;
+            double2 a0 = z0(), a1 = z0(), a2 = z0(), a3 = z0();
+            if (r < T.ni) {
+                const int len = tile_row_len(T, r);
+                const int k0 = split && h ? (len + 1) >> 1 : 0, k1 = split && !h ? (len + 1) >> 1 : len;
+                const int L = k1 - k0;
+                const double2* zr = zt + tile_row_start(T, r) + k0;
+                const double2* xk = xc + k0;
+                // rows nj apart with nj even share banks: start each row at its
+                // own offset (any fixed order of the sum is as good)
+                const int q = (T.mode != 1 && !(T.nj & 1) && L > 0) ? r % L : 0;
+                int n = 0;
+                for (; n + 3 < L; n += 4) {
+                    int k = q + n;
+                    k -= k >= L ? L : 0;
+                    a0 = cfma(zr[k], xk[k], a0);
+                    k = k + 1 == L ? 0 : k + 1;
+                    a1 = cfma(zr[k], xk[k], a1);
+                    k = k + 1 == L ? 0 : k + 1;
+                    a2 = cfma(zr[k], xk[k], a2);
+                    k = k + 1 == L ? 0 : k + 1;
+                    a3 = cfma(zr[k], xk[k], a3);
+                }
+                for (; n < L; ++n) {
+                    int k = q + n;
+                    k -= k >= L ? L : 0;
+                    a0 = cfma(zr[k], xk[k], a0);
+                }
+                if (h == 0) my_slot = sl[r];
+            }
+            rowp[b][h][r] = cadd(cadd(a0, a1), cadd(a2, a3));
+            if (!split) rowp[b][1][r] = z0();
+        } else {  // column sums: two threads per column when the tile has at most 32 columns
+            const int cc = ct - 64;
+            const bool split = T.nj <= 32;
+            const int c = split ? (cc & 31) : cc, h = split ? (cc >> 5) : 0;
+            idx = c;
+            double2 a0 = z0(), a1 = z0(), a2 = z0(), a3 = z0();
+            if (c < T.nj) {
+                const int rs = tile_col_start(T, c);
+                const int mid = (rs + T.ni + 1) >> 1;
+                const int ra = split && h ? mid : rs, rb = split && !h ? mid : T.ni;
+                // walk down the column: rows nj apart, or (packed) one longer each
+                const int inc = T.mode == 1 ? 1 : 0;
+                int stride = T.mode == 1 ? T.i0 + ra + (T.kind == 2 ? 1 : 0) : T.nj;
+                const double2* zc = zt + tile_row_start(T, ra) + c;
+                int r = ra;
+                for (; r + 3 < rb; r += 4) {
+                    a0 = cfma(*zc, xr[r], a0);
+                    zc += stride;
+                    stride += inc;
+                    a1 = cfma(*zc, xr[r + 1], a1);
+                    zc += stride;
+                    stride += inc;
+                    a2 = cfma(*zc, xr[r + 2], a2);
+                    zc += stride;
+                    stride += inc;
+                    a3 = cfma(*zc, xr[r + 3], a3);
+                    zc += stride;
+                    stride += inc;
+                }
+                for (; r < rb; ++r) {
+                    a0 = cfma(*zc, xr[r], a0);
+                    zc += stride;
+                    stride += inc;
+                }
+                if (h == 0) my_slot = sl[T.ni + c];
+            }
+            colp[b][h][c] = cadd(cadd(a0, a1), cadd(a2, a3));
+            if (!split) colp[b][1][c] = z0();
+        }
+        consumers_sync();  // stage s read, partial halves complete
+        if (ct == 0) mbar_arrive(smem_addr(&empty[s]));
+        if (my_slot >= 0)
+            part[my_slot] = ct < 64 ? cadd(rowp[b][0][idx], rowp[b][1][idx]) : cadd(colp[b][0][idx], colp[b][1][idx]);
+    }
+}
+
+// y[t] = sum of target t's consecutive partial slots: eight lanes per target,
+// a fixed shuffle tree, so the order never changes.
+constexpr int kReduceLanes = 8;
+
+__global__ void k_near_reduce(const int* __restrict__ ptr, const double2* __restrict__ part, int n,
+                              double2* __restrict__ y) {
+    const long long g = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int t = static_cast<int>(g / kReduceLanes);
+    const int l = static_cast<int>(g % kReduceLanes);
+    double2 acc = z0();
+    if (t < n) {
+        const int p0 = ptr[t] + l, p1 = ptr[t + 1];
+        double2 v[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) v[u] = p0 + u * kReduceLanes < p1 ? part[p0 + u * kReduceLanes] : z0();
+        acc = cadd(cadd(v[0], v[1]), cadd(v[2], v[3]));
+        for (int p = p0 + 4 * kReduceLanes; p < p1; p += kReduceLanes) acc = cadd(acc, part[p]);
+    }
+#pragma unroll
+    for (int o = kReduceLanes / 2; o > 0; o >>= 1) {
+        acc.x += __shfl_xor_sync(0xffffffffu, acc.x, o);
+        acc.y += __shfl_xor_sync(0xffffffffu, acc.y, o);
+    }
+    if (t < n && l == 0) y[t] = acc;
 }
 
 // ------------------------------------------------------------ setup kernels
@@ -229,6 +508,37 @@ __global__ void k_farfield_adj(DevSources S, const int* __restrict__ perm, int n
     }
     const zd r = zd{ck.x, -ck.y} * acc;
     g[perm[t]] = make_double2(r.x, r.y);
+}
+
+// Entries of the stored blocks: thread per entry.  A self block is packed
+// lower-triangular: row i starts at i(i-1)/2 (strict) or i(i+1)/2 (with its
+// diagonal).  Each value is Z_mn for the block's row m and column n, used as
+// Z_nm as well.
+__global__ void k_near_blocks_assemble(const DevNearBlock* __restrict__ blocks, int nblocks, long long total,
+                                       DevSources S, double2* __restrict__ Z) {
+    const long long e = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (e >= total) return;
+    int lo = 0, hi = nblocks - 1;
+    while (lo < hi) {  // last block with off <= e
+        const int mid = (lo + hi + 1) >> 1;
+        if (blocks[mid].off <= e) lo = mid; else hi = mid - 1;
+    }
+    const DevNearBlock B = blocks[lo];
+    const long long loc = e - B.off;
+    int i, j;
+    if (B.kind == 0) {
+        i = static_cast<int>(loc / B.ncol);
+        j = static_cast<int>(loc - static_cast<long long>(i) * B.ncol);
+    } else {
+        // largest i with packed_row(i) <= loc (estimate, then correct by one)
+        const double q = sqrt(1.0 + 8.0 * static_cast<double>(loc));
+        i = static_cast<int>(B.kind == 1 ? (1.0 + q) * 0.5 : (q - 1.0) * 0.5);
+        while (i > 0 && packed_row(i, B.kind) > loc) --i;
+        while (packed_row(i + 1, B.kind) <= loc) ++i;
+        j = static_cast<int>(loc - packed_row(i, B.kind));
+    }
+    const zd z = near_entry(S, B.row0 + i, B.col0 + j);
+    Z[e] = make_double2(z.x, z.y);
 }
 
 // Entries of the block rows: thread per entry.

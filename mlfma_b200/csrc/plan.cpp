@@ -7,6 +7,7 @@
 #include <deque>
 #include <thread>
 #include <functional>
+#include <limits>
 #include <stdexcept>
 #include <unordered_map>
 
@@ -922,6 +923,76 @@ void Plan::build_near_plan() {
     for (int a : leaves) {
         const Node& A = nodes[a];
         add(A.src_begin, A.src_count, A.src_begin, A.src_count, 1);
+    }
+
+    // Tiles of the stored blocks and the partial sums they write.  A self block
+    // is packed lower-triangular (row i holds columns 0..i-1, or 0..i with the
+    // diagonal).  Partials are numbered tile by tile (rows, then columns), then
+    // given slots sorted by target, ties in that order.
+    near_tiles.clear();
+    long long parts = 0;
+    std::vector<int> part_tgt;
+    auto tri = [](long long i, int kind) { return kind == 1 ? i * (i - 1) / 2 : i * (i + 1) / 2; };
+    auto push = [&](const NearBlock& b, int kind, int mode, long long z, int i0, int ni, int j0, int nj) {
+        NearTile t;
+        t.z = z;
+        t.r0 = b.row0;
+        t.c0 = b.col0;
+        t.i0 = i0;
+        t.ni = ni;
+        t.j0 = j0;
+        t.nj = nj;
+        t.ld = kind == 0 ? b.ncol : 0;
+        t.kind = kind;
+        t.slot = 0;
+        t.mode = mode;
+        parts += ni + nj;
+        if (parts > std::numeric_limits<int>::max() / 2) throw std::runtime_error("near field: too many partial sums");
+        for (int i = 0; i < ni; ++i) part_tgt.push_back(b.row0 + i0 + i);
+        for (int j = 0; j < nj; ++j) part_tgt.push_back(b.col0 + j0 + j);
+        near_tiles.push_back(t);
+    };
+    for (const NearBlock& b : near_blocks) {
+        const int kind = b.self ? (cfg.self_terms ? 2 : 1) : 0;
+        const int d = kind == 2 ? 1 : 0;
+        if (kind == 0 && b.ncol <= kNearTileCols) {  // whole rows
+            const int rows = std::min(kNearTileRows, kNearTileEntries / b.ncol);
+            for (int i0 = 0; i0 < b.nrow; i0 += rows)
+                push(b, 0, 0, b.off + static_cast<long long>(i0) * b.ncol, i0, std::min(rows, b.nrow - i0), 0, b.ncol);
+        } else if (kind != 0 && b.nrow <= kNearTileCols) {  // whole packed rows
+            for (int i0 = 0; i0 < b.nrow;) {
+                int ni = 1;
+                while (i0 + ni < b.nrow && ni < kNearTileRows && tri(i0 + ni + 1, kind) - tri(i0, kind) <= kNearTileEntries)
+                    ++ni;
+                const int nj = i0 + ni - 1 + d;  // columns 0 .. nj - 1
+                if (nj > 0) push(b, kind, 1, b.off + tri(i0, kind), i0, ni, 0, nj);
+                i0 += ni;
+            }
+        } else {  // column ranges, row by row
+            for (int i0 = 0; i0 < b.nrow; i0 += kNearTileRowsSplit) {
+                const int ni = std::min(kNearTileRowsSplit, b.nrow - i0);
+                for (int j0 = 0; j0 < b.ncol; j0 += kNearTileCols) {
+                    if (kind != 0 && j0 >= i0 + ni - 1 + d) break;  // no entries from here on
+                    push(b, kind, 2, b.off, i0, ni, j0, std::min(kNearTileCols, b.ncol - j0));
+                }
+            }
+        }
+    }
+    near_parts = static_cast<int>(parts);
+    near_red_ptr.assign(n + 1, 0);
+    for (int t : part_tgt) ++near_red_ptr[t + 1];
+    for (int t = 0; t < n; ++t) near_red_ptr[t + 1] += near_red_ptr[t];
+    {
+        std::vector<int> fill(near_red_ptr.begin(), near_red_ptr.end() - 1);
+        near_slot.clear();
+        int p = 0;
+        for (NearTile& t : near_tiles) {
+            t.slot = static_cast<int>(near_slot.size());
+            const int cnt = t.ni + t.nj;
+            for (int q = 0; q < cnt; ++q) near_slot.push_back(fill[part_tgt[p + q]]++);
+            while (near_slot.size() % 4) near_slot.push_back(0);
+            p += cnt;
+        }
     }
 
     // Block rows: every stored block in both orientations.

@@ -107,6 +107,32 @@ struct NearRow {
     long long col_off;  // offset into near_cols
 };
 
+// One tile of a stored near-field block for the symmetric application: the
+// tile's entries are read once and give both its row sums (Z x) and its column
+// sums (Z^T x).  Each sum is a partial written to its slot; a target's
+// partials occupy consecutive slots (near_red_ptr), added in a second pass in a
+// fixed order.  A tile holds at most kNearTileEntries entries, kNearTileRows
+// rows and kNearTileCols columns, laid out in one of three ways:
+//   mode 0: whole rows of a rectangular block, one contiguous span (row stride nj);
+//   mode 1: whole rows of a packed self block, one contiguous span (row i0 + r
+//           has i0 + r entries, i0 + r + 1 with the diagonal, from column 0);
+//   mode 2: a column range of some rows (wide or large self blocks), row by row,
+//           rows nj apart in the tile.
+constexpr int kNearTileRows = 64;
+constexpr int kNearTileCols = 64;
+constexpr int kNearTileEntries = 1024;
+constexpr int kNearTileRowsSplit = kNearTileEntries / kNearTileCols;  // rows of a mode-2 tile
+
+struct NearTile {
+    long long z;          // first entry (modes 0, 1) or the block's first entry (mode 2)
+    int r0, c0;           // block's first row and first column source (tree order)
+    int i0, ni, j0, nj;   // tile rows [i0, i0 + ni) and columns [j0, j0 + nj) within the block
+    int ld;               // row stride of a rectangular block in the block storage (0 for a self block)
+    int kind;             // 0 rectangular; 1 strict-lower self; 2 lower self with its diagonal
+    int slot;             // near_slot offset (a multiple of 4): ni row slots, then nj column slots
+    int mode;             // layout, above
+};
+
 struct FarLeaf {
     int level, box, src0, nsrc;
     long long pat_off;  // offset in units of (direction, 2 components)
@@ -144,7 +170,11 @@ struct Plan {
     // Near field
     std::vector<NearBlock> near_blocks;   // each interaction once (reference storage)
     long long near_entries = 0;
-    std::vector<NearRow> near_rows;       // both orientations, per leaf (device storage)
+    std::vector<NearTile> near_tiles;     // symmetric application of near_blocks
+    int near_parts = 0;                   // partial sums the tiles write
+    std::vector<int> near_slot;           // per tile, padded to 4: slot of each partial
+    std::vector<int> near_red_ptr;        // [n + 1]: target t's partials are slots ptr[t]..ptr[t+1]
+    std::vector<NearRow> near_rows;       // both orientations, per leaf (many-rhs storage)
     std::vector<int> near_cols;
     long long near_row_entries = 0;
     // Stats
