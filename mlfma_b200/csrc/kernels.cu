@@ -538,7 +538,9 @@ std::string DeviceOp::setup(const Plan& plan, int device, int precision, int max
                 int per_sm = 0, sms = 0;
                 MLFMA_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_near_sym, kSymThreads, kSymSmemBytes));
                 MLFMA_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_));
-                near_grid_ = std::max(1, std::min(n_near_tiles_, std::max(1, per_sm) * sms));
+                // at least four tiles per block, so that a small operator leaves
+                // room for the kernels of others running beside it
+                near_grid_ = std::max(1, std::min({n_near_tiles_ / 4, std::max(1, per_sm) * sms}));
                 DevNearBlock* d_nb = upload(nb);
                 k_near_blocks_assemble<<<blocks_for(near_block_entries_, 128), 128, 0, stream_>>>(
                     d_nb, static_cast<int>(nb.size()), near_block_entries_, S, near_bz_);

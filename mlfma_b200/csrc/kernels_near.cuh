@@ -42,7 +42,7 @@ namespace {
 // copies it still has in flight.
 constexpr int kSymConsumers = 128;
 constexpr int kSymThreads = 32 + kSymConsumers;
-constexpr int kSymStages = 3;
+constexpr int kSymStages = 2;
 constexpr int kSymXc = kNearTileEntries;  // entry offsets within a stage
 constexpr int kSymXr = kSymXc + kNearTileCols;
 constexpr int kSymSlot = kSymXr + kNearTileRows;
@@ -125,7 +125,7 @@ __device__ __forceinline__ void consumers_sync() {
     asm volatile("bar.sync 1, %0;" ::"n"(kSymConsumers) : "memory");
 }
 
-__global__ void __launch_bounds__(kSymThreads, 3)
+__global__ void __launch_bounds__(kSymThreads, 4)
 k_near_sym(const DevNearTile* __restrict__ tiles, int ntiles, const double2* __restrict__ Z,
            const double2* __restrict__ x, const int* __restrict__ slots, double2* __restrict__ part,
            int* __restrict__ err) {
