@@ -42,6 +42,7 @@ struct DevLevelT {
     const int* m2l_ptr;          // [nbox+1]
     const int* m2l_src;
     const int* m2l_off;
+    const int* anti;             // [ndir]: element of the antipodal direction, for elements e < ndir
 };
 
 // Stencil rows padded to a fixed width (padding entries have coefficient 0):
@@ -152,7 +153,8 @@ struct FarField {
     DevLevelT<R> lv[kMaxLevels] = {};
     DevLevelT<R>* lv_dev = nullptr;
     std::vector<DevTransT<R>> trans;  // index = parent level
-    C* pat = nullptr;                 // radiation patterns [pat_elems][2]
+    C* pat = nullptr;                 // radiation patterns [pat_elems][2] (FP64; many right-hand sides)
+    C* hpat = nullptr;                // complex float: directions d < ndir/2 of each source, [pat_elems / 2][2]
     C* m2l_t8 = nullptr;              // many-rhs M2L: pre-gathered weighted transfer values
 };
 
@@ -290,9 +292,12 @@ private:
     std::vector<int> n_l2l_pairs_, npar_, up_w_, dn_w_;
     int4* s2m_items_ = nullptr;          // (leaf, first element, element count)
     int n_s2m_items_ = 0;
+    int4* s2m_items_h_ = nullptr;        // the same over the stored half (half patterns)
+    int n_s2m_items_h_ = 0;
     int4* l2t_items_ = nullptr;          // (leaf, first source, source count)
     int n_l2t_items_ = 0;
     int max_src_ = 0;                    // largest far leaf
+    int max_leaf_ndir_ = 0;              // most directions on a level holding far leaves
     DevFarLeaf* leaves_ = nullptr;
     int n_leaves_ = 0;
     FarField<double> f64_;

@@ -135,10 +135,20 @@ T* DeviceOp::alloc(size_t count) {
     return static_cast<T*>(p);
 }
 
+// Host-to-device copy that has landed when it returns.  cudaMemcpy from
+// pageable memory may return once the data is staged, before the DMA (on the
+// legacy default stream) reaches device memory, and kernels on this operator's
+// non-blocking streams are not ordered after it.
+static cudaError_t h2d_landed(void* dst, const void* src, size_t bytes) {
+    cudaError_t e = cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(cudaStreamLegacy);
+    return e;
+}
+
 template <class T>
 T* DeviceOp::upload(const std::vector<T>& v) {
     T* p = alloc<T>(v.size());
-    if (!v.empty() && cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice) != cudaSuccess)
+    if (!v.empty() && h2d_landed(p, v.data(), v.size() * sizeof(T)) != cudaSuccess)
         throw std::runtime_error("cudaMemcpy failed");
     return p;
 }
@@ -171,7 +181,7 @@ void DeviceOp::build_m2l_items(int max_chunk) {
     }
     n_m2l_items_ = static_cast<int>(items.size());
     m2l_chunk_ = max_chunk;
-    if (!items.empty()) cudaMemcpy(m2l_items_, items.data(), sizeof(int4) * items.size(), cudaMemcpyHostToDevice);
+    if (!items.empty()) h2d_landed(m2l_items_, items.data(), sizeof(int4) * items.size());
 }
 
 // Far-field arrays in precision R (levels, transitions, patterns).
@@ -204,6 +214,14 @@ std::string DeviceOp::setup_far(const Plan& plan, FarField<R>& F, const double2*
         d.m2l_ptr = upload(L.m2l_ptr);
         d.m2l_src = upload(L.m2l_src);
         d.m2l_off = upload(L.m2l_off);
+        // antipode of direction (ith, iph): (nth - 1 - ith, iph + nph / 2); the
+        // first half of the directions (d < ndir / 2) meets every pair once
+        std::vector<int> anti(L.ndir);
+        for (int e = 0; e < L.ndir; ++e) {
+            const int dd = e >> 1, ith = dd / L.nph, iph = dd % L.nph;
+            anti[e] = (((L.nth - 1 - ith) * L.nph + (iph + L.nph / 2) % L.nph) << 1) | (e & 1);
+        }
+        d.anti = upload(anti);
     }
     F.lv_dev = upload(std::vector<DevLevelT<R>>(F.lv, F.lv + kMaxLevels));
     F.trans.assign(std::max(lmax_, 0) + 1, DevTransT<R>{});
@@ -271,10 +289,15 @@ std::string DeviceOp::setup_far(const Plan& plan, FarField<R>& F, const double2*
     }
     if (std::is_same<R, double>::value) {
         F.pat = reinterpret_cast<C*>(const_cast<double2*>(pat64));
-    } else {
+    } else if (max_rhs_ > 1) {
         const long long cnt = plan.pat_elems * 2;
         F.pat = alloc<C>(static_cast<size_t>(cnt));
         if (cnt) k_narrow<C><<<blocks_for(cnt, 256), 256, 0, stream_>>>(pat64, F.pat, cnt);
+        MLFMA_CK(cudaGetLastError());
+    }
+    if constexpr (!std::is_same<R, double>::value) {  // half patterns for the complex-float far field
+        F.hpat = alloc<C>(static_cast<size_t>(plan.pat_elems));
+        if (n_leaves_) k_half_patterns<R><<<n_leaves_, 256, 0, stream_>>>(F.lv_dev, leaves_, pat64, F.hpat);
         MLFMA_CK(cudaGetLastError());
     }
     // Shared-memory limits.
@@ -286,8 +309,11 @@ std::string DeviceOp::setup_far(const Plan& plan, FarField<R>& F, const double2*
     int dev_smem = 0;
     MLFMA_CK(cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, device_));
     const size_t s2m_smem = static_cast<size_t>(std::max(1, max_src_)) * sizeof(C);
+    // k_l2t_half (complex-float far field) stages a leaf's local pattern twice
+    const size_t l2t_smem = 2 * sizeof(C) * static_cast<size_t>(max_leaf_ndir_);
     if (m2m_smem > static_cast<size_t>(dev_smem) || l2l_smem > static_cast<size_t>(dev_smem) ||
-        s2m_smem > static_cast<size_t>(dev_smem))
+        s2m_smem > static_cast<size_t>(dev_smem) ||
+        (!std::is_same<R, double>::value && l2t_smem > static_cast<size_t>(dev_smem)))
         return "angular grid or leaf too large for the kernels' shared memory";
     // The limit is a property of the kernel, shared by every operator in the
     // process: set it to the device's opt-in maximum (this operator's needs
@@ -308,6 +334,10 @@ std::string DeviceOp::setup_far(const Plan& plan, FarField<R>& F, const double2*
         MLFMA_CK(cudaFuncSetAttribute(t ? k_l2l<R, 24, true> : k_l2l<R, 24, false>, attr, dev_smem));
         MLFMA_CK(cudaFuncSetAttribute(t ? k_l2l<R, 32, true> : k_l2l<R, 32, false>, attr, dev_smem));
         MLFMA_CK(cudaFuncSetAttribute(t ? k_s2m<R, true> : k_s2m<R, false>, attr, dev_smem));
+        if constexpr (!std::is_same<R, double>::value) {
+            MLFMA_CK(cudaFuncSetAttribute(t ? k_s2m_half<R, true> : k_s2m_half<R, false>, attr, dev_smem));
+            MLFMA_CK(cudaFuncSetAttribute(t ? k_l2t_half<R, true> : k_l2t_half<R, false>, attr, dev_smem));
+        }
     }
     if (max_rhs_ > 1) {
         // dynamic shared memory up to the opt-in limit less the kernel's static part
@@ -441,7 +471,7 @@ std::string DeviceOp::setup(const Plan& plan, int device, int precision, int max
         // ---- far leaves and work items
         std::vector<DevFarLeaf> h_leaves;
         std::vector<DevFarLeafGeom> geo;
-        std::vector<int4> s2m_items, l2t_items;
+        std::vector<int4> s2m_items, s2m_items_h, l2t_items;
         max_src_ = 0;
         for (const FarLeaf& f : plan.far_leaves) {
             h_leaves.push_back(DevFarLeaf{f.level, f.box, f.src0, f.nsrc, f.pat_off});
@@ -450,9 +480,16 @@ std::string DeviceOp::setup(const Plan& plan, int device, int precision, int max
             const int nchunk = (ne + kS2MThreads - 1) / kS2MThreads;
             const int chunk = (ne + nchunk - 1) / nchunk;
             for (int e0 = 0; e0 < ne; e0 += chunk) s2m_items.push_back(make_int4(li, e0, std::min(chunk, ne - e0), 0));
+            // half patterns (complex-float far field): elements of the first half of the directions
+            const int nh = ne / 2;
+            const int nchunk_h = (nh + kS2MThreads - 1) / kS2MThreads;
+            const int chunk_h = (nh + nchunk_h - 1) / nchunk_h;
+            for (int e0 = 0; e0 < nh; e0 += chunk_h)
+                s2m_items_h.push_back(make_int4(li, e0, std::min(chunk_h, nh - e0), 0));
             for (int s0 = 0; s0 < f.nsrc; s0 += kL2TSrcPerBlock)
                 l2t_items.push_back(make_int4(li, s0, std::min(kL2TSrcPerBlock, f.nsrc - s0), 0));
             max_src_ = std::max(max_src_, f.nsrc);
+            max_leaf_ndir_ = std::max(max_leaf_ndir_, plan.levels[f.level].ndir);
             const Node& nd = plan.nodes[plan.levels[f.level].boxes[f.box]];
             geo.push_back(DevFarLeafGeom{{nd.center[0], nd.center[1], nd.center[2]}});
         }
@@ -460,10 +497,14 @@ std::string DeviceOp::setup(const Plan& plan, int device, int precision, int max
         leaves_ = upload(h_leaves);
         n_s2m_items_ = static_cast<int>(s2m_items.size());
         s2m_items_ = upload(s2m_items);
+        n_s2m_items_h_ = static_cast<int>(s2m_items_h.size());
+        if (precision != kFp64) s2m_items_h_ = upload(s2m_items_h);
         n_l2t_items_ = static_cast<int>(l2t_items.size());
         l2t_items_ = upload(l2t_items);
-        traffic_.s2m = plan.pat_elems * 2.0 * cbytes + n_ * 16.0;
-        traffic_.l2t = plan.pat_elems * 2.0 * cbytes + n_ * 16.0;
+        // the complex-float far field keeps half the patterns (antipodes by symmetry)
+        const double pat_copies = precision == kFp64 ? 2.0 : 1.0;
+        traffic_.s2m = plan.pat_elems * pat_copies * cbytes + n_ * 16.0;
+        traffic_.l2t = plan.pat_elems * pat_copies * cbytes + n_ * 16.0;
 
         // ---- radiation patterns (complex double first)
         DevSources S{};
@@ -493,7 +534,7 @@ std::string DeviceOp::setup(const Plan& plan, int device, int precision, int max
             // the host with the reference's exact rounding and uploaded.
             std::vector<cplx> hp;
             plan.rwg_patterns_host(hp);
-            MLFMA_CK(cudaMemcpy(pat64, hp.data(), hp.size() * sizeof(cplx), cudaMemcpyHostToDevice));
+            MLFMA_CK(h2d_landed(pat64, hp.data(), hp.size() * sizeof(cplx)));
         } else if (n_leaves_ > 0) {
             std::vector<DevGeomLevel> gl(kMaxLevels, DevGeomLevel{nullptr, nullptr, 0});
             for (int l = lmin_; l <= lmax_; ++l)
@@ -571,6 +612,7 @@ std::string DeviceOp::setup(const Plan& plan, int device, int precision, int max
             if (!err.empty()) return err;
         }
         MLFMA_CK(cudaStreamSynchronize(stream_));
+        MLFMA_CK(cudaStreamSynchronize(cudaStreamLegacy));  // the memsets above run there
         MLFMA_CK(cudaGetLastError());
         ready_ = true;
         return {};
@@ -602,9 +644,14 @@ int DeviceOp::launches_per_matvec() const {
 template <class R, bool TR>
 void DeviceOp::far_s2m(FarField<R>& F, const double2* xt, cudaStream_t s) {
     using C = typename Cx<R>::T;
-    if (n_s2m_items_)
-        k_s2m<R, TR><<<n_s2m_items_, kS2MThreads, sizeof(C) * std::max(1, max_src_), s>>>(F.lv_dev, s2m_items_,
-                                                                                            leaves_, F.pat, xt);
+    if constexpr (std::is_same<R, double>::value) {
+        if (n_s2m_items_)
+            k_s2m<R, TR><<<n_s2m_items_, kS2MThreads, sizeof(C) * std::max(1, max_src_), s>>>(F.lv_dev, s2m_items_,
+                                                                                                leaves_, F.pat, xt);
+    } else if (n_s2m_items_h_) {
+        k_s2m_half<R, TR><<<n_s2m_items_h_, kS2MThreads, sizeof(C) * std::max(1, max_src_), s>>>(
+            F.lv_dev, s2m_items_h_, leaves_, F.hpat, xt);
+    }
 }
 
 template <class R, bool TR>
@@ -651,8 +698,12 @@ void DeviceOp::far_l2l(FarField<R>& F, int p, cudaStream_t s) {
 
 template <class R, bool TR>
 void DeviceOp::far_l2t(FarField<R>& F, cudaStream_t s) {
-    if (n_l2t_items_)
+    if (!n_l2t_items_) return;
+    if constexpr (std::is_same<R, double>::value)
         k_l2t<R, !TR><<<n_l2t_items_, kL2TThreads, 0, s>>>(F.lv_dev, l2t_items_, leaves_, F.pat, yfar_);
+    else
+        k_l2t_half<R, !TR><<<n_l2t_items_, kL2TThreads, 2 * sizeof(typename Cx<R>::T) * max_leaf_ndir_, s>>>(
+            F.lv_dev, l2t_items_, leaves_, F.hpat, yfar_);
 }
 
 // stage: -1 all, 0 S2M, 1 M2M, 2 M2L, 3 L2L, 4 L2T, in sequence on s.
@@ -768,7 +819,7 @@ std::string DeviceOp::set_loads(const double2* z_user) {
         return {};
     }
     if (!loads_) loads_ = alloc<double2>(n_);
-    MLFMA_CK(cudaMemcpy(yt_, z_user, sizeof(double2) * n_, cudaMemcpyHostToDevice));
+    MLFMA_CK(cudaMemcpyAsync(yt_, z_user, sizeof(double2) * n_, cudaMemcpyHostToDevice, stream_));
     k_gather<<<blocks_for(n_, 256), 256, 0, stream_>>>(yt_, perm_, loads_, n_, 0);
     MLFMA_CK(cudaStreamSynchronize(stream_));
     has_loads_ = true;
@@ -968,7 +1019,7 @@ std::string DeviceOp::setup_multi(const Plan& plan) {
         for (int d = 0; d < L.ndir; ++d)
             for (int gi : gl) items.push_back(make_int2(gi, d));
     }
-    MLFMA_CK(cudaMemcpy(m2l_groups_, h_groups_.data(), sizeof(DevM2LGroup) * h_groups_.size(), cudaMemcpyHostToDevice));
+    MLFMA_CK(h2d_landed(m2l_groups_, h_groups_.data(), sizeof(DevM2LGroup) * h_groups_.size()));
     f64_.m2l_t8 = upload(conv_c<double2>(t8));
     if (precision_ != kFp64) f32_.m2l_t8 = upload(conv_c<float2>(t8));
     n_m2l_items_m_ = static_cast<int>(items.size());

@@ -127,6 +127,161 @@ k_l2t(const DevLevelT<R>* __restrict__ lvs, const int4* __restrict__ items, cons
     if (lane == 0) yfar[lf.src0 + s] = to_d2(acc);
 }
 
+// Half patterns (the complex-float far field of the mixed operator): patterns
+// are kept for the first half of the directions only (d < ndir/2,
+// `hpat`: per source, ndir elements (direction, component)).  The direction
+// grid is symmetric under k -> -k (Gauss-Legendre theta rows in mirror pairs,
+// an even number of phi columns), and for a real basis function
+// R(-k) = conj(R(k)) as a vector; theta-hat is the same at -k and phi-hat flips,
+// so the antipodal element anti[e] holds sgn(e) conj(R[e]), sgn = +1 for the
+// theta component and -1 for the phi component.  S2M and L2T read each stored
+// value once and use it for both directions: half the pattern bytes.  The
+// closed-form RWG integrals are ill-conditioned enough that the derived
+// antipodal values differ from directly computed ones by about 1e-8 relative:
+// far below complex-float rounding, but above the 1e-10 agreement the FP64
+// operator keeps with the reference, so the FP64 far field stores every
+// direction and uses k_s2m / k_l2t.
+// hpat from the full patterns: the first ndir elements of every source.
+template <class R>
+__global__ void k_half_patterns(const DevLevelT<R>* __restrict__ lvs, const DevFarLeaf* __restrict__ leaves,
+                                const double2* __restrict__ pat, typename Cx<R>::T* __restrict__ hpat) {
+    using C = typename Cx<R>::T;
+    const DevFarLeaf lf = leaves[blockIdx.x];
+    const int ne = lvs[lf.level].ndir;
+    for (int i = threadIdx.x; i < lf.nsrc * ne; i += blockDim.x) {
+        const int s = i / ne, e = i - s * ne;
+        hpat[lf.pat_off + static_cast<long long>(s) * ne + e] =
+            from_d2<C>(pat[(lf.pat_off + static_cast<long long>(s) * ne) * 2 + e]);
+    }
+}
+
+// ------------------------------------------------------------ S2M, half patterns
+// a_B[e] = sum_n x_n R_n[e]  (Leaf::buildMpoleCoeffs, src/fmm/leaf.cpp:212-230).
+// One block per work item (leaf, run of at most kS2MThreads elements of the
+// first half), all leaf levels in one launch; one thread per element e, which
+// also forms the antipodal element a_B[anti[e]] = sgn sum_n x_n conj(R_n[e]);
+// every stored pattern row is read once with coalesced loads; eight sources
+// are in flight per thread.
+// CJ: conjugated patterns, a_B[e] = sum_n x_n conj(R_n[e]) -- the transpose of
+// L2T, first stage of the transposed product.
+template <class R, bool CJ>
+__global__ void __launch_bounds__(kS2MThreads)
+k_s2m_half(const DevLevelT<R>* __restrict__ lvs, const int4* __restrict__ items, const DevFarLeaf* __restrict__ leaves,
+      const typename Cx<R>::T* __restrict__ hpat, const double2* __restrict__ x) {
+    using C = typename Cx<R>::T;
+    extern __shared__ unsigned char smraw[];
+    C* xs = reinterpret_cast<C*>(smraw);
+    const int4 it = items[blockIdx.x];  // leaf, first element, element count
+    const DevFarLeaf lf = leaves[it.x];
+    const DevLevelT<R> lv = lvs[lf.level];
+    const int ne = lv.ndir;  // stored elements per source
+    C* A = lv.A + static_cast<size_t>(lf.box) * 2 * ne;
+    for (int i = threadIdx.x; i < lf.nsrc; i += blockDim.x) xs[i] = from_d2<C>(x[lf.src0 + i]);
+    __syncthreads();
+    if (static_cast<int>(threadIdx.x) >= it.z) return;
+    const int e = it.y + threadIdx.x;
+    const C* r = hpat + lf.pat_off + e;
+    // a: this element, b: sum of x conj(v) (or x v), the antipodal one up to its sign
+    C a0 = zero<C>(), a1 = zero<C>(), a2 = zero<C>(), a3 = zero<C>();
+    C b0 = zero<C>(), b1 = zero<C>(), b2 = zero<C>(), b3 = zero<C>();
+    int s = 0;
+    for (; s + 8 <= lf.nsrc; s += 8) {
+        C v[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) v[u] = ldg_stream(r + static_cast<size_t>(s + u) * ne);
+#pragma unroll
+        for (int u = 0; u < 8; u += 4) {
+            if (CJ) {
+                a0 = cjfma(v[u], xs[s + u], a0);
+                a1 = cjfma(v[u + 1], xs[s + u + 1], a1);
+                a2 = cjfma(v[u + 2], xs[s + u + 2], a2);
+                a3 = cjfma(v[u + 3], xs[s + u + 3], a3);
+                b0 = cfma(xs[s + u], v[u], b0);
+                b1 = cfma(xs[s + u + 1], v[u + 1], b1);
+                b2 = cfma(xs[s + u + 2], v[u + 2], b2);
+                b3 = cfma(xs[s + u + 3], v[u + 3], b3);
+            } else {
+                a0 = cfma(xs[s + u], v[u], a0);
+                a1 = cfma(xs[s + u + 1], v[u + 1], a1);
+                a2 = cfma(xs[s + u + 2], v[u + 2], a2);
+                a3 = cfma(xs[s + u + 3], v[u + 3], a3);
+                b0 = cjfma(v[u], xs[s + u], b0);
+                b1 = cjfma(v[u + 1], xs[s + u + 1], b1);
+                b2 = cjfma(v[u + 2], xs[s + u + 2], b2);
+                b3 = cjfma(v[u + 3], xs[s + u + 3], b3);
+            }
+        }
+    }
+    for (; s < lf.nsrc; ++s) {
+        const C v = ldg_stream(r + static_cast<size_t>(s) * ne);
+        a0 = CJ ? cjfma(v, xs[s], a0) : cfma(xs[s], v, a0);
+        b0 = CJ ? cfma(xs[s], v, b0) : cjfma(v, xs[s], b0);
+    }
+    A[e] = cadd(cadd(a0, a1), cadd(a2, a3));
+    const C b = cadd(cadd(b0, b1), cadd(b2, b3));
+    A[lv.anti[e]] = (e & 1) ? C{-b.x, -b.y} : b;
+}
+
+// ------------------------------------------------------------ L2T, half patterns
+// y_m = sum_e conj(R_m[e]) b_B[e] over the stored half:
+// y_m = sum_{e < ndir} conj(R_m[e]) b_B[e] + R_m[e] b'_B[e], b'_B[e] =
+// sgn(e) b_B[anti[e]].  One block per work item (leaf, run of up to eight
+// sources): the block first stages b_B and b'_B in shared memory, then one warp
+// per source streams its stored patterns (eight loads in flight per lane).
+// CJ = false: plain patterns (the transpose of S2M).
+template <class R, bool CJ>
+__global__ void __launch_bounds__(kL2TThreads)
+k_l2t_half(const DevLevelT<R>* __restrict__ lvs, const int4* __restrict__ items, const DevFarLeaf* __restrict__ leaves,
+           const typename Cx<R>::T* __restrict__ hpat, double2* __restrict__ yfar) {
+    using C = typename Cx<R>::T;
+    extern __shared__ unsigned char smraw[];
+    const int4 it = items[blockIdx.x];  // leaf, first source, source count
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const DevFarLeaf lf = leaves[it.x];
+    const DevLevelT<R> lv = lvs[lf.level];
+    const int ne = lv.ndir;  // stored elements per source
+    C* bs = reinterpret_cast<C*>(smraw);
+    C* bp = bs + ne;
+    {
+        const C* Bb = lv.B + static_cast<size_t>(lf.box) * 2 * ne;
+        for (int e = threadIdx.x; e < ne; e += blockDim.x) {
+            bs[e] = Bb[e];
+            const C q = Bb[lv.anti[e]];
+            bp[e] = (e & 1) ? C{-q.x, -q.y} : q;
+        }
+    }
+    __syncthreads();
+    if (warp >= it.z) return;
+    const int s = it.y + warp;
+    const C* r = hpat + lf.pat_off + static_cast<long long>(s) * ne;
+    C a0 = zero<C>(), a1 = zero<C>(), a2 = zero<C>(), a3 = zero<C>();
+    int e = lane;
+    for (; e + 224 < ne; e += 256) {
+        C v[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) v[u] = ldg_stream(r + e + 32 * u);
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int ee = e + 32 * u;
+            C& acc = (u & 3) == 0 ? a0 : (u & 3) == 1 ? a1 : (u & 3) == 2 ? a2 : a3;
+            if (CJ) {
+                acc = cjfma(v[u], bs[ee], acc);
+                acc = cfma(v[u], bp[ee], acc);
+            } else {
+                acc = cfma(v[u], bs[ee], acc);
+                acc = cjfma(v[u], bp[ee], acc);
+            }
+        }
+    }
+    for (; e < ne; e += 32) {
+        const C v = ldg_stream(r + e);
+        a0 = CJ ? cjfma(v, bs[e], a0) : cfma(v, bs[e], a0);
+        a0 = CJ ? cfma(v, bp[e], a0) : cjfma(v, bp[e], a0);
+    }
+    const C acc = warp_sum(cadd(cadd(a0, a1), cadd(a2, a3)));
+    if (lane == 0) yfar[lf.src0 + s] = to_d2(acc);
+}
+
 // ------------------------------------------------------------ M2M
 // Parent outgoing pattern = sum over non-empty children of Interp[shift(child)]:
 // shift on the child grid, theta pass with pole reflection, periodic phi pass
