@@ -393,6 +393,10 @@ std::string DeviceOp::setup(const Plan& plan, int device, int precision, int max
         MLFMA_CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
         MLFMA_CK(cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking));
         MLFMA_CK(cudaStreamCreateWithFlags(&side2_, cudaStreamNonBlocking));
+        // error word of the kernels with bounded waits, read by the host after a sync
+        MLFMA_CK(cudaHostAlloc(reinterpret_cast<void**>(&err_host_), sizeof(int), cudaHostAllocMapped));
+        *err_host_ = 0;
+        MLFMA_CK(cudaHostGetDevicePointer(reinterpret_cast<void**>(&err_dev_), err_host_, 0));
         MLFMA_CK(cudaEventCreateWithFlags(&ev_fork_, cudaEventDisableTiming));
         MLFMA_CK(cudaEventCreateWithFlags(&ev_join_, cudaEventDisableTiming));
         MLFMA_CK(cudaEventCreateWithFlags(&ev_m2l_done_, cudaEventDisableTiming));
@@ -495,6 +499,7 @@ std::string DeviceOp::setup(const Plan& plan, int device, int precision, int max
         }
         n_leaves_ = static_cast<int>(h_leaves.size());
         leaves_ = upload(h_leaves);
+
         n_s2m_items_ = static_cast<int>(s2m_items.size());
         s2m_items_ = upload(s2m_items);
         n_s2m_items_h_ = static_cast<int>(s2m_items_h.size());
@@ -571,9 +576,6 @@ std::string DeviceOp::setup(const Plan& plan, int device, int precision, int max
                 near_part_ = alloc<double2>(static_cast<size_t>(plan.near_parts));
                 near_red_ptr_ = upload(plan.near_red_ptr);
                 near_slot_ = upload(plan.near_slot);
-                MLFMA_CK(cudaHostAlloc(reinterpret_cast<void**>(&err_host_), sizeof(int), cudaHostAllocMapped));
-                *err_host_ = 0;
-                MLFMA_CK(cudaHostGetDevicePointer(reinterpret_cast<void**>(&err_dev_), err_host_, 0));
                 MLFMA_CK(cudaFuncSetAttribute(k_near_sym, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                               static_cast<int>(kSymSmemBytes)));
                 int per_sm = 0, sms = 0;

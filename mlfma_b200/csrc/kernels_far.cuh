@@ -11,6 +11,7 @@
 
 #include "device.cuh"
 #include "zmath.cuh"
+#include "bulk_copy.cuh"
 
 namespace mlfma {
 namespace {
