@@ -166,6 +166,14 @@ int mlfma_gmres(mlfma_handle h, const double* b, double* x, const mlfma_solver_o
  * on the root's angular grid).  Allocates device scratch for the directions. */
 int mlfma_farfield(mlfma_handle h, const double* x, int ndir, const double* khat, double* out);
 
+/* Rows of the operator evaluated densely: y[i] = (A x)[rows[i]] with every
+ * interaction computed directly in FP64 (O(N) work per row; the near-field
+ * entry of every pair, diagonal loads not included).  The dense FP64
+ * reference for the relative error of an MLFMA product or of a solution's
+ * residual on sampled rows.  rows: caller-order indices; x (n) and y (nrows)
+ * interleaved complex.  No counterpart in the reference. */
+int mlfma_dense_rows(mlfma_handle h, int nrows, const int* rows, const double* x, double* y);
+
 /* GMRES that allocates no device memory.  No counterpart in the reference.
  * mlfma_gmres allocates its Krylov basis with cudaMalloc on first use; a
  * caller that cannot allocate device memory during a solve (a fixed memory

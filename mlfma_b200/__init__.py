@@ -321,6 +321,16 @@ class MLFMA:
                                    kh.ctypes.data_as(_dp), out.view(np.float64).ctypes.data_as(_dp)))
         return out
 
+    def dense_rows(self, rows, x) -> np.ndarray:
+        """(A x)[rows] with every interaction evaluated directly in FP64
+        (mlfma_dense_rows): the dense reference for sampled rows."""
+        r = np.ascontiguousarray(np.asarray(rows, dtype=np.int32).ravel())
+        xv = _cvec(x, self.n)
+        out = np.zeros(r.shape[0], dtype=np.complex128)
+        check(lib().mlfma_dense_rows(self._h, r.shape[0], r.ctypes.data_as(_ip), xv.view(np.float64).ctypes.data_as(_dp),
+                                     out.view(np.float64).ctypes.data_as(_dp)))
+        return out
+
     @staticmethod
     def phi_cut(n: int = 360, theta: float = np.pi / 2) -> np.ndarray:
         """Unit directions of a phi cut at fixed theta (n equally spaced phi)."""

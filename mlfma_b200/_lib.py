@@ -87,6 +87,7 @@ SIGNATURES = {
     "mlfma_gmres": (ctypes.c_int, [ctypes.c_void_p, _dp, _dp, ctypes.POINTER(SolverOpts),
                                    ctypes.POINTER(SolveInfo)]),
     "mlfma_farfield": (ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_int, _dp, _dp]),
+    "mlfma_dense_rows": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _ip, _dp, _dp]),
     "mlfma_gmres_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                            ctypes.POINTER(SolverOpts), ctypes.POINTER(SolveInfo)]),
     "mlfma_rhs_planewave": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(PlaneWaveC), _dp]),

@@ -260,6 +260,40 @@ int mlfma_gmres(mlfma_handle h, const double* b, double* x, const mlfma_solver_o
     return MLFMA_OK;
 }
 
+int mlfma_dense_rows(mlfma_handle h, int nrows, const int* rows, const double* x, double* y) {
+    if (!h || nrows < 0 || (nrows > 0 && (!rows || !x || !y))) return fail(MLFMA_ERR_ARG, "null argument");
+    if (!ready(h)) return fail(MLFMA_ERR_STATE, "mlfma_setup has not run");
+    if (nrows == 0) return MLFMA_OK;
+    const int n = h->plan.n;
+    std::vector<int> slot(n), tree(nrows);
+    for (int t = 0; t < n; ++t) slot[h->plan.perm[t]] = t;
+    for (int i = 0; i < nrows; ++i) {
+        if (rows[i] < 0 || rows[i] >= n) return fail(MLFMA_ERR_ARG, "row index out of range");
+        tree[i] = slot[rows[i]];
+    }
+    if (cudaSetDevice(h->device) != cudaSuccess) return fail(MLFMA_ERR_CUDA, "cudaSetDevice failed");
+    cudaStream_t s = h->dev->stream();
+    int* d_rows = nullptr;
+    double2* d_y = nullptr;
+    if (cudaMalloc(&d_rows, sizeof(int) * nrows) != cudaSuccess ||
+        cudaMalloc(&d_y, sizeof(double2) * nrows) != cudaSuccess) {
+        cudaFree(d_rows);
+        return fail(MLFMA_ERR_CUDA, "cudaMalloc failed");
+    }
+    std::string e;
+    if (cudaMemcpyAsync(d_rows, tree.data(), sizeof(int) * nrows, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+        cudaMemcpyAsync(h->d_x, x, sizeof(double2) * n, cudaMemcpyHostToDevice, s) != cudaSuccess)
+        e = "copy failed";
+    if (e.empty()) e = h->dev->dense_rows(d_rows, nrows, h->d_x, d_y, s);
+    if (e.empty() && (cudaMemcpyAsync(y, d_y, sizeof(double2) * nrows, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+                      cudaStreamSynchronize(s) != cudaSuccess))
+        e = "copy of y failed";
+    cudaFree(d_rows);
+    cudaFree(d_y);
+    if (!e.empty()) return fail(MLFMA_ERR_CUDA, e);
+    return MLFMA_OK;
+}
+
 int mlfma_farfield(mlfma_handle h, const double* x, int ndir, const double* khat, double* out) {
     if (!h || !x || (ndir > 0 && (!khat || !out)) || ndir < 0) return fail(MLFMA_ERR_ARG, "null argument");
     if (!ready(h)) return fail(MLFMA_ERR_STATE, "mlfma_setup has not run");

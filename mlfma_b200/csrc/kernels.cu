@@ -918,6 +918,15 @@ std::string DeviceOp::farfield(const double2* cur, int ndir, const double* khat,
     return {};
 }
 
+std::string DeviceOp::dense_rows(const int* rows, int nrows, const double2* x, double2* y, cudaStream_t s) {
+    if (!ready_) return "operator not set up";
+    if (nrows <= 0) return {};
+    MLFMA_CK(cudaSetDevice(device_));
+    k_dense_rows<<<nrows, kDenseThreads, 0, s>>>(src_, rows, perm_, x, n_, ck_, y);
+    MLFMA_CK(cudaGetLastError());
+    return {};
+}
+
 std::string DeviceOp::farfield_adjoint(const double2* F, int ndir, const double* khat, double2* g, cudaStream_t s) {
     if (!ready_) return "operator not set up";
     MLFMA_CK(cudaSetDevice(device_));

@@ -387,6 +387,31 @@ __device__ zd near_entry(const DevSources& S, int m, int n) {
     return (go.leng * gs.leng) * acc;
 }
 
+// Rows of the dense operator: y_i = C k sum_n Z(m_i, n) x_n with every
+// interaction evaluated directly by near_entry (FP64, O(N) work per row), the
+// reference against which the MLFMA product's error is stated.  rows: tree
+// slots; x in caller order.  One block per row, a fixed reduction tree.
+constexpr int kDenseThreads = 256;
+
+__global__ void __launch_bounds__(kDenseThreads)
+k_dense_rows(DevSources S, const int* __restrict__ rows, const int* __restrict__ perm, const double2* __restrict__ x,
+             int n, double2 ck, double2* __restrict__ y) {
+    __shared__ double2 red[kDenseThreads];
+    const int m = rows[blockIdx.x];
+    zd acc = mkz(0);
+    for (int t = threadIdx.x; t < n; t += blockDim.x) {
+        const double2 xv = x[perm[t]];
+        acc += near_entry(S, m, t) * zd{xv.x, xv.y};
+    }
+    red[threadIdx.x] = make_double2(acc.x, acc.y);
+    __syncthreads();
+    for (int w = kDenseThreads / 2; w > 0; w >>= 1) {
+        if (static_cast<int>(threadIdx.x) < w) red[threadIdx.x] = cadd(red[threadIdx.x], red[threadIdx.x + w]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) y[blockIdx.x] = cmul(ck, red[0]);
+}
+
 // Far field of currents I (caller order) along unit directions khat:
 // F = C k (I - khat khat^T) sum_n I_n f_n(k khat), with f_n = e^{-i r_n . k khat}
 // phat_n for a dipole (Dipole::getFarAlongDir, src/sources/dipole.h:53-57)
