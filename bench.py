@@ -510,6 +510,7 @@ def main():
             "config": config_dict({"parallelism": f"replicas{world}", "levels": st["max_level"],
                                    "near_entries": st["near_entries"], "setup_s": r64["setup_s"],
                                    "autotuned": {"m2l_chunk": r64["tuning"]["m2l_chunk"],
+                                                 "near_blocks_per_sm": r64["tuning"]["near_blocks_per_sm"],
                                                  "m2m_rows": [v for v in r64["tuning"]["m2m_rows"] if v]}}),
             "e2e": {"value": world * 1000.0 / e2e_ms, "unit": UNIT, "h2d_bytes_per_step": n * 16,
                     "d2h_bytes_per_step": n * 16},

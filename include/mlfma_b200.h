@@ -263,6 +263,7 @@ typedef struct {
     int multi_l2l_pairs;       /* many-rhs anterpolation: column pairs per block */
     float product_ms_before;   /* one product (nrhs right-hand sides) before and after, ms */
     float product_ms_after;
+    int near_blocks_per_sm;    /* one-vector near field: persistent blocks per SM (it runs beside the far field) */
 } mlfma_tuning;
 
 /* Autotuner: times the candidate launch shapes of the stages on this operator

@@ -343,7 +343,7 @@ class MLFMA:
         check(lib().mlfma_autotune(self._h, nrhs, reps, ctypes.byref(t)))
         return {"m2l_chunk": t.m2l_chunk, "m2m_rows": list(t.m2m_rows), "multi_m2m_rows_fast": t.multi_m2m_rows_fast,
                 "multi_l2l_pairs": t.multi_l2l_pairs, "product_ms_before": t.product_ms_before,
-                "product_ms_after": t.product_ms_after}
+                "product_ms_after": t.product_ms_after, "near_blocks_per_sm": t.near_blocks_per_sm}
 
     def stream(self) -> int:
         s = ctypes.c_void_p()

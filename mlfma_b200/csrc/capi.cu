@@ -653,6 +653,7 @@ int mlfma_autotune(mlfma_handle h, int nrhs, int reps, mlfma_tuning* out) {
         out->multi_l2l_pairs = r.multi_l2l_pairs;
         out->product_ms_before = r.before_ms;
         out->product_ms_after = r.after_ms;
+        out->near_blocks_per_sm = r.near_blocks_per_sm;
     }
     return MLFMA_OK;
 }

@@ -140,6 +140,7 @@ struct TuneReport {
     int multi_rows_fast;           // many-rhs M2M grid order (1 rows fastest, 0 parents fastest)
     int multi_l2l_pairs;           // many-rhs L2L column pairs per block
     float before_ms, after_ms;     // product time before and after
+    int near_blocks_per_sm;        // one-vector near field: persistent blocks per SM
 };
 
 struct StageTimes {
@@ -313,6 +314,9 @@ private:
     long long near_block_entries_ = 0;
     double2* near_part_ = nullptr;        // partial sums (near_parts)
     int near_grid_ = 0;                   // persistent blocks of k_near_sym
+    int near_occ_ = 0;                    // its resident blocks per SM at most (occupancy)
+    int near_per_sm_ = 0, sms_ = 0;       // its blocks per SM (the bound, or tuned) and the SM count
+    void set_near_grid(int per_sm);
     int* err_host_ = nullptr;             // error word in mapped host memory
     int* err_dev_ = nullptr;              //   and its device address
     int* near_slot_ = nullptr;            // per tile: slots of its partials

@@ -119,6 +119,13 @@ DeviceOp::~DeviceOp() {
     if (err_host_) cudaFreeHost(err_host_);
 }
 
+// Persistent blocks of k_near_sym: per_sm per SM, but at least four tiles per
+// block, so that a small operator leaves room for the kernels of others
+// running beside it.
+void DeviceOp::set_near_grid(int per_sm) {
+    near_grid_ = std::max(1, std::min(n_near_tiles_ / 4, std::max(1, per_sm) * sms_));
+}
+
 std::string DeviceOp::device_error() const {
     if (err_host_ && *static_cast<volatile int*>(err_host_))
         return "near-field kernel: a bulk copy did not complete within its bounded wait";
@@ -578,12 +585,12 @@ std::string DeviceOp::setup(const Plan& plan, int device, int precision, int max
                 near_slot_ = upload(plan.near_slot);
                 MLFMA_CK(cudaFuncSetAttribute(k_near_sym, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                               static_cast<int>(kSymSmemBytes)));
-                int per_sm = 0, sms = 0;
-                MLFMA_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_near_sym, kSymThreads, kSymSmemBytes));
-                MLFMA_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_));
-                // at least four tiles per block, so that a small operator leaves
-                // room for the kernels of others running beside it
-                near_grid_ = std::max(1, std::min({n_near_tiles_ / 4, std::max(1, per_sm) * sms}));
+                MLFMA_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&near_occ_, k_near_sym, kSymThreads,
+                                                                       kSymSmemBytes));
+                near_occ_ = std::max(1, near_occ_);
+                near_per_sm_ = near_occ_;
+                MLFMA_CK(cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, device_));
+                set_near_grid(near_per_sm_);
                 DevNearBlock* d_nb = upload(nb);
                 k_near_blocks_assemble<<<blocks_for(near_block_entries_, 128), 128, 0, stream_>>>(
                     d_nb, static_cast<int>(nb.size()), near_block_entries_, S, near_bz_);
@@ -1294,6 +1301,7 @@ std::string DeviceOp::autotune(int nr, int reps, TuneReport* rep) {
         return ms / reps;
     };
     TuneReport r{};
+    r.near_blocks_per_sm = near_per_sm_;
     if (nr == 1) {
         auto product = [&] { enqueue_core(s, precision_, false); };
         r.before_ms = timed(product);
@@ -1324,6 +1332,20 @@ std::string DeviceOp::autotune(int nr, int reps, TuneReport* rep) {
             m2m_rows_[p] = brows;
             r.m2m_rows[p] = brows;
         }
+        // near field: persistent blocks per SM, timed on the whole product (it
+        // runs beside the far-field chain and competes with it for the SMs)
+        if (n_near_tiles_) {
+            float bt = 1e30f;
+            int bk = near_per_sm_;
+            for (int k = 1; k <= near_occ_; ++k) {
+                set_near_grid(k);
+                const float t = timed(product);
+                if (t < bt) { bt = t; bk = k; }
+            }
+            near_per_sm_ = bk;
+            set_near_grid(bk);
+        }
+        r.near_blocks_per_sm = near_per_sm_;
         r.after_ms = timed(product);
     } else {
         auto product = [&] { enqueue_multi(nr, s, precision_); };
