@@ -166,6 +166,14 @@ int mlfma_gmres(mlfma_handle h, const double* b, double* x, const mlfma_solver_o
  * on the root's angular grid).  Allocates device scratch for the directions. */
 int mlfma_farfield(mlfma_handle h, const double* x, int ndir, const double* khat, double* out);
 
+/* Self-check of the failure path of the kernels' bounded waits (the
+ * near-field kernel waits on mbarriers for its bulk copies; every wait gives
+ * up after about a second and raises the operator's error word, which the
+ * synchronous calls report, instead of hanging).  Runs one wait on a barrier nothing arrives
+ * on, limited to about 8 ms, on `device`; *timed_out = 1 when it ran out and
+ * the kernel returned.  No GPU fault is involved; the context stays usable. */
+int mlfma_check_bounded_wait(int device, int* timed_out);
+
 /* Rows of the operator evaluated densely: y[i] = (A x)[rows[i]] with every
  * interaction computed directly in FP64 (O(N) work per row; the near-field
  * entry of every pair, diagonal loads not included).  The dense FP64

@@ -88,6 +88,7 @@ SIGNATURES = {
                                    ctypes.POINTER(SolveInfo)]),
     "mlfma_farfield": (ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_int, _dp, _dp]),
     "mlfma_dense_rows": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _ip, _dp, _dp]),
+    "mlfma_check_bounded_wait": (ctypes.c_int, [ctypes.c_int, _ip]),
     "mlfma_gmres_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                            ctypes.POINTER(SolverOpts), ctypes.POINTER(SolveInfo)]),
     "mlfma_rhs_planewave": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(PlaneWaveC), _dp]),

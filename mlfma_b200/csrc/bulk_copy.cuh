@@ -33,12 +33,24 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
     return ok != 0;
 }
 constexpr long long kWaitCycles = 1ll << 31;  // about a second at the B200 clock
-__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity) {
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity, long long limit = kWaitCycles) {
     if (mbar_try_wait(bar, parity)) return true;
     const long long t0 = clock64();
     while (!mbar_try_wait(bar, parity))
-        if (clock64() - t0 > kWaitCycles) return false;
+        if (clock64() - t0 > limit) return false;
     return true;
+}
+
+// Self-check of the bounded wait: one thread waits on a barrier that nothing
+// arrives on, for `limit` cycles, and reports 1 in *status when the wait ran
+// out (0 if it had completed, which cannot happen).  No copy is in flight, so
+// the block exits cleanly and the context stays usable.
+__global__ void k_wait_runs_out(long long limit, int* status) {
+    __shared__ __align__(8) unsigned long long bar;
+    if (threadIdx.x != 0) return;
+    mbar_init(smem_addr(&bar), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    *status = mbar_wait_bounded(smem_addr(&bar), 0, limit) ? 0 : 1;
 }
 // Global -> this block's shared memory, completion counted on bar (bytes and
 // both addresses multiples of 16).

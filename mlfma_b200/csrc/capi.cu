@@ -260,6 +260,20 @@ int mlfma_gmres(mlfma_handle h, const double* b, double* x, const mlfma_solver_o
     return MLFMA_OK;
 }
 
+int mlfma_check_bounded_wait(int device, int* timed_out) {
+    if (!timed_out) return fail(MLFMA_ERR_ARG, "null argument");
+    if (cudaSetDevice(device) != cudaSuccess) return fail(MLFMA_ERR_CUDA, "cudaSetDevice failed");
+    int* d = nullptr;
+    if (cudaMalloc(&d, sizeof(int)) != cudaSuccess) return fail(MLFMA_ERR_CUDA, "cudaMalloc failed");
+    cudaMemset(d, 0xff, sizeof(int));
+    mlfma::launch_wait_runs_out(1ll << 24, d);  // about 8 ms
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = cudaMemcpy(timed_out, d, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) return fail(MLFMA_ERR_CUDA, cudaGetErrorString(e));
+    return MLFMA_OK;
+}
+
 int mlfma_dense_rows(mlfma_handle h, int nrows, const int* rows, const double* x, double* y) {
     if (!h || nrows < 0 || (nrows > 0 && (!rows || !x || !y))) return fail(MLFMA_ERR_ARG, "null argument");
     if (!ready(h)) return fail(MLFMA_ERR_STATE, "mlfma_setup has not run");

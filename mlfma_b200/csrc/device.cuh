@@ -106,6 +106,10 @@ struct DevNearTile {
     int r0, c0, i0, ni, j0, nj, ld, kind, slot, mode;
 };
 
+// Runs k_wait_runs_out (a bounded mbarrier wait on a barrier nothing arrives
+// on) on the current device's default stream.
+void launch_wait_runs_out(long long limit, int* status);
+
 struct DevNearRow {
     int row0, nrow, ncol, pad;
     long long off, col_off;

@@ -126,6 +126,8 @@ void DeviceOp::set_near_grid(int per_sm) {
     near_grid_ = std::max(1, std::min(n_near_tiles_ / 4, std::max(1, per_sm) * sms_));
 }
 
+void launch_wait_runs_out(long long limit, int* status) { k_wait_runs_out<<<1, 32>>>(limit, status); }
+
 std::string DeviceOp::device_error() const {
     if (err_host_ && *static_cast<volatile int*>(err_host_))
         return "near-field kernel: a bulk copy did not complete within its bounded wait";
