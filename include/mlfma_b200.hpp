@@ -106,6 +106,15 @@ public:
     // Diagonal impedance loads z (n complex) added to the operator.
     void setLoads(const std::vector<cplx>& z) { check(mlfma_set_loads(h_, reinterpret_cast<const double*>(z.data()))); }
 
+    // (A x)[rows] with every interaction evaluated directly in FP64: the dense
+    // reference for sampled rows (rows: caller-order indices).
+    std::vector<cplx> denseRows(const std::vector<int>& rows, const std::vector<cplx>& x) {
+        std::vector<cplx> y(rows.size());
+        check(mlfma_dense_rows(h_, static_cast<int>(rows.size()), rows.data(), reinterpret_cast<const double*>(x.data()),
+                               reinterpret_cast<double*>(y.data())));
+        return y;
+    }
+
     // Launch shapes timed on this operator (nrhs = 1: one-vector product).
     mlfma_tuning autotune(int nrhs = 1, int reps = 5) {
         mlfma_tuning t{};
