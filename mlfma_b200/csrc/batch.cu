@@ -75,7 +75,7 @@ int capture(mlfma_batch_s* b) {
         }
     }
     B_CK(cudaStreamEndCapture(b->stream, &b->graph));
-    B_CK(cudaGraphInstantiate(&b->exec, b->graph, 0));
+    B_CK(cudaGraphInstantiate(&b->exec, b->graph, cudaGraphInstantiateFlagUseNodePriority));
     return MLFMA_OK;
 }
 

@@ -399,9 +399,14 @@ std::string DeviceOp::setup(const Plan& plan, int device, int precision, int max
         if (max_rhs < 1 || max_rhs > kMaxRhs) return "max_rhs must be 1..64";
         max_rhs_ = max_rhs;
         MLFMA_CK(cudaSetDevice(device));
-        MLFMA_CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
-        MLFMA_CK(cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking));
-        MLFMA_CK(cudaStreamCreateWithFlags(&side2_, cudaStreamNonBlocking));
+        // The far-field chain (the product's critical path) gets the highest
+        // priority; the near field and the finer levels' translations, which
+        // run beside it, the lowest: pending chain blocks are scheduled first.
+        int prio_low = 0, prio_high = 0;
+        MLFMA_CK(cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high));
+        MLFMA_CK(cudaStreamCreateWithPriority(&stream_, cudaStreamNonBlocking, prio_high));
+        MLFMA_CK(cudaStreamCreateWithPriority(&side_, cudaStreamNonBlocking, prio_low));
+        MLFMA_CK(cudaStreamCreateWithPriority(&side2_, cudaStreamNonBlocking, prio_low));
         // error word of the kernels with bounded waits, read by the host after a sync
         MLFMA_CK(cudaHostAlloc(reinterpret_cast<void**>(&err_host_), sizeof(int), cudaHostAllocMapped));
         *err_host_ = 0;
@@ -813,7 +818,7 @@ std::string DeviceOp::ensure_graph(int prec, bool tr) {
     MLFMA_CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
     enqueue_core(stream_, prec, tr);
     MLFMA_CK(cudaStreamEndCapture(stream_, &graph_[prec][t]));
-    MLFMA_CK(cudaGraphInstantiate(&graph_exec_[prec][t], graph_[prec][t], 0));
+    MLFMA_CK(cudaGraphInstantiate(&graph_exec_[prec][t], graph_[prec][t], cudaGraphInstantiateFlagUseNodePriority));
     return {};
 }
 
