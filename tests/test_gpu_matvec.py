@@ -135,3 +135,26 @@ def test_single_leaf_and_single_source(cuda_device):
     ck = O.PHYS_C * PW.wavenum
     assert abs(op1.matvec(np.array([1.0 + 2.0j]))[0] - ck * (1.0 + 2.0j)) <= 1e-12 * abs(ck)
     op1.close()
+
+
+def test_matvec_large_leaves_and_wide_blocks_match_oracle(cuda_device):
+    # Leaves of up to 150 sources and a dense cluster beside a sparse cloud:
+    # self blocks of more than 64 sources and (leaf, node) blocks wider than 64
+    # columns, which the near-field kernel moves row by row (its third tile
+    # layout), besides whole-row tiles.
+    from oracle import mlfma_oracle as O
+    rng = np.random.default_rng(21)
+    n = 2400
+    pos = rng.uniform(-1.9, 1.9, (n, 3))
+    pos[: n // 2] *= 0.08  # half the sources in a small ball at the centre
+    mom = rng.standard_normal((n, 3))
+    mom /= np.linalg.norm(mom, axis=1)[:, None]
+    d = inputs.Dipoles(pos=pos, mom=mom)
+    for self_terms in (0, 1):
+        op = MLFMA.dipoles(d, PW, max_node_srcs=150, self_terms=self_terms, ref_compat=1 - self_terms).setup()
+        src = O.DipoleSources(d.pos, d.mom, PW)
+        src.self_terms = bool(self_terms)
+        orc = O.Oracle(src, max_node_srcs=150)
+        x = cvec(op.n, 22)
+        assert rel(op.matvec(x), orc.matvec(x)) <= 1e-12
+        op.close()
