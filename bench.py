@@ -12,8 +12,9 @@ matrix-vector product y = A x on one right-hand side.
 
 `value` is device-resident throughput (x and y already in HBM), timed with
 CUDA events on the launching stream; `e2e` is the same product through the
-public host-buffer call mlfma_matvec, with the host->device copy of x and the
-device->host copy of y (pinned buffers) inside the timed region.  The operator
+C-ABI host-buffer call mlfma_matvec (called through ctypes, pointers prepared
+once), with the host->device copy of x and the device->host copy of y (pinned
+buffers) inside the timed region.  The operator
 reads 0.41 GB per matvec, more than the 126 MB L2, so no flush runs between
 steps.  With N > 1 every rank runs an independent replica of the product
 (there is no data exchange on this path); rank 0 reports N * K / max time.
@@ -199,17 +200,30 @@ def measure(torch, dev, rank, world, args, precision: int, clocks=None) -> dict:
     ms = e0.elapsed_time(e1) / args.steps
     y_dev = y.cpu().numpy().copy()
 
-    # End to end through the public host-buffer call (pinned buffers).
+    # End to end through the C-ABI host-buffer call mlfma_matvec (the drop-in
+    # boundary a C or C++ caller uses), pinned buffers, pointers prepared once;
+    # each call copies x in, runs the product, copies y out and synchronises.
+    import ctypes
+    from mlfma_b200 import _lib
     xp = torch.empty(n, dtype=torch.complex128, pin_memory=True)
     yp = torch.empty(n, dtype=torch.complex128, pin_memory=True)
     xp.copy_(xh)
     xn, yn = xp.numpy(), yp.numpy()
+    dp = ctypes.POINTER(ctypes.c_double)
+    c_matvec, handle = _lib.lib().mlfma_matvec, op._h
+    px, py = xn.view(np.float64).ctypes.data_as(dp), yn.view(np.float64).ctypes.data_as(dp)
+
+    def e2e_step():
+        rc = c_matvec(handle, px, py, 0)
+        if rc:
+            raise RuntimeError(f"mlfma_matvec returned {rc}")
+
     for _ in range(args.warmup):
-        op.matvec(xn, out=yn)
+        e2e_step()
     f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     f0.record(stream)
     for _ in range(args.steps):
-        op.matvec(xn, out=yn)
+        e2e_step()
     f1.record(stream)
     torch.cuda.synchronize(dev)
     e2e_ms = f0.elapsed_time(f1) / args.steps
