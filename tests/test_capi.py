@@ -74,6 +74,9 @@ def test_device_calls_before_setup_are_state_errors():
     assert e.value.code == _lib.MLFMA_ERR_STATE
     with pytest.raises(MlfmaError):
         op.stage_times()
+    with pytest.raises(MlfmaError) as e:
+        op.dense_rows([0, 1], np.zeros(50))
+    assert e.value.code == _lib.MLFMA_ERR_STATE
     op.close()
 
 
@@ -83,6 +86,9 @@ def test_null_arguments():
     assert L.mlfma_config_default(None) == _lib.MLFMA_ERR_ARG
     assert L.mlfma_destroy(None) == _lib.MLFMA_OK
     assert L.mlfma_last_error()  # message set by the failing call
+    assert L.mlfma_dense_rows(None, 1, None, None, None) == _lib.MLFMA_ERR_ARG
+    assert L.mlfma_check_bounded_wait(0, None) == _lib.MLFMA_ERR_ARG
+    assert L.mlfma_batch_create(0, None, None) == _lib.MLFMA_ERR_ARG
 
 
 def test_host_plan_stats_without_gpu():
