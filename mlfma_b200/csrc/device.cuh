@@ -305,6 +305,7 @@ private:
     int n_l2t_items_ = 0;
     int max_src_ = 0;                    // largest far leaf
     int max_leaf_ndir_ = 0;              // most directions on a level holding far leaves
+    bool far_covers_all_ = false;        // every source sits in a far leaf (L2T writes all of yfar_)
     DevFarLeaf* leaves_ = nullptr;
     int n_leaves_ = 0;
     FarField<double> f64_;

@@ -520,6 +520,9 @@ std::string DeviceOp::setup(const Plan& plan, int device, int precision, int max
         if (precision != kFp64) s2m_items_h_ = upload(s2m_items_h);
         n_l2t_items_ = static_cast<int>(l2t_items.size());
         l2t_items_ = upload(l2t_items);
+        long long far_srcs = 0;
+        for (const FarLeaf& f : plan.far_leaves) far_srcs += f.nsrc;
+        far_covers_all_ = n_leaves_ > 0 && far_srcs == n_;
         // the complex-float far field keeps half the patterns (antipodes by symmetry)
         const double pat_copies = precision == kFp64 ? 2.0 : 1.0;
         traffic_.s2m = plan.pat_elems * pat_copies * cbytes + n_ * 16.0;
@@ -803,7 +806,9 @@ void DeviceOp::run_near(const double2* xt, cudaStream_t s) {
 // is symmetric (each stored block is applied as Z and Z^T), so the transposed
 // product reuses it; run_near writes every entry of ynear_.
 void DeviceOp::enqueue_core(cudaStream_t s, int prec, bool tr) {
-    cudaMemsetAsync(yfar_, 0, sizeof(double2) * n_, s);
+    // L2T writes (not adds) every far-leaf source's entry: zero yfar_ only
+    // when some source sits in a leaf without far interactions
+    if (!far_covers_all_) cudaMemsetAsync(yfar_, 0, sizeof(double2) * n_, s);
     cudaEventRecord(ev_fork_, s);
     cudaStreamWaitEvent(side_, ev_fork_, 0);
     run_near(xt_, side_);
