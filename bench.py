@@ -130,7 +130,13 @@ class ClockSampler:
 
 # ------------------------------------------------------------------ reference arm
 
-def run_reference(steps: int, warmup: int, quiet=False) -> dict:
+def parity_vector(n):
+    """The seeded input vector of the reference arm's products (and of the GPU
+    arm's parity check against them)."""
+    return np.random.default_rng(7).standard_normal(n) + 1j * np.random.default_rng(8).standard_normal(n)
+
+
+def run_reference(steps: int, warmup: int, save_y: str | None = None) -> dict:
     sys.path.insert(0, HERE)
     from oracle import ref_lib
     mesh, pw = make_problem()
@@ -139,14 +145,42 @@ def run_reference(steps: int, warmup: int, quiet=False) -> dict:
                            over_interp=WORKLOAD["over_interp"], root_leng=WORKLOAD["root_leng"],
                            max_node_srcs=WORKLOAD["max_node_srcs"], quad_prec=WORKLOAD["quad_prec"])
     setup_s = time.perf_counter() - t0
-    x = np.random.default_rng(7).standard_normal(P.n) + 1j * np.random.default_rng(8).standard_normal(P.n)
+    x = parity_vector(P.n)
+    y = None
     for _ in range(warmup):
-        P.matvec(x)
+        y = P.matvec(x)
     t0 = time.perf_counter()
     for _ in range(steps):
-        P.matvec(x)
+        y = P.matvec(x)
     dt = time.perf_counter() - t0
+    if save_y:
+        # the last product and how many products of x led to it (the reference
+        # carries state from one product to the next)
+        np.savez(save_y, y=y, products=warmup + steps)
     return {"value": steps / dt, "ms_per_step": dt / steps * 1e3, "setup_s": setup_s, "steps": steps}
+
+
+def parity_vs_reference(dev, saved: str) -> dict:
+    """Replays the reference arm's products of the seeded vector on a fresh
+    plain-FP64 operator with the reference's rules and compares the last one
+    with the reference's (the 1e-10 contract, on the benchmark workload)."""
+    from mlfma_b200 import MLFMA, default_config
+    f = np.load(saved)
+    y_ref, count = f["y"], int(f["products"])
+    mesh, pw = make_problem()
+    cfg = default_config(quad_prec=WORKLOAD["quad_prec"], digits=WORKLOAD["digits"],
+                         interp_order=WORKLOAD["interp_order"], over_interp=WORKLOAD["over_interp"],
+                         root_leng=WORKLOAD["root_leng"], max_node_srcs=WORKLOAD["max_node_srcs"],
+                         device=dev.index, precision=0)
+    op = MLFMA.rwg(mesh, pw, config=cfg).setup()
+    x = parity_vector(op.n)
+    for _ in range(count):
+        y = op.matvec(x)
+    op.close()
+    return {"rel_err": float(np.linalg.norm(y - y_ref) / np.linalg.norm(y_ref)), "products": count,
+            "tolerance": 1e-10,
+            "what": "the reference's own product (oracle/_ref, same seeded x, same call sequence) against "
+                    "mlfma_matvec, plain FP64, reference rules"}
 
 
 # ------------------------------------------------------------------ our arm
@@ -458,6 +492,7 @@ def main():
     ap.add_argument("--no-solve", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=3)
+    ap.add_argument("--save-y", default=None, help="reference arm: save its last product here (.npz)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -466,7 +501,7 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return 0
-        r = run_reference(args.steps, max(args.warmup, 0))
+        r = run_reference(args.steps, max(args.warmup, 0), save_y=args.save_y)
         line = {"metric": METRIC, "value": r["value"], "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms_per_step"],
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
@@ -491,9 +526,12 @@ def main():
 
     # CPU baseline in a child process (rank 0, N = 1), overlapping GPU setup.
     cpu_proc = None
+    ref_y = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        fd, ref_y = tempfile.mkstemp(suffix=".npz")
+        os.close(fd)
         cpu_proc = subprocess.Popen([sys.executable, os.path.abspath(__file__), "--impl", "reference",
-                                     "--steps", str(args.cpu_steps), "--warmup", "1"],
+                                     "--steps", str(args.cpu_steps), "--warmup", "1", "--save-y", ref_y],
                                     stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
     sys.path.insert(0, HERE)
 
@@ -516,6 +554,14 @@ def main():
                                  f"{r['config'].get('reference_setup_s', 0):.0f} s setup"}
             except Exception as e:  # noqa: BLE001
                 cpu = {"value": None, "unit": UNIT, "cores": 1, "kind": "reference", "sample": f"failed: {e}"}
+        parity = None
+        if ref_y is not None:
+            try:
+                parity = parity_vs_reference(dev, ref_y)
+            except Exception as e:  # noqa: BLE001
+                parity = {"rel_err": None, "error": str(e)}
+            finally:
+                os.unlink(ref_y)
         st, n, ms, e2e_ms = r64["stats"], r64["n"], r64["ms"], r64["e2e_ms"]
         line = {
             "metric": METRIC, "value": world * 1000.0 / ms, "unit": UNIT, "n_gpus": world,
@@ -534,6 +580,8 @@ def main():
             "matvec_alg_bytes": r64["traffic"]["total"],
             "clocks": r64["clocks"],
             "cpu_baseline": cpu,
+            "parity_rel_err_vs_reference": parity["rel_err"] if parity else None,
+            "parity_vs_reference": parity,
             "dense_check": {"rows": DENSE_ROWS, "matvec_rel_err_fp64": r64["dense_err"],
                             "reference": "the same rows of the operator with every interaction evaluated "
                                          "directly in FP64 (mlfma_dense_rows)"},

@@ -190,13 +190,15 @@ int mlfma_dense_rows(mlfma_handle h, int nrows, const int* rows, const double* x
  * mlfma_gmres; b and x are DEVICE buffers of n complex values in the caller's
  * source order; the solve runs on the handle's stream and returns when done.
  * The workspace is one fixed array in device memory that is part of the
- * library (32 MiB, held on every GPU that loads the library until exit): n *
- * (restart + 5) must not exceed 2,097,152 complex values (restart = max_iter
- * when restart is 0; restart + 7 with refinement on a mixed operator),
- * otherwise MLFMA_ERR_ARG.  All calls share that array and
- * it keeps the last call's contents, so calls that overlap on the GPU race.
- * The first call on a device looks up the array's device address; make that
- * first call before any stream capture. */
+ * library (32 MiB).  CUDA creates it on a device when the library's solver
+ * module is first used there; mlfma_setup does that on the operator's device,
+ * so the 32 MiB are taken at setup (not during a solve, and not merely by
+ * loading the library) and held until the process exits.  A solve of n
+ * unknowns with m = restart (max_iter when restart is 0) needs
+ * n (m + 5) + (m + 2)(2 + ceil(n / 8192)) complex values, n (m + 7) + ... with
+ * refinement on a mixed operator; more than 2,097,152 gives MLFMA_ERR_ARG with
+ * the count in mlfma_last_error().  All calls share the array and it keeps the
+ * last call's contents, so calls that overlap on the GPU race. */
 int mlfma_gmres_noalloc(mlfma_handle h, const void* d_b, void* d_x, const mlfma_solver_opts* opts,
                         mlfma_solve_info* info);
 

@@ -155,6 +155,10 @@ int mlfma_setup(mlfma_handle h) {
         if (cudaMalloc(&h->d_x, sizeof(double2) * h->plan.n) != cudaSuccess ||
             cudaMalloc(&h->d_y, sizeof(double2) * h->plan.n) != cudaSuccess)
             return fail(MLFMA_ERR_CUDA, "cudaMalloc failed");
+        // The fixed workspace of mlfma_gmres_noalloc is created on this device
+        // now (first use of its module), not inside a solve.
+        e = mlfma::noalloc_workspace_prepare();
+        if (!e.empty()) return fail(MLFMA_ERR_CUDA, e);
         h->dev = std::move(dev);
         h->gmres = std::make_unique<mlfma::Gmres>();
         return MLFMA_OK;
@@ -356,10 +360,13 @@ int mlfma_gmres_noalloc(mlfma_handle h, const void* d_b, void* d_x, const mlfma_
     const int m = o.restart > 0 ? o.restart : o.max_iter;
     std::string e = h->gmres_fixed->use_static_workspace(
         h->plan.n, m + 1, (o.refine && h->precision != MLFMA_FP64) ? 2 : 0);
-    if (!e.empty()) return fail(e.rfind("size:", 0) == 0 ? MLFMA_ERR_ARG : MLFMA_ERR_CUDA, e);
+    if (!e.empty()) return e.rfind("size:", 0) == 0 ? fail(MLFMA_ERR_ARG, e.substr(5)) : fail(MLFMA_ERR_CUDA, e);
     mlfma::SolveResult r;
     e = h->gmres_fixed->solve(*h->dev, static_cast<const double2*>(d_b), static_cast<double2*>(d_x), o, &r);
     if (!e.empty()) return from_msg(e);
+    // a kernel that gave up a bounded wait leaves x invalid (as in mlfma_gmres)
+    e = h->dev->device_error();
+    if (!e.empty()) return fail(MLFMA_ERR_CUDA, e);
     if (info) {
         info->iterations = r.iterations;
         info->residual = r.residual;

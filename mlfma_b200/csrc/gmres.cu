@@ -196,44 +196,69 @@ void Gmres::apply(DeviceOp& op, const double2* x, double2* y, cudaStream_t s, in
 // Some callers cannot allocate device memory while they solve: code that runs
 // with a device memory budget fixed at start-up, or under an allocator policy
 // that forbids cudaMalloc outside initialisation.  For them the library keeps
-// one fixed GMRES workspace in device memory that is part of the loaded module
-// (it exists on every GPU that loads the library, until the process exits):
-// kNoAllocWorkspace complex doubles (32 MiB) for the Krylov basis and work
-// vectors, and kNoAllocNorm doubles for norm partial sums.  Every solve shares
-// it and it keeps the previous solve's contents (every element is written
-// before it is read); two solves that overlap on the GPU race on it.
+// one fixed GMRES workspace in device memory that is part of this file's
+// module: kNoAllocWorkspace complex doubles (32 MiB) for the Krylov basis and
+// work vectors, and kNoAllocNorm doubles for norm partial sums.  CUDA loads
+// modules lazily, so the arrays are created on a device when the module is
+// first used there; mlfma_setup forces that (noalloc_workspace_prepare) on the
+// operator's device, and the memory stays until the process exits.  Every
+// solve shares the arrays and they keep the previous solve's contents (every
+// element is written before it is read); two solves that overlap on the GPU
+// race on them.
 constexpr size_t kNoAllocWorkspace = size_t(1) << 21;
 constexpr int kNoAllocNorm = 4096;
 static __device__ __align__(256) double2 g_noalloc_ws[kNoAllocWorkspace];
 static __device__ __align__(256) double g_noalloc_norm[kNoAllocNorm];
 
-std::string Gmres::use_static_workspace(int n, int ncols, int extra) {
-    // Device addresses of the arrays, looked up once per device (with that
-    // device current); host code only sees host-side stand-ins for them.
+namespace {
+// Device addresses of the arrays, looked up once per device (with that device
+// current); host code only sees host-side stand-ins for them.
+std::string noalloc_addresses(double2** ws, double** nws) {
     static std::mutex mu;
     static std::map<int, std::pair<double2*, double*>> addr;
     int dev = 0;
     GM_CK(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = addr.find(dev);
+    if (it == addr.end()) {
+        double2* w = nullptr;
+        double* nw = nullptr;
+        GM_CK(cudaGetSymbolAddress(reinterpret_cast<void**>(&w), g_noalloc_ws));
+        GM_CK(cudaGetSymbolAddress(reinterpret_cast<void**>(&nw), g_noalloc_norm));
+        it = addr.emplace(dev, std::make_pair(w, nw)).first;
+    }
+    *ws = it->second.first;
+    *nws = it->second.second;
+    return {};
+}
+}  // namespace
+
+std::string noalloc_workspace_prepare() {
     double2* ws = nullptr;
     double* nws = nullptr;
-    {
-        std::lock_guard<std::mutex> lock(mu);
-        auto it = addr.find(dev);
-        if (it == addr.end()) {
-            GM_CK(cudaGetSymbolAddress(reinterpret_cast<void**>(&ws), g_noalloc_ws));
-            GM_CK(cudaGetSymbolAddress(reinterpret_cast<void**>(&nws), g_noalloc_norm));
-            addr.emplace(dev, std::make_pair(ws, nws));
-        } else {
-            ws = it->second.first;
-            nws = it->second.second;
-        }
-    }
+    return noalloc_addresses(&ws, &nws);
+}
+
+size_t noalloc_workspace_need(int n, int ncols, int extra) {
+    const size_t nchunks = (static_cast<size_t>(n) + kDotChunk - 1) / kDotChunk;
+    return static_cast<size_t>(n) * ncols + (4 + extra) * static_cast<size_t>(n) + 2 * static_cast<size_t>(ncols + 1) +
+           nchunks * (ncols + 1);
+}
+
+std::string Gmres::use_static_workspace(int n, int ncols, int extra) {
+    double2* ws = nullptr;
+    double* nws = nullptr;
+    std::string err = noalloc_addresses(&ws, &nws);
+    if (!err.empty()) return err;
     const int nchunks = (n + kDotChunk - 1) / kDotChunk;
-    const size_t need = static_cast<size_t>(n) * ncols + (4 + extra) * static_cast<size_t>(n) +
-                        2 * static_cast<size_t>(ncols + 1) + static_cast<size_t>(nchunks) * (ncols + 1);
-    if (need > kNoAllocWorkspace || nchunks > kNoAllocNorm)
-        return extra ? "size:N x (restart + 7) exceeds the fixed workspace of 2097152 complex values"
-                     : "size:N x (restart + 5) exceeds the fixed workspace of 2097152 complex values";
+    const size_t need = noalloc_workspace_need(n, ncols, extra);
+    if (need > kNoAllocWorkspace || nchunks > kNoAllocNorm) {
+        // need = n (m + 5 + extra) + (m + 2)(2 + ceil(n / 8192)), m = ncols - 1
+        return "size:the solve needs " + std::to_string(need) + " complex values = N x (m + " +
+               std::to_string(5 + extra) + ") + (m + 2) x (2 + ceil(N / 8192)) with N = " + std::to_string(n) +
+               ", m = " + std::to_string(ncols - 1) +
+               " (restart, or max_iter without restart); the fixed workspace holds 2097152";
+    }
     if (!external_) release();
     external_ = true;
     n_ = n;

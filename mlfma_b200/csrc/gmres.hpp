@@ -76,6 +76,14 @@ private:
     double2* bo_ = nullptr;   // refinement: right-hand side
 };
 
+// The fixed workspace of Gmres::use_static_workspace: makes sure it exists on
+// the current device (CUDA creates a module's device arrays when the module is
+// first used on a device) and looks up its address; mlfma_setup calls it.
+std::string noalloc_workspace_prepare();
+// Complex values the fixed workspace must hold for a solve of n unknowns with
+// ncols basis vectors (restart + 1) and `extra` refinement vectors.
+size_t noalloc_workspace_need(int n, int ncols, int extra);
+
 // GMRES on nr right-hand sides sharing every product (gmres_multi.cu).
 class GmresMulti {
 public:

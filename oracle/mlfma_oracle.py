@@ -155,8 +155,15 @@ OFFSET_ID = {o: i for i, o in enumerate(OFFSETS)}
 # ------------------------------------------------------------------ sources
 
 def dyadic_uv(X, k, u, v):
-    """u^T G(X) v (Math::dyadicG, src/math.h:132-142), vectorised over rows of X."""
-    r = np.linalg.norm(X, axis=-1)
+    """u^T G(X) v (Math::dyadicG, src/math.h:132-142), vectorised over rows of X.
+
+    G is singular at X = 0; those entries come back as 0 (every caller masks
+    coincident points: the zero diagonal, coincident triangles), so no
+    divide-by-zero is evaluated and a NaN elsewhere stays visible."""
+    r0 = np.linalg.norm(X, axis=-1)
+    at0 = r0 == 0.0
+    r = np.where(at0, 1.0, r0)
+    X = np.where(at0[..., None], 1.0, X)
     kr = k * r
     invkrsq = 1.0 / (kr * kr)
     iinvkr = 1j / kr
@@ -165,7 +172,7 @@ def dyadic_uv(X, k, u, v):
     b = 1.0 + 3.0 * iinvkr - 3.0 * invkrsq
     uv = np.sum(u * v, axis=-1)
     urv = np.sum(u * rh, axis=-1) * np.sum(rh * v, axis=-1)
-    return np.exp(1j * kr) / r * (a * uv - b * urv)
+    return np.where(at0, 0.0, np.exp(1j * kr) / r * (a * uv - b * urv))
 
 
 QUAD_RULES = {  # Triangle::buildQuads (src/sources/triangle.cpp:45-130): (bary or None, weight)

@@ -62,6 +62,26 @@ def test_matvec_matches_reference(cuda_device, kind, geo, mns):
     op.close()
 
 
+@needs_ref
+def test_benchmark_workload_matches_reference(cuda_device):
+    # The workload every benchmark ratio is quoted on: the r = 2 wavelength
+    # icosphere-5 sphere (30,720 RWGs), root box 4, boxes split above 54 RWGs
+    # (5 levels), 7-point quadrature, 3 digits, 6-point interpolation, plain
+    # FP64 with the reference's rules.  Two consecutive products on different
+    # vectors keep the reference's state between products (stale locals) in step.
+    # The reference's own setup takes about 80 s on one core.
+    from oracle import ref_lib
+    m = inputs.make_icosphere(5, radius=2.0)
+    kw = dict(quad_prec=2, digits=3, interp_order=3, over_interp=2.0, root_leng=4.0, max_node_srcs=54)
+    op = MLFMA.rwg(m, PW, **kw).setup()
+    assert op.n == 30720 and op.stats()["max_level"] == 4
+    P = ref_lib.RefProblem("rwg", m, PW, **kw)
+    for seed in (11, 12):
+        x = cvec(op.n, seed)
+        assert rel(op.matvec(x), P.matvec(x)) <= TOL
+    op.close()
+
+
 def test_matvec_matches_numpy_oracle(cuda_device):
     from oracle import mlfma_oracle as O
     d = inputs.make_dipoles(1800, seed=8)

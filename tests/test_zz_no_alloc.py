@@ -22,7 +22,8 @@ def rel(a, b):
 
 
 def solve_noalloc(op, b_dev, x_dev, **kw):
-    o = SolverOpts(max_iter=kw["max_iter"], tol=kw["tol"], restart=kw["restart"], ref_givens=kw["ref_givens"])
+    o = SolverOpts(max_iter=kw["max_iter"], tol=kw["tol"], restart=kw["restart"], ref_givens=kw["ref_givens"],
+                   refine=int(kw.get("refine", False)))
     info = SolveInfo()
     code = _lib.lib().mlfma_gmres_noalloc(op._h, ctypes.c_void_p(b_dev.data_ptr()), ctypes.c_void_p(x_dev.data_ptr()),
                                           ctypes.byref(o), ctypes.byref(info))
@@ -45,6 +46,29 @@ def test_gmres_noalloc_matches_gmres(cuda_device):
         assert (code == _lib.MLFMA_OK) == info_ref.converged
         assert info.iterations == info_ref.iterations
         assert rel(x_dev.cpu().numpy(), x_ref) <= TOL
+    op.close()
+
+
+def test_gmres_noalloc_refined_mixed_matches_gmres(cuda_device):
+    # A mixed-precision operator with refinement uses the two extra vectors of
+    # the workspace (outer solution and right-hand side) and the FP64 far field
+    # for its outer residuals.
+    import torch
+    op = MLFMA.rwg(inputs.make_icosphere(3, radius=1.0), inputs.PlaneWave(), max_node_srcs=16, ref_compat=0,
+                   precision=1, self_terms=1).setup()
+    b = op.rhs()
+    opts = dict(max_iter=300, tol=1e-4, restart=30, ref_givens=False, refine=True)
+    x_ref, info_ref = op.solve(b, **opts)
+    assert info_ref.converged and info_ref.refinements >= 1
+    b_dev = torch.from_numpy(b).cuda()
+    for _ in range(2):
+        x_dev = torch.zeros_like(b_dev)
+        code, info = solve_noalloc(op, b_dev, x_dev, **opts)
+        assert code == _lib.MLFMA_OK
+        assert info.iterations == info_ref.iterations
+        assert info.refinements == info_ref.refinements
+        assert abs(info.true_residual - info_ref.true_residual) <= 1e-6 * info_ref.true_residual
+        assert rel(x_dev.cpu().numpy(), x_ref) <= 1e-8  # same float far field, same order of operations
     op.close()
 
 
