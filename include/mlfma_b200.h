@@ -274,6 +274,7 @@ typedef struct {
     float product_ms_before;   /* one product (nrhs right-hand sides) before and after, ms */
     float product_ms_after;
     int near_blocks_per_sm;    /* one-vector near field: persistent blocks per SM (it runs beside the far field) */
+    int interp_path;           /* interpolation/anterpolation kernels chosen (see mlfma_set_interp_path) */
 } mlfma_tuning;
 
 /* Autotuner: times the candidate launch shapes of the stages on this operator
@@ -283,6 +284,21 @@ typedef struct {
  * operator's state (the reference's stale locals) is preserved.  Call outside
  * any stream capture; out may be NULL. */
 int mlfma_autotune(mlfma_handle h, int nrhs, int reps, mlfma_tuning* out);
+
+/* Interpolation (M2M; Stem::buildMpoleCoeffs + addInterpCoeffs,
+ * src/fmm/stem.cpp:72-184) and anterpolation (L2L; getShiftedLocalCoeffs +
+ * addAnterpCoeffs, stem.cpp:109-244) of the complex-float far field on the
+ * tensor cores: every box of a level at once as separable theta and phi
+ * contractions (tcgen05 MMAs, split-precision 3xTF32, FP32 accumulation),
+ * children shifted and summed before the interpolation.  mode bit 0: the
+ * one-vector product, bit 1: the many-right-hand-side product; 0 = the
+ * CUDA-core kernels.  Defaults: bit 1 set when max_rhs > 1; mlfma_autotune
+ * times both and keeps the faster.  Products of the FP64 far field and
+ * transposed products always use the CUDA-core kernels.  MLFMA_ERR_ARG when
+ * the operator has no complex-float far field or a grid exceeds the kernels'
+ * shared memory.  Results agree with the CUDA-core kernels to float rounding. */
+int mlfma_set_interp_path(mlfma_handle h, int mode);
+int mlfma_get_interp_path(mlfma_handle h, int* mode);
 
 /* ---- Many independent operators of uneven size (no counterpart in the
  * reference, which holds one problem per process).  A batch refers to set-up

@@ -343,7 +343,21 @@ class MLFMA:
         check(lib().mlfma_autotune(self._h, nrhs, reps, ctypes.byref(t)))
         return {"m2l_chunk": t.m2l_chunk, "m2m_rows": list(t.m2m_rows), "multi_m2m_rows_fast": t.multi_m2m_rows_fast,
                 "multi_l2l_pairs": t.multi_l2l_pairs, "product_ms_before": t.product_ms_before,
-                "product_ms_after": t.product_ms_after, "near_blocks_per_sm": t.near_blocks_per_sm}
+                "product_ms_after": t.product_ms_after, "near_blocks_per_sm": t.near_blocks_per_sm,
+                "interp_path": t.interp_path}
+
+    @property
+    def interp_path(self) -> int:
+        """Interpolation/anterpolation kernels of the complex-float far field
+        (mlfma_set_interp_path): bit 0 tensor cores for one vector, bit 1 for
+        many right-hand sides; 0 = CUDA cores."""
+        m = ctypes.c_int()
+        check(lib().mlfma_get_interp_path(self._h, ctypes.byref(m)))
+        return m.value
+
+    @interp_path.setter
+    def interp_path(self, mode: int) -> None:
+        check(lib().mlfma_set_interp_path(self._h, int(mode)))
 
     def stream(self) -> int:
         s = ctypes.c_void_p()

@@ -67,7 +67,8 @@ class SolveInfo(ctypes.Structure):
 class Tuning(ctypes.Structure):
     _fields_ = [("m2l_chunk", ctypes.c_int), ("m2m_rows", ctypes.c_int * 20), ("multi_m2m_rows_fast", ctypes.c_int),
                 ("multi_l2l_pairs", ctypes.c_int), ("product_ms_before", ctypes.c_float),
-                ("product_ms_after", ctypes.c_float), ("near_blocks_per_sm", ctypes.c_int)]
+                ("product_ms_after", ctypes.c_float), ("near_blocks_per_sm", ctypes.c_int),
+                ("interp_path", ctypes.c_int)]
 
 
 # name -> (restype, argtypes); every symbol the header declares.
@@ -107,6 +108,8 @@ SIGNATURES = {
                                                 ctypes.c_int, _dp, ctypes.POINTER(SolverOpts), _dp, _dp, _dp, _dp,
                                                 ctypes.POINTER(SolveInfo)]),
     "mlfma_autotune": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(Tuning)]),
+    "mlfma_set_interp_path": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "mlfma_get_interp_path": (ctypes.c_int, [ctypes.c_void_p, _ip]),
     "mlfma_batch_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_void_p),
                                           ctypes.POINTER(ctypes.c_void_p)]),
     "mlfma_batch_size": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong)]),

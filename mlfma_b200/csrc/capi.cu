@@ -675,7 +675,21 @@ int mlfma_autotune(mlfma_handle h, int nrhs, int reps, mlfma_tuning* out) {
         out->product_ms_before = r.before_ms;
         out->product_ms_after = r.after_ms;
         out->near_blocks_per_sm = r.near_blocks_per_sm;
+        out->interp_path = r.interp_path;
     }
+    return MLFMA_OK;
+}
+
+int mlfma_set_interp_path(mlfma_handle h, int mode) {
+    if (!h) return fail(MLFMA_ERR_ARG, "null handle");
+    if (!ready(h)) return fail(MLFMA_ERR_STATE, "mlfma_setup has not run");
+    return from_msg(h->dev->set_tc(mode));
+}
+
+int mlfma_get_interp_path(mlfma_handle h, int* mode) {
+    if (!h || !mode) return fail(MLFMA_ERR_ARG, "null argument");
+    if (!ready(h)) return fail(MLFMA_ERR_STATE, "mlfma_setup has not run");
+    *mode = h->dev->tc_mode();
     return MLFMA_OK;
 }
 

@@ -145,6 +145,21 @@ struct TuneReport {
     int multi_l2l_pairs;           // many-rhs L2L column pairs per block
     float before_ms, after_ms;     // product time before and after
     int near_blocks_per_sm;        // one-vector near field: persistent blocks per SM
+    int interp_path;               // tensor-core interpolation: bit 0 one vector, bit 1 many
+};
+
+// Tensor-core interpolation and anterpolation of one level transition
+// (complex-float far field; kernels_tc.cuh): per pass (THETA, PHI, PHI_T,
+// THETA_T) the dense weight matrix split hi + lo in the MMA's canonical layout,
+// its contraction length K (reflected source rows included) and output count
+// N, both padded, and for the theta passes the source row of every
+// contraction index.
+struct TcTrans {
+    float* w[4] = {};
+    int K[4] = {}, Kpad[4] = {}, N[4] = {}, Npad[4] = {};
+    int* krow[4] = {};
+    size_t smem[4] = {};
+    int grid[4] = {};
 };
 
 struct StageTimes {
@@ -234,6 +249,13 @@ public:
     long long bytes_allocated() const { return bytes_; }
     int launches_per_matvec() const;
 
+    // Interpolation and anterpolation of the complex-float far field on the
+    // tensor cores (bit 0: one right-hand side, bit 1: many); false when the
+    // operator has no complex-float far field or a grid is too large for them.
+    bool tc_available() const { return tc_ok_; }
+    std::string set_tc(int mode);
+    int tc_mode() const { return (use_tc_ ? 1 : 0) | (use_tc_multi_ ? 2 : 0); }
+
     // Diagnostic copies of per-level patterns (level, which: 0 outgoing, 1 local),
     // widened to complex double.
     std::string copy_level(int level, int which, double2* host, long long count);
@@ -268,6 +290,10 @@ private:
     size_t m2l_item_capacity(int min_chunk) const;
     void build_m2l_items(int max_chunk);
     std::string ensure_graph(int prec, bool tr);
+    std::string setup_tc(const Plan& plan);
+    void far_m2m_tc(int p, int nr, cudaStream_t s);
+    void far_l2l_tc(int p, int nr, cudaStream_t s);
+    void drop_graphs();
     static int m2m_rows(int nth, int nph);
 
     int device_ = 0;
@@ -357,6 +383,12 @@ private:
     int* m2l_cand_src_ = nullptr;
     int2* m2l_items_m_ = nullptr;
     int n_m2l_items_m_ = 0;
+    // Tensor-core interpolation (complex-float far field), per transition.
+    std::vector<TcTrans> tc_;
+    float* tc_scratch_ = nullptr;       // intermediate of the two passes of a stage
+    size_t tc_scratch_floats_ = 0;
+    bool tc_ok_ = false;
+    bool use_tc_ = false, use_tc_multi_ = false;
     double2 ck_{};             // Phys::C * k
     double2* loads_ = nullptr; // diagonal loads, tree order
     bool has_loads_ = false;

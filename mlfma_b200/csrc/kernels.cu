@@ -33,6 +33,7 @@
 #include "kernels_far.cuh"
 #include "kernels_multi.cuh"
 #include "kernels_near.cuh"
+#include "kernels_tc.cuh"
 #include "zmath.cuh"
 
 namespace mlfma {
@@ -129,8 +130,9 @@ void DeviceOp::set_near_grid(int per_sm) {
 void launch_wait_runs_out(long long limit, int* status) { k_wait_runs_out<<<1, 32>>>(limit, status); }
 
 std::string DeviceOp::device_error() const {
-    if (err_host_ && *static_cast<volatile int*>(err_host_))
-        return "near-field kernel: a bulk copy did not complete within its bounded wait";
+    const int e = err_host_ ? *static_cast<volatile int*>(err_host_) : 0;
+    if (e == 1) return "near-field kernel: a bulk copy did not complete within its bounded wait";
+    if (e == 2) return "tensor-core interpolation kernel: a copy or an MMA did not complete within its bounded wait";
     return {};
 }
 
@@ -573,6 +575,8 @@ std::string DeviceOp::setup(const Plan& plan, int device, int precision, int max
         if (precision != kFp64) {
             err = setup_far<float>(plan, f32_, pat64);
             if (!err.empty()) return err;
+            err = setup_tc(plan);
+            if (!err.empty()) return err;
         }
 
         // ---- near field: the stored blocks (each interaction once), applied
@@ -733,12 +737,17 @@ void DeviceOp::far_l2t(FarField<R>& F, cudaStream_t s) {
 template <class R, bool TR>
 void DeviceOp::run_far_t(FarField<R>& F, const double2* xt, cudaStream_t s, int stage) {
     if (n_leaves_ == 0) return;
+    const bool tc = std::is_same<R, float>::value && !TR && use_tc_;
     if (stage < 0 || stage == 0) far_s2m<R, TR>(F, xt, s);
     if (stage < 0 || stage == 1)
-        for (int p = lmax_ - 1; p >= lmin_; --p) far_m2m<R, TR>(F, p, s);
+        for (int p = lmax_ - 1; p >= lmin_; --p) {
+            if (tc) far_m2m_tc(p, 1, s); else far_m2m<R, TR>(F, p, s);
+        }
     if (stage < 0 || stage == 2) far_m2l<R, TR>(F, lmin_, lmax_, s);
     if (stage < 0 || stage == 3)
-        for (int p = lmin_; p < lmax_; ++p) far_l2l<R, TR>(F, p, s);
+        for (int p = lmin_; p < lmax_; ++p) {
+            if (tc) far_l2l_tc(p, 1, s); else far_l2l<R, TR>(F, p, s);
+        }
     if (stage < 0 || stage == 4) far_l2t<R, TR>(F, s);
 }
 
@@ -754,10 +763,11 @@ void DeviceOp::run_far_overlap_t(FarField<R>& F, const double2* xt, cudaStream_t
         run_far_t<R, TR>(F, xt, s, -1);
         return;
     }
+    const bool tc = std::is_same<R, float>::value && !TR && use_tc_;
     far_s2m<R, TR>(F, xt, s);
     cudaEventRecord(ev_level_[lmax_], s);
     for (int p = lmax_ - 1; p >= lmin_; --p) {
-        far_m2m<R, TR>(F, p, s);
+        if (tc) far_m2m_tc(p, 1, s); else far_m2m<R, TR>(F, p, s);
         cudaEventRecord(ev_level_[p], s);
     }
     for (int l = lmax_; l > lmin_; --l) {
@@ -767,7 +777,9 @@ void DeviceOp::run_far_overlap_t(FarField<R>& F, const double2* xt, cudaStream_t
     cudaEventRecord(ev_m2l_done_, s2);
     far_m2l<R, TR>(F, lmin_, lmin_, s);
     cudaStreamWaitEvent(s, ev_m2l_done_, 0);
-    for (int p = lmin_; p < lmax_; ++p) far_l2l<R, TR>(F, p, s);
+    for (int p = lmin_; p < lmax_; ++p) {
+        if (tc) far_l2l_tc(p, 1, s); else far_l2l<R, TR>(F, p, s);
+    }
     far_l2t<R, TR>(F, s);
 }
 
@@ -1125,7 +1137,10 @@ void DeviceOp::run_far_multi_t(FarField<R>& F, int nr, cudaStream_t s, int stage
     if (n_leaves_ == 0) return;
     if ((stage < 0 || stage == 0) && n_s2m_items_m_)
         k_s2m_m<R><<<n_s2m_items_m_, kGemmThreads, 0, s>>>(F.lv_dev, s2m_items_m_, leaves_, F.pat, xtm_, nr);
-    if (stage < 0 || stage == 1)
+    const bool tc = std::is_same<R, float>::value && use_tc_multi_;
+    if ((stage < 0 || stage == 1) && tc)
+        for (int p = lmax_ - 1; p >= lmin_; --p) far_m2m_tc(p, nr, s);
+    if ((stage < 0 || stage == 1) && !tc)
         for (int p = lmax_ - 1; p >= lmin_; --p) {
             if (npar_[p] == 0) continue;
             constexpr int rc = 16 * m2m_rpl<R>();
@@ -1152,7 +1167,9 @@ void DeviceOp::run_far_multi_t(FarField<R>& F, int nr, cudaStream_t s, int stage
         k_m2l_m<R><<<n_m2l_items_m_, threads, 0, s>>>(F.lv_dev, m2l_items_m_, m2l_groups_, m2l_cand_src_,
                                                       F.m2l_t8, nr, ref_compat_ ? 0 : 1);
     }
-    if (stage < 0 || stage == 3)
+    if ((stage < 0 || stage == 3) && tc)
+        for (int p = lmin_; p < lmax_; ++p) far_l2l_tc(p, nr, s);
+    if ((stage < 0 || stage == 3) && !tc)
         for (int p = lmin_; p < lmax_; ++p) {
             const int g = n_l2l_pairs_[p];
             if (!g) continue;
@@ -1258,6 +1275,207 @@ std::string DeviceOp::time_stages_multi(int nr, StageTimes* out) {
     return {};
 }
 
+// ================================================================= tensor-core interpolation
+
+namespace {
+
+// The shared-memory limit is a property of the kernel, shared by every
+// operator: set it to the device's opt-in maximum.
+template <int KIND>
+cudaError_t tc_prepare(int smem) {
+    return cudaFuncSetAttribute(k_tc_pass<KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+}
+
+}  // namespace
+
+// Weights, contraction tables and the intermediate buffer of the tensor-core
+// passes of every transition; tc_ok_ stays false (the CUDA-core kernels run)
+// when a grid needs more shared memory than a CTA has.
+std::string DeviceOp::setup_tc(const Plan& plan) {
+    tc_ok_ = false;
+    tc_.assign(std::max(lmax_, 0) + 1, TcTrans{});
+    int dev_smem = 0;
+    MLFMA_CK(cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, device_));
+    if (!sms_) MLFMA_CK(cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, device_));
+    size_t scr_one = 1, scr_many = 1;
+    for (int p = lmin_; p < lmax_; ++p) {
+        const Transition& T = plan.trans[p];
+        TcTrans& t = tc_[p];
+        TcDense d[4];
+        std::string e;
+        if ((e = tc_dense_weights(T.up_th, nth_[p + 1], true, d[kTcTheta])).size() ||
+            (e = tc_dense_weights(T.up_ph, nph_[p + 1], false, d[kTcPhi])).size() ||
+            (e = tc_dense_weights(T.dn_ph, nph_[p], false, d[kTcPhiT])).size() ||
+            (e = tc_dense_weights(T.dn_th, nth_[p], true, d[kTcThetaT])).size())
+            return {};  // not expressible: keep the CUDA-core kernels
+        for (int k = 0; k < 4; ++k) {
+            t.K[k] = d[k].K;
+            t.Kpad[k] = (d[k].K + 7) / 8 * 8;
+            t.N[k] = d[k].N;
+            t.Npad[k] = (d[k].N + 15) / 16 * 16;
+            if (t.Npad[k] > 256) return {};
+            t.smem[k] = tc_smem_bytes(t.Npad[k], t.Kpad[k], t.K[k]);
+            if (t.smem[k] > static_cast<size_t>(dev_smem)) return {};
+        }
+        for (int k = 0; k < 4; ++k) {
+            t.w[k] = upload(tc_pack_weights(d[k], t.Npad[k], t.Kpad[k]));
+            if (k == kTcTheta || k == kTcThetaT) t.krow[k] = upload(d[k].krow);
+        }
+        const size_t per_item = static_cast<size_t>(nth_[p]) * nph_[p + 1] * 4;  // one vector: [nth_p][mph][4]
+        const size_t items = static_cast<size_t>(std::max(npar_[p], n_l2l_pairs_[p]));
+        scr_one = std::max(scr_one, per_item * items);
+        scr_many = std::max(scr_many, per_item * items * max_rhs_);
+    }
+    // many right-hand sides: items in chunks whose intermediate fits the buffer
+    // (at most 64 MB beyond what one vector needs)
+    tc_scratch_floats_ = std::max(scr_one, std::min(scr_many, static_cast<size_t>(16) << 20));
+    for (int p = lmin_; p < lmax_; ++p)  // one item's intermediate must fit (chunks of at least one item)
+        if (static_cast<size_t>(nth_[p]) * nph_[p + 1] * 4 * max_rhs_ > tc_scratch_floats_) return {};
+    tc_scratch_ = alloc<float>(tc_scratch_floats_);
+    MLFMA_CK(tc_prepare<kTcTheta>(dev_smem));
+    MLFMA_CK(tc_prepare<kTcPhi>(dev_smem));
+    MLFMA_CK(tc_prepare<kTcPhiT>(dev_smem));
+    MLFMA_CK(tc_prepare<kTcThetaT>(dev_smem));
+    const auto ncols_of = [](int npad) { int c = 32; while (c < npad) c <<= 1; return c; };
+    const void* fns[4] = {reinterpret_cast<const void*>(k_tc_pass<kTcTheta>),
+                          reinterpret_cast<const void*>(k_tc_pass<kTcPhi>),
+                          reinterpret_cast<const void*>(k_tc_pass<kTcPhiT>),
+                          reinterpret_cast<const void*>(k_tc_pass<kTcThetaT>)};
+    for (int p = lmin_; p < lmax_; ++p)
+        for (int k = 0; k < 4; ++k) {
+            // persistent CTAs: as many per SM as shared memory and the 512
+            // tensor-memory columns of an SM allow
+            TcTrans& t = tc_[p];
+            int occ = 0;
+            MLFMA_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fns[k], kTcThreads, static_cast<int>(t.smem[k])));
+            occ = std::max(1, std::min(occ, 512 / ncols_of(t.Npad[k])));
+            t.grid[k] = occ * sms_;
+        }
+    tc_ok_ = true;
+    use_tc_multi_ = max_rhs_ > 1;
+    return {};
+}
+
+namespace {
+TcArgs tc_args_common(int nr, const DevTransT<float>& T, const TcTrans& t, int kind, int mth, int mph, int nth,
+                      int nph) {
+    TcArgs a{};
+    a.K = t.K[kind];
+    a.Kpad = t.Kpad[kind];
+    a.N = t.N[kind];
+    a.Npad = t.Npad[kind];
+    a.w = t.w[kind];
+    a.krow = t.krow[kind];
+    a.nr = nr;
+    a.Q = 4 * nr;
+    a.mth = mth;
+    a.mph = mph;
+    a.nth = nth;
+    a.nph = nph;
+    a.child_ptr = T.child_ptr;
+    a.child_box = T.child_box;
+    a.child_oct = T.child_oct;
+    a.par_box = T.par_box;
+    return a;
+}
+
+template <int KIND>
+void tc_launch(const TcArgs& a, const TcTrans& t, int* err, cudaStream_t s) {
+    const long long rows = static_cast<long long>(a.J) * a.Q * a.nitems;
+    const long long tiles = (rows + kTcRows - 1) / kTcRows;
+    if (tiles <= 0) return;
+    const int grid = static_cast<int>(std::min<long long>(tiles, t.grid[KIND]));
+    k_tc_pass<KIND><<<grid, kTcThreads, t.smem[KIND], s>>>(a, err);
+}
+}  // namespace
+
+// M2M of transition p on nr right-hand sides (nr = 1: the one-vector
+// patterns A; nr > 1: the many-rhs patterns Am), parents in chunks whose
+// intermediate fits the buffer.
+void DeviceOp::far_m2m_tc(int p, int nr, cudaStream_t s) {
+    if (npar_[p] == 0) return;
+    const TcTrans& t = tc_[p];
+    const DevTransT<float>& T = f32_.trans[p];
+    const DevLevelT<float>& P = f32_.lv[p];
+    const DevLevelT<float>& C = f32_.lv[p + 1];
+    const size_t per_item = static_cast<size_t>(nth_[p]) * nph_[p + 1] * 4 * nr;
+    const int chunk = static_cast<int>(std::max<size_t>(1, std::min<size_t>(npar_[p], tc_scratch_floats_ / per_item)));
+    for (int i0 = 0; i0 < npar_[p]; i0 += chunk) {
+        const int ni = std::min(chunk, npar_[p] - i0);
+        TcArgs a = tc_args_common(nr, T, t, kTcTheta, nth_[p + 1], nph_[p + 1], nth_[p], nph_[p]);
+        a.item0 = i0;
+        a.nitems = ni;
+        a.J = nph_[p + 1];
+        a.pat_in = nr == 1 ? C.A : C.Am;
+        a.shift = C.shift_up;
+        a.scr_out = tc_scratch_;
+        tc_launch<kTcTheta>(a, t, err_dev_, s);
+        TcArgs b = tc_args_common(nr, T, t, kTcPhi, nth_[p + 1], nph_[p + 1], nth_[p], nph_[p]);
+        b.item0 = i0;
+        b.nitems = ni;
+        b.J = nth_[p];
+        b.scr_in = tc_scratch_;
+        b.pat_out = nr == 1 ? P.A : P.Am;
+        tc_launch<kTcPhi>(b, t, err_dev_, s);
+    }
+}
+
+// L2L of transition p on nr right-hand sides, (parent, child) pairs in chunks.
+void DeviceOp::far_l2l_tc(int p, int nr, cudaStream_t s) {
+    const int npairs = n_l2l_pairs_[p];
+    if (npairs == 0) return;
+    const TcTrans& t = tc_[p];
+    const DevTransT<float>& T = f32_.trans[p];
+    const DevLevelT<float>& P = f32_.lv[p];
+    const DevLevelT<float>& C = f32_.lv[p + 1];
+    const size_t per_item = static_cast<size_t>(nth_[p]) * nph_[p + 1] * 4 * nr;
+    const int chunk = static_cast<int>(std::max<size_t>(1, std::min<size_t>(npairs, tc_scratch_floats_ / per_item)));
+    for (int i0 = 0; i0 < npairs; i0 += chunk) {
+        const int ni = std::min(chunk, npairs - i0);
+        TcArgs a = tc_args_common(nr, T, t, kTcPhiT, nth_[p + 1], nph_[p + 1], nth_[p], nph_[p]);
+        a.item0 = i0;
+        a.nitems = ni;
+        a.J = nth_[p];
+        a.pat_in = nr == 1 ? P.B : P.Bm;
+        a.shift = P.shift_down;
+        a.pairs = l2l_pairs_[p];
+        a.scr_out = tc_scratch_;
+        tc_launch<kTcPhiT>(a, t, err_dev_, s);
+        TcArgs b = tc_args_common(nr, T, t, kTcThetaT, nth_[p + 1], nph_[p + 1], nth_[p], nph_[p]);
+        b.item0 = i0;
+        b.nitems = ni;
+        b.J = nph_[p + 1];
+        b.pairs = l2l_pairs_[p];
+        b.scr_in = tc_scratch_;
+        b.pat_out = nr == 1 ? C.B : C.Bm;
+        tc_launch<kTcThetaT>(b, t, err_dev_, s);
+    }
+}
+
+void DeviceOp::drop_graphs() {
+    for (int p = 0; p < 2; ++p)
+        for (int t = 0; t < 2; ++t) {
+            if (graph_exec_[p][t]) cudaGraphExecDestroy(graph_exec_[p][t]);
+            if (graph_[p][t]) cudaGraphDestroy(graph_[p][t]);
+            graph_exec_[p][t] = nullptr;
+            graph_[p][t] = nullptr;
+        }
+}
+
+std::string DeviceOp::set_tc(int mode) {
+    if (!ready_) return "operator not set up";
+    if (mode < 0 || mode > 3) return "arg:mode must be 0..3";
+    if (mode && !tc_ok_)
+        return "arg:no tensor-core interpolation on this operator (FP64 far field only, or a grid too large)";
+    if ((mode & 2) && max_rhs_ < 2) return "arg:the many-right-hand-side mode needs max_rhs > 1";
+    MLFMA_CK(cudaSetDevice(device_));
+    MLFMA_CK(cudaStreamSynchronize(stream_));
+    use_tc_ = (mode & 1) != 0;
+    use_tc_multi_ = (mode & 2) != 0;
+    drop_graphs();  // recaptured with the chosen kernels on the next product
+    return {};
+}
+
 // ================================================================= autotuner
 
 // Times the candidate launch shapes of the stages on this operator (CUDA
@@ -1358,6 +1576,15 @@ std::string DeviceOp::autotune(int nr, int reps, TuneReport* rep) {
             set_near_grid(bk);
         }
         r.near_blocks_per_sm = near_per_sm_;
+        // interpolation and anterpolation: tensor cores or CUDA cores (the
+        // complex-float far field), timed on the whole product
+        if (tc_ok_ && precision_ != kFp64) {
+            use_tc_ = false;
+            const float t_cc = timed(product);
+            use_tc_ = true;
+            const float t_tc = timed(product);
+            use_tc_ = t_tc < t_cc;
+        }
         r.after_ms = timed(product);
     } else {
         auto product = [&] { enqueue_multi(nr, s, precision_); };
@@ -1386,8 +1613,16 @@ std::string DeviceOp::autotune(int nr, int reps, TuneReport* rep) {
         m_l2l_pairs_ = bpairs;
         r.multi_rows_fast = border;
         r.multi_l2l_pairs = bpairs;
+        if (tc_ok_ && precision_ != kFp64) {
+            use_tc_multi_ = false;
+            const float t_cc = timed(product);
+            use_tc_multi_ = true;
+            const float t_tc = timed(product);
+            use_tc_multi_ = t_tc < t_cc;
+        }
         r.after_ms = timed(product);
     }
+    r.interp_path = tc_mode();
     r.m2l_chunk = m2l_chunk_;
     for (int p = lmin_; p < lmax_; ++p) r.m2m_rows[p] = m2m_rows_[p];
     if (r.multi_rows_fast == 0 && m_m2m_rows_fast_ < 0) r.multi_rows_fast = -1;
@@ -1398,13 +1633,7 @@ std::string DeviceOp::autotune(int nr, int reps, TuneReport* rep) {
     for (void* t : tmp) cudaFree(t);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    for (int p = 0; p < 2; ++p)
-        for (int t = 0; t < 2; ++t) {
-            if (graph_exec_[p][t]) cudaGraphExecDestroy(graph_exec_[p][t]);
-            if (graph_[p][t]) cudaGraphDestroy(graph_[p][t]);
-            graph_exec_[p][t] = nullptr;
-            graph_[p][t] = nullptr;
-        }
+    drop_graphs();
     if (rep) *rep = r;
     MLFMA_CK(cudaGetLastError());
     return {};
