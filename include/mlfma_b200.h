@@ -101,7 +101,15 @@ typedef struct {
                             mixed operator, outer residual r = b - A x in FP64, x += correction;
                             stops on the FP64 residual); 0 = GMRES on the mixed operator alone.
                             Ignored by MLFMA_FP64 operators. */
-    double inner_tol;    /* refinement: inner relative residual target (0 = automatic) */
+    double inner_tol;    /* refinement: inner relative residual target (0 = automatic); flexible:
+                            an inner solve stops early below this relative residual (0 = never) */
+    int flexible;        /* 1: flexible GMRES (FGMRES(restart), restart 0 = max_iter outer steps):
+                            outer Krylov space, products and residual in FP64; each outer step's
+                            preconditioner is inner_iters GMRES iterations from zero on the
+                            operator's own far field (the complex-float one on a mixed operator).
+                            iterations counts inner products, refinements outer products.
+                            No counterpart in the reference. */
+    int inner_iters;     /* flexible: GMRES iterations per inner solve (0 = 20) */
 } mlfma_solver_opts;
 
 typedef struct {

@@ -185,14 +185,17 @@ class MLFMA:
                                         int(accumulate), ctypes.c_void_p(stream)))
 
     def solve(self, b=None, max_iter: int = 500, tol: float = 1e-6, restart: int = 0,
-              ref_givens: bool = True, raise_on_fail: bool = False, refine: bool = False, inner_tol: float = 0.0):
+              ref_givens: bool = True, raise_on_fail: bool = False, refine: bool = False, inner_tol: float = 0.0,
+              flexible: bool = False, inner_iters: int = 0):
         """GMRES (Solver::solve).  On a mixed operator, refine=True runs
         iterative refinement: inner GMRES on the mixed operator, outer FP64
-        residual; tol then holds for the FP64 residual."""
+        residual; tol then holds for the FP64 residual.  flexible=True runs
+        FGMRES(restart): FP64 outer Krylov space, each outer step preconditioned
+        by inner_iters GMRES iterations on the operator's own far field."""
         bv = self.rhs() if b is None else _cvec(b, self.n)
         x = np.zeros(self.n, dtype=np.complex128)
         o = SolverOpts(max_iter=max_iter, tol=tol, restart=restart, ref_givens=int(ref_givens),
-                       refine=int(refine), inner_tol=inner_tol)
+                       refine=int(refine), inner_tol=inner_tol, flexible=int(flexible), inner_iters=inner_iters)
         info = SolveInfo()
         code = lib().mlfma_gmres(self._h, bv.view(np.float64).ctypes.data_as(_dp),
                                  x.view(np.float64).ctypes.data_as(_dp), ctypes.byref(o), ctypes.byref(info))

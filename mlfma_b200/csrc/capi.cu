@@ -239,6 +239,8 @@ int mlfma_gmres(mlfma_handle h, const double* b, double* x, const mlfma_solver_o
         o.ref_givens = opts->ref_givens;
         o.refine = opts->refine;
         o.inner_tol = opts->inner_tol;
+        o.flexible = opts->flexible;
+        o.inner_iters = opts->inner_iters;
     }
     const size_t bytes = sizeof(double2) * h->plan.n;
     cudaStream_t s = h->dev->stream();
@@ -353,8 +355,11 @@ int mlfma_gmres_noalloc(mlfma_handle h, const void* d_b, void* d_x, const mlfma_
         o.ref_givens = opts->ref_givens;
         o.refine = opts->refine;
         o.inner_tol = opts->inner_tol;
+        o.flexible = opts->flexible;
+        o.inner_iters = opts->inner_iters;
     }
     if (o.max_iter < 1 || o.restart < 0) return fail(MLFMA_ERR_ARG, "max_iter and restart must be positive");
+    if (o.flexible) return fail(MLFMA_ERR_ARG, "the flexible solve needs its own workspace (use mlfma_gmres)");
     if (cudaSetDevice(h->device) != cudaSuccess) return fail(MLFMA_ERR_CUDA, "cudaSetDevice failed");
     if (!h->gmres_fixed) h->gmres_fixed = std::make_unique<mlfma::Gmres>();
     const int m = o.restart > 0 ? o.restart : o.max_iter;
@@ -437,7 +442,10 @@ int mlfma_gmres_multi(mlfma_handle h, int nrhs, const double* b, double* x, cons
         o.ref_givens = opts->ref_givens;
         o.refine = opts->refine;
         o.inner_tol = opts->inner_tol;
+        o.flexible = opts->flexible;
+        o.inner_iters = opts->inner_iters;
     }
+    if (o.flexible) return fail(MLFMA_ERR_ARG, "flexible GMRES runs one right-hand side at a time (mlfma_gmres)");
     if (cudaSetDevice(h->device) != cudaSuccess) return fail(MLFMA_ERR_CUDA, "cudaSetDevice failed");
     int code = ensure_multi_staging(h);
     if (code != MLFMA_OK) return code;
@@ -528,6 +536,8 @@ static mlfma::SolveOpts to_opts(const mlfma_solver_opts* opts) {
         o.ref_givens = opts->ref_givens;
         o.refine = opts->refine;
         o.inner_tol = opts->inner_tol;
+        o.flexible = opts->flexible;
+        o.inner_iters = opts->inner_iters;
     }
     return o;
 }

@@ -186,7 +186,34 @@ void Gmres::release() {
     n_ = cap_ = extra_ = 0;
 }
 
-Gmres::~Gmres() { release(); }
+Gmres::~Gmres() {
+    release();
+    release_outer();
+}
+
+std::string Gmres::ensure_outer(int n, int ncols) {
+    if (n == on_ && ncols <= ocap_) return {};
+    release_outer();
+    on_ = n;
+    ocap_ = ncols;
+    const int nch = (n + kDotChunk - 1) / kDotChunk;
+    GM_CK(cudaMalloc(&V_, sizeof(double2) * static_cast<size_t>(n) * (ncols + 1)));
+    GM_CK(cudaMalloc(&Z_, sizeof(double2) * static_cast<size_t>(n) * ncols));
+    GM_CK(cudaMalloc(&wo_, sizeof(double2) * n));
+    GM_CK(cudaMalloc(&xf_, sizeof(double2) * n));
+    GM_CK(cudaMalloc(&bf_, sizeof(double2) * n));
+    GM_CK(cudaMalloc(&ho_, sizeof(double2) * (ncols + 2)));
+    GM_CK(cudaMalloc(&to_, sizeof(double2) * (ncols + 2)));
+    GM_CK(cudaMalloc(&po_, sizeof(double2) * static_cast<size_t>(nch) * (ncols + 2)));
+    return {};
+}
+
+void Gmres::release_outer() {
+    for (void* p : {(void*)V_, (void*)Z_, (void*)wo_, (void*)xf_, (void*)bf_, (void*)ho_, (void*)to_, (void*)po_})
+        if (p) cudaFree(p);
+    V_ = Z_ = wo_ = xf_ = bf_ = ho_ = to_ = po_ = nullptr;
+    on_ = ocap_ = 0;
+}
 
 void Gmres::apply(DeviceOp& op, const double2* x, double2* y, cudaStream_t s, int prec) {
     if (external_) op.apply_tree_direct(x, y, s, prec, adj_); else op.apply_tree(x, y, s, prec, adj_);
@@ -433,6 +460,10 @@ std::string Gmres::solve(DeviceOp& op, const double2* d_b_user, double2* d_x_use
                          SolveResult* res) {
     if (o.adjoint && op.ref_compat()) return "arg:the adjoint needs ref_compat = 0";
     adj_ = o.adjoint != 0;
+    if (o.flexible) {
+        if (external_) return "arg:the flexible solve needs its own workspace (use mlfma_gmres)";
+        return solve_flexible(op, d_b_user, d_x_user, o, res);
+    }
     if (o.refine && op.precision() != kFp64) return solve_refined(op, d_b_user, d_x_user, o, res);
     const auto t_start = std::chrono::steady_clock::now();
     const int n = op.n();
@@ -534,6 +565,151 @@ std::string Gmres::solve_refined(DeviceOp& op, const double2* d_b_user, double2*
     }
     res->true_residual = rn / bnorm;
     k_scatter_perm<<<nblk(n, 256), 256, 0, s>>>(xo_, perm, d_x_user, n);
+    GM_CK(cudaStreamSynchronize(s));
+    res->converged = converged;
+    res->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
+    return {};
+}
+
+// Flexible GMRES (FGMRES(m), right preconditioning that may change at every
+// step): the outer Krylov space, its products, the Hessenberg matrix, the
+// unitary Givens rotations and the residual are FP64; the preconditioner of
+// outer step j is an inner GMRES of `inner_iters` iterations from zero on
+// A z = v_j on the operator's own far field (complex float on a mixed
+// operator), so every inner solve's result z_j enters the solution
+// x = x0 + Z y exactly, and the inner precision only changes how good a
+// preconditioner it is.  The outer space keeps what restarted GMRES(m) throws
+// away at each restart; the stopping test is the FP64 residual.
+std::string Gmres::solve_flexible(DeviceOp& op, const double2* d_b_user, double2* d_x_user, const SolveOpts& o,
+                                  SolveResult* res) {
+    using cd = std::complex<double>;
+    const auto t_start = std::chrono::steady_clock::now();
+    const int n = op.n();
+    const int mo = o.restart > 0 ? o.restart : o.max_iter;
+    const int mi = o.inner_iters > 0 ? o.inner_iters : 20;
+    if (mo < 1 || o.max_iter < 1) return "max_iter and restart must be positive";
+    std::string err = ensure(n, mi + 1, 0);
+    if (!err.empty()) return err;
+    err = ensure_outer(n, mo);
+    if (!err.empty()) return err;
+    cudaStream_t s = op.stream();
+    const int* perm = op.perm();
+    const int nch = nchunks_;
+    const int prec_in = op.precision();
+    k_gather_perm<<<nblk(n, 256), 256, 0, s>>>(d_b_user, perm, bf_, n);
+    GM_CK(cudaMemsetAsync(xf_, 0, sizeof(double2) * n, s));
+    double bnorm = 0;
+    err = norm(bf_, s, &bnorm);
+    if (!err.empty()) return err;
+    if (!std::isfinite(bnorm)) return "nonfinite:right-hand side";
+    *res = SolveResult{};
+    if (bnorm == 0.0) {
+        GM_CK(cudaMemsetAsync(d_x_user, 0, sizeof(double2) * n, s));
+        GM_CK(cudaStreamSynchronize(s));
+        res->converged = true;
+        return {};
+    }
+    const double tol_abs = o.tol * bnorm;
+    // CGS2 of w against the first ncols outer basis vectors: h (device) = V^H w
+    // summed over both passes, w orthogonalised in place.
+    auto cgs2 = [&](int ncols) {
+        const dim3 grid(nch, ncols);
+        for (int pass = 0; pass < 2; ++pass) {
+            k_multi_dot<<<grid, kDotThreads, 0, s>>>(V_, n, ncols, wo_, n, po_, nch);
+            k_reduce_partials<<<nblk(ncols, 128), 128, 0, s>>>(po_, nch, ncols, to_, 0);
+            k_sub_qh<<<nblk(n, 256), 256, 0, s>>>(V_, n, ncols, to_, wo_, n);
+            k_reduce_partials<<<nblk(ncols, 128), 128, 0, s>>>(po_, nch, ncols, ho_, pass);
+        }
+    };
+    std::vector<cd> H(static_cast<size_t>(mo + 1) * mo), cs(mo), sn(mo), g(mo + 1);
+    std::vector<double2> hcol(mo + 2);
+    double beta = bnorm;
+    bool converged = false;
+    SolveOpts oi = o;
+    oi.restart = mi;
+    oi.flexible = 0;
+    GM_CK(cudaMemcpyAsync(r_, bf_, sizeof(double2) * n, cudaMemcpyDeviceToDevice, s));  // r = b (x = 0)
+    while (res->iterations < o.max_iter && !converged) {
+        k_scale<<<nblk(n, 256), 256, 0, s>>>(r_, make_double2(1.0 / beta, 0.0), V_, n);
+        std::fill(g.begin(), g.end(), cd(0));
+        g[0] = beta;
+        int k = 0;
+        for (; k < mo && res->iterations < o.max_iter; ++k) {
+            double2* vk = V_ + static_cast<size_t>(k) * n;
+            double2* zk = Z_ + static_cast<size_t>(k) * n;
+            // inner solve A z = v_k from zero (||v_k|| = 1)
+            GM_CK(cudaMemcpyAsync(b_, vk, sizeof(double2) * n, cudaMemcpyDeviceToDevice, s));
+            int it = 0;
+            double est = 0;
+            bool c = false;
+            err = cycles(op, prec_in, oi, 1.0, o.inner_tol > 0 ? o.inner_tol : 0.0,
+                         std::min(mi, o.max_iter - res->iterations), false, &it, &est, &c);
+            if (!err.empty()) return err;
+            res->iterations += it;
+            GM_CK(cudaMemcpyAsync(zk, x_, sizeof(double2) * n, cudaMemcpyDeviceToDevice, s));
+            // w = A z_k in FP64, orthogonalised against v_0..v_k
+            apply(op, zk, wo_, s, kFp64);
+            ++res->refinements;
+            cgs2(k + 1);
+            k_norm2<<<nch, kDotThreads, 0, s>>>(wo_, n, npartial_);
+            k_sum_into<<<1, 1, 0, s>>>(npartial_, nch, ho_ + k + 1);
+            GM_CK(cudaMemcpyAsync(hcol.data(), ho_, sizeof(double2) * (k + 2), cudaMemcpyDeviceToHost, s));
+            GM_CK(cudaStreamSynchronize(s));
+            const double hn = std::sqrt(hcol[k + 1].x);
+            if (!std::isfinite(hn)) return "nonfinite:Arnoldi";
+            std::vector<cd> hc(k + 2);
+            for (int i = 0; i <= k; ++i) hc[i] = cd(hcol[i].x, hcol[i].y);
+            hc[k + 1] = hn;
+            if (hn > 0)
+                k_scale<<<nblk(n, 256), 256, 0, s>>>(wo_, make_double2(1.0 / hn, 0.0), V_ + static_cast<size_t>(k + 1) * n, n);
+            for (int i = 0; i < k; ++i) {  // previous unitary rotations
+                const cd a = hc[i], b = hc[i + 1];
+                hc[i] = cs[i] * a + sn[i] * b;
+                hc[i + 1] = -std::conj(sn[i]) * a + cs[i] * b;
+            }
+            const double az = std::abs(hc[k]);
+            const double t = std::sqrt(az * az + std::norm(hc[k + 1]));
+            cd cr, sr;
+            if (az == 0.0) {
+                cr = 0.0;
+                sr = 1.0;
+            } else {
+                cr = az / t;
+                sr = (hc[k] / az) * std::conj(hc[k + 1]) / t;
+            }
+            hc[k] = cr * hc[k] + sr * hc[k + 1];
+            g[k + 1] = -std::conj(sr) * g[k];
+            g[k] = cr * g[k];
+            cs[k] = cr;
+            sn[k] = sr;
+            for (int i = 0; i <= k; ++i) H[static_cast<size_t>(k) * (mo + 1) + i] = hc[i];
+            res->residual = std::abs(g[k + 1]) / bnorm;
+            if (!(std::abs(g[k + 1]) > tol_abs) || hn == 0.0) {
+                ++k;
+                break;
+            }
+        }
+        // x += Z y, R y = g
+        std::vector<cd> yv(k);
+        for (int i = k - 1; i >= 0; --i) {
+            cd acc = g[i];
+            for (int j = i + 1; j < k; ++j) acc -= H[static_cast<size_t>(j) * (mo + 1) + i] * yv[j];
+            yv[i] = acc / H[static_cast<size_t>(i) * (mo + 1) + i];
+        }
+        std::vector<double2> yd(k);
+        for (int i = 0; i < k; ++i) yd[i] = make_double2(-yv[i].real(), -yv[i].imag());
+        GM_CK(cudaMemcpyAsync(to_, yd.data(), sizeof(double2) * k, cudaMemcpyHostToDevice, s));
+        k_sub_qh<<<nblk(n, 256), 256, 0, s>>>(Z_, n, k, to_, xf_, n);
+        // true FP64 residual
+        apply(op, xf_, wo_, s, kFp64);
+        k_sub<<<nblk(n, 256), 256, 0, s>>>(bf_, wo_, r_, n);
+        err = norm(r_, s, &beta);
+        if (!err.empty()) return err;
+        if (!std::isfinite(beta)) return "nonfinite:residual";
+        res->true_residual = beta / bnorm;
+        if (beta <= tol_abs) converged = true;
+    }
+    k_scatter_perm<<<nblk(n, 256), 256, 0, s>>>(xf_, perm, d_x_user, n);
     GM_CK(cudaStreamSynchronize(s));
     res->converged = converged;
     res->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();

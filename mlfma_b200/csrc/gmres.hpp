@@ -19,6 +19,8 @@ struct SolveOpts {
                          // outer loop on the FP64 residual
     double inner_tol = 0;  // refinement: inner relative target (0 = automatic)
     int adjoint = 0;       // solve A^H x = b (operator set up with ref_compat = 0)
+    int flexible = 0;      // FGMRES: FP64 outer Krylov space over inner GMRES solves
+    int inner_iters = 0;   // flexible: iterations per inner solve (0 = 20)
 };
 
 struct SolveResult {
@@ -55,6 +57,10 @@ private:
                        bool refg, int* iters, double* resid, bool* conv);
     std::string solve_refined(DeviceOp& op, const double2* d_b_user, double2* d_x_user, const SolveOpts& o,
                               SolveResult* res);
+    std::string solve_flexible(DeviceOp& op, const double2* d_b_user, double2* d_x_user, const SolveOpts& o,
+                               SolveResult* res);
+    std::string ensure_outer(int n, int ncols);
+    void release_outer();
     bool external_ = false;   // workspace not owned (static device array)
     bool adj_ = false;        // products with A^H (SolveOpts::adjoint)
     std::string ensure(int n, int ncols, int extra);
@@ -74,6 +80,11 @@ private:
     double* npartial_ = nullptr;
     double2* xo_ = nullptr;   // refinement: accumulated solution
     double2* bo_ = nullptr;   // refinement: right-hand side
+    // Flexible GMRES: outer basis V (ncols + 1), preconditioned directions Z
+    // (ncols), outer work vector, Hessenberg column and dot partials.
+    int on_ = 0, ocap_ = 0;
+    double2 *V_ = nullptr, *Z_ = nullptr, *wo_ = nullptr, *ho_ = nullptr, *to_ = nullptr, *po_ = nullptr;
+    double2 *xf_ = nullptr, *bf_ = nullptr;
 };
 
 // The fixed workspace of Gmres::use_static_workspace: makes sure it exists on

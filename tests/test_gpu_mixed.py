@@ -80,3 +80,27 @@ def test_refined_mixed_solve_meets_fp64_residual(cuda_device):
     assert rel(xmx, x64) < 10 * tol
     op64.close()
     opmx.close()
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_flexible_gmres_meets_fp64_residual(cuda_device, precision):
+    # FGMRES: FP64 outer Krylov space over inner GMRES solves on the operator's
+    # own far field (complex float on the mixed operator).  The answer must meet
+    # the tolerance on the FP64 operator and agree with the FP64 GMRES solution.
+    m = inputs.make_icosphere(3, radius=1.0)
+    op64 = MLFMA.rwg(m, PW, max_node_srcs=16, ref_compat=0, precision=0, self_terms=1).setup()
+    op = op64 if precision == 0 else MLFMA.rwg(m, PW, max_node_srcs=16, ref_compat=0, precision=1,
+                                               self_terms=1).setup()
+    b = op64.rhs()
+    tol = 1e-6
+    x64, i64 = op64.solve(b, max_iter=600, tol=tol, restart=50, ref_givens=False)
+    xf, inf = op.solve(b, max_iter=600, tol=tol, restart=30, flexible=True, inner_iters=10)
+    assert i64.converged and inf.converged
+    assert inf.refinements >= 1 and inf.iterations >= inf.refinements
+    r = rel(op64.matvec(xf), b)
+    assert r <= tol * 1.0001, r
+    assert abs(r - inf.true_residual) <= 1e-3 * r + 1e-12
+    assert rel(xf, x64) < 100 * tol
+    if op is not op64:
+        op.close()
+    op64.close()
