@@ -46,6 +46,13 @@ WORKLOAD = dict(name="rwg_sphere_r2lambda_ico5", kind="rwg", level=5, radius=2.0
                 max_node_srcs=54, quad_prec=2, digits=3, interp_order=3, over_interp=2.0)
 HERE = os.path.dirname(os.path.abspath(__file__))
 SOLVE = dict(restart=50, tol=1e-4, max_iter=3000)
+# The large benchmark: PEC sphere of radius 8 wavelengths, level-7 icosphere
+# (327,680 triangles, 491,520 RWGs), root box 16, leaves 0.25 wavelength.
+LARGE = dict(name="rwg_sphere_r8lambda_ico7", level=7, radius=8.0, root_leng=16.0, max_node_srcs=54, quad_prec=2,
+             digits=3, interp_order=3, over_interp=2.0)
+LARGE_SOLVE = dict(restart=50, tol=1e-4, max_iter=6000)
+LARGE_FLEX = dict(restart=40, inner_iters=25)  # flexible GMRES: outer steps per cycle, inner iterations
+LARGE_NRHS = 16
 NRHS = 64
 NPROB = 32
 DENSE_ROWS = 64
@@ -450,6 +457,155 @@ def measure_problems(torch, dev, args) -> dict:
             "speedup": ms_seq / ms_batch, "problem_products_per_s": NPROB * 1000.0 / ms_batch}
 
 
+def measure_large(torch, dev, args) -> dict:
+    """The 8-wavelength sphere (491,520 RWGs, 7 levels) on the EFIE with self
+    terms: products (FP64 and mixed), the FP64 GMRES(50) solve to 1e-4, the
+    mixed solves (iterative refinement; flexible GMRES) and the mixed batched
+    solve of LARGE_NRHS plane waves, each to 1e-4 on the FP64 residual; far
+    field of every solution against the FP64 solution on 360 phi-cut angles."""
+    from mlfma_b200 import MLFMA, default_config, inputs
+    t0 = time.perf_counter()
+    mesh = inputs.make_icosphere(LARGE["level"], radius=LARGE["radius"])
+    pw = inputs.PlaneWave(amplitude=1.0, pol=(1.0, 0.0, 0.0), khat=(0.0, 0.0, -1.0), wavenum=2.0 * np.pi)
+    mesh_s = time.perf_counter() - t0
+
+    def cfg(precision, max_rhs=1):
+        return default_config(quad_prec=LARGE["quad_prec"], digits=LARGE["digits"],
+                              interp_order=LARGE["interp_order"], over_interp=LARGE["over_interp"],
+                              root_leng=LARGE["root_leng"], max_node_srcs=LARGE["max_node_srcs"], device=dev.index,
+                              precision=precision, self_terms=1, ref_compat=0, max_rhs=max_rhs)
+
+    def products(op, steps):
+        x = torch.randn(op.n, dtype=torch.complex128, device=dev)
+        y = torch.zeros_like(x)
+        stream = torch.cuda.ExternalStream(op.stream(), device=dev)
+        for _ in range(3):
+            op.matvec_device(x.data_ptr(), y.data_ptr(), False, stream.cuda_stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            op.matvec_device(x.data_ptr(), y.data_ptr(), False, stream.cuda_stream)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        return e0.elapsed_time(e1) / steps
+
+    steps = max(5, min(args.steps, 20))
+    out = {"workload": f"{LARGE['name']}: PEC sphere r = 8 wavelengths, icosphere level 7, root box 16, "
+                       f"boxes split above {LARGE['max_node_srcs']} RWGs, EFIE with self terms",
+           "mesh_s": mesh_s}
+    rows = np.random.default_rng(91).choice(491520, 32, replace=False)
+    phi = None
+    # ---- FP64
+    t0 = time.perf_counter()
+    op = MLFMA.rwg(mesh, pw, config=cfg(0)).setup()
+    out["unknowns"], out["levels"] = op.n, op.stats()["max_level"] + 1
+    setup64 = time.perf_counter() - t0
+    op.autotune(1, reps=3)
+    ms64 = products(op, steps)
+    st64 = op.stage_times()
+    tr64 = op.traffic()
+    b = op.rhs()
+    xr = np.random.default_rng(92).standard_normal(op.n) + 1j * np.random.default_rng(93).standard_normal(op.n)
+    yr = op.matvec(xr)
+    dense_err = float(np.linalg.norm(yr[rows] - op.dense_rows(rows, xr)) / np.linalg.norm(op.dense_rows(rows, xr)))
+    op.solve(b, max_iter=3, tol=1e-12, restart=LARGE_SOLVE["restart"], ref_givens=False)  # workspace, graphs
+    t0 = time.perf_counter()
+    x64, i64 = op.solve(b, max_iter=LARGE_SOLVE["max_iter"], tol=LARGE_SOLVE["tol"],
+                        restart=LARGE_SOLVE["restart"], ref_givens=False)
+    s64 = time.perf_counter() - t0
+    phi = op.phi_cut(360)
+    far64 = op.farfield(x64, phi)
+    op.close()
+    out["fp64"] = {"setup_s": setup64, "ms_per_product": ms64, "matvecs_per_s": 1000.0 / ms64, "stage_ms": st64,
+                   "matvec_alg_bytes": tr64["total"], "roofline": roofline(st64, tr64, "", LARGE["name"]),
+                   "dense_rel_err_32_rows": dense_err,
+                   "solve": {"seconds": s64, "iterations": i64.iterations, "true_residual_fp64": i64.true_residual,
+                             "converged": i64.converged,
+                             "method": f"GMRES({LARGE_SOLVE['restart']}) to {LARGE_SOLVE['tol']:g}, FP64"}}
+
+    def farerr(x):
+        return float(np.linalg.norm(op.farfield(x, phi) - far64) / np.linalg.norm(far64))
+
+    # ---- mixed precision, one right-hand side
+    t0 = time.perf_counter()
+    op = MLFMA.rwg(mesh, pw, config=cfg(1)).setup()
+    setupmx = time.perf_counter() - t0
+    tune = op.autotune(1, reps=3)
+    msmx = products(op, steps)
+    stmx = op.stage_times()
+    trmx = op.traffic()
+    op.solve(b, max_iter=3, tol=1e-12, restart=LARGE_SOLVE["restart"], ref_givens=False, refine=True)
+    t0 = time.perf_counter()
+    xir, iir = op.solve(b, max_iter=LARGE_SOLVE["max_iter"], tol=LARGE_SOLVE["tol"],
+                        restart=LARGE_SOLVE["restart"], ref_givens=False, refine=True)
+    sir = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    xfl, ifl = op.solve(b, max_iter=LARGE_SOLVE["max_iter"], tol=LARGE_SOLVE["tol"], restart=LARGE_FLEX["restart"],
+                        flexible=True, inner_iters=LARGE_FLEX["inner_iters"])
+    sfl = time.perf_counter() - t0
+    out["mixed"] = {"setup_s": setupmx, "ms_per_product": msmx, "matvecs_per_s": 1000.0 / msmx,
+                    "speedup_vs_fp64": ms64 / msmx, "stage_ms": stmx, "matvec_alg_bytes": trmx["total"],
+                    "interp_path": tune["interp_path"],
+                    "solve_refined": {"seconds": sir, "iterations": iir.iterations,
+                                      "refinements": iir.refinements, "true_residual_fp64": iir.true_residual,
+                                      "converged": iir.converged, "speedup_vs_fp64": s64 / sir,
+                                      "farfield_rel_err_vs_fp64": farerr(xir),
+                                      "method": f"iterative refinement, inner GMRES({LARGE_SOLVE['restart']}) "
+                                                "on the complex-float far field, FP64 residual"},
+                    "solve_flexible": {"seconds": sfl, "inner_iterations": ifl.iterations,
+                                       "outer_iterations": ifl.refinements, "true_residual_fp64": ifl.true_residual,
+                                       "converged": ifl.converged, "speedup_vs_fp64": s64 / sfl,
+                                       "farfield_rel_err_vs_fp64": farerr(xfl),
+                                       "method": f"FGMRES({LARGE_FLEX['restart']}) in FP64 over inner GMRES of "
+                                                 f"{LARGE_FLEX['inner_iters']} iterations on the complex-float "
+                                                 "far field"}}
+    op.close()
+    # ---- mixed precision, many right-hand sides (the benchmark's plane wave first)
+    if not args.no_batched:
+        t0 = time.perf_counter()
+        op = MLFMA.rwg(mesh, pw, config=cfg(1, LARGE_NRHS)).setup()
+        setupb = time.perf_counter() - t0
+        op.autotune(1, reps=3)
+        tb = op.autotune(LARGE_NRHS, reps=2)
+        B = np.stack([b] + [op.rhs_planewave(p) for p in inputs.fibonacci_planewaves(LARGE_NRHS - 1)])
+        X = torch.from_numpy(B).to(dev)
+        Y = torch.zeros_like(X)
+        stream = torch.cuda.ExternalStream(op.stream(), device=dev)
+        for _ in range(2):
+            op.matvec_multi_device(LARGE_NRHS, X.data_ptr(), Y.data_ptr(), False, stream.cuda_stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(3):
+            op.matvec_multi_device(LARGE_NRHS, X.data_ptr(), Y.data_ptr(), False, stream.cuda_stream)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        msb = e0.elapsed_time(e1) / 3
+        stb = op.stage_times_multi(LARGE_NRHS)
+        op.solve_multi(B, max_iter=2, tol=1e-12, restart=LARGE_SOLVE["restart"], refine=True)
+        t0 = time.perf_counter()
+        Xs, infos = op.solve_multi(B, max_iter=LARGE_SOLVE["max_iter"], tol=LARGE_SOLVE["tol"],
+                                   restart=LARGE_SOLVE["restart"], refine=True)
+        sb = time.perf_counter() - t0
+        out["batched"] = {"nrhs": LARGE_NRHS, "setup_s": setupb, "ms_per_product": msb,
+                          "us_per_rhs": msb * 1000.0 / LARGE_NRHS, "stage_ms": stb,
+                          "matvec_speedup_per_rhs_vs_fp64": ms64 * LARGE_NRHS / msb,
+                          "interp_path": tb["interp_path"],
+                          "solve": {"seconds": sb, "seconds_per_rhs": sb / LARGE_NRHS,
+                                    "iterations_max": max(i.iterations for i in infos),
+                                    "true_residual_fp64_max": max(i.true_residual for i in infos),
+                                    "converged": all(i.converged for i in infos),
+                                    "speedup_per_rhs_vs_fp64_single": s64 * LARGE_NRHS / sb,
+                                    "farfield_rel_err_vs_fp64_rhs0": farerr(Xs[0]),
+                                    "method": f"{LARGE_NRHS} simultaneous GMRES({LARGE_SOLVE['restart']}) with "
+                                              "iterative refinement, complex-float far field, FP64 residual"}}
+        op.close()
+    best = max([out["mixed"]["solve_refined"]["speedup_vs_fp64"], out["mixed"]["solve_flexible"]["speedup_vs_fp64"]] +
+               ([out["batched"]["solve"]["speedup_per_rhs_vs_fp64_single"]] if "batched" in out else []))
+    out["target"] = {"what": "mixed/batched solve to 1e-4 at least 4x faster than the FP64 GPU solve, far-field "
+                             "error below 1e-3", "best_speedup": best, "met": bool(best >= 4.0)}
+    return out
+
+
 def solve_summary(sv):
     return {"seconds": sv["seconds"], "iterations": sv["iterations"], "true_residual_fp64": sv["true_residual"],
             "dense_residual": sv["dense_residual"], "converged": sv["converged"], "refinements": sv["refinements"],
@@ -457,7 +613,7 @@ def solve_summary(sv):
             "operator": "EFIE with self terms (self_terms=1, ref_compat=0)"}
 
 
-def roofline(avg, traffic, precision_name):
+def roofline(avg, traffic, precision_name, workload=None):
     # The near field's tile kernel is the longest single kernel of a product
     # (launch list in profiles/); the stage time also holds its per-target sum.
     dom = "near_field"
@@ -473,7 +629,7 @@ def roofline(avg, traffic, precision_name):
     ncu_traffic = None
     try:
         with open(os.path.join(HERE, "profiles", "traffic.json")) as f:
-            ncu_traffic = json.load(f).get(WORKLOAD["name"] + precision_name, {}).get(dom)
+            ncu_traffic = json.load(f).get((workload or WORKLOAD["name"]) + precision_name, {}).get(dom)
     except (OSError, ValueError):
         pass
     return {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
@@ -491,6 +647,7 @@ def main():
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-solve", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--no-large", action="store_true", help="skip the 8-wavelength sphere (491,520 unknowns)")
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--save-y", default=None, help="reference arm: save its last product here (.npz)")
     args = ap.parse_args()
@@ -541,6 +698,7 @@ def main():
     if not args.no_batched:
         bat = {p: measure_batched(torch, dev, args, p) for p in ((0, 1) if not args.no_mixed else (0,))}
     probs = None if args.no_batched else measure_problems(torch, dev, args)
+    large = None if args.no_large else measure_large(torch, dev, args)
 
     if rank == 0:
         cpu = None
@@ -606,6 +764,8 @@ def main():
             line["batched"] = batched_summary(bat, r64)
         if probs is not None:
             line["problems"] = probs
+        if large is not None:
+            line["large"] = large
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()

@@ -137,6 +137,28 @@ int mlfma_create_dipoles(const mlfma_config* cfg, const mlfma_planewave* pw, int
 int mlfma_create_rwg(const mlfma_config* cfg, const mlfma_planewave* pw, int nv, const double* verts,
                      int nf, const int* faces, int ne, const int* rwgs, mlfma_handle* out);
 
+/* The reference's text formats (no GPU needed).  Errors: MLFMA_ERR_ARG with
+ * "Unable to find file" or "Unable to parse line" in mlfma_last_error(), the
+ * reference's messages.  Each line is parsed as the reference parses it: the
+ * values it needs are read and the rest of the line ignored; a line without
+ * them (a blank line included) is an error.
+ * Plane wave: the first line holds amplitude, pol (3), khat (3), wavenumber
+ * (importPlaneWave, src/fileio.h:8-27). */
+int mlfma_read_planewave(const char* path, mlfma_planewave* pw);
+/* Dipoles: one line per dipole, position (3) and moment (3) (importDipoles,
+ * src/fileio.h:110-131), then as mlfma_create_dipoles. */
+int mlfma_create_dipoles_from_file(const mlfma_config* cfg, const mlfma_planewave* pw, const char* path,
+                                   mlfma_handle* out);
+/* RWG mesh: vertices (x y z per line), faces (three 0-based vertex indices),
+ * rwgs (v0 v1 t+ t-) (importVertices, importTriangles, importRWG,
+ * src/fileio.h:134-202), then as mlfma_create_rwg. */
+int mlfma_create_rwg_from_files(const mlfma_config* cfg, const mlfma_planewave* pw, const char* vertices_path,
+                                const char* faces_path, const char* rwgs_path, mlfma_handle* out);
+/* Solution file: one complex current per line as "(re,im)", 15 significant
+ * digits, scientific (Solver::printSols, src/solver.cpp:149-165; the caller
+ * chooses the path).  x: n interleaved complex values. */
+int mlfma_write_solution(const char* path, int n, const double* x);
+
 /* Upload to the GPU and assemble radiation patterns and near-field blocks
  * there (Leaf::buildNearRads, src/fmm/leaf.cpp:108-180; root->resizeCoeffs;
  * Leaf::buildRadPats, src/fmm/leaf.cpp:185-207). */

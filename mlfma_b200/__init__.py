@@ -47,6 +47,19 @@ def _pw(p: inputs.PlaneWave) -> PlaneWaveC:
     return c
 
 
+def read_planewave(path: str) -> inputs.PlaneWave:
+    """The plane wave of the reference's text format (mlfma_read_planewave)."""
+    c = PlaneWaveC()
+    check(lib().mlfma_read_planewave(str(path).encode(), ctypes.byref(c)))
+    return inputs.PlaneWave(amplitude=c.amplitude, pol=tuple(c.pol), khat=tuple(c.khat), wavenum=c.wavenum)
+
+
+def write_solution(path: str, x) -> None:
+    """Currents in the reference's solution format (mlfma_write_solution)."""
+    a = np.ascontiguousarray(np.asarray(x, dtype=np.complex128).reshape(-1))
+    check(lib().mlfma_write_solution(str(path).encode(), a.shape[0], a.view(np.float64).ctypes.data_as(_dp)))
+
+
 def _cvec(x, n):
     a = np.ascontiguousarray(np.asarray(x, dtype=np.complex128).reshape(-1))
     if a.shape[0] != n:
@@ -97,6 +110,31 @@ class MLFMA:
                                      F.shape[0], F.ctypes.data_as(_ip), E.shape[0], E.ctypes.data_as(_ip),
                                      ctypes.byref(h)))
         return cls(h, m.n, "rwg")
+
+    @classmethod
+    def dipoles_from_file(cls, path: str, pw: inputs.PlaneWave, config: Config | None = None, **kw) -> "MLFMA":
+        """Dipoles from the reference's text format (mlfma_create_dipoles_from_file)."""
+        cfg = config or default_config(**kw)
+        h = ctypes.c_void_p()
+        p = _pw(pw)
+        check(lib().mlfma_create_dipoles_from_file(ctypes.byref(cfg), ctypes.byref(p), str(path).encode(),
+                                                   ctypes.byref(h)))
+        n = ctypes.c_int()
+        check(lib().mlfma_num_unknowns(h, ctypes.byref(n)))
+        return cls(h, n.value, "dipole")
+
+    @classmethod
+    def rwg_from_files(cls, vertices: str, faces: str, rwgs: str, pw: inputs.PlaneWave,
+                       config: Config | None = None, **kw) -> "MLFMA":
+        """RWG mesh from the reference's text files (mlfma_create_rwg_from_files)."""
+        cfg = config or default_config(**kw)
+        h = ctypes.c_void_p()
+        p = _pw(pw)
+        check(lib().mlfma_create_rwg_from_files(ctypes.byref(cfg), ctypes.byref(p), str(vertices).encode(),
+                                                str(faces).encode(), str(rwgs).encode(), ctypes.byref(h)))
+        n = ctypes.c_int()
+        check(lib().mlfma_num_unknowns(h, ctypes.byref(n)))
+        return cls(h, n.value, "rwg")
 
     def setup(self) -> "MLFMA":
         check(lib().mlfma_setup(self._h))

@@ -110,6 +110,13 @@ SIGNATURES = {
                                                 ctypes.POINTER(SolveInfo)]),
     "mlfma_autotune": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(Tuning)]),
     "mlfma_set_interp_path": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "mlfma_read_planewave": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(PlaneWaveC)]),
+    "mlfma_create_dipoles_from_file": (ctypes.c_int, [ctypes.POINTER(Config), ctypes.POINTER(PlaneWaveC),
+                                                      ctypes.c_char_p, ctypes.POINTER(ctypes.c_void_p)]),
+    "mlfma_create_rwg_from_files": (ctypes.c_int, [ctypes.POINTER(Config), ctypes.POINTER(PlaneWaveC),
+                                                   ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p,
+                                                   ctypes.POINTER(ctypes.c_void_p)]),
+    "mlfma_write_solution": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, _dp]),
     "mlfma_get_interp_path": (ctypes.c_int, [ctypes.c_void_p, _ip]),
     "mlfma_batch_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_void_p),
                                           ctypes.POINTER(ctypes.c_void_p)]),

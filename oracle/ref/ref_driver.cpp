@@ -173,6 +173,42 @@ int ref_create_rwg(const double* verts, int nv, const int* faces, int nf, const 
     }
 }
 
+// From the reference's text files, read by its own importers
+// (importPlaneWave, src/fileio.h:8-27; importDipoles, fileio.h:110-131;
+// importRWG, fileio.h:174-202).  Returns 1 when an importer throws.
+int ref_create_dipoles_file(const char* path, const char* pw_path, int digits, int interp_order,
+                            double over_interp, double root_leng, int max_node_srcs) {
+    QuietCout q;
+    try {
+        reset_statics();
+        g.einc = importPlaneWave(pw_path);
+        g.srcs = importDipoles(path, g.einc);
+        build_operator(make_config(0, digits, interp_order, over_interp, root_leng, max_node_srcs,
+                                   static_cast<int>(g.srcs.size())));
+        return 0;
+    } catch (const std::exception& e) {
+        std::cerr << "ref_create_dipoles_file: " << e.what() << '\n';
+        return 1;
+    }
+}
+
+int ref_create_rwg_files(const char* vpath, const char* fpath, const char* rpath, const char* pw_path,
+                         int quad_prec, int digits, int interp_order, double over_interp, double root_leng,
+                         int max_node_srcs) {
+    QuietCout q;
+    try {
+        reset_statics();
+        g.einc = importPlaneWave(pw_path);
+        g.srcs = importRWG(vpath, fpath, rpath, static_cast<Precision>(quad_prec), g.einc);
+        build_operator(make_config(quad_prec, digits, interp_order, over_interp, root_leng, max_node_srcs,
+                                   static_cast<int>(g.srcs.size())));
+        return 0;
+    } catch (const std::exception& e) {
+        std::cerr << "ref_create_rwg_files: " << e.what() << '\n';
+        return 1;
+    }
+}
+
 int ref_num_srcs() { return static_cast<int>(g.srcs.size()); }
 
 // [numNodes, numLeaves, maxLevel]

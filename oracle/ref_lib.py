@@ -46,6 +46,11 @@ def lib():
         L.ref_leaf.argtypes = [ctypes.c_int, _ip, _dp, _ip, _ip]
         L.ref_list_stats.argtypes = [_lp]
         L.ref_entry.argtypes = [ctypes.c_int, ctypes.c_int, _dp]
+        L.ref_create_dipoles_file.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_int,
+                                              ctypes.c_double, ctypes.c_double, ctypes.c_int]
+        L.ref_create_rwg_files.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p,
+                                           ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                           ctypes.c_double, ctypes.c_int]
         _lib = L
     return _lib
 
@@ -84,6 +89,28 @@ class RefProblem:
             raise RuntimeError("reference setup failed")
         self.n = L.ref_num_srcs()
         self.order = interp_order
+
+    @classmethod
+    def from_files(cls, kind, paths, pw_path, digits=3, interp_order=3, over_interp=2.0, root_leng=4.0,
+                   max_node_srcs=64, quad_prec=2):
+        """The reference's own importers on its text files (src/fileio.h):
+        paths = dipole file, or (vertices, faces, rwgs).  Raises when an
+        importer throws."""
+        L = lib()
+        self = cls.__new__(cls)
+        enc = lambda p: str(p).encode()  # noqa: E731
+        if kind == "dipole":
+            rc = L.ref_create_dipoles_file(enc(paths), enc(pw_path), digits, interp_order, over_interp, root_leng,
+                                           max_node_srcs)
+        else:
+            v, f, r = paths
+            rc = L.ref_create_rwg_files(enc(v), enc(f), enc(r), enc(pw_path), quad_prec, digits, interp_order,
+                                        over_interp, root_leng, max_node_srcs)
+        if rc != 0:
+            raise RuntimeError("reference importer failed")
+        self.n = L.ref_num_srcs()
+        self.order = interp_order
+        return self
 
     def info(self):
         out = np.zeros(3, dtype=np.int32)
