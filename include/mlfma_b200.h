@@ -212,6 +212,14 @@ int mlfma_check_bounded_wait(int device, int* timed_out);
  * interleaved complex.  No counterpart in the reference. */
 int mlfma_dense_rows(mlfma_handle h, int nrows, const int* rows, const double* x, double* y);
 
+/* The same operator's entries themselves: d_out[i * ld + j] = A[rows[i]][j]
+ * (caller order, j < n, ld >= n) in a DEVICE buffer, every interaction
+ * evaluated directly in FP64 (diagonal loads not included).  A dense reference
+ * for the adjoint and the solution (all rows of a 30,720-unknown operator are
+ * 15 GB).  Returns when written.  No counterpart in the reference (its direct
+ * path, src/mlfma.cpp:84-107, applies the entries without keeping them). */
+int mlfma_dense_block_device(mlfma_handle h, int nrows, const int* rows, void* d_out, long long ld);
+
 /* GMRES that allocates no device memory.  No counterpart in the reference.
  * mlfma_gmres allocates its Krylov basis with cudaMalloc on first use; a
  * caller that cannot allocate device memory during a solve (a fixed memory

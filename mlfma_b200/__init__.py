@@ -372,6 +372,13 @@ class MLFMA:
                                      out.view(np.float64).ctypes.data_as(_dp)))
         return out
 
+    def dense_block_device(self, rows, out_ptr: int, ld: int | None = None) -> None:
+        """Rows of the operator's matrix (every interaction direct, FP64) into
+        device memory at out_ptr: entry (i, j) at out_ptr + 16 (i ld + j)."""
+        r = np.ascontiguousarray(np.asarray(rows, dtype=np.int32).reshape(-1))
+        check(lib().mlfma_dense_block_device(self._h, r.shape[0], r.ctypes.data_as(_ip), ctypes.c_void_p(out_ptr),
+                                             int(ld if ld is not None else self.n)))
+
     @staticmethod
     def phi_cut(n: int = 360, theta: float = np.pi / 2) -> np.ndarray:
         """Unit directions of a phi cut at fixed theta (n equally spaced phi)."""

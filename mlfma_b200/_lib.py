@@ -117,6 +117,8 @@ SIGNATURES = {
                                                    ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p,
                                                    ctypes.POINTER(ctypes.c_void_p)]),
     "mlfma_write_solution": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, _dp]),
+    "mlfma_dense_block_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _ip, ctypes.c_void_p,
+                                                ctypes.c_longlong]),
     "mlfma_get_interp_path": (ctypes.c_int, [ctypes.c_void_p, _ip]),
     "mlfma_batch_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_void_p),
                                           ctypes.POINTER(ctypes.c_void_p)]),

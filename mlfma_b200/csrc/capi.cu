@@ -27,13 +27,16 @@ struct mlfma_op_s {
     double2* d_ym = nullptr;
     double2* d_x = nullptr;  // staging for host-buffer calls
     double2* d_y = nullptr;
+    void* d_stage = nullptr;  // small per-call inputs and outputs (directions, rows, far fields); grows only
+    size_t stage_bytes = 0;
     ~mlfma_op_s() {
-        if (d_x || d_y || d_xm || d_ym) {
+        if (d_x || d_y || d_xm || d_ym || d_stage) {
             cudaSetDevice(device);
             if (d_x) cudaFree(d_x);
             if (d_y) cudaFree(d_y);
             if (d_xm) cudaFree(d_xm);
             if (d_ym) cudaFree(d_ym);
+            if (d_stage) cudaFree(d_stage);
         }
     }
 };
@@ -52,6 +55,22 @@ int from_msg(const std::string& msg) {
     if (msg.rfind("nonfinite", 0) == 0) return fail(MLFMA_ERR_NONFINITE, msg);
     if (msg.rfind("arg:", 0) == 0) return fail(MLFMA_ERR_ARG, msg);
     return fail(MLFMA_ERR_CUDA, msg);
+}
+
+// The handle's staging buffer, at least `bytes` long: reallocated (after the
+// handle's stream has drained) only when a call needs more than any before.
+int ensure_stage(mlfma_handle h, size_t bytes) {
+    if (bytes <= h->stage_bytes) return MLFMA_OK;
+    bytes = std::max<size_t>(bytes, 2 * h->stage_bytes);
+    if (h->d_stage) {
+        cudaStreamSynchronize(h->dev->stream());
+        cudaFree(h->d_stage);
+        h->d_stage = nullptr;
+        h->stage_bytes = 0;
+    }
+    if (cudaMalloc(&h->d_stage, bytes) != cudaSuccess) return fail(MLFMA_ERR_CUDA, "cudaMalloc failed");
+    h->stage_bytes = bytes;
+    return MLFMA_OK;
 }
 
 mlfma::Config to_cfg(const mlfma_config* c) {
@@ -293,13 +312,11 @@ int mlfma_dense_rows(mlfma_handle h, int nrows, const int* rows, const double* x
     }
     if (cudaSetDevice(h->device) != cudaSuccess) return fail(MLFMA_ERR_CUDA, "cudaSetDevice failed");
     cudaStream_t s = h->dev->stream();
-    int* d_rows = nullptr;
-    double2* d_y = nullptr;
-    if (cudaMalloc(&d_rows, sizeof(int) * nrows) != cudaSuccess ||
-        cudaMalloc(&d_y, sizeof(double2) * nrows) != cudaSuccess) {
-        cudaFree(d_rows);
-        return fail(MLFMA_ERR_CUDA, "cudaMalloc failed");
-    }
+    const size_t yb = (sizeof(double2) * nrows + 255) & ~static_cast<size_t>(255);
+    const int code = ensure_stage(h, yb + sizeof(int) * nrows);
+    if (code != MLFMA_OK) return code;
+    double2* d_y = static_cast<double2*>(h->d_stage);
+    int* d_rows = reinterpret_cast<int*>(static_cast<char*>(h->d_stage) + yb);
     std::string e;
     if (cudaMemcpyAsync(d_rows, tree.data(), sizeof(int) * nrows, cudaMemcpyHostToDevice, s) != cudaSuccess ||
         cudaMemcpyAsync(h->d_x, x, sizeof(double2) * n, cudaMemcpyHostToDevice, s) != cudaSuccess)
@@ -308,9 +325,33 @@ int mlfma_dense_rows(mlfma_handle h, int nrows, const int* rows, const double* x
     if (e.empty() && (cudaMemcpyAsync(y, d_y, sizeof(double2) * nrows, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
                       cudaStreamSynchronize(s) != cudaSuccess))
         e = "copy of y failed";
-    cudaFree(d_rows);
-    cudaFree(d_y);
     if (!e.empty()) return fail(MLFMA_ERR_CUDA, e);
+    return MLFMA_OK;
+}
+
+int mlfma_dense_block_device(mlfma_handle h, int nrows, const int* rows, void* d_out, long long ld) {
+    if (!h || nrows < 0 || (nrows > 0 && (!rows || !d_out))) return fail(MLFMA_ERR_ARG, "null argument");
+    if (!ready(h)) return fail(MLFMA_ERR_STATE, "mlfma_setup has not run");
+    const int n = h->plan.n;
+    if (ld < n) return fail(MLFMA_ERR_ARG, "ld must be at least n");
+    if (nrows == 0) return MLFMA_OK;
+    std::vector<int> slot(n), tree(nrows);
+    for (int t = 0; t < n; ++t) slot[h->plan.perm[t]] = t;
+    for (int i = 0; i < nrows; ++i) {
+        if (rows[i] < 0 || rows[i] >= n) return fail(MLFMA_ERR_ARG, "row index out of range");
+        tree[i] = slot[rows[i]];
+    }
+    if (cudaSetDevice(h->device) != cudaSuccess) return fail(MLFMA_ERR_CUDA, "cudaSetDevice failed");
+    cudaStream_t s = h->dev->stream();
+    const int code = ensure_stage(h, sizeof(int) * nrows);
+    if (code != MLFMA_OK) return code;
+    int* d_rows = static_cast<int*>(h->d_stage);
+    if (cudaMemcpyAsync(d_rows, tree.data(), sizeof(int) * nrows, cudaMemcpyHostToDevice, s) != cudaSuccess)
+        return fail(MLFMA_ERR_CUDA, "copy of rows failed");
+    std::string e = h->dev->dense_block(d_rows, nrows, static_cast<double2*>(d_out), ld, s);
+    if (!e.empty()) return fail(MLFMA_ERR_CUDA, e);
+    const cudaError_t ce = cudaStreamSynchronize(s);
+    if (ce != cudaSuccess) return fail(MLFMA_ERR_CUDA, cudaGetErrorString(ce));
     return MLFMA_OK;
 }
 
@@ -320,13 +361,11 @@ int mlfma_farfield(mlfma_handle h, const double* x, int ndir, const double* khat
     if (ndir == 0) return MLFMA_OK;
     if (cudaSetDevice(h->device) != cudaSuccess) return fail(MLFMA_ERR_CUDA, "cudaSetDevice failed");
     cudaStream_t s = h->dev->stream();
-    double* d_k = nullptr;
-    double2* d_o = nullptr;
-    if (cudaMalloc(&d_k, sizeof(double) * 3 * ndir) != cudaSuccess ||
-        cudaMalloc(&d_o, sizeof(double2) * 3 * ndir) != cudaSuccess) {
-        cudaFree(d_k);
-        return fail(MLFMA_ERR_CUDA, "cudaMalloc failed");
-    }
+    const size_t ob = (sizeof(double2) * 3 * ndir + 255) & ~static_cast<size_t>(255);
+    const int code = ensure_stage(h, ob + sizeof(double) * 3 * ndir);
+    if (code != MLFMA_OK) return code;
+    double2* d_o = static_cast<double2*>(h->d_stage);
+    double* d_k = reinterpret_cast<double*>(static_cast<char*>(h->d_stage) + ob);
     std::string e;
     if (cudaMemcpyAsync(h->d_x, x, sizeof(double2) * h->plan.n, cudaMemcpyHostToDevice, s) != cudaSuccess ||
         cudaMemcpyAsync(d_k, khat, sizeof(double) * 3 * ndir, cudaMemcpyHostToDevice, s) != cudaSuccess)
@@ -335,8 +374,6 @@ int mlfma_farfield(mlfma_handle h, const double* x, int ndir, const double* khat
     if (e.empty() && (cudaMemcpyAsync(out, d_o, sizeof(double2) * 3 * ndir, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
                       cudaStreamSynchronize(s) != cudaSuccess))
         e = "copy of the far field failed";
-    cudaFree(d_k);
-    cudaFree(d_o);
     if (!e.empty()) return fail(MLFMA_ERR_CUDA, e);
     return MLFMA_OK;
 }
@@ -586,24 +623,22 @@ int mlfma_farfield_adjoint(mlfma_handle h, int ndir, const double* khat, const d
     if (!ready(h)) return fail(MLFMA_ERR_STATE, "mlfma_setup has not run");
     if (cudaSetDevice(h->device) != cudaSuccess) return fail(MLFMA_ERR_CUDA, "cudaSetDevice failed");
     cudaStream_t s = h->dev->stream();
-    double* d_k = nullptr;
-    double2* d_F = nullptr;
     const int nd = ndir > 0 ? ndir : 1;
-    if (cudaMalloc(&d_k, sizeof(double) * 3 * nd) != cudaSuccess ||
-        cudaMalloc(&d_F, sizeof(double2) * 3 * nd) != cudaSuccess) {
-        cudaFree(d_k);
-        return fail(MLFMA_ERR_CUDA, "cudaMalloc failed");
-    }
+    // F, its projection (k_project), the directions
+    const size_t fb = (sizeof(double2) * 3 * nd + 255) & ~static_cast<size_t>(255);
+    const int code = ensure_stage(h, 2 * fb + sizeof(double) * 3 * nd);
+    if (code != MLFMA_OK) return code;
+    double2* d_F = static_cast<double2*>(h->d_stage);
+    double2* d_P = reinterpret_cast<double2*>(static_cast<char*>(h->d_stage) + fb);
+    double* d_k = reinterpret_cast<double*>(static_cast<char*>(h->d_stage) + 2 * fb);
     std::string e;
     if (ndir > 0 && (cudaMemcpyAsync(d_k, khat, sizeof(double) * 3 * ndir, cudaMemcpyHostToDevice, s) != cudaSuccess ||
                      cudaMemcpyAsync(d_F, F, sizeof(double2) * 3 * ndir, cudaMemcpyHostToDevice, s) != cudaSuccess))
         e = "copy failed";
-    if (e.empty()) e = h->dev->farfield_adjoint(d_F, ndir, d_k, h->d_y, s);
+    if (e.empty()) e = h->dev->farfield_adjoint(d_F, ndir, d_k, h->d_y, s, d_P);
     if (e.empty() && (cudaMemcpyAsync(g, h->d_y, sizeof(double2) * h->plan.n, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
                       cudaStreamSynchronize(s) != cudaSuccess))
         e = "copy of g failed";
-    cudaFree(d_k);
-    cudaFree(d_F);
     if (!e.empty()) return fail(MLFMA_ERR_CUDA, e);
     return MLFMA_OK;
 }

@@ -238,8 +238,13 @@ public:
     std::string farfield(const double2* cur, int ndir, const double* khat, double2* out, cudaStream_t s);
     // y[i] = (A x)[row i] with every interaction evaluated directly (rows: tree slots).
     std::string dense_rows(const int* rows, int nrows, const double2* x, double2* y, cudaStream_t s);
-    // Its adjoint: g (caller order, device, n) = M^H F for F (device, ndir x 3).
-    std::string farfield_adjoint(const double2* F, int ndir, const double* khat, double2* g, cudaStream_t s);
+    // Its adjoint: g (caller order, device, n) = M^H F for F (device, ndir x 3);
+    // work: ndir x 3 complex (device).
+    std::string farfield_adjoint(const double2* F, int ndir, const double* khat, double2* g, cudaStream_t s,
+                                 double2* work);
+    // out[i * ld + j] = A[row i][column j] (caller order), every interaction
+    // evaluated directly (rows: tree slots).
+    std::string dense_block(const int* rows, int nrows, double2* out, long long ld, cudaStream_t s);
 
     int n() const { return n_; }
     int precision() const { return precision_; }

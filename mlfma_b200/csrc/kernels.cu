@@ -958,18 +958,26 @@ std::string DeviceOp::dense_rows(const int* rows, int nrows, const double2* x, d
     return {};
 }
 
-std::string DeviceOp::farfield_adjoint(const double2* F, int ndir, const double* khat, double2* g, cudaStream_t s) {
+std::string DeviceOp::farfield_adjoint(const double2* F, int ndir, const double* khat, double2* g, cudaStream_t s,
+                                       double2* PF) {
     if (!ready_) return "operator not set up";
     MLFMA_CK(cudaSetDevice(device_));
     if (ndir <= 0) {
         MLFMA_CK(cudaMemsetAsync(g, 0, sizeof(double2) * n_, s));
         return {};
     }
-    double2* PF = nullptr;
-    MLFMA_CK(cudaMallocAsync(&PF, sizeof(double2) * 3 * ndir, s));
     k_project<<<blocks_for(ndir, 128), 128, 0, s>>>(khat, F, ndir, PF);
     k_farfield_adj<<<blocks_for(n_, 128), 128, 0, s>>>(src_, perm_, n_, khat, PF, ndir, ck_, g);
-    MLFMA_CK(cudaFreeAsync(PF, s));
+    MLFMA_CK(cudaGetLastError());
+    return {};
+}
+
+std::string DeviceOp::dense_block(const int* rows, int nrows, double2* out, long long ld, cudaStream_t s) {
+    if (!ready_) return "operator not set up";
+    if (nrows <= 0) return {};
+    MLFMA_CK(cudaSetDevice(device_));
+    const dim3 grid(blocks_for(n_, kDenseThreads), nrows);
+    k_dense_block<<<grid, kDenseThreads, 0, s>>>(src_, rows, perm_, n_, ck_, out, ld);
     MLFMA_CK(cudaGetLastError());
     return {};
 }
@@ -1280,10 +1288,15 @@ std::string DeviceOp::time_stages_multi(int nr, StageTimes* out) {
 namespace {
 
 // The shared-memory limit is a property of the kernel, shared by every
-// operator: set it to the device's opt-in maximum.
+// operator: set it to the device's opt-in maximum less the kernel's static
+// shared memory; *dyn_max receives that limit.
 template <int KIND>
-cudaError_t tc_prepare(int smem) {
-    return cudaFuncSetAttribute(k_tc_pass<KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+cudaError_t tc_prepare(int smem, int* dyn_max) {
+    cudaFuncAttributes fa{};
+    cudaError_t e = cudaFuncGetAttributes(&fa, k_tc_pass<KIND>);
+    if (e != cudaSuccess) return e;
+    *dyn_max = smem - static_cast<int>(fa.sharedSizeBytes);
+    return cudaFuncSetAttribute(k_tc_pass<KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize, *dyn_max);
 }
 
 }  // namespace
@@ -1332,10 +1345,14 @@ std::string DeviceOp::setup_tc(const Plan& plan) {
     for (int p = lmin_; p < lmax_; ++p)  // one item's intermediate must fit (chunks of at least one item)
         if (static_cast<size_t>(nth_[p]) * nph_[p + 1] * 4 * max_rhs_ > tc_scratch_floats_) return {};
     tc_scratch_ = alloc<float>(tc_scratch_floats_);
-    MLFMA_CK(tc_prepare<kTcTheta>(dev_smem));
-    MLFMA_CK(tc_prepare<kTcPhi>(dev_smem));
-    MLFMA_CK(tc_prepare<kTcPhiT>(dev_smem));
-    MLFMA_CK(tc_prepare<kTcThetaT>(dev_smem));
+    int dyn[4] = {};
+    MLFMA_CK(tc_prepare<kTcTheta>(dev_smem, &dyn[kTcTheta]));
+    MLFMA_CK(tc_prepare<kTcPhi>(dev_smem, &dyn[kTcPhi]));
+    MLFMA_CK(tc_prepare<kTcPhiT>(dev_smem, &dyn[kTcPhiT]));
+    MLFMA_CK(tc_prepare<kTcThetaT>(dev_smem, &dyn[kTcThetaT]));
+    for (int p = lmin_; p < lmax_; ++p)
+        for (int k = 0; k < 4; ++k)
+            if (tc_[p].smem[k] > static_cast<size_t>(dyn[k])) return {};  // keep the CUDA-core kernels
     const auto ncols_of = [](int npad) { int c = 32; while (c < npad) c <<= 1; return c; };
     const void* fns[4] = {reinterpret_cast<const void*>(k_tc_pass<kTcTheta>),
                           reinterpret_cast<const void*>(k_tc_pass<kTcPhi>),

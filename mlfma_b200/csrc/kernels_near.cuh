@@ -412,6 +412,18 @@ k_dense_rows(DevSources S, const int* __restrict__ rows, const int* __restrict__
     if (threadIdx.x == 0) y[blockIdx.x] = cmul(ck, red[0]);
 }
 
+// The same entries written out: out[i * ld + perm[t]] = C k Z[rows[i]][t],
+// one thread per column.
+__global__ void __launch_bounds__(kDenseThreads)
+k_dense_block(DevSources S, const int* __restrict__ rows, const int* __restrict__ perm, int n, double2 ck,
+              double2* __restrict__ out, long long ld) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const int m = rows[blockIdx.y];
+    const zd z = near_entry(S, m, t);
+    out[static_cast<long long>(blockIdx.y) * ld + perm[t]] = cmul(ck, make_double2(z.x, z.y));
+}
+
 // Far field of currents I (caller order) along unit directions khat:
 // F = C k (I - khat khat^T) sum_n I_n f_n(k khat), with f_n = e^{-i r_n . k khat}
 // phat_n for a dipole (Dipole::getFarAlongDir, src/sources/dipole.h:53-57)
