@@ -383,6 +383,10 @@ int mlfma_level_patterns(mlfma_handle h, int level, int which, double* out, long
 /* Transfer functions of a level: 316 x ndir complex in the order of
  * Math::getINodeDistVecs (src/math.cpp:106-122). */
 int mlfma_level_transl(mlfma_handle h, int level, double* out);
+/* The same table as the operator uses it: built on the GPU at setup
+ * (Tables::getAlpha, getInterpPsi, buildTranslationTable,
+ * src/fmm/tables.cpp:90-220), complex double, same layout. */
+int mlfma_level_transl_gpu(mlfma_handle h, int level, double* out);
 
 /* Far-field leaves in tree order: count, then per leaf (level, box, first
  * source in tree order, source count) and the tree-order -> caller-order

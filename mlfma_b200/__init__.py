@@ -192,6 +192,14 @@ class MLFMA:
         check(lib().mlfma_level_transl(self._h, level, out.view(np.float64).ctypes.data_as(_dp)))
         return out.reshape(316, ndir)
 
+    def level_transl_gpu(self, level: int) -> np.ndarray:
+        """The level's transfer functions as built on the GPU (after setup)."""
+        info = self.level_info(level)
+        ndir = info["nth"] * info["nph"]
+        out = np.zeros(316 * ndir, dtype=np.complex128)
+        check(lib().mlfma_level_transl_gpu(self._h, level, out.view(np.float64).ctypes.data_as(_dp)))
+        return out.reshape(316, ndir)
+
     def far_leaves(self):
         """(info[:, (level, box, src0, nsrc)], perm) with perm[tree slot] = caller index."""
         cnt = ctypes.c_int()

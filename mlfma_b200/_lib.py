@@ -135,6 +135,7 @@ SIGNATURES = {
     "mlfma_level_boxes": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _ip, _ip]),
     "mlfma_level_patterns": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp, ctypes.c_longlong]),
     "mlfma_level_transl": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _dp]),
+    "mlfma_level_transl_gpu": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _dp]),
     "mlfma_far_leaves": (ctypes.c_int, [ctypes.c_void_p, _ip, _ip, _ip]),
     "mlfma_rwg_patterns_host": (ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_longlong]),
     "mlfma_destroy": (ctypes.c_int, [ctypes.c_void_p]),

@@ -824,6 +824,14 @@ int mlfma_level_transl(mlfma_handle h, int level, double* out) {
     return MLFMA_OK;
 }
 
+int mlfma_level_transl_gpu(mlfma_handle h, int level, double* out) {
+    if (!h || !out) return fail(MLFMA_ERR_ARG, "null argument");
+    if (!ready(h)) return fail(MLFMA_ERR_STATE, "mlfma_setup has not run");
+    const std::string e = h->dev->copy_transl(level, reinterpret_cast<double2*>(out));
+    if (!e.empty()) return fail(e == "level out of range" ? MLFMA_ERR_ARG : MLFMA_ERR_CUDA, e);
+    return MLFMA_OK;
+}
+
 int mlfma_far_leaves(mlfma_handle h, int* count, int* info, int* perm) {
     if (!h || !count) return fail(MLFMA_ERR_ARG, "null argument");
     const mlfma::Plan& p = h->plan;

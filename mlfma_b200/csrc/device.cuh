@@ -206,6 +206,14 @@ public:
     void apply_tree(const double2* xt, double2* yt, cudaStream_t s, int prec = -1, bool adj = false);
     // Same, never capturing a graph (launches the captured one if it exists).
     void apply_tree_direct(const double2* xt, double2* yt, cudaStream_t s, int prec = -1, bool adj = false);
+    // The product of what is already in the operator's input buffer (xt_buffer(),
+    // tree order; for the adjoint it holds conj(x)) into yt, with plain
+    // launches (for capture into a solver's step graph).
+    void enqueue_apply_from_input(double2* yt, cudaStream_t s, int prec, bool adj);
+    double2* input_buffer() const { return xt_; }
+    // Changes whenever something a captured product depends on changes
+    // (loads, launch shapes, kernel choice).
+    int generation() const { return generation_; }
 
     // Diagonal loads z (host, caller order, n complex) added to the operator:
     // A x + z .* x (A^H x + conj(z) .* x for the adjoint).  nullptr removes them.
@@ -261,6 +269,9 @@ public:
     std::string set_tc(int mode);
     int tc_mode() const { return (use_tc_ ? 1 : 0) | (use_tc_multi_ ? 2 : 0); }
 
+    // The level's FP64 transfer functions as built on the GPU, [316][ndir].
+    std::string copy_transl(int level, double2* host);
+
     // Diagnostic copies of per-level patterns (level, which: 0 outgoing, 1 local),
     // widened to complex double.
     std::string copy_level(int level, int which, double2* host, long long count);
@@ -296,6 +307,7 @@ private:
     void build_m2l_items(int max_chunk);
     std::string ensure_graph(int prec, bool tr);
     std::string setup_tc(const Plan& plan);
+    std::string build_transl_device(const Level& L, double2* t);
     void far_m2m_tc(int p, int nr, cudaStream_t s);
     void far_l2l_tc(int p, int nr, cudaStream_t s);
     void drop_graphs();
@@ -316,6 +328,8 @@ private:
 
     // Shared by both precisions.
     int lmin_ = 2, lmax_ = 0, ref_compat_ = 1;
+    int plan_order_ = 3;      // interp_order (2 order interpolation points)
+    double wavenum_ = 0;
     int nbox_[kMaxLevels] = {}, ndir_[kMaxLevels] = {}, nth_[kMaxLevels] = {}, nph_[kMaxLevels] = {};
     int4* m2l_items_ = nullptr;          // (level, box, first direction, count)
     int n_m2l_items_ = 0;
@@ -357,6 +371,7 @@ private:
     int* err_dev_ = nullptr;              //   and its device address
     int* near_slot_ = nullptr;            // per tile: slots of its partials
     int* near_red_ptr_ = nullptr;         // [n + 1]: target t's slots
+    int* near_cnt_ = nullptr;             // [n]: partials arrived for target t (0 between products)
     // Near field, many right-hand sides: block rows (both orientations).
     DevNearRow* near_rows_ = nullptr;
     int n_near_rows_ = 0;
@@ -394,6 +409,7 @@ private:
     size_t tc_scratch_floats_ = 0;
     bool tc_ok_ = false;
     bool use_tc_ = false, use_tc_multi_ = false;
+    int generation_ = 0;
     double2 ck_{};             // Phys::C * k
     double2* loads_ = nullptr; // diagonal loads, tree order
     bool has_loads_ = false;

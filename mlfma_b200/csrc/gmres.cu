@@ -141,6 +141,128 @@ __global__ void k_scatter_perm(const double2* __restrict__ xt, const int* __rest
 
 inline int nblk(long long n, int bs) { return static_cast<int>((n + bs - 1) / bs); }
 
+// ---------------------------------------------------------------- device-resident Arnoldi step
+// The step index k lives in device memory, so one captured graph serves every
+// step of a cycle.
+constexpr int kMaxDeviceSteps = 256;  // basis vectors per cycle that the step kernels handle
+constexpr int kStepBatch = 8;         // device steps between host reads of the Hessenberg columns
+struct StepStateD {
+    int k;
+    unsigned cnt;
+    double hn;
+};
+
+// q_k = w (1 / hn) for k > 0 (q_0 is set by the cycle), and the product's input
+// xt = q_k (conj(q_k) for the adjoint).
+__global__ void k_step_prep(StepStateD* __restrict__ st, double2* __restrict__ Q, const double2* __restrict__ w,
+                            double2* __restrict__ xt, int n, int adj) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int k = st->k;
+    double2 q;
+    if (k == 0) {
+        q = Q[i];
+    } else {
+        const double hn = st->hn;
+        const double2 v = w[i];
+        const double a = hn > 0 ? 1.0 / hn : 0.0;
+        q = make_double2(a * v.x, a * v.y);
+        Q[static_cast<long long>(k) * n + i] = q;
+    }
+    xt[i] = adj ? make_double2(q.x, -q.y) : q;
+}
+
+// One CGS pass, dots: partial[j][c] = sum_{i in chunk c} conj(Q_j[i]) w[i] for
+// j <= k (block (c, j)); the last block to finish sums each j's partials in a
+// fixed order into t[j] and into column k of the Hessenberg matrix (pass 0
+// sets it, pass 1 adds).
+__global__ void k_step_dots(StepStateD* __restrict__ st, const double2* __restrict__ Q, int n,
+                            const double2* __restrict__ w, double2* __restrict__ partial, int nchunks,
+                            double2* __restrict__ t, double2* __restrict__ hcols, int ldh, int pass) {
+    __shared__ double2 red[kDotThreads];
+    __shared__ bool last;
+    const int c = blockIdx.x, j = blockIdx.y;
+    const int k = st->k;
+    if (j <= k) {
+        const double2* q = Q + static_cast<long long>(j) * n;
+        const int i0 = c * kDotChunk, i1 = min(n, i0 + kDotChunk);
+        double2 acc = make_double2(0.0, 0.0);
+        for (int i = i0 + threadIdx.x; i < i1; i += blockDim.x) acc = cj_mul_add(q[i], w[i], acc);
+        red[threadIdx.x] = acc;
+        __syncthreads();
+        for (int s2 = blockDim.x / 2; s2 > 0; s2 >>= 1) {
+            if (threadIdx.x < s2) {
+                red[threadIdx.x].x += red[threadIdx.x + s2].x;
+                red[threadIdx.x].y += red[threadIdx.x + s2].y;
+            }
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) partial[static_cast<long long>(j) * nchunks + c] = red[0];
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(&st->cnt, 1u) == gridDim.x * gridDim.y - 1;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    double2* h = hcols + static_cast<long long>(k) * ldh;
+    for (int jj = threadIdx.x; jj <= k; jj += blockDim.x) {
+        double2 sum = make_double2(0.0, 0.0);
+        for (int cc = 0; cc < nchunks; ++cc) {
+            const double2 p = __ldcg(partial + static_cast<long long>(jj) * nchunks + cc);
+            sum.x += p.x;
+            sum.y += p.y;
+        }
+        t[jj] = sum;
+        h[jj] = pass ? make_double2(h[jj].x + sum.x, h[jj].y + sum.y) : sum;
+    }
+    if (threadIdx.x == 0) st->cnt = 0;
+}
+
+// One CGS pass, update: w -= sum_{j <= k} Q_j t[j].  The second pass also
+// forms ||w||^2 (block partials, the last block sums them in a fixed order):
+// h[k+1] = (||w||^2, 0), hn = ||w||, and the step index moves on.
+__global__ void k_step_update(StepStateD* __restrict__ st, const double2* __restrict__ Q, int n,
+                              const double2* __restrict__ t, double2* __restrict__ w, double* __restrict__ npart,
+                              double2* __restrict__ hcols, int ldh, int norm) {
+    __shared__ double red[256];
+    __shared__ bool last;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = st->k;
+    double nn = 0.0;
+    if (i < n) {
+        double2 v = w[i];
+        for (int j = 0; j <= k; ++j) {
+            const double2 q = Q[static_cast<long long>(j) * n + i];
+            const double2 hj = t[j];
+            v.x -= q.x * hj.x - q.y * hj.y;
+            v.y -= q.x * hj.y + q.y * hj.x;
+        }
+        w[i] = v;
+        nn = fma(v.x, v.x, v.y * v.y);
+    }
+    if (!norm) return;
+    red[threadIdx.x] = nn;
+    __syncthreads();
+    for (int s2 = blockDim.x / 2; s2 > 0; s2 >>= 1) {
+        if (threadIdx.x < s2) red[threadIdx.x] += red[threadIdx.x + s2];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) npart[blockIdx.x] = red[0];
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(&st->cnt, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!last || threadIdx.x != 0) return;
+    __threadfence();
+    double acc = 0.0;
+    for (int b = 0; b < static_cast<int>(gridDim.x); ++b) acc += __ldcg(npart + b);
+    hcols[static_cast<long long>(k) * ldh + k + 1] = make_double2(acc, 0.0);
+    st->hn = sqrt(acc);
+    st->k = k + 1;
+    st->cnt = 0;
+}
+
 }  // namespace
 
 #define GM_CK(call)                                                                \
@@ -173,10 +295,64 @@ std::string Gmres::ensure(int n, int ncols, int extra) {
         GM_CK(cudaMalloc(&xo_, sizeof(double2) * n));
         GM_CK(cudaMalloc(&bo_, sizeof(double2) * n));
     }
+    if (ncols <= kMaxDeviceSteps + 1) {
+        GM_CK(cudaMalloc(&st_, sizeof(StepStateD)));
+        GM_CK(cudaMalloc(&hcols_, sizeof(double2) * static_cast<size_t>(ncols) * (ncols + 1)));
+        GM_CK(cudaMalloc(&tco_, sizeof(double2) * (ncols + 1)));
+        GM_CK(cudaMalloc(&npart2_, sizeof(double) * nblk(n, 256)));
+    }
+    return {};
+}
+
+void Gmres::release_steps() {
+    if (sgx_) cudaGraphExecDestroy(sgx_);
+    if (sg_) cudaGraphDestroy(sg_);
+    sgx_ = nullptr;
+    sg_ = nullptr;
+    sg_op_ = nullptr;
+    for (void* p : {st_, (void*)hcols_, (void*)tco_, (void*)npart2_})
+        if (p) cudaFree(p);
+    st_ = nullptr;
+    hcols_ = nullptr;
+    tco_ = nullptr;
+    npart2_ = nullptr;
+}
+
+// The captured Arnoldi step for this operator, precision and direction
+// (recaptured when any of them, the operator's generation or the workspace
+// changes).
+std::string Gmres::step_graph(DeviceOp& op, int prec) {
+    const int adj = adj_ ? 1 : 0;
+    if (sgx_ && sg_op_ == &op && sg_prec_ == prec && sg_adj_ == adj && sg_gen_ == op.generation() && sg_q_ == Q_)
+        return {};
+    if (sgx_) cudaGraphExecDestroy(sgx_);
+    if (sg_) cudaGraphDestroy(sg_);
+    sgx_ = nullptr;
+    sg_ = nullptr;
+    cudaStream_t s = op.stream();
+    StepStateD* st = static_cast<StepStateD*>(st_);
+    const int n = n_, ldh = cap_ + 1;
+    GM_CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    k_step_prep<<<nblk(n, 256), 256, 0, s>>>(st, Q_, w_, op.input_buffer(), n, adj);
+    op.enqueue_apply_from_input(w_, s, prec, adj_);
+    for (int pass = 0; pass < 2; ++pass) {
+        k_step_dots<<<dim3(nchunks_, cap_), kDotThreads, 0, s>>>(st, Q_, n, w_, partial_, nchunks_, tco_, hcols_, ldh,
+                                                                  pass);
+        k_step_update<<<nblk(n, 256), 256, 0, s>>>(st, Q_, n, tco_, w_, npart2_, hcols_, ldh, pass);
+    }
+    const cudaError_t ce = cudaStreamEndCapture(s, &sg_);
+    if (ce != cudaSuccess) return std::string("step capture: ") + cudaGetErrorString(ce);
+    GM_CK(cudaGraphInstantiate(&sgx_, sg_, cudaGraphInstantiateFlagUseNodePriority));
+    sg_op_ = &op;
+    sg_prec_ = prec;
+    sg_adj_ = adj;
+    sg_gen_ = op.generation();
+    sg_q_ = Q_;
     return {};
 }
 
 void Gmres::release() {
+    release_steps();
     if (!external_)
         for (void* p : {(void*)Q_, (void*)w_, (void*)b_, (void*)x_, (void*)r_, (void*)h_, (void*)y_,
                         (void*)partial_, (void*)npartial_, (void*)xo_, (void*)bo_})
@@ -372,29 +548,10 @@ std::string Gmres::cycles(DeviceOp& op, int prec, const SolveOpts& o, double bno
         k_scale<<<nblk(n, 256), 256, 0, s>>>(r_, make_double2(1.0 / beta, 0.0), Q_, n);
         std::fill(g.begin(), g.end(), cd(0));
         g[0] = beta;
-        int k = 0;
-        for (; k < m && total < max_iter; ++k) {
-            double2* qk = Q_ + static_cast<long long>(k) * n;
-            apply(op, qk, w_, s, prec);  // w = A q_k
-            err = cgs_pass(k + 1, s, false);
-            if (!err.empty()) return err;
-            err = cgs_pass(k + 1, s, true);
-            if (!err.empty()) return err;
-            // ||w||^2 into h_[k+1].x, then h_[0..k+1] to the host in one copy.
-            k_norm2<<<nchunks_, kDotThreads, 0, s>>>(w_, n, npartial_);
-            k_sum_into<<<1, 1, 0, s>>>(npartial_, nchunks_, h_ + k + 1);
-            GM_CK(cudaMemcpyAsync(hcol.data(), h_, sizeof(double2) * (k + 2), cudaMemcpyDeviceToHost, s));
-            GM_CK(cudaStreamSynchronize(s));
-            const double hn = std::sqrt(hcol[k + 1].x);
-            if (!std::isfinite(hn)) return "nonfinite:Arnoldi";
-            std::vector<cd> hc(k + 2);
-            for (int i = 0; i <= k; ++i) hc[i] = cd(hcol[i].x, hcol[i].y);
-            hc[k + 1] = hn;
-            if (hn > 0) {
-                double2* qn = Q_ + static_cast<long long>(k + 1) * n;
-                k_scale<<<nblk(n, 256), 256, 0, s>>>(w_, make_double2(1.0 / hn, 0.0), qn, n);
-            }
-            // Previous rotations, then a new one annihilating hc[k+1].
+        // Givens rotations of Hessenberg column k (hc[0..k], hc[k+1] = the new
+        // vector's norm); true when the cycle ends here.
+        auto absorb = [&](int k, std::vector<cd>& hc) -> bool {
+            const double hn = std::abs(hc[k + 1]);
             for (int i = 0; i < k; ++i) {
                 const cd a = hc[i], b = hc[i + 1];
                 if (refg) {
@@ -433,7 +590,66 @@ std::string Gmres::cycles(DeviceOp& op, int prec, const SolveOpts& o, double bno
             for (int i = 0; i <= k; ++i) H[static_cast<size_t>(k) * (m + 1) + i] = hc[i];
             ++total;
             last = std::abs(g[k + 1]) / bnorm;
-            if (!(std::abs(g[k + 1]) > tol_abs) || hn == 0.0) { ++k; converged = true; break; }
+            if (!(std::abs(g[k + 1]) > tol_abs) || hn == 0.0) {
+                converged = true;
+                return true;
+            }
+            return false;
+        };
+        int k = 0;
+        const bool device_steps = !external_ && st_ && m + 1 <= cap_ && m <= kMaxDeviceSteps;
+        if (device_steps) {
+            // batches of device-resident steps; the host takes the new columns once per batch
+            err = step_graph(op, prec);
+            if (!err.empty()) return err;
+            GM_CK(cudaMemsetAsync(st_, 0, sizeof(StepStateD), s));
+            const int ldh = cap_ + 1;
+            std::vector<double2> cols;
+            bool stop = false;
+            while (!stop && k < m && total < max_iter) {
+                const int batch = std::min(kStepBatch, std::min(m - k, max_iter - total));
+                for (int b = 0; b < batch; ++b) GM_CK(cudaGraphLaunch(sgx_, s));
+                cols.resize(static_cast<size_t>(batch) * ldh);
+                GM_CK(cudaMemcpyAsync(cols.data(), hcols_ + static_cast<size_t>(k) * ldh,
+                                      sizeof(double2) * cols.size(), cudaMemcpyDeviceToHost, s));
+                GM_CK(cudaStreamSynchronize(s));
+                for (int b = 0; b < batch && !stop; ++b, ++k) {
+                    const double2* col = cols.data() + static_cast<size_t>(b) * ldh;
+                    const double hn = std::sqrt(col[k + 1].x);
+                    if (!std::isfinite(hn)) return "nonfinite:Arnoldi";
+                    std::vector<cd> hc(k + 2);
+                    for (int i = 0; i <= k; ++i) hc[i] = cd(col[i].x, col[i].y);
+                    hc[k + 1] = hn;
+                    stop = absorb(k, hc);
+                }
+            }
+        } else {
+            for (; k < m && total < max_iter; ++k) {
+                double2* qk = Q_ + static_cast<long long>(k) * n;
+                apply(op, qk, w_, s, prec);  // w = A q_k
+                err = cgs_pass(k + 1, s, false);
+                if (!err.empty()) return err;
+                err = cgs_pass(k + 1, s, true);
+                if (!err.empty()) return err;
+                // ||w||^2 into h_[k+1].x, then h_[0..k+1] to the host in one copy.
+                k_norm2<<<nchunks_, kDotThreads, 0, s>>>(w_, n, npartial_);
+                k_sum_into<<<1, 1, 0, s>>>(npartial_, nchunks_, h_ + k + 1);
+                GM_CK(cudaMemcpyAsync(hcol.data(), h_, sizeof(double2) * (k + 2), cudaMemcpyDeviceToHost, s));
+                GM_CK(cudaStreamSynchronize(s));
+                const double hn = std::sqrt(hcol[k + 1].x);
+                if (!std::isfinite(hn)) return "nonfinite:Arnoldi";
+                std::vector<cd> hc(k + 2);
+                for (int i = 0; i <= k; ++i) hc[i] = cd(hcol[i].x, hcol[i].y);
+                hc[k + 1] = hn;
+                if (hn > 0) {
+                    double2* qn = Q_ + static_cast<long long>(k + 1) * n;
+                    k_scale<<<nblk(n, 256), 256, 0, s>>>(w_, make_double2(1.0 / hn, 0.0), qn, n);
+                }
+                if (absorb(k, hc)) {
+                    ++k;
+                    break;
+                }
+            }
         }
         // Solve the k x k upper-triangular system R y = g (solver.cpp:143-145).
         std::vector<cd> yv(k);

@@ -68,6 +68,22 @@ private:
     std::string norm(const double2* v, cudaStream_t s, double* out);
     std::string cgs_pass(int ncols, cudaStream_t s, bool add);
 
+    // Device-resident Arnoldi steps (allocated workspace, restart <= kMaxDeviceSteps):
+    // one step = a captured graph (next basis vector, product, CGS2, norm)
+    // that reads the step index from device memory; the host takes the new
+    // Hessenberg columns once per batch of steps.
+    std::string step_graph(DeviceOp& op, int prec);
+    void release_steps();
+    void* st_ = nullptr;         // step index, block counter, last norm (device)
+    double2* hcols_ = nullptr;   // [cap_][cap_ + 1]: Hessenberg column k at k (cap_ + 1)
+    double2* tco_ = nullptr;     // [cap_]: coefficients of the current CGS pass
+    double* npart2_ = nullptr;   // norm partials, one per update block
+    cudaGraph_t sg_ = nullptr;
+    cudaGraphExec_t sgx_ = nullptr;
+    const DeviceOp* sg_op_ = nullptr;
+    int sg_prec_ = -1, sg_adj_ = -1, sg_gen_ = -1;
+    const double2* sg_q_ = nullptr;
+
     int n_ = 0, cap_ = 0, extra_ = 0, nchunks_ = 0;
     double2* Q_ = nullptr;
     double2* w_ = nullptr;

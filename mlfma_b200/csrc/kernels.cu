@@ -33,6 +33,7 @@
 #include "kernels_far.cuh"
 #include "kernels_multi.cuh"
 #include "kernels_near.cuh"
+#include "kernels_tables.cuh"
 #include "kernels_tc.cuh"
 #include "zmath.cuh"
 
@@ -195,6 +196,45 @@ void DeviceOp::build_m2l_items(int max_chunk) {
     if (!items.empty()) h2d_landed(m2l_items_, items.data(), sizeof(int4) * items.size());
 }
 
+// The 316 x ndir transfer functions of level L on the GPU (k_tables_alpha,
+// k_tables_transl), complex double, into t.
+std::string DeviceOp::build_transl_device(const Level& L, double2* t) {
+    // offsets in the order of Math::getINodeDistVecs (src/math.cpp:106-122);
+    // the distinct squared lengths index the alpha rows
+    std::vector<int> r2list, rix;
+    std::vector<double> uhat;
+    for (int dz = -3; dz <= 3; ++dz)
+        for (int dy = -3; dy <= 3; ++dy)
+            for (int dx = -3; dx <= 3; ++dx) {
+                if (std::max({std::abs(dx), std::abs(dy), std::abs(dz)}) <= 1) continue;
+                const int r2 = dx * dx + dy * dy + dz * dz;
+                auto it = std::find(r2list.begin(), r2list.end(), r2);
+                if (it == r2list.end()) {
+                    r2list.push_back(r2);
+                    it = r2list.end() - 1;
+                }
+                rix.push_back(static_cast<int>(it - r2list.begin()));
+                const double r = std::sqrt(static_cast<double>(r2));
+                uhat.push_back(dx / r);
+                uhat.push_back(dy / r);
+                uhat.push_back(dz / r);
+            }
+    const int order = plan_order_;
+    if (2 * order > 2 * kTabMaxOrder || L.nps < 2 * order || L.nps < 2) return "interp_order out of range for the tables";
+    const int nr = static_cast<int>(r2list.size());
+    int* d_r2 = upload(r2list);
+    int* d_rix = upload(rix);
+    double* d_u = upload(uhat);
+    double* d_kh = upload(L.khat);
+    double2* d_alpha = alloc<double2>(static_cast<size_t>(nr) * L.nps);
+    k_tables_alpha<<<blocks_for(static_cast<long long>(nr) * L.nps, kTabThreads), kTabThreads, 0, stream_>>>(
+        d_r2, nr, L.nps, L.L, wavenum_, L.leng, d_alpha);
+    k_tables_transl<<<blocks_for(316ll * L.ndir, kTabThreads), kTabThreads, 0, stream_>>>(d_u, d_rix, d_alpha, L.nps,
+                                                                                         order, d_kh, L.ndir, t);
+    MLFMA_CK(cudaGetLastError());
+    return {};
+}
+
 // Far-field arrays in precision R (levels, transitions, patterns).
 template <class R>
 std::string DeviceOp::setup_far(const Plan& plan, FarField<R>& F, const double2* pat64) {
@@ -218,7 +258,20 @@ std::string DeviceOp::setup_far(const Plan& plan, FarField<R>& F, const double2*
             MLFMA_CK(cudaMemset(d.Am, 0, cnt * max_rhs_ * sizeof(C)));
             MLFMA_CK(cudaMemset(d.Bm, 0, cnt * max_rhs_ * sizeof(C)));
         }
-        d.transl = upload(conv_c<C>(L.transl));
+        if constexpr (std::is_same<R, double>::value) {
+            // transfer functions built on the GPU (kernels_tables.cuh)
+            double2* t = alloc<double2>(static_cast<size_t>(316) * L.ndir);
+            std::string e = build_transl_device(L, t);
+            if (!e.empty()) return e;
+            d.transl = t;
+        } else {
+            // the complex-float far field narrows the FP64 table
+            C* t = alloc<C>(static_cast<size_t>(316) * L.ndir);
+            const long long cnt = 316ll * L.ndir;
+            k_narrow<C><<<blocks_for(cnt, 256), 256, 0, stream_>>>(f64_.lv[l].transl, t, cnt);
+            MLFMA_CK(cudaGetLastError());
+            d.transl = t;
+        }
         d.w = upload(conv_r<R>(L.m2l_w));
         d.shift_up = upload(conv_c<C>(L.shift_up));
         d.shift_down = upload(conv_c<C>(L.shift_down));
@@ -428,6 +481,8 @@ std::string DeviceOp::setup(const Plan& plan, int device, int precision, int max
         yt_ = alloc<double2>(n_);
         lmin_ = plan.lmin;
         lmax_ = plan.max_level;
+        plan_order_ = plan.cfg.interp_order;
+        wavenum_ = plan.pw.wavenum;
         ref_compat_ = plan.cfg.ref_compat;
         traffic_ = Traffic{};
         const double cbytes = precision == kFp64 ? 16.0 : 8.0;  // one far-field complex value
@@ -597,6 +652,9 @@ std::string DeviceOp::setup(const Plan& plan, int device, int precision, int max
                 near_part_ = alloc<double2>(static_cast<size_t>(plan.near_parts));
                 near_red_ptr_ = upload(plan.near_red_ptr);
                 near_slot_ = upload(plan.near_slot);
+                near_cnt_ = alloc<int>(n_);
+                MLFMA_CK(cudaMemset(near_cnt_, 0, sizeof(int) * n_));
+                MLFMA_CK(cudaMemset(ynear_, 0, sizeof(double2) * n_));  // targets without entries stay 0
                 MLFMA_CK(cudaFuncSetAttribute(k_near_sym, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                               static_cast<int>(kSymSmemBytes)));
                 MLFMA_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&near_occ_, k_near_sym, kSymThreads,
@@ -655,7 +713,7 @@ int DeviceOp::launches_per_matvec() const {
         for (int l = lmin_; l <= lmax_; ++l)
             if (m2l_count_[l]) n += 1;  // one M2L launch per level
     }
-    if (n_near_tiles_) n += 2;  // tiles + per-target sums
+    if (n_near_tiles_) n += 1;  // tiles, per-target sums fused
     return n;
 }
 
@@ -807,9 +865,7 @@ void DeviceOp::run_near(const double2* xt, cudaStream_t s) {
         return;
     }
     k_near_sym<<<near_grid_, kSymThreads, kSymSmemBytes, s>>>(near_tiles_, n_near_tiles_, near_bz_, xt, near_slot_,
-                                                             near_part_, err_dev_);
-    k_near_reduce<<<blocks_for(static_cast<long long>(n_) * kReduceLanes, 256), 256, 0, s>>>(near_red_ptr_, near_part_,
-                                                                                           n_, ynear_);
+                                                             near_part_, near_red_ptr_, near_cnt_, ynear_, err_dev_);
 }
 
 // The tree-ordered product xt_ -> (yfar_, ynear_): near field on the side
@@ -848,9 +904,11 @@ std::string DeviceOp::set_loads(const double2* z_user) {
     if (!ready_) return "operator not set up";
     MLFMA_CK(cudaSetDevice(device_));
     if (!z_user) {
+        if (has_loads_) ++generation_;
         has_loads_ = false;
         return {};
     }
+    ++generation_;
     if (!loads_) loads_ = alloc<double2>(n_);
     MLFMA_CK(cudaMemcpyAsync(yt_, z_user, sizeof(double2) * n_, cudaMemcpyHostToDevice, stream_));
     k_gather<<<blocks_for(n_, 256), 256, 0, stream_>>>(yt_, perm_, loads_, n_, 0);
@@ -866,6 +924,13 @@ void DeviceOp::apply_tree(const double2* xt, double2* yt, cudaStream_t s, int pr
     if (adj) k_conj_copy<<<blocks_for(n_, 256), 256, 0, s>>>(xt, xt_, n_);
     else if (xt != xt_) cudaMemcpyAsync(xt_, xt, sizeof(double2) * n_, cudaMemcpyDeviceToDevice, s);
     launch_core(s, prec, adj);
+    k_finish<<<blocks_for(n_, 256), 256, 0, s>>>(yfar_, ynear_, nullptr, yt, n_, ck_, 0, xt_,
+                                                 has_loads_ ? loads_ : nullptr, adj ? 1 : 0);
+}
+
+void DeviceOp::enqueue_apply_from_input(double2* yt, cudaStream_t s, int prec, bool adj) {
+    if (prec < 0) prec = precision_;
+    enqueue_core(s, prec, adj);
     k_finish<<<blocks_for(n_, 256), 256, 0, s>>>(yfar_, ynear_, nullptr, yt, n_, ck_, 0, xt_,
                                                  has_loads_ ? loads_ : nullptr, adj ? 1 : 0);
 }
@@ -989,6 +1054,14 @@ __global__ void k_widen(const C* __restrict__ src, double2* __restrict__ dst, lo
     if (i < n) dst[i] = to_d2(src[i]);
 }
 }  // namespace
+
+std::string DeviceOp::copy_transl(int level, double2* host) {
+    if (level < lmin_ || level > lmax_) return "level out of range";
+    MLFMA_CK(cudaSetDevice(device_));
+    MLFMA_CK(cudaStreamSynchronize(stream_));
+    MLFMA_CK(cudaMemcpy(host, f64_.lv[level].transl, sizeof(double2) * 316 * ndir_[level], cudaMemcpyDeviceToHost));
+    return {};
+}
 
 std::string DeviceOp::copy_level(int level, int which, double2* host, long long count) {
     if (level < lmin_ || level > lmax_) return "level out of range";
@@ -1490,6 +1563,7 @@ std::string DeviceOp::set_tc(int mode) {
     use_tc_ = (mode & 1) != 0;
     use_tc_multi_ = (mode & 2) != 0;
     drop_graphs();  // recaptured with the chosen kernels on the next product
+    ++generation_;
     return {};
 }
 
@@ -1651,6 +1725,7 @@ std::string DeviceOp::autotune(int nr, int reps, TuneReport* rep) {
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     drop_graphs();
+    ++generation_;
     if (rep) *rep = r;
     MLFMA_CK(cudaGetLastError());
     return {};
