@@ -330,8 +330,8 @@ int mlfma_autotune(mlfma_handle h, int nrhs, int reps, mlfma_tuning* out);
  * contractions (tcgen05 MMAs, split-precision 3xTF32, FP32 accumulation),
  * children shifted and summed before the interpolation.  mode bit 0: the
  * one-vector product, bit 1: the many-right-hand-side product; 0 = the
- * CUDA-core kernels.  Defaults: bit 1 set when max_rhs > 1; mlfma_autotune
- * times both and keeps the faster.  Products of the FP64 far field and
+ * CUDA-core kernels (the default); mlfma_autotune times both and keeps the
+ * faster.  Products of the FP64 far field and
  * transposed products always use the CUDA-core kernels.  MLFMA_ERR_ARG when
  * the operator has no complex-float far field or a grid exceeds the kernels'
  * shared memory.  Results agree with the CUDA-core kernels to float rounding. */

@@ -1442,7 +1442,6 @@ std::string DeviceOp::setup_tc(const Plan& plan) {
             t.grid[k] = occ * sms_;
         }
     tc_ok_ = true;
-    use_tc_multi_ = max_rhs_ > 1;
     return {};
 }
 

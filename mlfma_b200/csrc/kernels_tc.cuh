@@ -24,8 +24,8 @@
 //
 // One CTA = 4 warps, persistent over 128-row tiles.  Every thread stages one
 // row of the tile (loads, shift, child sum, hi/lo split) into shared memory;
-// thread 0 issues the MMAs (A: the tile, MN-major, 128-byte swizzle; B: the
-// weights, K-major, no swizzle, bulk-copied once per CTA) and commits them to
+// thread 0 issues the MMAs (A: the tile; B: the weights, bulk-copied once per
+// CTA; both K-major without swizzle, the layout valid for TF32) and commits them to
 // an mbarrier; then each warp reads its 32 TMEM lanes (one row per thread) and
 // writes the outputs.  Every mbarrier wait is bounded: a CTA that gives up sets
 // *err, releases its tensor memory and returns.
@@ -93,10 +93,46 @@ __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint
     return static_cast<uint64_t>((saddr >> 4) & 0x3FFF) | (static_cast<uint64_t>((lbo >> 4) & 0x3FFF) << 16) |
            (static_cast<uint64_t>((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46) | (static_cast<uint64_t>(layout) << 61);
 }
-// Instruction descriptor: kind::tf32, FP32 accumulator, A MN-major, B K-major, M = 128.
+// Instruction descriptor: kind::tf32, FP32 accumulator, A and B K-major, M = 128.
 __host__ __device__ constexpr uint32_t tc_idesc(int npad) {
-    return (1u << 4) | (2u << 7) | (2u << 10) | (1u << 15) | (0u << 16) | (static_cast<uint32_t>(npad >> 3) << 17) |
+    return (1u << 4) | (2u << 7) | (2u << 10) | (0u << 15) | (0u << 16) | (static_cast<uint32_t>(npad >> 3) << 17) |
            (static_cast<uint32_t>(kTcRows >> 4) << 24);
+}
+
+// Stages four consecutive contraction values of row m (kq: their 16-byte
+// piece within the chunk), split hi + lo, as two 16-byte stores.
+__device__ __forceinline__ void tc_stage4(unsigned char* a_hi, unsigned char* a_lo, int m, int kq, int kc_max,
+                                          const float* v) {
+    uint4 h, l;
+    uint32_t* hp = &h.x;
+    uint32_t* lp = &l.x;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        hp[u] = tf32_rna(v[u]);
+        lp[u] = tf32_rna(v[u] - __uint_as_float(hp[u]));
+    }
+    const uint32_t o = tc_a_offset(m, kq, kc_max);
+    *reinterpret_cast<uint4*>(a_hi + o) = h;
+    *reinterpret_cast<uint4*>(a_lo + o) = l;
+}
+
+// One thread: the 3xTF32 MMAs of a staged chunk, D (+)= A_chunk W_chunk^T with
+// D = A_hi W_lo + A_lo W_hi + A_hi W_hi (small products first); k0: the
+// chunk's first contraction index; first: the chunk starts the accumulation.
+__device__ __forceinline__ void tc_issue_chunk(uint32_t tmem, uint32_t s_ahi, uint32_t s_alo, uint32_t s_w,
+                                               uint32_t wbytes, int Kpad, int k0, int kc, int kc_max, uint32_t idesc,
+                                               bool first) {
+    const uint32_t sbo_a = static_cast<uint32_t>(kc_max) * 32u, sbo_w = static_cast<uint32_t>(Kpad) * 32u;
+    for (int kk = 0; kk < kc / 8; ++kk) {
+        const uint64_t ahi = umma_desc(s_ahi + kk * 256, 128, sbo_a, 0);
+        const uint64_t alo = umma_desc(s_alo + kk * 256, 128, sbo_a, 0);
+        const uint32_t kb = static_cast<uint32_t>(k0 / 8 + kk) * 256u;  // two 16-byte K pieces
+        const uint64_t bhi = umma_desc(s_w + kb, 128, sbo_w, 0);
+        const uint64_t blo = umma_desc(s_w + wbytes + kb, 128, sbo_w, 0);
+        umma_tf32(tmem, alo, bhi, idesc, (first && kk == 0) ? 0u : 1u);
+        umma_tf32(tmem, ahi, blo, idesc, 1u);
+        umma_tf32(tmem, ahi, bhi, idesc, 1u);
+    }
 }
 
 constexpr int kTcThreads = 128;
@@ -141,7 +177,7 @@ k_tc_pass(TcArgs a, int* __restrict__ err) {
     ok = __syncthreads_and(ok);
     bool w_done = ok, mma_pending = false;
     const uint32_t idesc = tc_idesc(a.Npad);
-    const uint32_t sbo_w = static_cast<uint32_t>(a.Kpad) * 32u;
+    const int kc_max = a.Kpad < kTcKChunk ? a.Kpad : kTcKChunk;
     const long long nrows = static_cast<long long>(a.J) * a.Q * a.nitems;
     const long long ntiles = (nrows + kTcRows - 1) / kTcRows;
     uint32_t phase = 0;
@@ -150,31 +186,19 @@ k_tc_pass(TcArgs a, int* __restrict__ err) {
         const TcItem it = tc_item<KIND>(a, r);
         for (int k0 = 0; k0 < a.Kpad && ok; k0 += kTcKChunk) {
             const int kc = min(kTcKChunk, a.Kpad - k0);
-            // this row's contraction values of the chunk, split hi + lo
-            for (int k = 0; k < kc; ++k) {
-                const float v = tc_load<KIND>(a, r, k0 + k, krow_s, it);
-                const uint32_t hi = tf32_rna(v);
-                const uint32_t lo = tf32_rna(v - __uint_as_float(hi));
-                const uint32_t o = tc_a_offset(tid, k);
-                *reinterpret_cast<uint32_t*>(a_hi + o) = hi;
-                *reinterpret_cast<uint32_t*>(a_lo + o) = lo;
+            // this row's contraction values of the chunk, four at a time, split hi + lo
+            for (int kq = 0; kq < kc / 4; ++kq) {
+                float v[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) v[u] = tc_load<KIND>(a, r, k0 + 4 * kq + u, krow_s, it);
+                tc_stage4(a_hi, a_lo, tid, kq, kc_max, v);
             }
             fence_async_smem();
             tc_fence_before();
             __syncthreads();
             tc_fence_after();
             if (tid == 0) {
-                for (int kk = 0; kk < kc / 8; ++kk) {
-                    const uint64_t ahi = umma_desc(s_ahi + kk * 4096, 1024, 4096, 2);
-                    const uint64_t alo = umma_desc(s_alo + kk * 4096, 1024, 4096, 2);
-                    const uint32_t kb = static_cast<uint32_t>(k0 / 8 + kk) * 256u;  // two 16-byte K chunks
-                    const uint64_t bhi = umma_desc(s_w + kb, 128, sbo_w, 0);
-                    const uint64_t blo = umma_desc(s_w + wbytes + kb, 128, sbo_w, 0);
-                    // small products first
-                    umma_tf32(tmem, alo, bhi, idesc, (k0 | kk) ? 1u : 0u);
-                    umma_tf32(tmem, ahi, blo, idesc, 1u);
-                    umma_tf32(tmem, ahi, bhi, idesc, 1u);
-                }
+                tc_issue_chunk(tmem, s_ahi, s_alo, s_w, wbytes, a.Kpad, k0, kc, kc_max, idesc, k0 == 0);
                 umma_commit(smem_addr(&bar_mma));
             }
             mma_pending = true;

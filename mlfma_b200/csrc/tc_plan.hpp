@@ -162,13 +162,13 @@ MLFMA_HD void tc_store(const TcArgs& a, const TcRow& r, int i, float v, const Tc
     }
 }
 
-// Shared-memory byte offset of tile element (row m, contraction index k within
-// the staged chunk): MN-major with the 128-byte swizzle, atoms of 8 K rows x
-// 32 M values (1 KB), the four 32-row groups of a K group 1 KB apart (the
-// descriptor's leading offset), K groups 4 KB apart (its stride offset).
-MLFMA_HD uint32_t tc_a_offset(int m, int k) {
-    return static_cast<uint32_t>((k >> 3) * 4096 + (m >> 5) * 1024 + (k & 7) * 128 +
-                                 ((((m & 31) >> 2) ^ (k & 7)) << 4) + (m & 3) * 4);
+// Shared-memory byte offset of the four contraction values [4 kq, 4 kq + 4)
+// of tile row m within the staged chunk: K-major without swizzle, core
+// matrices of 8 rows x 16 bytes, the chunk's 16-byte K pieces of one 8-row
+// group 128 bytes apart (the descriptor's leading offset), 8-row groups
+// kc_max * 32 bytes apart (its stride offset; kc_max = the largest chunk).
+MLFMA_HD uint32_t tc_a_offset(int m, int kq, int kc_max) {
+    return static_cast<uint32_t>((m >> 3) * (kc_max * 32) + kq * 128 + (m & 7) * 16);
 }
 // Element (output n, contraction k) of a weight matrix with Kpad columns in the
 // K-major layout without swizzle: 8-row groups Kpad * 32 bytes apart (stride
@@ -177,8 +177,9 @@ MLFMA_HD size_t tc_w_index(int n, int k, int Kpad) {
     return static_cast<size_t>(n / 8) * (Kpad * 8) + (k / 4) * 32 + (n % 8) * 4 + (k % 4);
 }
 
-// Bytes of one A tile half (hi or lo): at least 16 KB, so that the tile region
-// exceeds every span an operand descriptor of this layout covers.
+// Bytes of one A tile half (hi or lo): 128 rows x kc_max values, at least
+// 16 KB, so that the region exceeds any span an operand descriptor over it
+// could cover.
 MLFMA_HD size_t tc_a_bytes(int Kpad) {
     const size_t b = static_cast<size_t>(Kpad < kTcKChunk ? Kpad : kTcKChunk) * 512;
     return b > 16384 ? b : 16384;

@@ -61,14 +61,23 @@ static int check_layout(const TcDense& d, int Npad, int Kpad, const char* what) 
     if (smem > 232448) { printf("%s: shared memory %zu too large\n", what, smem); return 1; }
     const size_t ab = tc_a_bytes(Kpad);
     const int kc = std::min(Kpad, kTcKChunk);
-    uint32_t mx = 0;
+    // every 16-byte piece written once, all inside the tile
+    std::vector<int> hit(ab / 16, 0);
     for (int m = 0; m < kTcRows; ++m)
-        for (int k = 0; k < kc; ++k) mx = std::max(mx, tc_a_offset(m, k) + 4);
-    // each MMA reads K group kk: 4 row groups of 1 KB from kk * 4 KB; any
-    // reading of the leading/stride offsets (1 KB, 4 KB) stays below 16 KB + span
-    const size_t span = static_cast<size_t>(kc / 8 - 1) * 4096 + 4096;
-    if (mx > ab || span > ab || 3 * 4096 + 1024 + static_cast<size_t>(kc / 8 - 1) * 1024 > ab) {
-        printf("%s: A tile offsets exceed the tile (%u, %zu, %zu)\n", what, mx, span, ab);
+        for (int kq = 0; kq < kc / 4; ++kq) {
+            const uint32_t o = tc_a_offset(m, kq, kc);
+            if (o % 16 || o + 16 > ab || hit[o / 16]++) {
+                printf("%s: A tile piece (%d, %d) at %u outside the tile or written twice\n", what, m, kq, o);
+                return 1;
+            }
+        }
+    // an MMA reads K step kk: 16 row groups (stride kc * 32) of two 16-byte
+    // pieces (leading offset 128) from kk * 256; with the offsets swapped it
+    // would reach 15 * 128 + 128 + kk * 256 + kc * 32 -- both inside the region
+    const size_t span1 = static_cast<size_t>(15) * kc * 32 + (kc / 8 - 1) * 256 + 256;
+    const size_t span2 = static_cast<size_t>(15) * 128 + (kc / 8 - 1) * 256 + static_cast<size_t>(kc) * 32 + 128;
+    if (span1 > ab || span2 > ab) {
+        printf("%s: A descriptor spans exceed the tile (%zu, %zu, %zu)\n", what, span1, span2, ab);
         return 1;
     }
     size_t wmax = 0;
