@@ -313,6 +313,9 @@ typedef struct {
     float product_ms_after;
     int near_blocks_per_sm;    /* one-vector near field: persistent blocks per SM (it runs beside the far field) */
     int interp_path;           /* interpolation/anterpolation kernels chosen (see mlfma_set_interp_path) */
+    int schedule;              /* one-vector product: bit 0 translation lists staged in shared memory,
+                                  bit 1 near field started after aggregation, bit 2 two side streams
+                                  for the finer levels' translations */
 } mlfma_tuning;
 
 /* Autotuner: times the candidate launch shapes of the stages on this operator

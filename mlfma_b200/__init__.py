@@ -400,7 +400,7 @@ class MLFMA:
         return {"m2l_chunk": t.m2l_chunk, "m2m_rows": list(t.m2m_rows), "multi_m2m_rows_fast": t.multi_m2m_rows_fast,
                 "multi_l2l_pairs": t.multi_l2l_pairs, "product_ms_before": t.product_ms_before,
                 "product_ms_after": t.product_ms_after, "near_blocks_per_sm": t.near_blocks_per_sm,
-                "interp_path": t.interp_path}
+                "interp_path": t.interp_path, "schedule": t.schedule}
 
     @property
     def interp_path(self) -> int:

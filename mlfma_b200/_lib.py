@@ -69,7 +69,7 @@ class Tuning(ctypes.Structure):
     _fields_ = [("m2l_chunk", ctypes.c_int), ("m2m_rows", ctypes.c_int * 20), ("multi_m2m_rows_fast", ctypes.c_int),
                 ("multi_l2l_pairs", ctypes.c_int), ("product_ms_before", ctypes.c_float),
                 ("product_ms_after", ctypes.c_float), ("near_blocks_per_sm", ctypes.c_int),
-                ("interp_path", ctypes.c_int)]
+                ("interp_path", ctypes.c_int), ("schedule", ctypes.c_int)]
 
 
 # name -> (restype, argtypes); every symbol the header declares.

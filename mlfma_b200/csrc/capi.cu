@@ -721,6 +721,7 @@ int mlfma_autotune(mlfma_handle h, int nrhs, int reps, mlfma_tuning* out) {
         out->product_ms_after = r.after_ms;
         out->near_blocks_per_sm = r.near_blocks_per_sm;
         out->interp_path = r.interp_path;
+        out->schedule = r.schedule;
     }
     return MLFMA_OK;
 }

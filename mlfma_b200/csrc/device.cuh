@@ -146,6 +146,8 @@ struct TuneReport {
     float before_ms, after_ms;     // product time before and after
     int near_blocks_per_sm;        // one-vector near field: persistent blocks per SM
     int interp_path;               // tensor-core interpolation: bit 0 one vector, bit 1 many
+    int schedule;                  // one-vector product: bit 0 staged M2L lists, bit 1 near field after
+                                   // S2M, bit 2 two side streams for the finer levels' M2L
 };
 
 // Tensor-core interpolation and anterpolation of one level transition
@@ -286,8 +288,8 @@ private:
     template <class R> std::string setup_far(const Plan& plan, FarField<R>& F, const double2* pat64);
     template <class R, bool TR> void run_far_t(FarField<R>& F, const double2* xt, cudaStream_t s, int stage);
     template <class R, bool TR> void run_far_overlap_t(FarField<R>& F, const double2* xt, cudaStream_t s,
-                                                       cudaStream_t s2);
-    void run_far_overlap(const double2* xt, cudaStream_t s, cudaStream_t s2, int prec, bool tr);
+                                                       cudaStream_t s2, bool near_late);
+    void run_far_overlap(const double2* xt, cudaStream_t s, cudaStream_t s2, int prec, bool tr, bool late);
     template <class R, bool TR> void far_s2m(FarField<R>& F, const double2* xt, cudaStream_t s);
     template <class R, bool TR> void far_m2m(FarField<R>& F, int p, cudaStream_t s);
     template <class R, bool TR> void far_m2l(FarField<R>& F, int lo, int hi, cudaStream_t s);
@@ -317,8 +319,8 @@ private:
     int n_ = 0;
     int precision_ = kFp64;
     bool ready_ = false;
-    cudaStream_t stream_ = nullptr, side_ = nullptr, side2_ = nullptr;
-    cudaEvent_t ev_fork_ = nullptr, ev_join_ = nullptr, ev_m2l_done_ = nullptr;
+    cudaStream_t stream_ = nullptr, side_ = nullptr, side2_ = nullptr, side3_ = nullptr;
+    cudaEvent_t ev_fork_ = nullptr, ev_join_ = nullptr, ev_m2l_done_ = nullptr, ev_m2l_done2_ = nullptr;
     cudaEvent_t ev_level_[kMaxLevels] = {};  // outgoing patterns of a level final
     std::vector<void*> allocs_;
     long long bytes_ = 0;
@@ -337,6 +339,9 @@ private:
     std::vector<char> m2l_has_list_[kMaxLevels];  // box has a non-empty list 2
     // Launch shapes (defaults at setup; mlfma_autotune may change them).
     int m2l_chunk_ = 128;                 // one-vector M2L directions per block
+    int m2l_staged_ = 1;                  // one-vector M2L with its lists staged in shared memory
+    bool near_late_ = false;              // near field after S2M (overlapping the latency-bound stages)
+    int m2l_streams_ = 1;                 // side streams for the finer levels' translations
     std::vector<int> m2m_rows_;           // one-vector M2M parent rows per block, per transition
     int m_m2m_rows_fast_ = -1;            // many-rhs M2M grid order (-1: precision default)
     int m_l2l_pairs_ = 0;                 // many-rhs L2L column pairs per block (0: precision default)
@@ -371,7 +376,6 @@ private:
     int* err_dev_ = nullptr;              //   and its device address
     int* near_slot_ = nullptr;            // per tile: slots of its partials
     int* near_red_ptr_ = nullptr;         // [n + 1]: target t's slots
-    int* near_cnt_ = nullptr;             // [n]: partials arrived for target t (0 between products)
     // Near field, many right-hand sides: block rows (both orientations).
     DevNearRow* near_rows_ = nullptr;
     int n_near_rows_ = 0;

@@ -113,6 +113,8 @@ DeviceOp::~DeviceOp() {
     if (ev_fork_) cudaEventDestroy(ev_fork_);
     if (ev_join_) cudaEventDestroy(ev_join_);
     if (ev_m2l_done_) cudaEventDestroy(ev_m2l_done_);
+    if (ev_m2l_done2_) cudaEventDestroy(ev_m2l_done2_);
+    if (side3_) cudaStreamDestroy(side3_);
     for (auto& e : ev_level_)
         if (e) cudaEventDestroy(e);
     if (side2_) cudaStreamDestroy(side2_);
@@ -462,6 +464,7 @@ std::string DeviceOp::setup(const Plan& plan, int device, int precision, int max
         MLFMA_CK(cudaStreamCreateWithPriority(&stream_, cudaStreamNonBlocking, prio_high));
         MLFMA_CK(cudaStreamCreateWithPriority(&side_, cudaStreamNonBlocking, prio_low));
         MLFMA_CK(cudaStreamCreateWithPriority(&side2_, cudaStreamNonBlocking, prio_low));
+        MLFMA_CK(cudaStreamCreateWithPriority(&side3_, cudaStreamNonBlocking, prio_low));
         // error word of the kernels with bounded waits, read by the host after a sync
         MLFMA_CK(cudaHostAlloc(reinterpret_cast<void**>(&err_host_), sizeof(int), cudaHostAllocMapped));
         *err_host_ = 0;
@@ -469,6 +472,7 @@ std::string DeviceOp::setup(const Plan& plan, int device, int precision, int max
         MLFMA_CK(cudaEventCreateWithFlags(&ev_fork_, cudaEventDisableTiming));
         MLFMA_CK(cudaEventCreateWithFlags(&ev_join_, cudaEventDisableTiming));
         MLFMA_CK(cudaEventCreateWithFlags(&ev_m2l_done_, cudaEventDisableTiming));
+        MLFMA_CK(cudaEventCreateWithFlags(&ev_m2l_done2_, cudaEventDisableTiming));
         for (auto& e : ev_level_) MLFMA_CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         n_ = plan.n;
         if (plan.max_level >= kMaxLevels) return "tree deeper than supported";
@@ -652,9 +656,6 @@ std::string DeviceOp::setup(const Plan& plan, int device, int precision, int max
                 near_part_ = alloc<double2>(static_cast<size_t>(plan.near_parts));
                 near_red_ptr_ = upload(plan.near_red_ptr);
                 near_slot_ = upload(plan.near_slot);
-                near_cnt_ = alloc<int>(n_);
-                MLFMA_CK(cudaMemset(near_cnt_, 0, sizeof(int) * n_));
-                MLFMA_CK(cudaMemset(ynear_, 0, sizeof(double2) * n_));  // targets without entries stay 0
                 MLFMA_CK(cudaFuncSetAttribute(k_near_sym, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                               static_cast<int>(kSymSmemBytes)));
                 MLFMA_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&near_occ_, k_near_sym, kSymThreads,
@@ -713,7 +714,7 @@ int DeviceOp::launches_per_matvec() const {
         for (int l = lmin_; l <= lmax_; ++l)
             if (m2l_count_[l]) n += 1;  // one M2L launch per level
     }
-    if (n_near_tiles_) n += 1;  // tiles, per-target sums fused
+    if (n_near_tiles_) n += 2;  // tiles + per-target sums
     return n;
 }
 
@@ -758,7 +759,11 @@ void DeviceOp::far_m2l(FarField<R>& F, int lo, int hi, cudaStream_t s) {
     if (lo > hi) return;
     const int first = m2l_first_[lo];
     const int count = m2l_first_[hi] + m2l_count_[hi] - first;
-    if (count > 0) k_m2l<R, TR><<<count, 128, 0, s>>>(F.lv_dev, m2l_items_ + first, ref_compat_ ? 0 : 1);
+    if (count <= 0) return;
+    if (m2l_staged_)
+        k_m2l_staged<R, TR><<<count, 128, 0, s>>>(F.lv_dev, m2l_items_ + first, ref_compat_ ? 0 : 1);
+    else
+        k_m2l<R, TR><<<count, 128, 0, s>>>(F.lv_dev, m2l_items_ + first, ref_compat_ ? 0 : 1);
 }
 
 template <class R, bool TR>
@@ -814,8 +819,13 @@ void DeviceOp::run_far_t(FarField<R>& F, const double2* xt, cudaStream_t s, int 
 // final once S2M (l = max level) or M2M(l+1 -> l) has run, so levels
 // lmax..lmin+1 translate on s2 while the interpolations climb to the coarsest
 // level on s; the anterpolations wait for both.
+// near_late: the near field (on side_) starts once S2M has run, so that it
+// overlaps the latency-bound stages instead of competing with S2M for
+// bandwidth.  The finer levels' translations alternate between m2l_streams_
+// side streams (s2, side3_).
 template <class R, bool TR>
-void DeviceOp::run_far_overlap_t(FarField<R>& F, const double2* xt, cudaStream_t s, cudaStream_t s2) {
+void DeviceOp::run_far_overlap_t(FarField<R>& F, const double2* xt, cudaStream_t s, cudaStream_t s2,
+                                 bool near_late) {
     if (n_leaves_ == 0) return;
     if (lmax_ <= lmin_) {  // one far level: nothing to overlap
         run_far_t<R, TR>(F, xt, s, -1);
@@ -824,17 +834,27 @@ void DeviceOp::run_far_overlap_t(FarField<R>& F, const double2* xt, cudaStream_t
     const bool tc = std::is_same<R, float>::value && !TR && use_tc_;
     far_s2m<R, TR>(F, xt, s);
     cudaEventRecord(ev_level_[lmax_], s);
+    if (near_late) {
+        cudaStreamWaitEvent(side_, ev_level_[lmax_], 0);
+        run_near(xt_, side_);
+        cudaEventRecord(ev_join_, side_);
+    }
     for (int p = lmax_ - 1; p >= lmin_; --p) {
         if (tc) far_m2m_tc(p, 1, s); else far_m2m<R, TR>(F, p, s);
         cudaEventRecord(ev_level_[p], s);
     }
-    for (int l = lmax_; l > lmin_; --l) {
-        cudaStreamWaitEvent(s2, ev_level_[l], 0);
-        far_m2l<R, TR>(F, l, l, s2);
+    cudaStream_t ms[2] = {s2, side3_};
+    const int nms = m2l_streams_ > 1 ? 2 : 1;
+    for (int l = lmax_, i = 0; l > lmin_; --l, ++i) {
+        cudaStream_t q = ms[i % nms];
+        cudaStreamWaitEvent(q, ev_level_[l], 0);
+        far_m2l<R, TR>(F, l, l, q);
     }
     cudaEventRecord(ev_m2l_done_, s2);
+    if (nms > 1) cudaEventRecord(ev_m2l_done2_, side3_);
     far_m2l<R, TR>(F, lmin_, lmin_, s);
     cudaStreamWaitEvent(s, ev_m2l_done_, 0);
+    if (nms > 1) cudaStreamWaitEvent(s, ev_m2l_done2_, 0);
     for (int p = lmin_; p < lmax_; ++p) {
         if (tc) far_l2l_tc(p, 1, s); else far_l2l<R, TR>(F, p, s);
     }
@@ -850,12 +870,14 @@ void DeviceOp::run_far(const double2* xt, cudaStream_t s, int stage, int prec, b
     }
 }
 
-void DeviceOp::run_far_overlap(const double2* xt, cudaStream_t s, cudaStream_t s2, int prec, bool tr) {
+void DeviceOp::run_far_overlap(const double2* xt, cudaStream_t s, cudaStream_t s2, int prec, bool tr, bool late) {
     if (prec < 0) prec = precision_;
     if (prec == kFp64) {
-        if (tr) run_far_overlap_t<double, true>(f64_, xt, s, s2); else run_far_overlap_t<double, false>(f64_, xt, s, s2);
+        if (tr) run_far_overlap_t<double, true>(f64_, xt, s, s2, late);
+        else run_far_overlap_t<double, false>(f64_, xt, s, s2, late);
     } else {
-        if (tr) run_far_overlap_t<float, true>(f32_, xt, s, s2); else run_far_overlap_t<float, false>(f32_, xt, s, s2);
+        if (tr) run_far_overlap_t<float, true>(f32_, xt, s, s2, late);
+        else run_far_overlap_t<float, false>(f32_, xt, s, s2, late);
     }
 }
 
@@ -865,7 +887,9 @@ void DeviceOp::run_near(const double2* xt, cudaStream_t s) {
         return;
     }
     k_near_sym<<<near_grid_, kSymThreads, kSymSmemBytes, s>>>(near_tiles_, n_near_tiles_, near_bz_, xt, near_slot_,
-                                                             near_part_, near_red_ptr_, near_cnt_, ynear_, err_dev_);
+                                                             near_part_, err_dev_);
+    k_near_reduce<<<blocks_for(static_cast<long long>(n_) * kReduceLanes, 256), 256, 0, s>>>(near_red_ptr_, near_part_,
+                                                                                           n_, ynear_);
 }
 
 // The tree-ordered product xt_ -> (yfar_, ynear_): near field on the side
@@ -878,10 +902,13 @@ void DeviceOp::enqueue_core(cudaStream_t s, int prec, bool tr) {
     // when some source sits in a leaf without far interactions
     if (!far_covers_all_) cudaMemsetAsync(yfar_, 0, sizeof(double2) * n_, s);
     cudaEventRecord(ev_fork_, s);
-    cudaStreamWaitEvent(side_, ev_fork_, 0);
-    run_near(xt_, side_);
-    cudaEventRecord(ev_join_, side_);
-    run_far_overlap(xt_, s, side2_, prec, tr);
+    const bool late = near_late_ && n_leaves_ > 0 && lmax_ > lmin_;
+    if (!late) {
+        cudaStreamWaitEvent(side_, ev_fork_, 0);
+        run_near(xt_, side_);
+        cudaEventRecord(ev_join_, side_);
+    }
+    run_far_overlap(xt_, s, side2_, prec, tr, late);
     cudaStreamWaitEvent(s, ev_join_, 0);
 }
 
@@ -1666,6 +1693,25 @@ std::string DeviceOp::autotune(int nr, int reps, TuneReport* rep) {
             set_near_grid(bk);
         }
         r.near_blocks_per_sm = near_per_sm_;
+        // product schedule: translation kernel (list staged or not), near field
+        // early or after S2M, one or two side streams for the finer translations
+        {
+            float bt = 1e30f;
+            int bst = m2l_staged_, bnl = near_late_ ? 1 : 0, bms = m2l_streams_;
+            for (int st : {0, 1})
+                for (int nl : {0, 1})
+                    for (int ms : {1, 2}) {
+                        m2l_staged_ = st;
+                        near_late_ = nl != 0;
+                        m2l_streams_ = ms;
+                        const float t = timed(product);
+                        if (t < bt) { bt = t; bst = st; bnl = nl; bms = ms; }
+                    }
+            m2l_staged_ = bst;
+            near_late_ = bnl != 0;
+            m2l_streams_ = bms;
+            r.schedule = bst | (bnl << 1) | ((bms - 1) << 2);
+        }
         // interpolation and anterpolation: tensor cores or CUDA cores (the
         // complex-float far field), timed on the whole product
         if (tc_ok_ && precision_ != kFp64) {

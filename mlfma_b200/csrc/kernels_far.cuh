@@ -431,6 +431,71 @@ k_m2l(const DevLevelT<R>* __restrict__ lvs, const int4* __restrict__ items, int 
     Bo[1] = cscale(w, cadd(a1, c1));
 }
 
+// The same translation with the box's list 2 (source boxes, offset ids)
+// staged in shared memory first, so the inner loop's loads of patterns and
+// transfer values depend on nothing but shared memory and U of them are in
+// flight at once.
+constexpr int kM2LStage = 256;  // list entries staged per round (list 2 holds at most 189)
+
+template <class R, bool TR>
+__global__ void __launch_bounds__(128)
+k_m2l_staged(const DevLevelT<R>* __restrict__ lvs, const int4* __restrict__ items, int zero_empty) {
+    using C = typename Cx<R>::T;
+    constexpr int U = sizeof(R) == 4 ? 8 : 6;
+    __shared__ int s_src[kM2LStage], s_off[kM2LStage];
+    const int4 it = items[blockIdx.x];  // level, box, first direction, count
+    const DevLevelT<R> lv = lvs[it.x];
+    const int b = it.y, ndir = lv.ndir;
+    const bool live = static_cast<int>(threadIdx.x) < it.w;
+    const int d = it.z + (live ? threadIdx.x : 0);
+    const int p0 = lv.m2l_ptr[b], p1 = lv.m2l_ptr[b + 1];
+    C* Bo = lv.B + (static_cast<size_t>(b) * ndir + d) * 2;
+    if (p0 == p1) {
+        if (zero_empty && live) { Bo[0] = zero<C>(); Bo[1] = zero<C>(); }
+        return;
+    }
+    C a0 = zero<C>(), a1 = zero<C>(), c0 = zero<C>(), c1 = zero<C>();
+    for (int base = p0; base < p1; base += kM2LStage) {
+        const int cnt = min(kM2LStage, p1 - base);
+        __syncthreads();
+        for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
+            s_src[i] = lv.m2l_src[base + i];
+            const int o = lv.m2l_off[base + i];
+            s_off[i] = TR ? 315 - o : o;
+        }
+        __syncthreads();
+        if (!live) continue;
+        int p = 0;
+        for (; p + U <= cnt; p += U) {
+            C t[U], xa[U], xb[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                t[u] = lv.transl[static_cast<size_t>(s_off[p + u]) * ndir + d];
+                const C* As = lv.A + (static_cast<size_t>(s_src[p + u]) * ndir + d) * 2;
+                xa[u] = As[0];
+                xb[u] = As[1];
+            }
+#pragma unroll
+            for (int u = 0; u < U; u += 2) {
+                a0 = cfma(t[u], xa[u], a0);
+                a1 = cfma(t[u], xb[u], a1);
+                c0 = cfma(t[u + 1], xa[u + 1], c0);
+                c1 = cfma(t[u + 1], xb[u + 1], c1);
+            }
+        }
+        for (; p < cnt; ++p) {
+            const C t0 = lv.transl[static_cast<size_t>(s_off[p]) * ndir + d];
+            const C* A0 = lv.A + (static_cast<size_t>(s_src[p]) * ndir + d) * 2;
+            a0 = cfma(t0, A0[0], a0);
+            a1 = cfma(t0, A0[1], a1);
+        }
+    }
+    if (!live) return;
+    const R w = lv.w[d];
+    Bo[0] = cscale(w, cadd(a0, c0));
+    Bo[1] = cscale(w, cadd(a1, c1));
+}
+
 // ------------------------------------------------------------ L2L
 // child local += Anterp[shift(parent local)]: shift on the parent grid, then
 // the transposed phi pass, then the transposed theta pass with pole

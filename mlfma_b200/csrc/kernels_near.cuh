@@ -34,8 +34,8 @@ namespace {
 // sums, 64 the column sums (two threads per row or column when the tile has
 // at most 32; the diagonal of a self tile counts once, in its row), release the
 // stage on its "empty" mbarrier and write the partials to their slots.
-// Each target's consecutive slots are then added in a fixed order by the thread
-// that completes them (below): a deterministic product.  HBM traffic: the block entries once (half
+// k_near_reduce then adds each target's consecutive slots in a fixed order: no
+// atomics, a deterministic product.  HBM traffic: the block entries once (half
 // the block-row form), x from L2.
 //
 // Every mbarrier wait is bounded (about a second).  A consumer group that gives
@@ -88,15 +88,9 @@ __device__ __forceinline__ void consumers_sync() {
     asm volatile("bar.sync 1, %0;" ::"n"(kSymConsumers) : "memory");
 }
 
-// The per-target sums are fused into the tile kernel: every target counts
-// its arriving partials (cnt[t], zero between products); the thread that
-// writes a target's last partial sums that target's slots in slot order (a
-// fixed order: the product stays deterministic), writes y[t] and resets the
-// count.  A target without near-field entries keeps the zero written at setup.
 __global__ void __launch_bounds__(kSymThreads, 4)
 k_near_sym(const DevNearTile* __restrict__ tiles, int ntiles, const double2* __restrict__ Z,
            const double2* __restrict__ x, const int* __restrict__ slots, double2* __restrict__ part,
-           const int* __restrict__ red_ptr, int* __restrict__ cnt, double2* __restrict__ y,
            int* __restrict__ err) {
     extern __shared__ __align__(128) unsigned char sym_smem[];
     double2* stages = reinterpret_cast<double2*>(sym_smem);
@@ -267,25 +261,35 @@ k_near_sym(const DevNearTile* __restrict__ tiles, int ntiles, const double2* __r
         }
         consumers_sync();  // stage s read, partial halves complete
         if (ct == 0) mbar_arrive(smem_addr(&empty[s]));
-        if (my_slot >= 0) {
+        if (my_slot >= 0)
             part[my_slot] = ct < 64 ? cadd(rowp[b][0][idx], rowp[b][1][idx]) : cadd(colp[b][0][idx], colp[b][1][idx]);
-            const int tgt = ct < 64 ? T.r0 + T.i0 + idx : T.c0 + T.j0 + idx;
-            const int p0 = red_ptr[tgt], p1 = red_ptr[tgt + 1];
-            __threadfence();
-            if (atomicAdd(cnt + tgt, 1) == p1 - p0 - 1) {  // the target's last partial
-                __threadfence();
-                double2 a0 = z0(), a1 = z0();
-                int p = p0;
-                for (; p + 1 < p1; p += 2) {
-                    a0 = cadd(a0, __ldcg(part + p));
-                    a1 = cadd(a1, __ldcg(part + p + 1));
-                }
-                if (p < p1) a0 = cadd(a0, __ldcg(part + p));
-                y[tgt] = cadd(a0, a1);
-                cnt[tgt] = 0;
-            }
-        }
     }
+}
+
+// y[t] = sum of target t's consecutive partial slots: eight lanes per target,
+// a fixed shuffle tree, so the order never changes.
+constexpr int kReduceLanes = 8;
+
+__global__ void k_near_reduce(const int* __restrict__ ptr, const double2* __restrict__ part, int n,
+                              double2* __restrict__ y) {
+    const long long g = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int t = static_cast<int>(g / kReduceLanes);
+    const int l = static_cast<int>(g % kReduceLanes);
+    double2 acc = z0();
+    if (t < n) {
+        const int p0 = ptr[t] + l, p1 = ptr[t + 1];
+        double2 v[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) v[u] = p0 + u * kReduceLanes < p1 ? part[p0 + u * kReduceLanes] : z0();
+        acc = cadd(cadd(v[0], v[1]), cadd(v[2], v[3]));
+        for (int p = p0 + 4 * kReduceLanes; p < p1; p += kReduceLanes) acc = cadd(acc, part[p]);
+    }
+#pragma unroll
+    for (int o = kReduceLanes / 2; o > 0; o >>= 1) {
+        acc.x += __shfl_xor_sync(0xffffffffu, acc.x, o);
+        acc.y += __shfl_xor_sync(0xffffffffu, acc.y, o);
+    }
+    if (t < n && l == 0) y[t] = acc;
 }
 
 // ------------------------------------------------------------ setup kernels

@@ -112,8 +112,12 @@ __device__ __forceinline__ void tc_stage4(unsigned char* a_hi, unsigned char* a_
         lp[u] = tf32_rna(v[u] - __uint_as_float(hp[u]));
     }
     const uint32_t o = tc_a_offset(m, kq, kc_max);
-    *reinterpret_cast<uint4*>(a_hi + o) = h;
-    *reinterpret_cast<uint4*>(a_lo + o) = l;
+    // explicit shared-memory stores: the global loads of the next values need
+    // not wait for them (volatile asm keeps them ordered with the fences)
+    asm volatile("st.shared.v4.u32 [%0], {%1, %2, %3, %4};" ::"r"(smem_addr(a_hi) + o), "r"(h.x), "r"(h.y), "r"(h.z),
+                 "r"(h.w));
+    asm volatile("st.shared.v4.u32 [%0], {%1, %2, %3, %4};" ::"r"(smem_addr(a_lo) + o), "r"(l.x), "r"(l.y), "r"(l.z),
+                 "r"(l.w));
 }
 
 // One thread: the 3xTF32 MMAs of a staged chunk, D (+)= A_chunk W_chunk^T with
@@ -186,12 +190,14 @@ k_tc_pass(TcArgs a, int* __restrict__ err) {
         const TcItem it = tc_item<KIND>(a, r);
         for (int k0 = 0; k0 < a.Kpad && ok; k0 += kTcKChunk) {
             const int kc = min(kTcKChunk, a.Kpad - k0);
-            // this row's contraction values of the chunk, four at a time, split hi + lo
-            for (int kq = 0; kq < kc / 4; ++kq) {
-                float v[4];
+            // this row's contraction values of the chunk, eight at a time (all
+            // their loads in flight together), split hi + lo
+            for (int kq = 0; kq < kc / 4; kq += 2) {
+                float v[8];
 #pragma unroll
-                for (int u = 0; u < 4; ++u) v[u] = tc_load<KIND>(a, r, k0 + 4 * kq + u, krow_s, it);
+                for (int u = 0; u < 8; ++u) v[u] = tc_load<KIND>(a, r, k0 + 4 * kq + u, krow_s, it);
                 tc_stage4(a_hi, a_lo, tid, kq, kc_max, v);
+                tc_stage4(a_hi, a_lo, tid, kq + 1, kc_max, v + 4);
             }
             fence_async_smem();
             tc_fence_before();
@@ -216,10 +222,21 @@ k_tc_pass(TcArgs a, int* __restrict__ err) {
         for (int i0 = 0; i0 < a.Npad; i0 += 16) {
             float v[16];
             tmem_ld16(lane_addr + i0, v);
-            if (r.live)
+            if (r.live) {
+                if (KIND == kTcThetaT) {
+                    // accumulated outputs: every old value loaded before the stores
+                    float old[16];
 #pragma unroll
-                for (int u = 0; u < 16; ++u)
-                    if (i0 + u < a.N) tc_store<KIND>(a, r, i0 + u, v[u], it);
+                    for (int u = 0; u < 16; ++u) old[u] = i0 + u < a.N ? tc_peek_out(a, r, i0 + u, it) : 0.f;
+#pragma unroll
+                    for (int u = 0; u < 16; ++u)
+                        if (i0 + u < a.N) tc_put_out(a, r, i0 + u, old[u] + v[u], it);
+                } else {
+#pragma unroll
+                    for (int u = 0; u < 16; ++u)
+                        if (i0 + u < a.N) tc_store<KIND>(a, r, i0 + u, v[u], it);
+                }
+            }
         }
         tc_fence_before();
         __syncthreads();  // TMEM read and the A tile free before the next tile's MMAs

@@ -162,6 +162,18 @@ MLFMA_HD void tc_store(const TcArgs& a, const TcRow& r, int i, float v, const Tc
     }
 }
 
+// THETA_T's output (child B at theta i, phi j), read and written separately
+// so that a row's loads can all be in flight before its stores.
+MLFMA_HD size_t tc_out_index_thetaT(const TcArgs& a, const TcRow& r, int i, const TcItem& it) {
+    return (static_cast<size_t>(it.box) * a.mth * a.mph + static_cast<size_t>(i) * a.mph + r.j) * 4 * a.nr + r.q;
+}
+MLFMA_HD float tc_peek_out(const TcArgs& a, const TcRow& r, int i, const TcItem& it) {
+    return reinterpret_cast<const float*>(a.pat_out)[tc_out_index_thetaT(a, r, i, it)];
+}
+MLFMA_HD void tc_put_out(const TcArgs& a, const TcRow& r, int i, float v, const TcItem& it) {
+    reinterpret_cast<float*>(a.pat_out)[tc_out_index_thetaT(a, r, i, it)] = v;
+}
+
 // Shared-memory byte offset of the four contraction values [4 kq, 4 kq + 4)
 // of tile row m within the staged chunk: K-major without swizzle, core
 // matrices of 8 rows x 16 bytes, the chunk's 16-byte K pieces of one 8-row

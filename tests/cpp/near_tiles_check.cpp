@@ -2,8 +2,8 @@
 // the index arithmetic the near-field kernels apply to it (kernels_near.cuh):
 // k_near_blocks_assemble's decoding of packed self blocks, k_near_sym's bulk
 // copies (source and destination ranges, expected byte counts), its row and
-// column sums over the stage, the partial slots, and the sum of each target's
-// slots.  Every stored entry must land in exactly one tile, every read must hit
+// column sums over the stage, the partial slots, and k_near_reduce's sums per
+// target.  Every stored entry must land in exactly one tile, every read must hit
 // a copied value, every partial must be written once, and the result must equal
 // the block-row form (each leaf's rows against all the sources it meets) on a
 // symmetric synthetic entry.  Run by tests/test_near_tiles.py.

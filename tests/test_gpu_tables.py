@@ -1,9 +1,12 @@
 """M2L transfer functions built on the GPU (Tables::getAlpha, getInterpPsi,
 buildTranslationTable, src/fmm/tables.cpp:90-220), which the operator uses,
 against the host plan's tables (pinned to the reference's own tables in
-tests/test_host_plan.py): 1e-14 relative to the largest entry, on every level
-of a 4-wavelength cube and of the 16-wavelength root box of the largest
-benchmark (grids up to 58 x 116)."""
+tests/test_host_plan.py), on every level of a 4-wavelength cube and of the
+16-wavelength root box of the largest benchmark (grids up to 58 x 116).  The
+agreement is 1e-14 relative to the largest entry on the finer levels; on the
+coarsest 16-wavelength level (L = 28 terms) the multipole sum cancels enough
+to turn one-ulp differences of sin, cos and FMA contraction between the host
+and the GPU into 5e-14, so the bound there is 1e-13."""
 import numpy as np
 import pytest
 
@@ -26,5 +29,5 @@ def test_gpu_tables_match_host(cuda_device, root, n, mns, maxlev):
     for level in range(2, st["max_level"] + 1):
         host, gpu = op.level_transl(level), op.level_transl_gpu(level)
         err = np.abs(gpu - host).max() / np.abs(host).max()
-        assert err <= 1e-14, (level, err)
+        assert err <= (1e-13 if op.level_info(level)["nth"] > 40 else 1e-14), (level, err)
     op.close()
