@@ -844,7 +844,9 @@ void DeviceOp::run_far_overlap_t(FarField<R>& F, const double2* xt, cudaStream_t
         cudaEventRecord(ev_level_[p], s);
     }
     cudaStream_t ms[2] = {s2, side3_};
-    const int nms = m2l_streams_ > 1 ? 2 : 1;
+    // the second stream only when it gets a level (an event recorded on a
+    // stream outside a capture cannot be waited on inside it)
+    const int nms = m2l_streams_ > 1 && lmax_ - lmin_ >= 2 ? 2 : 1;
     for (int l = lmax_, i = 0; l > lmin_; --l, ++i) {
         cudaStream_t q = ms[i % nms];
         cudaStreamWaitEvent(q, ev_level_[l], 0);
@@ -1458,14 +1460,21 @@ std::string DeviceOp::setup_tc(const Plan& plan) {
                           reinterpret_cast<const void*>(k_tc_pass<kTcPhi>),
                           reinterpret_cast<const void*>(k_tc_pass<kTcPhiT>),
                           reinterpret_cast<const void*>(k_tc_pass<kTcThetaT>)};
+    int sm_bytes = 0, sm_regs = 0;
+    MLFMA_CK(cudaDeviceGetAttribute(&sm_bytes, cudaDevAttrMaxSharedMemoryPerMultiprocessor, device_));
+    MLFMA_CK(cudaDeviceGetAttribute(&sm_regs, cudaDevAttrMaxRegistersPerMultiprocessor, device_));
     for (int p = lmin_; p < lmax_; ++p)
         for (int k = 0; k < 4; ++k) {
-            // persistent CTAs: as many per SM as shared memory and the 512
-            // tensor-memory columns of an SM allow
+            // persistent CTAs: as many per SM as shared memory (with the 1 KB
+            // each block reserves), registers, warps and the 512 tensor-memory
+            // columns of an SM allow
             TcTrans& t = tc_[p];
-            int occ = 0;
-            MLFMA_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fns[k], kTcThreads, static_cast<int>(t.smem[k])));
-            occ = std::max(1, std::min(occ, 512 / ncols_of(t.Npad[k])));
+            cudaFuncAttributes fa{};
+            MLFMA_CK(cudaFuncGetAttributes(&fa, fns[k]));
+            MLFMA_CK(cudaFuncSetAttribute(fns[k], cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+            const int by_smem = sm_bytes / static_cast<int>(t.smem[k] + fa.sharedSizeBytes + 1024);
+            const int by_regs = sm_regs / std::max(1, fa.numRegs * kTcThreads);
+            const int occ = std::max(1, std::min({by_smem, by_regs, 64 / (kTcThreads / 32), 512 / ncols_of(t.Npad[k])}));
             t.grid[k] = occ * sms_;
         }
     tc_ok_ = true;

@@ -38,7 +38,7 @@ def problem():
 def test_vjp_full_size_matches_finite_differences(cuda_device, problem):
     op, z, kh, pws, w = problem
     J, gz, gw, _, infos = op.vjp_farfield_power(pws, w, kh, max_iter=8000, tol=1e-11, restart=200)
-    assert infos[0].converged and infos[1].converged
+    assert infos[0].true_residual <= 1e-11 and infos[1].true_residual <= 1e-11  # forward and adjoint solves
     B = [op.rhs_planewave(p) for p in pws]
 
     def J_of(zz, ww):
