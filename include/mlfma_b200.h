@@ -110,6 +110,10 @@ typedef struct {
                             iterations counts inner products, refinements outer products.
                             No counterpart in the reference. */
     int inner_iters;     /* flexible: GMRES iterations per inner solve (0 = 20) */
+    int precond;         /* 1: leaf block-Jacobi right preconditioner (each leaf's diagonal block of
+                            A, loads included, inverted on the GPU; with flexible = 1 it
+                            preconditions the inner solves).  Forward solves; no counterpart in
+                            the reference. */
 } mlfma_solver_opts;
 
 typedef struct {
@@ -331,13 +335,15 @@ int mlfma_autotune(mlfma_handle h, int nrhs, int reps, mlfma_tuning* out);
  * addAnterpCoeffs, stem.cpp:109-244) of the complex-float far field on the
  * tensor cores: every box of a level at once as separable theta and phi
  * contractions (tcgen05 MMAs, split-precision 3xTF32, FP32 accumulation),
- * children shifted and summed before the interpolation.  mode bit 0: the
- * one-vector product, bit 1: the many-right-hand-side product; 0 = the
- * CUDA-core kernels (the default); mlfma_autotune times both and keeps the
- * faster.  Products of the FP64 far field and
- * transposed products always use the CUDA-core kernels.  MLFMA_ERR_ARG when
- * the operator has no complex-float far field or a grid exceeds the kernels'
- * shared memory.  Results agree with the CUDA-core kernels to float rounding. */
+ * children shifted and summed before the interpolation.  mode bit 0: M2M of
+ * the one-vector product, bit 1: M2M of the many-right-hand-side product,
+ * bit 2: L2L of the one-vector product, bit 3: L2L of the many-rhs product;
+ * 0 = the CUDA-core kernels (the default); mlfma_autotune times both kernel
+ * families stage by stage and keeps the faster.  Products of the FP64 far
+ * field and transposed products always use the CUDA-core kernels.
+ * MLFMA_ERR_ARG when the operator has no complex-float far field or a grid
+ * exceeds the kernels' shared memory.  Results agree with the CUDA-core
+ * kernels to float rounding. */
 int mlfma_set_interp_path(mlfma_handle h, int mode);
 int mlfma_get_interp_path(mlfma_handle h, int* mode);
 

@@ -232,16 +232,19 @@ class MLFMA:
 
     def solve(self, b=None, max_iter: int = 500, tol: float = 1e-6, restart: int = 0,
               ref_givens: bool = True, raise_on_fail: bool = False, refine: bool = False, inner_tol: float = 0.0,
-              flexible: bool = False, inner_iters: int = 0):
+              flexible: bool = False, inner_iters: int = 0, precond: bool = False):
         """GMRES (Solver::solve).  On a mixed operator, refine=True runs
         iterative refinement: inner GMRES on the mixed operator, outer FP64
         residual; tol then holds for the FP64 residual.  flexible=True runs
         FGMRES(restart): FP64 outer Krylov space, each outer step preconditioned
-        by inner_iters GMRES iterations on the operator's own far field."""
+        by inner_iters GMRES iterations on the operator's own far field.
+        precond=True: leaf block-Jacobi right preconditioning (of the inner
+        solves when flexible)."""
         bv = self.rhs() if b is None else _cvec(b, self.n)
         x = np.zeros(self.n, dtype=np.complex128)
         o = SolverOpts(max_iter=max_iter, tol=tol, restart=restart, ref_givens=int(ref_givens),
-                       refine=int(refine), inner_tol=inner_tol, flexible=int(flexible), inner_iters=inner_iters)
+                       refine=int(refine), inner_tol=inner_tol, flexible=int(flexible), inner_iters=inner_iters,
+                       precond=int(precond))
         info = SolveInfo()
         code = lib().mlfma_gmres(self._h, bv.view(np.float64).ctypes.data_as(_dp),
                                  x.view(np.float64).ctypes.data_as(_dp), ctypes.byref(o), ctypes.byref(info))
@@ -405,8 +408,9 @@ class MLFMA:
     @property
     def interp_path(self) -> int:
         """Interpolation/anterpolation kernels of the complex-float far field
-        (mlfma_set_interp_path): bit 0 tensor cores for one vector, bit 1 for
-        many right-hand sides; 0 = CUDA cores."""
+        (mlfma_set_interp_path) on the tensor cores: bit 0 M2M one vector,
+        bit 1 M2M many right-hand sides, bit 2 L2L one vector, bit 3 L2L many;
+        0 = CUDA cores."""
         m = ctypes.c_int()
         check(lib().mlfma_get_interp_path(self._h, ctypes.byref(m)))
         return m.value

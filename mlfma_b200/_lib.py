@@ -56,7 +56,7 @@ class Traffic(ctypes.Structure):
 class SolverOpts(ctypes.Structure):
     _fields_ = [("max_iter", ctypes.c_int), ("tol", ctypes.c_double), ("restart", ctypes.c_int),
                 ("ref_givens", ctypes.c_int), ("refine", ctypes.c_int), ("inner_tol", ctypes.c_double),
-                ("flexible", ctypes.c_int), ("inner_iters", ctypes.c_int)]
+                ("flexible", ctypes.c_int), ("inner_iters", ctypes.c_int), ("precond", ctypes.c_int)]
 
 
 class SolveInfo(ctypes.Structure):

@@ -260,6 +260,7 @@ int mlfma_gmres(mlfma_handle h, const double* b, double* x, const mlfma_solver_o
         o.inner_tol = opts->inner_tol;
         o.flexible = opts->flexible;
         o.inner_iters = opts->inner_iters;
+        o.precond = opts->precond;
     }
     const size_t bytes = sizeof(double2) * h->plan.n;
     cudaStream_t s = h->dev->stream();
@@ -394,9 +395,11 @@ int mlfma_gmres_noalloc(mlfma_handle h, const void* d_b, void* d_x, const mlfma_
         o.inner_tol = opts->inner_tol;
         o.flexible = opts->flexible;
         o.inner_iters = opts->inner_iters;
+        o.precond = opts->precond;
     }
     if (o.max_iter < 1 || o.restart < 0) return fail(MLFMA_ERR_ARG, "max_iter and restart must be positive");
-    if (o.flexible) return fail(MLFMA_ERR_ARG, "the flexible solve needs its own workspace (use mlfma_gmres)");
+    if (o.flexible || o.precond)
+        return fail(MLFMA_ERR_ARG, "flexible and preconditioned solves need their own workspace (use mlfma_gmres)");
     if (cudaSetDevice(h->device) != cudaSuccess) return fail(MLFMA_ERR_CUDA, "cudaSetDevice failed");
     if (!h->gmres_fixed) h->gmres_fixed = std::make_unique<mlfma::Gmres>();
     const int m = o.restart > 0 ? o.restart : o.max_iter;
@@ -481,8 +484,10 @@ int mlfma_gmres_multi(mlfma_handle h, int nrhs, const double* b, double* x, cons
         o.inner_tol = opts->inner_tol;
         o.flexible = opts->flexible;
         o.inner_iters = opts->inner_iters;
+        o.precond = opts->precond;
     }
-    if (o.flexible) return fail(MLFMA_ERR_ARG, "flexible GMRES runs one right-hand side at a time (mlfma_gmres)");
+    if (o.flexible || o.precond)
+        return fail(MLFMA_ERR_ARG, "flexible and preconditioned GMRES run one right-hand side at a time (mlfma_gmres)");
     if (cudaSetDevice(h->device) != cudaSuccess) return fail(MLFMA_ERR_CUDA, "cudaSetDevice failed");
     int code = ensure_multi_staging(h);
     if (code != MLFMA_OK) return code;
@@ -575,6 +580,7 @@ static mlfma::SolveOpts to_opts(const mlfma_solver_opts* opts) {
         o.inner_tol = opts->inner_tol;
         o.flexible = opts->flexible;
         o.inner_iters = opts->inner_iters;
+        o.precond = opts->precond;
     }
     return o;
 }

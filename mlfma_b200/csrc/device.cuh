@@ -110,6 +110,14 @@ struct DevNearTile {
 // on) on the current device's default stream.
 void launch_wait_runs_out(long long limit, int* status);
 
+// A leaf of the block-Jacobi preconditioner: its sources [row0, row0 + nb)
+// (tree order), its stored self block (entry offset, kind 1 strict lower or 2
+// with the diagonal; zoff < 0: none) and its inverse's offset.
+struct DevBjLeaf {
+    int row0, nb, kind, pad;
+    long long zoff, ioff;
+};
+
 struct DevNearRow {
     int row0, nrow, ncol, pad;
     long long off, col_off;
@@ -268,8 +276,16 @@ public:
     // tensor cores (bit 0: one right-hand side, bit 1: many); false when the
     // operator has no complex-float far field or a grid is too large for them.
     bool tc_available() const { return tc_ok_; }
+    // mode bit 0: one-vector M2M, bit 1: many-rhs M2M, bit 2: one-vector L2L,
+    // bit 3: many-rhs L2L on the tensor cores.
     std::string set_tc(int mode);
-    int tc_mode() const { return (use_tc_ ? 1 : 0) | (use_tc_multi_ ? 2 : 0); }
+    int tc_mode() const { return tc_mode_; }
+
+    // Leaf block-Jacobi right preconditioner M (the diagonal blocks of A,
+    // loads included): built for the current loads on first use; y = M^{-1} x
+    // on tree-ordered device vectors.
+    std::string bj_prepare();
+    void bj_apply(const double2* x, double2* y, cudaStream_t s);
 
     // The level's FP64 transfer functions as built on the GPU, [316][ndir].
     std::string copy_transl(int level, double2* host);
@@ -412,8 +428,14 @@ private:
     float* tc_scratch_ = nullptr;       // intermediate of the two passes of a stage
     size_t tc_scratch_floats_ = 0;
     bool tc_ok_ = false;
-    bool use_tc_ = false, use_tc_multi_ = false;
+    int tc_mode_ = 0;  // see set_tc
     int generation_ = 0;
+    // Leaf block-Jacobi preconditioner
+    std::vector<DevBjLeaf> h_bj_;
+    DevBjLeaf* bj_leaves_ = nullptr;
+    int* bj_ok_ = nullptr;
+    double2* bj_inv_ = nullptr;
+    int bj_gen_ = -1;
     double2 ck_{};             // Phys::C * k
     double2* loads_ = nullptr; // diagonal loads, tree order
     bool has_loads_ = false;

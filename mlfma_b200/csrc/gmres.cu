@@ -291,6 +291,7 @@ std::string Gmres::ensure(int n, int ncols, int extra) {
     GM_CK(cudaMalloc(&y_, sizeof(double2) * (ncols + 1)));
     GM_CK(cudaMalloc(&partial_, sizeof(double2) * static_cast<size_t>(nchunks_) * (ncols + 1)));
     GM_CK(cudaMalloc(&npartial_, sizeof(double) * nchunks_));
+    GM_CK(cudaMalloc(&tq_, sizeof(double2) * n));
     if (extra >= 2) {
         GM_CK(cudaMalloc(&xo_, sizeof(double2) * n));
         GM_CK(cudaMalloc(&bo_, sizeof(double2) * n));
@@ -323,7 +324,9 @@ void Gmres::release_steps() {
 // changes).
 std::string Gmres::step_graph(DeviceOp& op, int prec) {
     const int adj = adj_ ? 1 : 0;
-    if (sgx_ && sg_op_ == &op && sg_prec_ == prec && sg_adj_ == adj && sg_gen_ == op.generation() && sg_q_ == Q_)
+    const int pc = pc_ ? 1 : 0;
+    if (sgx_ && sg_op_ == &op && sg_prec_ == prec && sg_adj_ == adj && sg_gen_ == op.generation() && sg_q_ == Q_ &&
+        sg_pc_ == pc)
         return {};
     if (sgx_) cudaGraphExecDestroy(sgx_);
     if (sg_) cudaGraphDestroy(sg_);
@@ -333,7 +336,12 @@ std::string Gmres::step_graph(DeviceOp& op, int prec) {
     StepStateD* st = static_cast<StepStateD*>(st_);
     const int n = n_, ldh = cap_ + 1;
     GM_CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-    k_step_prep<<<nblk(n, 256), 256, 0, s>>>(st, Q_, w_, op.input_buffer(), n, adj);
+    if (pc) {  // the product's input is M^{-1} q_k
+        k_step_prep<<<nblk(n, 256), 256, 0, s>>>(st, Q_, w_, tq_, n, 0);
+        op.bj_apply(tq_, op.input_buffer(), s);
+    } else {
+        k_step_prep<<<nblk(n, 256), 256, 0, s>>>(st, Q_, w_, op.input_buffer(), n, adj);
+    }
     op.enqueue_apply_from_input(w_, s, prec, adj_);
     for (int pass = 0; pass < 2; ++pass) {
         k_step_dots<<<dim3(nchunks_, cap_), kDotThreads, 0, s>>>(st, Q_, n, w_, partial_, nchunks_, tco_, hcols_, ldh,
@@ -348,6 +356,7 @@ std::string Gmres::step_graph(DeviceOp& op, int prec) {
     sg_adj_ = adj;
     sg_gen_ = op.generation();
     sg_q_ = Q_;
+    sg_pc_ = pc;
     return {};
 }
 
@@ -355,9 +364,9 @@ void Gmres::release() {
     release_steps();
     if (!external_)
         for (void* p : {(void*)Q_, (void*)w_, (void*)b_, (void*)x_, (void*)r_, (void*)h_, (void*)y_,
-                        (void*)partial_, (void*)npartial_, (void*)xo_, (void*)bo_})
+                        (void*)partial_, (void*)npartial_, (void*)xo_, (void*)bo_, (void*)tq_})
             if (p) cudaFree(p);
-    Q_ = w_ = b_ = x_ = r_ = h_ = y_ = partial_ = xo_ = bo_ = nullptr;
+    Q_ = w_ = b_ = x_ = r_ = h_ = y_ = partial_ = xo_ = bo_ = tq_ = nullptr;
     npartial_ = nullptr;
     n_ = cap_ = extra_ = 0;
 }
@@ -538,7 +547,12 @@ std::string Gmres::cycles(DeviceOp& op, int prec, const SolveOpts& o, double bno
             GM_CK(cudaMemcpyAsync(r_, b_, sizeof(double2) * n, cudaMemcpyDeviceToDevice, s));
             beta = bnorm;
         } else {
-            apply(op, x_, w_, s, prec);
+            if (pc_) {  // x_ holds u with x = M^{-1} u
+                op.bj_apply(x_, tq_, s);
+                apply(op, tq_, w_, s, prec);
+            } else {
+                apply(op, x_, w_, s, prec);
+            }
             k_sub<<<nblk(n, 256), 256, 0, s>>>(b_, w_, r_, n);
             err = norm(r_, s, &beta);
             if (!err.empty()) return err;
@@ -626,7 +640,12 @@ std::string Gmres::cycles(DeviceOp& op, int prec, const SolveOpts& o, double bno
         } else {
             for (; k < m && total < max_iter; ++k) {
                 double2* qk = Q_ + static_cast<long long>(k) * n;
-                apply(op, qk, w_, s, prec);  // w = A q_k
+                if (pc_) {  // w = A M^{-1} q_k
+                    op.bj_apply(qk, tq_, s);
+                    apply(op, tq_, w_, s, prec);
+                } else {
+                    apply(op, qk, w_, s, prec);  // w = A q_k
+                }
                 err = cgs_pass(k + 1, s, false);
                 if (!err.empty()) return err;
                 err = cgs_pass(k + 1, s, true);
@@ -666,6 +685,11 @@ std::string Gmres::cycles(DeviceOp& op, int prec, const SolveOpts& o, double bno
         GM_CK(cudaStreamSynchronize(s));
         if (o.restart <= 0) break;  // unrestarted: one cycle (the reference)
     }
+    if (pc_) {  // back from the preconditioned space: x = M^{-1} u
+        op.bj_apply(x_, tq_, s);
+        GM_CK(cudaMemcpyAsync(x_, tq_, sizeof(double2) * n, cudaMemcpyDeviceToDevice, s));
+        GM_CK(cudaStreamSynchronize(s));
+    }
     *iters = total;
     *resid = last;
     *conv = converged;
@@ -676,6 +700,13 @@ std::string Gmres::solve(DeviceOp& op, const double2* d_b_user, double2* d_x_use
                          SolveResult* res) {
     if (o.adjoint && op.ref_compat()) return "arg:the adjoint needs ref_compat = 0";
     adj_ = o.adjoint != 0;
+    pc_ = o.precond != 0;
+    if (pc_) {
+        if (adj_) return "arg:the block-Jacobi preconditioner serves forward solves";
+        if (external_) return "arg:the preconditioned solve needs its own workspace (use mlfma_gmres)";
+        const std::string e = op.bj_prepare();
+        if (!e.empty()) return e;
+    }
     if (o.flexible) {
         if (external_) return "arg:the flexible solve needs its own workspace (use mlfma_gmres)";
         return solve_flexible(op, d_b_user, d_x_user, o, res);

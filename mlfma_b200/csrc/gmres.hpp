@@ -21,6 +21,7 @@ struct SolveOpts {
     int adjoint = 0;       // solve A^H x = b (operator set up with ref_compat = 0)
     int flexible = 0;      // FGMRES: FP64 outer Krylov space over inner GMRES solves
     int inner_iters = 0;   // flexible: iterations per inner solve (0 = 20)
+    int precond = 0;       // 1: leaf block-Jacobi right preconditioner (DeviceOp::bj_*)
 };
 
 struct SolveResult {
@@ -81,7 +82,9 @@ private:
     cudaGraph_t sg_ = nullptr;
     cudaGraphExec_t sgx_ = nullptr;
     const DeviceOp* sg_op_ = nullptr;
-    int sg_prec_ = -1, sg_adj_ = -1, sg_gen_ = -1;
+    int sg_prec_ = -1, sg_adj_ = -1, sg_gen_ = -1, sg_pc_ = -1;
+    bool pc_ = false;            // right preconditioning in this solve
+    double2* tq_ = nullptr;      // preconditioner scratch vector
     const double2* sg_q_ = nullptr;
 
     int n_ = 0, cap_ = 0, extra_ = 0, nchunks_ = 0;

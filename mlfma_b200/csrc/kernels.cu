@@ -670,6 +670,25 @@ std::string DeviceOp::setup(const Plan& plan, int device, int precision, int max
                 MLFMA_CK(cudaGetLastError());
             }
         }
+        // leaves of the block-Jacobi preconditioner (built on first use)
+        {
+            std::vector<long long> self_off(n_ + 1, -1);
+            std::vector<int> self_kind(n_ + 1, 0);
+            for (const NearBlock& b : plan.near_blocks)
+                if (b.self) {
+                    self_off[b.row0] = b.off;
+                    self_kind[b.row0] = plan.cfg.self_terms ? 2 : 1;
+                }
+            h_bj_.clear();
+            long long ioff = 0;
+            for (int id : plan.leaves) {
+                const Node& nd = plan.nodes[id];
+                if (nd.src_count <= 0) continue;
+                DevBjLeaf L{nd.src_begin, nd.src_count, self_kind[nd.src_begin], 0, self_off[nd.src_begin], ioff};
+                if (L.nb <= kBjMax) ioff += static_cast<long long>(L.nb) * L.nb;
+                h_bj_.push_back(L);
+            }
+        }
         // many right-hand sides: block rows (both orientations), gather-only GEMM tiles
         if (max_rhs > 1) {
             std::vector<DevNearRow> nr;
@@ -800,16 +819,17 @@ void DeviceOp::far_l2t(FarField<R>& F, cudaStream_t s) {
 template <class R, bool TR>
 void DeviceOp::run_far_t(FarField<R>& F, const double2* xt, cudaStream_t s, int stage) {
     if (n_leaves_ == 0) return;
-    const bool tc = std::is_same<R, float>::value && !TR && use_tc_;
+    const bool tcf = std::is_same<R, float>::value && !TR;
+    const bool tc_up = tcf && (tc_mode_ & 1), tc_dn = tcf && (tc_mode_ & 4);
     if (stage < 0 || stage == 0) far_s2m<R, TR>(F, xt, s);
     if (stage < 0 || stage == 1)
         for (int p = lmax_ - 1; p >= lmin_; --p) {
-            if (tc) far_m2m_tc(p, 1, s); else far_m2m<R, TR>(F, p, s);
+            if (tc_up) far_m2m_tc(p, 1, s); else far_m2m<R, TR>(F, p, s);
         }
     if (stage < 0 || stage == 2) far_m2l<R, TR>(F, lmin_, lmax_, s);
     if (stage < 0 || stage == 3)
         for (int p = lmin_; p < lmax_; ++p) {
-            if (tc) far_l2l_tc(p, 1, s); else far_l2l<R, TR>(F, p, s);
+            if (tc_dn) far_l2l_tc(p, 1, s); else far_l2l<R, TR>(F, p, s);
         }
     if (stage < 0 || stage == 4) far_l2t<R, TR>(F, s);
 }
@@ -831,7 +851,8 @@ void DeviceOp::run_far_overlap_t(FarField<R>& F, const double2* xt, cudaStream_t
         run_far_t<R, TR>(F, xt, s, -1);
         return;
     }
-    const bool tc = std::is_same<R, float>::value && !TR && use_tc_;
+    const bool tcf = std::is_same<R, float>::value && !TR;
+    const bool tc_up = tcf && (tc_mode_ & 1), tc_dn = tcf && (tc_mode_ & 4);
     far_s2m<R, TR>(F, xt, s);
     cudaEventRecord(ev_level_[lmax_], s);
     if (near_late) {
@@ -840,7 +861,7 @@ void DeviceOp::run_far_overlap_t(FarField<R>& F, const double2* xt, cudaStream_t
         cudaEventRecord(ev_join_, side_);
     }
     for (int p = lmax_ - 1; p >= lmin_; --p) {
-        if (tc) far_m2m_tc(p, 1, s); else far_m2m<R, TR>(F, p, s);
+        if (tc_up) far_m2m_tc(p, 1, s); else far_m2m<R, TR>(F, p, s);
         cudaEventRecord(ev_level_[p], s);
     }
     cudaStream_t ms[2] = {s2, side3_};
@@ -858,7 +879,7 @@ void DeviceOp::run_far_overlap_t(FarField<R>& F, const double2* xt, cudaStream_t
     cudaStreamWaitEvent(s, ev_m2l_done_, 0);
     if (nms > 1) cudaStreamWaitEvent(s, ev_m2l_done2_, 0);
     for (int p = lmin_; p < lmax_; ++p) {
-        if (tc) far_l2l_tc(p, 1, s); else far_l2l<R, TR>(F, p, s);
+        if (tc_dn) far_l2l_tc(p, 1, s); else far_l2l<R, TR>(F, p, s);
     }
     far_l2t<R, TR>(F, s);
 }
@@ -1084,6 +1105,39 @@ __global__ void k_widen(const C* __restrict__ src, double2* __restrict__ dst, lo
 }
 }  // namespace
 
+std::string DeviceOp::bj_prepare() {
+    if (!ready_) return "operator not set up";
+    if (bj_gen_ == generation_ && bj_leaves_) return {};
+    MLFMA_CK(cudaSetDevice(device_));
+    if (h_bj_.empty()) return "arg:no leaves to precondition";
+    if (!bj_leaves_) {
+        long long entries = 0;
+        for (const DevBjLeaf& L : h_bj_)
+            if (L.nb <= kBjMax) entries += static_cast<long long>(L.nb) * L.nb;
+        bj_leaves_ = upload(h_bj_);
+        bj_ok_ = alloc<int>(h_bj_.size());
+        bj_inv_ = alloc<double2>(static_cast<size_t>(std::max(1ll, entries)));
+        int dev_smem = 0;
+        MLFMA_CK(cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, device_));
+        cudaFuncAttributes fa{};
+        MLFMA_CK(cudaFuncGetAttributes(&fa, k_bj_build));
+        MLFMA_CK(cudaFuncSetAttribute(k_bj_build, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      dev_smem - static_cast<int>(fa.sharedSizeBytes)));
+    }
+    const size_t smem = sizeof(double2) * 2 * kBjMax * kBjMax;
+    k_bj_build<<<static_cast<int>(h_bj_.size()), kBjThreads, smem, stream_>>>(bj_leaves_, near_bz_, ck_,
+                                                                             has_loads_ ? loads_ : nullptr, bj_inv_,
+                                                                             bj_ok_);
+    MLFMA_CK(cudaGetLastError());
+    MLFMA_CK(cudaStreamSynchronize(stream_));
+    bj_gen_ = generation_;
+    return {};
+}
+
+void DeviceOp::bj_apply(const double2* x, double2* y, cudaStream_t s) {
+    k_bj_apply<<<static_cast<int>(h_bj_.size()), kBjThreads, 0, s>>>(bj_leaves_, bj_ok_, bj_inv_, x, y);
+}
+
 std::string DeviceOp::copy_transl(int level, double2* host) {
     if (level < lmin_ || level > lmax_) return "level out of range";
     MLFMA_CK(cudaSetDevice(device_));
@@ -1247,10 +1301,11 @@ void DeviceOp::run_far_multi_t(FarField<R>& F, int nr, cudaStream_t s, int stage
     if (n_leaves_ == 0) return;
     if ((stage < 0 || stage == 0) && n_s2m_items_m_)
         k_s2m_m<R><<<n_s2m_items_m_, kGemmThreads, 0, s>>>(F.lv_dev, s2m_items_m_, leaves_, F.pat, xtm_, nr);
-    const bool tc = std::is_same<R, float>::value && use_tc_multi_;
-    if ((stage < 0 || stage == 1) && tc)
+    const bool tc_up = std::is_same<R, float>::value && (tc_mode_ & 2);
+    const bool tc_dn = std::is_same<R, float>::value && (tc_mode_ & 8);
+    if ((stage < 0 || stage == 1) && tc_up)
         for (int p = lmax_ - 1; p >= lmin_; --p) far_m2m_tc(p, nr, s);
-    if ((stage < 0 || stage == 1) && !tc)
+    if ((stage < 0 || stage == 1) && !tc_up)
         for (int p = lmax_ - 1; p >= lmin_; --p) {
             if (npar_[p] == 0) continue;
             constexpr int rc = 16 * m2m_rpl<R>();
@@ -1277,9 +1332,9 @@ void DeviceOp::run_far_multi_t(FarField<R>& F, int nr, cudaStream_t s, int stage
         k_m2l_m<R><<<n_m2l_items_m_, threads, 0, s>>>(F.lv_dev, m2l_items_m_, m2l_groups_, m2l_cand_src_,
                                                       F.m2l_t8, nr, ref_compat_ ? 0 : 1);
     }
-    if ((stage < 0 || stage == 3) && tc)
+    if ((stage < 0 || stage == 3) && tc_dn)
         for (int p = lmin_; p < lmax_; ++p) far_l2l_tc(p, nr, s);
-    if ((stage < 0 || stage == 3) && !tc)
+    if ((stage < 0 || stage == 3) && !tc_dn)
         for (int p = lmin_; p < lmax_; ++p) {
             const int g = n_l2l_pairs_[p];
             if (!g) continue;
@@ -1589,14 +1644,13 @@ void DeviceOp::drop_graphs() {
 
 std::string DeviceOp::set_tc(int mode) {
     if (!ready_) return "operator not set up";
-    if (mode < 0 || mode > 3) return "arg:mode must be 0..3";
+    if (mode < 0 || mode > 15) return "arg:mode must be 0..15";
     if (mode && !tc_ok_)
         return "arg:no tensor-core interpolation on this operator (FP64 far field only, or a grid too large)";
-    if ((mode & 2) && max_rhs_ < 2) return "arg:the many-right-hand-side mode needs max_rhs > 1";
+    if ((mode & 10) && max_rhs_ < 2) return "arg:the many-right-hand-side modes need max_rhs > 1";
     MLFMA_CK(cudaSetDevice(device_));
     MLFMA_CK(cudaStreamSynchronize(stream_));
-    use_tc_ = (mode & 1) != 0;
-    use_tc_multi_ = (mode & 2) != 0;
+    tc_mode_ = mode;
     drop_graphs();  // recaptured with the chosen kernels on the next product
     ++generation_;
     return {};
@@ -1723,13 +1777,15 @@ std::string DeviceOp::autotune(int nr, int reps, TuneReport* rep) {
         }
         // interpolation and anterpolation: tensor cores or CUDA cores (the
         // complex-float far field), timed on the whole product
-        if (tc_ok_ && precision_ != kFp64) {
-            use_tc_ = false;
-            const float t_cc = timed(product);
-            use_tc_ = true;
-            const float t_tc = timed(product);
-            use_tc_ = t_tc < t_cc;
-        }
+        if (tc_ok_ && precision_ != kFp64)
+            for (int bit : {1, 4}) {  // M2M, then L2L: each stage on the faster kernels
+                const int st = bit == 1 ? 1 : 3;
+                tc_mode_ &= ~bit;
+                const float t_cc = timed([&] { run_far(xt_, s, st, precision_, false); });
+                tc_mode_ |= bit;
+                const float t_tc = timed([&] { run_far(xt_, s, st, precision_, false); });
+                if (!(t_tc < t_cc)) tc_mode_ &= ~bit;
+            }
         r.after_ms = timed(product);
     } else {
         auto product = [&] { enqueue_multi(nr, s, precision_); };
@@ -1758,13 +1814,15 @@ std::string DeviceOp::autotune(int nr, int reps, TuneReport* rep) {
         m_l2l_pairs_ = bpairs;
         r.multi_rows_fast = border;
         r.multi_l2l_pairs = bpairs;
-        if (tc_ok_ && precision_ != kFp64) {
-            use_tc_multi_ = false;
-            const float t_cc = timed(product);
-            use_tc_multi_ = true;
-            const float t_tc = timed(product);
-            use_tc_multi_ = t_tc < t_cc;
-        }
+        if (tc_ok_ && precision_ != kFp64)
+            for (int bit : {2, 8}) {
+                const int st = bit == 2 ? 1 : 3;
+                tc_mode_ &= ~bit;
+                const float t_cc = timed([&] { run_far_multi(nr, s, st, precision_); });
+                tc_mode_ |= bit;
+                const float t_tc = timed([&] { run_far_multi(nr, s, st, precision_); });
+                if (!(t_tc < t_cc)) tc_mode_ &= ~bit;
+            }
         r.after_ms = timed(product);
     }
     r.interp_path = tc_mode();

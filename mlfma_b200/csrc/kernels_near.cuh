@@ -561,3 +561,132 @@ __global__ void k_near_rows_assemble(const DevNearRow* __restrict__ rows, int nr
 
 }  // namespace
 }  // namespace mlfma
+
+namespace mlfma {
+namespace {
+
+// ------------------------------------------------------------ leaf block-Jacobi preconditioner
+// M = the diagonal blocks of A = C k Z + diag(loads), one per leaf: its
+// inverse from the leaf's stored self block (packed lower triangle, used
+// symmetrically, as the near field applies it), by Gauss-Jordan elimination
+// with partial pivoting in shared memory.  A leaf larger than kBjMax sources,
+// without a self block, or with a (numerically) singular block keeps the
+// identity.
+constexpr int kBjMax = 64;
+constexpr int kBjThreads = 256;
+
+__global__ void __launch_bounds__(kBjThreads)
+k_bj_build(const DevBjLeaf* __restrict__ leaves, const double2* __restrict__ Z, double2 ck,
+           const double2* __restrict__ loads, double2* __restrict__ inv, int* __restrict__ ok) {
+    extern __shared__ double2 aug[];  // nb x 2 nb: [block | identity]
+    __shared__ double piv_v[kBjThreads];
+    __shared__ int piv_i[kBjThreads];
+    __shared__ int singular;
+    const DevBjLeaf L = leaves[blockIdx.x];
+    const int nb = L.nb, w = 2 * nb;
+    if (L.zoff < 0 || nb > kBjMax) {
+        if (threadIdx.x == 0) ok[blockIdx.x] = 0;
+        return;
+    }
+    for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
+        const int i = e / nb, j = e - i * nb;
+        const int hi = max(i, j), lo = min(i, j);
+        double2 z = make_double2(0.0, 0.0);
+        if (hi != lo || L.kind == 2) z = Z[L.zoff + packed_row(hi, L.kind) + lo];
+        double2 a = cmul(ck, z);
+        if (i == j && loads) a = cadd(a, loads[L.row0 + i]);
+        aug[i * w + j] = a;
+        aug[i * w + nb + j] = make_double2(i == j ? 1.0 : 0.0, 0.0);
+    }
+    if (threadIdx.x == 0) singular = 0;
+    __syncthreads();
+    for (int c = 0; c < nb; ++c) {
+        // pivot: largest |a_rc| for r >= c
+        double best = -1.0;
+        int bi = c;
+        for (int r = c + threadIdx.x; r < nb; r += blockDim.x) {
+            const double2 v = aug[r * w + c];
+            const double m = v.x * v.x + v.y * v.y;
+            if (m > best) { best = m; bi = r; }
+        }
+        piv_v[threadIdx.x] = best;
+        piv_i[threadIdx.x] = bi;
+        __syncthreads();
+        for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+            if (threadIdx.x < s && piv_v[threadIdx.x + s] > piv_v[threadIdx.x]) {
+                piv_v[threadIdx.x] = piv_v[threadIdx.x + s];
+                piv_i[threadIdx.x] = piv_i[threadIdx.x + s];
+            }
+            __syncthreads();
+        }
+        const int p = piv_i[0];
+        if (!(piv_v[0] > 1e-300)) {
+            if (threadIdx.x == 0) singular = 1;
+            break;  // uniform: every thread read the same piv_v[0]
+        }
+        if (p != c)
+            for (int j = threadIdx.x; j < w; j += blockDim.x) {
+                const double2 t = aug[c * w + j];
+                aug[c * w + j] = aug[p * w + j];
+                aug[p * w + j] = t;
+            }
+        __syncthreads();
+        const double2 d = aug[c * w + c];
+        const double dm = d.x * d.x + d.y * d.y;
+        const double2 dinv = make_double2(d.x / dm, -d.y / dm);
+        __syncthreads();
+        for (int j = threadIdx.x; j < w; j += blockDim.x) aug[c * w + j] = cmul(aug[c * w + j], dinv);
+        __syncthreads();
+        // eliminate column c from every other row (its factor read before the row changes)
+        for (int e = threadIdx.x; e < nb * w; e += blockDim.x) {
+            const int r = e / w, j = e - r * w;
+            if (r == c || j == c) continue;
+            const double2 f = aug[r * w + c];
+            aug[r * w + j] = cadd(aug[r * w + j], cmul(make_double2(-f.x, -f.y), aug[c * w + j]));
+        }
+        __syncthreads();
+        for (int r = threadIdx.x; r < nb; r += blockDim.x)
+            if (r != c) aug[r * w + c] = make_double2(0.0, 0.0);
+        __syncthreads();
+    }
+    __syncthreads();
+    const bool good = singular == 0;
+    if (good)
+        for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
+            const int i = e / nb, j = e - i * nb;
+            inv[L.ioff + e] = aug[i * w + nb + j];
+        }
+    if (threadIdx.x == 0) ok[blockIdx.x] = good ? 1 : 0;
+}
+
+// y = M^{-1} x (tree order): per leaf its inverse block, or a copy.
+__global__ void __launch_bounds__(kBjThreads)
+k_bj_apply(const DevBjLeaf* __restrict__ leaves, const int* __restrict__ ok, const double2* __restrict__ inv,
+           const double2* __restrict__ x, double2* __restrict__ y) {
+    __shared__ double2 xs[kBjMax];
+    const DevBjLeaf L = leaves[blockIdx.x];
+    const int nb = L.nb;
+    if (!ok[blockIdx.x]) {
+        for (int i = threadIdx.x; i < nb; i += blockDim.x) y[L.row0 + i] = x[L.row0 + i];
+        return;
+    }
+    for (int i = threadIdx.x; i < nb; i += blockDim.x) xs[i] = x[L.row0 + i];
+    __syncthreads();
+    // 4 threads per row, a shuffle sum
+    const int row = threadIdx.x >> 2, part = threadIdx.x & 3;
+    for (int r = row; r < nb + ((nb & 63) ? 64 - (nb & 63) : 0); r += kBjThreads / 4) {
+        double2 acc = make_double2(0.0, 0.0);
+        if (r < nb) {
+            const double2* m = inv + L.ioff + static_cast<long long>(r) * nb;
+            for (int j = part; j < nb; j += 4) acc = cfma(m[j], xs[j], acc);
+        }
+        acc.x += __shfl_xor_sync(0xffffffffu, acc.x, 1);
+        acc.y += __shfl_xor_sync(0xffffffffu, acc.y, 1);
+        acc.x += __shfl_xor_sync(0xffffffffu, acc.x, 2);
+        acc.y += __shfl_xor_sync(0xffffffffu, acc.y, 2);
+        if (r < nb && part == 0) y[L.row0 + r] = acc;
+    }
+}
+
+}  // namespace
+}  // namespace mlfma

@@ -55,8 +55,8 @@ def test_tc_one_vector_matches_cuda_cores(cuda_device, case):
     x = cvec(op.n, 1)
     op.interp_path = 0
     y_cc = op.matvec(x)
-    op.interp_path = 1
-    assert op.interp_path == 1
+    op.interp_path = 5  # M2M and L2L of the one-vector product
+    assert op.interp_path == 5
     y_tc = op.matvec(x)
     y_tc2 = op.matvec(x)  # graph replay, same result
     assert rel(y_tc, y_cc) <= TOL
@@ -71,14 +71,14 @@ def test_tc_one_vector_matches_cuda_cores(cuda_device, case):
 def test_tc_many_rhs_matches_cuda_cores(cuda_device, case):
     op = make(case, precision=1, max_rhs=8)
     X = cvec((5, op.n), 2)
-    op.interp_path = 2
+    op.interp_path = 10  # M2M and L2L of the many-rhs product
     Y_tc = op.matvec_multi(X)
     op.interp_path = 0
     Y_cc = op.matvec_multi(X)
     for r in range(5):
         assert rel(Y_tc[r], Y_cc[r]) <= TOL
     # each column equals the one-vector product on the tensor cores too
-    op.interp_path = 1
+    op.interp_path = 5
     assert rel(Y_tc[3], op.matvec(X[3])) <= TOL
     op.close()
 
@@ -87,7 +87,7 @@ def test_tc_refined_solve_meets_fp64_residual(cuda_device):
     m = inputs.make_icosphere(3, radius=1.0)
     op64 = MLFMA.rwg(m, PW, max_node_srcs=16, ref_compat=0, precision=0, self_terms=1).setup()
     opmx = MLFMA.rwg(m, PW, max_node_srcs=16, ref_compat=0, precision=1, self_terms=1).setup()
-    opmx.interp_path = 1
+    opmx.interp_path = 5
     b = op64.rhs()
     tol = 1e-4
     x64, i64 = op64.solve(b, max_iter=400, tol=tol, restart=50, ref_givens=False)
@@ -105,7 +105,7 @@ def test_tc_state_rule_and_fp64_operator(cuda_device):
     d = inputs.make_dipoles(4000, seed=8)
     a = MLFMA.dipoles(d, PW, max_node_srcs=8, precision=1).setup()
     b = MLFMA.dipoles(d, PW, max_node_srcs=8, precision=1).setup()
-    a.interp_path, b.interp_path = 0, 1
+    a.interp_path, b.interp_path = 0, 5
     for s in (3, 4, 5):
         x = cvec(a.n, s)
         assert rel(b.matvec(x), a.matvec(x)) <= TOL
@@ -115,5 +115,5 @@ def test_tc_state_rule_and_fp64_operator(cuda_device):
     op = MLFMA.dipoles(d, PW, max_node_srcs=8, precision=0).setup()
     assert op.interp_path == 0
     with pytest.raises(Exception):
-        op.interp_path = 1
+        op.interp_path = 5
     op.close()
