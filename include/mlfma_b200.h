@@ -62,6 +62,12 @@ typedef struct {
                             (symmetrised, FP64) */
     int max_rhs;         /* most right-hand sides of one product (1..64; mlfma_matvec_multi,
                             mlfma_gmres_multi); > 1 reserves their device work space */
+    int device_tree;     /* 1: build the octree and its lists on the device (Morton keys,
+                            radix sort, one thread per box for the lists): the same
+                            boxes, numbering, source order and lists as the host build
+                            (Stem ctor, src/fmm/stem.cpp:3-26; src/fmm/nbor.cpp:10-644;
+                            Node::buildInteractionList, src/fmm/node.cpp:61-84); trees
+                            deeper than 21 levels fall back to the host build */
 } mlfma_config;
 
 enum { MLFMA_FP64 = 0, MLFMA_MIXED = 1 };
@@ -401,6 +407,13 @@ int mlfma_level_transl_gpu(mlfma_handle h, int level, double* out);
  * source in tree order, source count) and the tree-order -> caller-order
  * permutation (n ints). */
 int mlfma_far_leaves(mlfma_handle h, int* count, int* info, int* perm);
+/* The octree and its lists, for inspection: which = 0 gives 14 ints per node
+ * in node order (level, parent, branch, child[8], leaf, src_begin, src_count),
+ * 1 the source order (perm[tree slot] = caller index), 2..5 per node the
+ * length and then the node ids of its equal-or-greater neighbours, list 1
+ * (near leaves), list 2 and list 4.  *count receives the ints needed; out ==
+ * NULL only asks for it. */
+int mlfma_tree_export(mlfma_handle h, int which, int* out, long long cap, long long* count);
 /* Reference-rounded RWG radiation patterns computed on the host, laid out as
  * the device array: per far leaf, per source, per direction, 2 complex. */
 int mlfma_rwg_patterns_host(mlfma_handle h, double* out, long long count);

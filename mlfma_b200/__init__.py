@@ -210,6 +210,16 @@ class MLFMA:
                                      perm.ctypes.data_as(_ip)))
         return info[: cnt.value], perm
 
+    def tree_export(self, which: int) -> np.ndarray:
+        """The octree (0: 14 ints per node), source order (1) or a list (2
+        neighbours, 3 list 1, 4 list 2, 5 list 4: per node its length, then
+        node ids) as one int32 array (mlfma_tree_export)."""
+        cnt = ctypes.c_longlong()
+        check(lib().mlfma_tree_export(self._h, which, None, 0, ctypes.byref(cnt)))
+        out = np.zeros(max(cnt.value, 1), dtype=np.int32)
+        check(lib().mlfma_tree_export(self._h, which, out.ctypes.data_as(_ip), out.size, ctypes.byref(cnt)))
+        return out[: cnt.value]
+
     def rwg_patterns_host(self) -> np.ndarray:
         n = self.stats()["pattern_elems"]
         out = np.zeros(2 * n, dtype=np.complex128)

@@ -28,7 +28,7 @@ class Config(ctypes.Structure):
                 ("over_interp", ctypes.c_double), ("root_leng", ctypes.c_double),
                 ("max_node_srcs", ctypes.c_int), ("max_level", ctypes.c_int),
                 ("ref_compat", ctypes.c_int), ("device", ctypes.c_int), ("precision", ctypes.c_int),
-                ("self_terms", ctypes.c_int), ("max_rhs", ctypes.c_int)]
+                ("self_terms", ctypes.c_int), ("max_rhs", ctypes.c_int), ("device_tree", ctypes.c_int)]
 
 
 class PlaneWaveC(ctypes.Structure):
@@ -137,6 +137,8 @@ SIGNATURES = {
     "mlfma_level_transl": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _dp]),
     "mlfma_level_transl_gpu": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _dp]),
     "mlfma_far_leaves": (ctypes.c_int, [ctypes.c_void_p, _ip, _ip, _ip]),
+    "mlfma_tree_export": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _ip, ctypes.c_longlong,
+                                         ctypes.POINTER(ctypes.c_longlong)]),
     "mlfma_rwg_patterns_host": (ctypes.c_int, [ctypes.c_void_p, _dp, ctypes.c_longlong]),
     "mlfma_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "mlfma_last_error": (ctypes.c_char_p, []),

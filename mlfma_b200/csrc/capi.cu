@@ -84,6 +84,7 @@ mlfma::Config to_cfg(const mlfma_config* c) {
     o.max_level = c->max_level;
     o.ref_compat = c->ref_compat;
     o.self_terms = c->self_terms;
+    o.device_tree = c->device_tree;
     return o;
 }
 
@@ -125,6 +126,7 @@ int mlfma_config_default(mlfma_config* cfg) {
     cfg->precision = MLFMA_FP64;
     cfg->self_terms = 0;
     cfg->max_rhs = 1;
+    cfg->device_tree = 0;
     return MLFMA_OK;
 }
 
@@ -137,6 +139,8 @@ int mlfma_create_dipoles(const mlfma_config* cfg, const mlfma_planewave* pw, int
         h->precision = cfg->precision;
         h->max_rhs = cfg->max_rhs < 1 ? 1 : cfg->max_rhs;
         if (h->max_rhs > 64) return fail(MLFMA_ERR_ARG, "max_rhs must be at most 64");
+        if (cfg->device_tree && cudaSetDevice(cfg->device) != cudaSuccess)
+            return fail(MLFMA_ERR_CUDA, "cudaSetDevice failed");
         const std::string e = h->plan.build_dipoles(to_cfg(cfg), to_pw(pw), n, pos, mom);
         if (!e.empty()) return fail(MLFMA_ERR_ARG, e);
         *out = h.release();
@@ -155,6 +159,8 @@ int mlfma_create_rwg(const mlfma_config* cfg, const mlfma_planewave* pw, int nv,
         h->precision = cfg->precision;
         h->max_rhs = cfg->max_rhs < 1 ? 1 : cfg->max_rhs;
         if (h->max_rhs > 64) return fail(MLFMA_ERR_ARG, "max_rhs must be at most 64");
+        if (cfg->device_tree && cudaSetDevice(cfg->device) != cudaSuccess)
+            return fail(MLFMA_ERR_CUDA, "cudaSetDevice failed");
         const std::string e = h->plan.build_rwg(to_cfg(cfg), to_pw(pw), nv, verts, nf, faces, ne, rwgs);
         if (!e.empty()) return fail(MLFMA_ERR_ARG, e);
         *out = h.release();
@@ -852,6 +858,34 @@ int mlfma_far_leaves(mlfma_handle h, int* count, int* info, int* perm) {
             info[4 * i + 3] = f.nsrc;
         }
     if (perm) std::memcpy(perm, p.perm.data(), sizeof(int) * p.perm.size());
+    return MLFMA_OK;
+}
+
+int mlfma_tree_export(mlfma_handle h, int which, int* out, long long cap, long long* count) {
+    if (!h || !count) return fail(MLFMA_ERR_ARG, "null argument");
+    if (which < 0 || which > 5) return fail(MLFMA_ERR_ARG, "which must be 0..5");
+    const mlfma::Plan& p = h->plan;
+    std::vector<int> v;
+    if (which == 1) {
+        v = p.perm;
+    } else {
+        for (const mlfma::Node& nd : p.nodes) {
+            if (which == 0) {
+                v.insert(v.end(), {nd.level, nd.parent, nd.branch});
+                v.insert(v.end(), nd.child, nd.child + 8);
+                v.insert(v.end(), {nd.leaf ? 1 : 0, nd.src_begin, nd.src_count});
+                continue;
+            }
+            const std::vector<int>& l = which == 2 ? nd.nbors : which == 3 ? nd.near_nbors
+                                        : which == 4 ? nd.ilist : nd.leaf_ilist;
+            v.push_back(static_cast<int>(l.size()));
+            v.insert(v.end(), l.begin(), l.end());
+        }
+    }
+    *count = static_cast<long long>(v.size());
+    if (!out) return MLFMA_OK;
+    if (cap < *count) return fail(MLFMA_ERR_ARG, "buffer too small");
+    std::memcpy(out, v.data(), sizeof(int) * v.size());
     return MLFMA_OK;
 }
 

@@ -195,6 +195,12 @@ double dot3_seq(const double* a, const double* b) {
 
 }  // namespace
 
+const int* plan_directions() { return &kDirs[0][0]; }
+
+// Weak, so that host-only programs built from this file alone still link; the
+// CUDA library defines it.
+std::string build_tree_lists_device(Plan& P, const std::vector<double>& centers) __attribute__((weak));
+
 // I(k) of one RWG in the closed form of RWG::getIntegratedPlaneWave
 // (src/sources/rwg.cpp:46-86), written operation for operation with
 // std::complex<double> so that, built without floating-point contraction,
@@ -447,8 +453,17 @@ std::string Plan::build_common(const std::vector<double>& centers) {
     for (int i = 0; i < n; ++i)
         for (int k = 0; k < 3; ++k)
             if (!(std::fabs(centers[3 * i + k]) <= h)) return "source outside the root box";
-    build_tree(centers);
-    build_lists();
+    bool host_tree = true;
+    if (cfg.device_tree) {
+        if (!&build_tree_lists_device) return "device_tree needs the CUDA library";
+        const std::string e = build_tree_lists_device(*this, centers);
+        if (e.empty()) host_tree = false;
+        else if (e.rfind("host:", 0) != 0) return e;
+    }
+    if (host_tree) {
+        build_tree(centers);
+        build_lists();
+    }
     build_levels();
     build_far_plan();
     build_near_plan();
@@ -653,6 +668,12 @@ void Plan::build_levels() {
         // src/fmm/tables.cpp:90-220).
         const int nps = L.nps;
         if (nps < 2 * order || nps < 2) throw std::runtime_error("over_interp too small for interp_order");
+        // The interpolation stencils reflect an index once at each pole and
+        // wrap it once in phi: a grid needs at least interp_order thetas.
+        if (L.nth < order)
+            throw std::runtime_error("level " + std::to_string(l) + " has " + std::to_string(L.nth) +
+                                     " thetas, fewer than interp_order: boxes too small for the wavelength "
+                                     "(lower max_level or raise max_node_srcs)");
         std::unordered_map<long long, std::vector<cplx>> alpha;  // key: r^2 (integer)
         std::vector<cplx> h;
         std::vector<double> P;

@@ -31,6 +31,8 @@ struct Config {
     int ref_compat = 1;       // 1: reproduce the reference's stale-local rule
     int self_terms = 0;       // 1: unit dipole diagonal; touching RWG pairs in
                               //    mixed-potential form, 1/R extracted
+    int device_tree = 0;      // 1: octree and lists built on the current CUDA
+                              //    device (same nodes, order and lists)
 };
 
 struct PlaneWave {
@@ -202,6 +204,16 @@ private:
     void build_far_plan();
     void build_near_plan();
 };
+
+// The 26 neighbour directions in the reference's order (FMM::Dir,
+// src/fmm/fmm.h:13-17), 3 ints (dx, dy, dz) each.
+const int* plan_directions();
+
+// The tree and lists of P (nodes, perm, src_center, leaves, max_level, list
+// counts) built on the current CUDA device from the source centres; empty on
+// success.  Defined with the CUDA sources; a message beginning "host:" asks
+// for the host build (a tree deeper than the device keys hold).
+std::string build_tree_lists_device(Plan& P, const std::vector<double>& centers);
 
 // Offset id of an integer M2L offset in Math::getINodeDistVecs order
 // (src/math.cpp:106-122), or -1.

@@ -43,7 +43,6 @@ constexpr int kHardCap = 30;        // the host's depth cap
 constexpr int kRsThreads = 256;
 constexpr int kRsItems = 4;         // elements per thread per block
 constexpr int kRsChunk = kRsThreads * kRsItems;
-constexpr int kBfsQueue = 1024;     // breadth-first queue of the near-leaf search
 
 using u64 = unsigned long long;
 
@@ -223,15 +222,31 @@ __global__ void k_splits(const u64* __restrict__ sk, const int* __restrict__ sv,
     if (!out_pk) count[i] = c;
 }
 
-__global__ void k_exclusive_scan_small(int* __restrict__ a, int n, int* __restrict__ total) {
-    // one thread: the counts are per sorted source (a few hundred thousand)
-    int run = 0;
-    for (int i = 0; i < n; ++i) {
+// exclusive scan of a[0, n) in place, one block of 1024 threads; *total = sum
+__global__ void k_scan_int(int* __restrict__ a, int n, int* __restrict__ total) {
+    __shared__ long long part[1024];
+    const int per = (n + blockDim.x - 1) / blockDim.x;
+    const int i0 = min(n, static_cast<int>(threadIdx.x) * per), i1 = min(n, i0 + per);
+    long long s = 0;
+    for (int i = i0; i < i1; ++i) s += a[i];
+    part[threadIdx.x] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        long long run = 0;
+        for (int t = 0; t < static_cast<int>(blockDim.x); ++t) {
+            const long long v = part[t];
+            part[t] = run;
+            run += v;
+        }
+        *total = run > 0x7fffffffLL ? -1 : static_cast<int>(run);
+    }
+    __syncthreads();
+    long long run = part[threadIdx.x];
+    for (int i = i0; i < i1; ++i) {
         const int v = a[i];
-        a[i] = run;
+        a[i] = static_cast<int>(run);
         run += v;
     }
-    *total = run;
 }
 
 // node records in depth-first order (padded key pk[id], level lv[id])
@@ -337,37 +352,69 @@ __global__ void k_nbors(int nn, const int* parent, const int* branch, const int*
                                                             c_dirs[i][2]);
 }
 
-// near leaves of leaf id (Node::getNeighborsLeqSize, breadth first), count or fill
+// near leaves of leaf id (Node::getNeighborsLeqSize), count or fill.  The
+// host's breadth-first queue emits the leaves inside a neighbour by depth and,
+// at one depth, in child-index path order; a depth-limited walk per depth
+// gives the same order with a stack of the tree's height.
 __global__ void k_near(int nn, const int* child, const int* leaf, const int* nb26, const int* base, int* count,
-                       int* out, int* err) {
+                       int* out) {
     const int id = blockIdx.x * blockDim.x + threadIdx.x;
-    if (id >= nn || !leaf[id]) {
-        if (id < nn && !out) count[id] = 0;
+    if (id >= nn) return;
+    if (!leaf[id]) {
+        if (!out) count[id] = 0;
         return;
     }
-    int q[kBfsQueue];
+    int stk[kHardCap + 1], nxt[kHardCap + 1];
     int c = 0;
     for (int i = 0; i < 26; ++i) {
         const int nb = nb26[id * 26 + i];
         if (nb < 0) continue;
-        int head = 0, tail = 0;
-        q[tail++] = nb;
-        while (head < tail) {
-            const int cur = q[head++];
-            if (leaf[cur]) {
-                if (out) out[base[id] + c] = cur;
-                ++c;
-                continue;
+        const int* d = c_dirs[i];
+        for (int depth = 0; depth <= kHardCap; ++depth) {
+            bool deeper = false;
+            int top = 0;
+            stk[0] = nb;
+            nxt[0] = -1;
+            while (top >= 0) {
+                const int cur = stk[top];
+                if (nxt[top] < 0) {  // first visit
+                    if (top == depth) {
+                        if (leaf[cur]) {
+                            if (out) out[base[id] + c] = cur;
+                            ++c;
+                        } else {
+                            deeper = true;
+                        }
+                        --top;
+                        continue;
+                    }
+                    if (leaf[cur]) {  // emitted at its own depth
+                        --top;
+                        continue;
+                    }
+                    nxt[top] = 0;
+                }
+                int cc = nxt[top];
+                for (; cc < 8; ++cc) {  // children on the face, edge or corner toward the box
+                    bool ok = true;
+                    for (int a = 0; a < 3; ++a) {
+                        const int ca = (cc >> a) & 1;
+                        if ((d[a] > 0 && ca != 0) || (d[a] < 0 && ca != 1)) ok = false;
+                    }
+                    if (ok) break;
+                }
+                if (cc >= 8) {
+                    --top;
+                    continue;
+                }
+                nxt[top] = cc + 1;
+                const int nx = child[cur * 8 + cc];
+                if (nx < 0) continue;  // not reached: a split box has all 8 children
+                ++top;
+                stk[top] = nx;
+                nxt[top] = -1;
             }
-            for (int cc = 0; cc < 8; ++cc) {
-                const int cb[3] = {cc & 1, (cc >> 1) & 1, (cc >> 2) & 1};
-                bool ok = true;
-                for (int a = 0; a < 3; ++a)
-                    if ((c_dirs[i][a] > 0 && cb[a] != 0) || (c_dirs[i][a] < 0 && cb[a] != 1)) ok = false;
-                if (!ok) continue;
-                if (tail >= kBfsQueue) { atomicExch(err, 2); return; }
-                q[tail++] = child[cur * 8 + cc];
-            }
+            if (!deeper) break;
         }
     }
     if (!out) count[id] = c;
@@ -399,7 +446,7 @@ __global__ void k_ilists(int nn, const int* parent, const int* child, const int*
             }
             for (int c = 0; c < 8; ++c) {
                 const int ch = child[bn * 8 + c];
-                if (!contains(ch) && scnt[ch] > 0) {
+                if (ch >= 0 && !contains(ch) && scnt[ch] > 0) {
                     if (out2) out2[base2[id] + c2] = ch;
                     ++c2;
                 }
@@ -422,8 +469,9 @@ struct DevBuf {
 std::string scan_counts(int* d, int n, int* total_h) {
     DevBuf<int> tot;
     TG_CK(tot.alloc(1));
-    k_exclusive_scan_small<<<1, 1>>>(d, n, tot.p);
+    k_scan_int<<<1, 1024>>>(d, n, tot.p);
     TG_CK(cudaMemcpy(total_h, tot.p, sizeof(int), cudaMemcpyDeviceToHost));
+    if (*total_h < 0) return "device tree: more than 2^31 list entries";
     return {};
 }
 
@@ -432,6 +480,7 @@ std::string scan_counts(int* d, int n, int* total_h) {
 std::string build_tree_lists_device(Plan& P, const std::vector<double>& centers) {
     const int n = P.n;
     const Config& cfg = P.cfg;
+    if (n < 2) return "host: fewer than two sources";
     const int T = 256;
     auto blocks = [&](long long m) { return static_cast<int>((m + T - 1) / T); };
     DevBuf<double> d_c;
@@ -458,6 +507,11 @@ std::string build_tree_lists_device(Plan& P, const std::vector<double>& centers)
     std::string e = radix_sort(ka, va, kb, vb, n, 3 * kDepth, hist.p);
     if (!e.empty()) return e;
     k_leaf_level<<<blocks(n), T>>>(ka, va, n, cfg.max_node_srcs, cfg.max_level, leafL.p, err.p);
+    {
+        int herr = 0;
+        TG_CK(cudaMemcpy(&herr, err.p, sizeof(int), cudaMemcpyDeviceToHost));
+        if (herr) return "host: the tree is deeper than the 21 levels of the device keys";
+    }
     // split boxes and the node records
     DevBuf<int> scount;
     TG_CK(scount.alloc(n));
@@ -485,8 +539,6 @@ std::string build_tree_lists_device(Plan& P, const std::vector<double>& centers)
     int* pv = pidx.p;
     u64* pb = kb;  // scratch of the key sort is free now
     int* pw = vb;
-    const bool pk_in_scratch = false;
-    (void)pk_in_scratch;
     e = radix_sort(pa, pv, pb, pw, n, 3 * kDepth, hist.p);
     if (!e.empty()) return e;
     // 4: nodes in depth-first pre-order: stable by level, then by padded key
@@ -565,7 +617,7 @@ std::string build_tree_lists_device(Plan& P, const std::vector<double>& centers)
     TG_CK(ncnt.alloc(nn));
     TG_CK(c2.alloc(nn));
     TG_CK(c4.alloc(nn));
-    k_near<<<blocks(nn), T>>>(nn, ch.p, lf.p, nb26.p, nullptr, ncnt.p, nullptr, err.p);
+    k_near<<<blocks(nn), T>>>(nn, ch.p, lf.p, nb26.p, nullptr, ncnt.p, nullptr);
     k_ilists<<<blocks(nn), T>>>(nn, par.p, ch.p, lf.p, sc.p, nb26.p, nullptr, nullptr, c2.p, c4.p, nullptr, nullptr);
     int nnear = 0, n2 = 0, n4 = 0;
     if (!(e = scan_counts(ncnt.p, nn, &nnear)).empty() || !(e = scan_counts(c2.p, nn, &n2)).empty() ||
@@ -575,12 +627,9 @@ std::string build_tree_lists_device(Plan& P, const std::vector<double>& centers)
     TG_CK(onear.alloc(nnear));
     TG_CK(o2.alloc(n2));
     TG_CK(o4.alloc(n4));
-    k_near<<<blocks(nn), T>>>(nn, ch.p, lf.p, nb26.p, ncnt.p, nullptr, onear.p, err.p);
+    k_near<<<blocks(nn), T>>>(nn, ch.p, lf.p, nb26.p, ncnt.p, nullptr, onear.p);
     k_ilists<<<blocks(nn), T>>>(nn, par.p, ch.p, lf.p, sc.p, nb26.p, c2.p, c4.p, nullptr, nullptr, o2.p, o4.p);
     TG_CK(cudaGetLastError());
-    int herr = 0;
-    TG_CK(cudaMemcpy(&herr, err.p, sizeof(int), cudaMemcpyDeviceToHost));
-    if (herr) return "device tree: deeper than 21 levels or a near-leaf search beyond its queue";
     // back to the host plan
     std::vector<int> hpar(nn), hbr(nn), hch(8 * static_cast<size_t>(nn)), hlf(nn), hsb(nn), hsc(nn),
         hnb(26 * static_cast<size_t>(nn)), hnc(nn), hc2(nn), hc4(nn), hnear(nnear), h2(n2), h4(n4), hperm(n);

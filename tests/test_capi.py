@@ -100,3 +100,23 @@ def test_host_plan_stats_without_gpu():
     assert sorted(perm.tolist()) == list(range(3000))
     assert info[:, 3].sum() == 3000
     op.close()
+
+
+def test_tree_export_and_device_tree_without_gpu():
+    op = MLFMA.dipoles(inputs.make_dipoles(3000, seed=2), inputs.PlaneWave(), max_node_srcs=16)
+    st = op.stats()
+    nodes = op.tree_export(0).reshape(-1, 14)
+    assert nodes.shape[0] == st["num_nodes"] and nodes[:, 11].sum() == st["num_leaves"]
+    assert nodes[0, 1] == -1 and nodes[0, 13] == 3000  # the root holds every source
+    assert sorted(op.tree_export(1).tolist()) == list(range(3000))
+    for which, key in ((4, "list2"), (5, "list4")):
+        a, total, i = op.tree_export(which), 0, 0
+        while i < a.size:  # per node: length, then ids
+            total += a[i]
+            i += a[i] + 1
+        assert i == a.size and total == st[key]
+    op.close()
+    import torch
+    if not torch.cuda.is_available():  # the device build needs a GPU: a clean error
+        with pytest.raises(MlfmaError, match="cudaSetDevice"):
+            MLFMA.dipoles(inputs.make_dipoles(300, seed=2), inputs.PlaneWave(), device_tree=1)
