@@ -51,7 +51,7 @@ SOLVE = dict(restart=50, tol=1e-4, max_iter=3000)
 LARGE = dict(name="rwg_sphere_r8lambda_ico7", level=7, radius=8.0, root_leng=16.0, max_node_srcs=54, quad_prec=2,
              digits=3, interp_order=3, over_interp=2.0)
 LARGE_SOLVE = dict(restart=50, tol=1e-4, max_iter=6000)
-LARGE_FLEX = dict(restart=40, inner_iters=25)  # flexible GMRES: outer steps per cycle, inner iterations
+LARGE_FLEX = dict(restart=30, inner_iters=50)  # flexible GMRES: outer steps per cycle, inner iterations
 LARGE_NRHS = 16
 NRHS = 64
 NPROB = 32

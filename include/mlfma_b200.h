@@ -199,6 +199,16 @@ int mlfma_matvec_device(mlfma_handle h, const void* d_x, void* d_y, int accumula
 int mlfma_gmres(mlfma_handle h, const double* b, double* x, const mlfma_solver_opts* opts,
                 mlfma_solve_info* info);
 
+/* Operator of the inner iterations of flexible solves (opts->flexible) on h:
+ * the outer FGMRES space and its products stay on h's FP64 far field, each
+ * outer step is preconditioned by opts->inner_iters GMRES iterations on
+ * `inner` instead of on h.  `inner` is a set-up operator on the same device
+ * with the same unknowns in the same source order (the same sources, root_leng,
+ * max_node_srcs and max_level); it may use fewer digits, a lower
+ * interpolation order or mixed precision, which makes each inner product
+ * cheaper.  NULL detaches it; destroying either handle detaches it too. */
+int mlfma_set_inner_operator(mlfma_handle h, mlfma_handle inner);
+
 /* Far field of the currents x (host, n complex, caller order) along ndir unit
  * directions khat (host, ndir x 3): out (host, ndir x 3 complex) =
  * C k (I - khat khat^T) sum_n x_n f_n(k khat), the sum of Node::printFarSols

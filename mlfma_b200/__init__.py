@@ -264,6 +264,12 @@ class MLFMA:
         return x, SolveResult(info.iterations, info.residual, info.true_residual, info.seconds, converged,
                               info.refinements)
 
+    def set_inner_operator(self, inner: "MLFMA | None") -> None:
+        """Operator of the inner iterations of flexible solves (mlfma_set_inner_operator):
+        same sources and tree, e.g. fewer digits or mixed precision.  None detaches it."""
+        check(lib().mlfma_set_inner_operator(self._h, inner._h if inner is not None else None))
+        self._inner = inner  # keeps it alive while registered
+
     # ---------------------------------------------------------------- many right-hand sides
     def rhs_planewave(self, pw: inputs.PlaneWave) -> np.ndarray:
         """-V for another incident plane wave (same wavenumber)."""

@@ -136,6 +136,7 @@ SIGNATURES = {
     "mlfma_level_patterns": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp, ctypes.c_longlong]),
     "mlfma_level_transl": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _dp]),
     "mlfma_level_transl_gpu": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _dp]),
+    "mlfma_set_inner_operator": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "mlfma_far_leaves": (ctypes.c_int, [ctypes.c_void_p, _ip, _ip, _ip]),
     "mlfma_tree_export": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _ip, ctypes.c_longlong,
                                          ctypes.POINTER(ctypes.c_longlong)]),

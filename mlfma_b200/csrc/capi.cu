@@ -1,6 +1,7 @@
 // C ABI of the operator (include/mlfma_b200.h).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstring>
 #include <complex>
 #include <cmath>
@@ -29,6 +30,8 @@ struct mlfma_op_s {
     double2* d_y = nullptr;
     void* d_stage = nullptr;  // small per-call inputs and outputs (directions, rows, far fields); grows only
     size_t stage_bytes = 0;
+    mlfma_op_s* inner = nullptr;        // operator of the flexible solve's inner iterations
+    std::vector<mlfma_op_s*> outers;    // operators that use this one as their inner operator
     ~mlfma_op_s() {
         if (d_x || d_y || d_xm || d_ym || d_stage) {
             cudaSetDevice(device);
@@ -268,6 +271,7 @@ int mlfma_gmres(mlfma_handle h, const double* b, double* x, const mlfma_solver_o
         o.inner_iters = opts->inner_iters;
         o.precond = opts->precond;
     }
+    if (o.flexible && h->inner) o.inner = h->inner->dev.get();
     const size_t bytes = sizeof(double2) * h->plan.n;
     cudaStream_t s = h->dev->stream();
     cudaSetDevice(h->device);
@@ -280,6 +284,7 @@ int mlfma_gmres(mlfma_handle h, const double* b, double* x, const mlfma_solver_o
         cudaStreamSynchronize(s) != cudaSuccess)
         return fail(MLFMA_ERR_CUDA, "copy of x failed");
     e = h->dev->device_error();
+    if (e.empty() && o.inner) e = o.inner->device_error();
     if (!e.empty()) return fail(MLFMA_ERR_CUDA, e);
     if (info) {
         info->iterations = r.iterations;
@@ -904,7 +909,34 @@ int mlfma_rwg_patterns_host(mlfma_handle h, double* out, long long count) {
     return MLFMA_OK;
 }
 
+int mlfma_set_inner_operator(mlfma_handle h, mlfma_handle inner) {
+    if (!h) return fail(MLFMA_ERR_ARG, "null handle");
+    if (!ready(h)) return fail(MLFMA_ERR_STATE, "mlfma_setup has not run");
+    if (inner == h) return fail(MLFMA_ERR_ARG, "an operator is not its own inner operator");
+    if (inner) {
+        if (!ready(inner)) return fail(MLFMA_ERR_STATE, "the inner operator is not set up");
+        if (inner->device != h->device) return fail(MLFMA_ERR_ARG, "the inner operator is on another device");
+        if (inner->plan.n != h->plan.n || inner->plan.perm != h->plan.perm)
+            return fail(MLFMA_ERR_ARG, "the inner operator has other unknowns or another source order (build it "
+                                       "from the same sources with the same root_leng, max_node_srcs, max_level)");
+    }
+    if (h->inner) {
+        auto& o = h->inner->outers;
+        o.erase(std::remove(o.begin(), o.end(), h), o.end());
+    }
+    h->inner = inner;
+    if (inner) inner->outers.push_back(h);
+    return MLFMA_OK;
+}
+
 int mlfma_destroy(mlfma_handle h) {
+    if (h) {
+        if (h->inner) {
+            auto& o = h->inner->outers;
+            o.erase(std::remove(o.begin(), o.end(), h), o.end());
+        }
+        for (mlfma_op_s* o : h->outers) o->inner = nullptr;
+    }
     delete h;
     return MLFMA_OK;
 }

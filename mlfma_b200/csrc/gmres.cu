@@ -701,10 +701,15 @@ std::string Gmres::solve(DeviceOp& op, const double2* d_b_user, double2* d_x_use
     if (o.adjoint && op.ref_compat()) return "arg:the adjoint needs ref_compat = 0";
     adj_ = o.adjoint != 0;
     pc_ = o.precond != 0;
+    if (o.inner) {
+        if (!o.flexible) return "arg:an inner operator serves the flexible solve";
+        if (adj_) return "arg:the flexible solve with an inner operator serves forward solves";
+        if (o.inner->n() != op.n()) return "arg:the inner operator has another number of unknowns";
+    }
     if (pc_) {
         if (adj_) return "arg:the block-Jacobi preconditioner serves forward solves";
         if (external_) return "arg:the preconditioned solve needs its own workspace (use mlfma_gmres)";
-        const std::string e = op.bj_prepare();
+        const std::string e = (o.inner ? *o.inner : op).bj_prepare();
         if (!e.empty()) return e;
     }
     if (o.flexible) {
@@ -842,7 +847,11 @@ std::string Gmres::solve_flexible(DeviceOp& op, const double2* d_b_user, double2
     cudaStream_t s = op.stream();
     const int* perm = op.perm();
     const int nch = nchunks_;
-    const int prec_in = op.precision();
+    // inner solves: on the inner operator when one is given (its own stream;
+    // the two streams meet at host synchronisations around each inner solve)
+    DeviceOp& iop = o.inner ? *o.inner : op;
+    const bool two_streams = iop.stream() != op.stream();
+    const int prec_in = iop.precision();
     k_gather_perm<<<nblk(n, 256), 256, 0, s>>>(d_b_user, perm, bf_, n);
     GM_CK(cudaMemsetAsync(xf_, 0, sizeof(double2) * n, s));
     double bnorm = 0;
@@ -886,12 +895,14 @@ std::string Gmres::solve_flexible(DeviceOp& op, const double2* d_b_user, double2
             double2* zk = Z_ + static_cast<size_t>(k) * n;
             // inner solve A z = v_k from zero (||v_k|| = 1)
             GM_CK(cudaMemcpyAsync(b_, vk, sizeof(double2) * n, cudaMemcpyDeviceToDevice, s));
+            if (two_streams) GM_CK(cudaStreamSynchronize(s));
             int it = 0;
             double est = 0;
             bool c = false;
-            err = cycles(op, prec_in, oi, 1.0, o.inner_tol > 0 ? o.inner_tol : 0.0,
+            err = cycles(iop, prec_in, oi, 1.0, o.inner_tol > 0 ? o.inner_tol : 0.0,
                          std::min(mi, o.max_iter - res->iterations), false, &it, &est, &c);
             if (!err.empty()) return err;
+            if (two_streams) GM_CK(cudaStreamSynchronize(iop.stream()));
             res->iterations += it;
             GM_CK(cudaMemcpyAsync(zk, x_, sizeof(double2) * n, cudaMemcpyDeviceToDevice, s));
             // w = A z_k in FP64, orthogonalised against v_0..v_k

@@ -22,6 +22,8 @@ struct SolveOpts {
     int flexible = 0;      // FGMRES: FP64 outer Krylov space over inner GMRES solves
     int inner_iters = 0;   // flexible: iterations per inner solve (0 = 20)
     int precond = 0;       // 1: leaf block-Jacobi right preconditioner (DeviceOp::bj_*)
+    DeviceOp* inner = nullptr;  // flexible: operator of the inner solves (same
+                                // unknowns and source order), null = the outer one
 };
 
 struct SolveResult {

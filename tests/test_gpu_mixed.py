@@ -104,3 +104,34 @@ def test_flexible_gmres_meets_fp64_residual(cuda_device, precision):
     if op is not op64:
         op.close()
     op64.close()
+
+
+def test_flexible_gmres_with_cheaper_inner_operator(cuda_device):
+    # FGMRES whose inner iterations run on another operator of the same
+    # sources and tree (here 1-digit angular sampling, 4-point interpolation,
+    # complex-float far field): the outer FP64 residual still meets tol, and the
+    # answer matches the FP64 GMRES solution.
+    m = inputs.make_icosphere(3, radius=1.0)
+    op64 = MLFMA.rwg(m, PW, max_node_srcs=16, ref_compat=0, precision=0, self_terms=1).setup()
+    cheap = MLFMA.rwg(m, PW, max_node_srcs=16, ref_compat=0, precision=1, self_terms=1, digits=1,
+                      interp_order=2).setup()
+    b = op64.rhs()
+    tol = 1e-6
+    x64, _ = op64.solve(b, max_iter=600, tol=tol, restart=50, ref_givens=False)
+    op64.set_inner_operator(cheap)
+    xf, inf = op64.solve(b, max_iter=600, tol=tol, restart=30, flexible=True, inner_iters=10)
+    assert inf.converged
+    assert rel(op64.matvec(xf), b) <= tol * 1.0001
+    assert rel(xf, x64) < 100 * tol
+    # the inner operator serves flexible solves only; a plain solve ignores it
+    x2, i2 = op64.solve(b, max_iter=600, tol=tol, restart=50, ref_givens=False)
+    assert i2.converged and rel(x2, x64) < 1e-12
+    # a different tree is refused; destroying the inner operator detaches it
+    other = MLFMA.rwg(m, PW, max_node_srcs=8, ref_compat=0, precision=1, self_terms=1).setup()
+    with pytest.raises(Exception):
+        op64.set_inner_operator(other)
+    other.close()
+    cheap.close()
+    xf2, inf2 = op64.solve(b, max_iter=600, tol=tol, restart=30, flexible=True, inner_iters=10)
+    assert inf2.converged and rel(op64.matvec(xf2), b) <= tol * 1.0001
+    op64.close()
