@@ -395,6 +395,12 @@ int mlfma_get_stream(mlfma_handle h, void** stream);
 
 /* CUDA-event time of each stage of one matvec on the handle's stream. */
 int mlfma_time_stages(mlfma_handle h, mlfma_stage_times* t);
+/* CUDA-event time (ms) of each level's far-field launches, one at a time on
+ * the handle's stream: for level l, ms[3l] the interpolation into l (M2M from
+ * l + 1), ms[3l + 1] the translation at l, ms[3l + 2] the anterpolation out of
+ * l (L2L to l + 1); 0 where a level has none.  *nlevels = max level + 1; ms ==
+ * NULL only asks for it; cap >= 3 * *nlevels. */
+int mlfma_time_levels(mlfma_handle h, int cap, float* ms, int* nlevels);
 int mlfma_get_traffic(mlfma_handle h, mlfma_traffic* t);
 
 /* Diagnostics: angular grid of a level (sizes: nth, nph, L) and the

@@ -445,6 +445,15 @@ class MLFMA:
         check(lib().mlfma_time_stages(self._h, ctypes.byref(t)))
         return {k: float(getattr(t, k)) for k, _ in StageTimes._fields_}
 
+    def level_times(self) -> dict:
+        """Per far level: {"m2m": ms into it, "m2l": ms at it, "l2l": ms out of it} (mlfma_time_levels)."""
+        nl = ctypes.c_int()
+        check(lib().mlfma_time_levels(self._h, 0, None, ctypes.byref(nl)))
+        buf = (ctypes.c_float * (3 * nl.value))()
+        check(lib().mlfma_time_levels(self._h, 3 * nl.value, buf, ctypes.byref(nl)))
+        return {l: {"m2m": buf[3 * l], "m2l": buf[3 * l + 1], "l2l": buf[3 * l + 2]}
+                for l in range(nl.value) if any(buf[3 * l + k] for k in range(3))}
+
     def traffic(self) -> dict:
         t = Traffic()
         check(lib().mlfma_get_traffic(self._h, ctypes.byref(t)))

@@ -130,6 +130,7 @@ SIGNATURES = {
     "mlfma_batch_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "mlfma_get_stream": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]),
     "mlfma_time_stages": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(StageTimes)]),
+    "mlfma_time_levels": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_float), _ip]),
     "mlfma_get_traffic": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Traffic)]),
     "mlfma_level_info": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _ip, _dp, _dp, _dp]),
     "mlfma_level_boxes": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _ip, _ip]),

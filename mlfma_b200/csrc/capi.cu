@@ -781,6 +781,19 @@ int mlfma_time_stages(mlfma_handle h, mlfma_stage_times* t) {
     return MLFMA_OK;
 }
 
+int mlfma_time_levels(mlfma_handle h, int cap, float* ms, int* nlevels) {
+    if (!h || !nlevels) return fail(MLFMA_ERR_ARG, "null argument");
+    if (!ready(h)) return fail(MLFMA_ERR_STATE, "mlfma_setup has not run");
+    *nlevels = h->plan.max_level + 1;
+    if (!ms) return MLFMA_OK;
+    if (cap < 3 * *nlevels) return fail(MLFMA_ERR_ARG, "buffer too small");
+    std::vector<float> v;
+    std::string e = h->dev->time_levels(v);
+    if (!e.empty()) return fail(MLFMA_ERR_CUDA, e);
+    std::copy(v.begin(), v.end(), ms);
+    return MLFMA_OK;
+}
+
 int mlfma_get_traffic(mlfma_handle h, mlfma_traffic* t) {
     if (!h || !t) return fail(MLFMA_ERR_ARG, "null argument");
     if (!ready(h)) return fail(MLFMA_ERR_STATE, "mlfma_setup has not run");

@@ -246,6 +246,8 @@ public:
 
     // Per-stage CUDA-event timing of one matvec on the operator's stream.
     std::string time_stages(StageTimes* out);
+    // per level l (index l): M2M into l, M2L at l, L2L out of l (ms; 0 where none)
+    std::string time_levels(std::vector<float>& out);
     // Chooses launch shapes by timing them on this operator (see kernels.cu).
     std::string autotune(int nr, int reps, TuneReport* rep);
     // Same for a product on nr right-hand sides.

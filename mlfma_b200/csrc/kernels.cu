@@ -1055,6 +1055,49 @@ std::string DeviceOp::time_stages(StageTimes* out) {
     return {};
 }
 
+std::string DeviceOp::time_levels(std::vector<float>& out) {
+    if (!ready_) return "operator not set up";
+    MLFMA_CK(cudaSetDevice(device_));
+    out.assign(3 * static_cast<size_t>(lmax_ + 1), 0.0f);
+    if (n_leaves_ == 0) return {};
+    const bool tcf = precision_ != kFp64;
+    const bool tc_up = tcf && (tc_mode_ & 1), tc_dn = tcf && (tc_mode_ & 4);
+    cudaStream_t s = stream_;
+    cudaEvent_t a, b;
+    MLFMA_CK(cudaEventCreate(&a));
+    MLFMA_CK(cudaEventCreate(&b));
+    auto timed = [&](auto&& fn) {
+        cudaEventRecord(a, s);
+        fn();
+        cudaEventRecord(b, s);
+        cudaEventSynchronize(b);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, a, b);
+        return ms;
+    };
+    if (precision_ == kFp64) far_s2m<double, false>(f64_, xt_, s); else far_s2m<float, false>(f32_, xt_, s);
+    for (int p = lmax_ - 1; p >= lmin_; --p)
+        out[3 * p] = timed([&] {
+            if (tc_up) far_m2m_tc(p, 1, s);
+            else if (precision_ == kFp64) far_m2m<double, false>(f64_, p, s);
+            else far_m2m<float, false>(f32_, p, s);
+        });
+    for (int l = lmax_; l >= lmin_; --l)
+        out[3 * l + 1] = timed([&] {
+            if (precision_ == kFp64) far_m2l<double, false>(f64_, l, l, s); else far_m2l<float, false>(f32_, l, l, s);
+        });
+    for (int p = lmin_; p < lmax_; ++p)
+        out[3 * p + 2] = timed([&] {
+            if (tc_dn) far_l2l_tc(p, 1, s);
+            else if (precision_ == kFp64) far_l2l<double, false>(f64_, p, s);
+            else far_l2l<float, false>(f32_, p, s);
+        });
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    MLFMA_CK(cudaGetLastError());
+    return {};
+}
+
 std::string DeviceOp::farfield(const double2* cur, int ndir, const double* khat, double2* out, cudaStream_t s) {
     if (!ready_) return "operator not set up";
     if (ndir <= 0) return {};
