@@ -336,6 +336,10 @@ typedef struct {
     int schedule;              /* one-vector product: bit 0 translation lists staged in shared memory,
                                   bit 1 near field started after aggregation, bit 2 two side streams
                                   for the finer levels' translations */
+    int m2m_staged;            /* one-vector interpolation: bit p = transition p+1 -> p sums the children
+                                  first in shared memory (else one interpolation per child) */
+    int l2l_staged;            /* one-vector anterpolation: bit p = transition p -> p+1 stages the parent's
+                                  local pattern in shared memory */
 } mlfma_tuning;
 
 /* Autotuner: times the candidate launch shapes of the stages on this operator
@@ -362,6 +366,14 @@ int mlfma_autotune(mlfma_handle h, int nrhs, int reps, mlfma_tuning* out);
  * kernels to float rounding. */
 int mlfma_set_interp_path(mlfma_handle h, int mode);
 int mlfma_get_interp_path(mlfma_handle h, int* mode);
+/* CUDA-core interpolation kernels of the one-vector product, on every level
+ * transition where their shared memory fits: bit 0, M2M with the children
+ * shifted and summed on the child grid first (one interpolation per parent,
+ * all taps from shared memory; rounding-level differences from the per-child
+ * kernel); bit 1, L2L with the parent's shifted local pattern staged in shared
+ * memory (the same arithmetic in the same order).  Both are on after setup;
+ * mlfma_autotune chooses per transition (mlfma_tuning.m2m_staged/l2l_staged). */
+int mlfma_set_staged_interp(mlfma_handle h, int mode);
 
 /* ---- Many independent operators of uneven size (no counterpart in the
  * reference, which holds one problem per process).  A batch refers to set-up

@@ -264,6 +264,11 @@ class MLFMA:
         return x, SolveResult(info.iterations, info.residual, info.true_residual, info.seconds, converged,
                               info.refinements)
 
+    def set_staged_interp(self, mode: int) -> None:
+        """bit 0: M2M children summed first in shared memory; bit 1: L2L with the parent
+        staged in shared memory (mlfma_set_staged_interp)."""
+        check(lib().mlfma_set_staged_interp(self._h, int(mode)))
+
     def set_inner_operator(self, inner: "MLFMA | None") -> None:
         """Operator of the inner iterations of flexible solves (mlfma_set_inner_operator):
         same sources and tree, e.g. fewer digits or mixed precision.  None detaches it."""
@@ -419,7 +424,8 @@ class MLFMA:
         return {"m2l_chunk": t.m2l_chunk, "m2m_rows": list(t.m2m_rows), "multi_m2m_rows_fast": t.multi_m2m_rows_fast,
                 "multi_l2l_pairs": t.multi_l2l_pairs, "product_ms_before": t.product_ms_before,
                 "product_ms_after": t.product_ms_after, "near_blocks_per_sm": t.near_blocks_per_sm,
-                "interp_path": t.interp_path, "schedule": t.schedule}
+                "interp_path": t.interp_path, "schedule": t.schedule, "m2m_staged": t.m2m_staged,
+                "l2l_staged": t.l2l_staged}
 
     @property
     def interp_path(self) -> int:

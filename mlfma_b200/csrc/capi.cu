@@ -739,6 +739,8 @@ int mlfma_autotune(mlfma_handle h, int nrhs, int reps, mlfma_tuning* out) {
         out->near_blocks_per_sm = r.near_blocks_per_sm;
         out->interp_path = r.interp_path;
         out->schedule = r.schedule;
+        out->m2m_staged = r.m2m_staged;
+        out->l2l_staged = r.l2l_staged;
     }
     return MLFMA_OK;
 }
@@ -747,6 +749,12 @@ int mlfma_set_interp_path(mlfma_handle h, int mode) {
     if (!h) return fail(MLFMA_ERR_ARG, "null handle");
     if (!ready(h)) return fail(MLFMA_ERR_STATE, "mlfma_setup has not run");
     return from_msg(h->dev->set_tc(mode));
+}
+
+int mlfma_set_staged_interp(mlfma_handle h, int mode) {
+    if (!h) return fail(MLFMA_ERR_ARG, "null handle");
+    if (!ready(h)) return fail(MLFMA_ERR_STATE, "mlfma_setup has not run");
+    return from_msg(h->dev->set_staged(mode));
 }
 
 int mlfma_get_interp_path(mlfma_handle h, int* mode) {

@@ -405,6 +405,27 @@ std::string DeviceOp::setup_far(const Plan& plan, FarField<R>& F, const double2*
             MLFMA_CK(cudaFuncSetAttribute(t ? k_l2t_half<R, true> : k_l2t_half<R, false>, attr, dev_smem));
         }
     }
+    {  // staged interpolation: dynamic shared memory up to the limit less the static part
+        auto dyn = [&](const void* fn) -> cudaError_t {
+            cudaFuncAttributes fa{};
+            cudaError_t e = cudaFuncGetAttributes(&fa, fn);
+            if (e != cudaSuccess) return e;
+            return cudaFuncSetAttribute(fn, attr, dev_smem - static_cast<int>(fa.sharedSizeBytes));
+        };
+        MLFMA_CK(dyn(reinterpret_cast<const void*>(k_m2m_sum<R, 2>)));
+        MLFMA_CK(dyn(reinterpret_cast<const void*>(k_m2m_sum<R, 4>)));
+        MLFMA_CK(dyn(reinterpret_cast<const void*>(k_m2m_sum<R, 6>)));
+        MLFMA_CK(dyn(reinterpret_cast<const void*>(k_m2m_sum<R, 8>)));
+        MLFMA_CK(dyn(reinterpret_cast<const void*>(k_m2m_sum<R, 10>)));
+        for (int tr = 0; tr < 2; ++tr) {
+            const bool t = tr != 0;
+            MLFMA_CK(dyn(reinterpret_cast<const void*>(t ? k_l2l_st<R, 8, true> : k_l2l_st<R, 8, false>)));
+            MLFMA_CK(dyn(reinterpret_cast<const void*>(t ? k_l2l_st<R, 12, true> : k_l2l_st<R, 12, false>)));
+            MLFMA_CK(dyn(reinterpret_cast<const void*>(t ? k_l2l_st<R, 16, true> : k_l2l_st<R, 16, false>)));
+            MLFMA_CK(dyn(reinterpret_cast<const void*>(t ? k_l2l_st<R, 24, true> : k_l2l_st<R, 24, false>)));
+            MLFMA_CK(dyn(reinterpret_cast<const void*>(t ? k_l2l_st<R, 32, true> : k_l2l_st<R, 32, false>)));
+        }
+    }
     if (max_rhs_ > 1) {
         // dynamic shared memory up to the opt-in limit less the kernel's static part
         auto dyn = [&](const void* fn) -> cudaError_t {
@@ -511,6 +532,9 @@ std::string DeviceOp::setup(const Plan& plan, int device, int precision, int max
         // ---- transitions: L2L pairs and stencil widths
         l2l_pairs_.assign(std::max(lmax_, 0) + 1, nullptr);
         m2m_rows_.assign(std::max(lmax_, 0) + 1, 1);
+        m2m_pref_.assign(std::max(lmax_, 0) + 1, 0);
+        l2l_pref_.assign(std::max(lmax_, 0) + 1, 0);
+        MLFMA_CK(cudaDeviceGetAttribute(&dev_smem_, cudaDevAttrMaxSharedMemoryPerBlockOptin, device_));
         n_l2l_pairs_.assign(std::max(lmax_, 0) + 1, 0);
         npar_.assign(std::max(lmax_, 0) + 1, 0);
         up_w_.assign(std::max(lmax_, 0) + 1, 0);
@@ -534,6 +558,8 @@ std::string DeviceOp::setup(const Plan& plan, int device, int precision, int max
             up_w_[p] = w_up;
             dn_w_[p] = w_dn;
             m2m_rows_[p] = m2m_rows(nth_[p], nph_[p]);
+            m2m_pref_[p] = 1;
+            l2l_pref_[p] = 1;
             npar_[p] = static_cast<int>(T.par_box.size());
             std::vector<int2> pairs;
             for (int q = 0; q < npar_[p]; ++q) {
@@ -761,8 +787,19 @@ void DeviceOp::far_m2m(FarField<R>& F, int p, cudaStream_t s) {
     if (npar_[p] == 0) return;
     const int rows = m2m_rows_[p];
     const dim3 grid(npar_[p], (nth_[p] + rows - 1) / rows);
-    const size_t smem = static_cast<size_t>(8) * rows * nph_[p + 1] * 2 * sizeof(C);
     const DevTransT<R>& T = F.trans[p];
+    const size_t ssum = m2m_sum_smem(nth_[p + 1], nph_[p + 1], rows, sizeof(C));
+    if (!TR && m2m_pref_[p] && ssum + 1024 <= static_cast<size_t>(dev_smem_)) {
+        switch (up_w_[p]) {
+            case 2: k_m2m_sum<R, 2><<<grid, 256, ssum, s>>>(F.lv_dev, T, rows); break;
+            case 4: k_m2m_sum<R, 4><<<grid, 256, ssum, s>>>(F.lv_dev, T, rows); break;
+            case 6: k_m2m_sum<R, 6><<<grid, 256, ssum, s>>>(F.lv_dev, T, rows); break;
+            case 8: k_m2m_sum<R, 8><<<grid, 256, ssum, s>>>(F.lv_dev, T, rows); break;
+            default: k_m2m_sum<R, 10><<<grid, 256, ssum, s>>>(F.lv_dev, T, rows); break;
+        }
+        return;
+    }
+    const size_t smem = static_cast<size_t>(8) * rows * nph_[p + 1] * 2 * sizeof(C);
     switch (up_w_[p]) {
         case 2: k_m2m<R, 2, TR><<<grid, 128, smem, s>>>(F.lv_dev, T, rows); break;
         case 4: k_m2m<R, 4, TR><<<grid, 128, smem, s>>>(F.lv_dev, T, rows); break;
@@ -790,8 +827,19 @@ void DeviceOp::far_l2l(FarField<R>& F, int p, cudaStream_t s) {
     using C = typename Cx<R>::T;
     const int g = n_l2l_pairs_[p];
     if (!g) return;
-    const size_t smem = static_cast<size_t>(nth_[p]) * nph_[p + 1] * 2 * sizeof(C);
     const DevTransT<R>& T = F.trans[p];
+    const size_t sst = l2l_st_smem(nth_[p], nph_[p], nph_[p + 1], sizeof(C));
+    if (l2l_pref_[p] && sst + 1024 <= static_cast<size_t>(dev_smem_)) {
+        switch (dn_w_[p]) {
+            case 8: k_l2l_st<R, 8, TR><<<g, 256, sst, s>>>(F.lv_dev, T, l2l_pairs_[p]); break;
+            case 12: k_l2l_st<R, 12, TR><<<g, 256, sst, s>>>(F.lv_dev, T, l2l_pairs_[p]); break;
+            case 16: k_l2l_st<R, 16, TR><<<g, 256, sst, s>>>(F.lv_dev, T, l2l_pairs_[p]); break;
+            case 24: k_l2l_st<R, 24, TR><<<g, 256, sst, s>>>(F.lv_dev, T, l2l_pairs_[p]); break;
+            default: k_l2l_st<R, 32, TR><<<g, 256, sst, s>>>(F.lv_dev, T, l2l_pairs_[p]); break;
+        }
+        return;
+    }
+    const size_t smem = static_cast<size_t>(nth_[p]) * nph_[p + 1] * 2 * sizeof(C);
     switch (dn_w_[p]) {
         case 8: k_l2l<R, 8, TR><<<g, 256, smem, s>>>(F.lv_dev, T, l2l_pairs_[p]); break;
         case 12: k_l2l<R, 12, TR><<<g, 256, smem, s>>>(F.lv_dev, T, l2l_pairs_[p]); break;
@@ -1699,6 +1747,20 @@ std::string DeviceOp::set_tc(int mode) {
     return {};
 }
 
+std::string DeviceOp::set_staged(int mode) {
+    if (!ready_) return "operator not set up";
+    if (mode < 0 || mode > 3) return "arg:mode must be 0..3";
+    MLFMA_CK(cudaSetDevice(device_));
+    MLFMA_CK(cudaStreamSynchronize(stream_));
+    for (int p = lmin_; p < lmax_; ++p) {
+        m2m_pref_[p] = mode & 1;
+        l2l_pref_[p] = (mode >> 1) & 1;
+    }
+    drop_graphs();
+    ++generation_;
+    return {};
+}
+
 // ================================================================= autotuner
 
 // Times the candidate launch shapes of the stages on this operator (CUDA
@@ -1768,22 +1830,40 @@ std::string DeviceOp::autotune(int nr, int reps, TuneReport* rep) {
         }
         build_m2l_items(best_chunk);
         r.m2l_chunk = best_chunk;
-        // M2M: parent rows per block, per transition
+        // M2M: kernel (per child or children summed first, staged) and parent
+        // rows per block, per transition; L2L: kernel (staged or not)
         for (int p = lmin_; p < lmax_; ++p) {
             if (!npar_[p]) continue;
             float bt = 1e30f;
-            int brows = m2m_rows_[p];
-            for (int rows : {1, 2, 4, 8, 16}) {
-                if (rows > nth_[p] || static_cast<size_t>(8) * rows * nph_[p + 1] * 2 * csize > static_cast<size_t>(dev_smem))
-                    continue;
-                m2m_rows_[p] = rows;
-                const float t = timed([&] {
-                    if (precision_ == kFp64) far_m2m<double, false>(f64_, p, s); else far_m2m<float, false>(f32_, p, s);
-                });
-                if (t < bt) { bt = t; brows = rows; }
-            }
+            int brows = m2m_rows_[p], bkind = m2m_pref_[p];
+            for (int kind : {0, 1})
+                for (int rows : {1, 2, 4, 8, 16, 32, 64}) {
+                    if (rows > nth_[p] && rows != 1) continue;
+                    const size_t need = kind ? m2m_sum_smem(nth_[p + 1], nph_[p + 1], rows, csize) + 1024
+                                             : static_cast<size_t>(8) * rows * nph_[p + 1] * 2 * csize;
+                    if (need > static_cast<size_t>(dev_smem) || (!kind && rows > 16)) continue;
+                    m2m_rows_[p] = rows;
+                    m2m_pref_[p] = kind;
+                    const float t = timed([&] {
+                        if (precision_ == kFp64) far_m2m<double, false>(f64_, p, s); else far_m2m<float, false>(f32_, p, s);
+                    });
+                    if (t < bt) { bt = t; brows = rows; bkind = kind; }
+                }
             m2m_rows_[p] = brows;
+            m2m_pref_[p] = bkind;
             r.m2m_rows[p] = brows;
+            if (n_l2l_pairs_[p]) {
+                float lt = 1e30f;
+                int lkind = l2l_pref_[p];
+                for (int kind : {0, 1}) {
+                    l2l_pref_[p] = kind;
+                    const float t = timed([&] {
+                        if (precision_ == kFp64) far_l2l<double, false>(f64_, p, s); else far_l2l<float, false>(f32_, p, s);
+                    });
+                    if (t < lt) { lt = t; lkind = kind; }
+                }
+                l2l_pref_[p] = lkind;
+            }
         }
         // near field: persistent blocks per SM, timed on the whole product (it
         // runs beside the far-field chain and competes with it for the SMs)
@@ -1870,6 +1950,11 @@ std::string DeviceOp::autotune(int nr, int reps, TuneReport* rep) {
     }
     r.interp_path = tc_mode();
     r.m2l_chunk = m2l_chunk_;
+    r.m2m_staged = r.l2l_staged = 0;
+    for (int p = lmin_; p < lmax_ && p < 31; ++p) {
+        if (m2m_pref_[p]) r.m2m_staged |= 1 << p;
+        if (l2l_pref_[p]) r.l2l_staged |= 1 << p;
+    }
     for (int p = lmin_; p < lmax_; ++p) r.m2m_rows[p] = m2m_rows_[p];
     if (r.multi_rows_fast == 0 && m_m2m_rows_fast_ < 0) r.multi_rows_fast = -1;
     // restore the local patterns, drop captured graphs

@@ -562,6 +562,171 @@ k_l2l(const DevLevelT<R>* __restrict__ lvs, DevTransT<R> T, const int2* __restri
     }
 }
 
+// ------------------------------------------------------------ staged interpolation
+// M2M with the children shifted and summed on the child grid first:
+// U = sum_c shift_up(oct_c) A_c over the child theta rows the block's
+// stencils read, then the theta pass (pole reflection as in k_m2m) into V,
+// then the phi pass to the parent.  Interpolation is linear and the same for
+// every child, so this is k_m2m's sum in another order (one interpolation per
+// parent instead of one per child).  Block = (parent, tile of `rows` parent
+// theta rows); each child value is read from global memory once per block and
+// every stencil tap reads shared memory.
+template <class R, int W>  // taps per row: 2 * interp_order (both passes)
+__global__ void __launch_bounds__(256)
+k_m2m_sum(const DevLevelT<R>* __restrict__ lvs, DevTransT<R> T, int rows) {
+    using C = typename Cx<R>::T;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    __shared__ int band[2];
+    const int par = blockIdx.x;
+    const DevLevelT<R> P = lvs[T.plevel];
+    const DevLevelT<R> Cl = lvs[T.plevel + 1];
+    const int nph = P.nph, mph = Cl.nph, halfm = Cl.nph / 2;
+    const int r0 = blockIdx.y * rows;
+    const int nrow = min(P.nth, r0 + rows) - r0;
+    if (nrow <= 0) return;  // the whole block
+    if (threadIdx.x == 0) {
+        band[0] = Cl.nth;
+        band[1] = -1;
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < nrow * W; q += blockDim.x) {
+        const int src = T.up_th.src[r0 * W + q];
+        atomicMin(&band[0], src);
+        atomicMax(&band[1], src);
+    }
+    __syncthreads();
+    const int lo = band[0], nb = band[1] - lo + 1;
+    C* U = reinterpret_cast<C*>(smraw);              // [nb * mph][2], child rows lo..lo+nb-1
+    C* V = U + 2 * static_cast<size_t>(nb) * mph;    // [nrow * mph][2]
+    const int c0 = T.child_ptr[par], nch = T.child_ptr[par + 1] - c0;
+    for (int e = threadIdx.x; e < nb * mph; e += blockDim.x) {
+        const int d = lo * mph + e;
+        C u0 = zero<C>(), u1 = zero<C>();
+#pragma unroll 8
+        for (int c = 0; c < nch; ++c) {
+            const C* Ac = Cl.A + static_cast<size_t>(T.child_box[c0 + c]) * Cl.ndir * 2;
+            const C ph = Cl.shift_up[static_cast<size_t>(T.child_oct[c0 + c]) * Cl.ndir + d];
+            u0 = cfma(ph, Ac[2 * d], u0);
+            u1 = cfma(ph, Ac[2 * d + 1], u1);
+        }
+        U[2 * e] = u0;
+        U[2 * e + 1] = u1;
+    }
+    __syncthreads();
+    for (int it = threadIdx.x; it < nrow * mph; it += blockDim.x) {
+        const int jr = it / mph, iph = it - jr * mph;
+        const int jth = r0 + jr;
+        C v0 = zero<C>(), v1 = zero<C>();
+#pragma unroll
+        for (int k = 0; k < W; ++k) {
+            const int q = jth * W + k;
+            const bool rf = T.up_th.refl[q];
+            const int sp = rf ? (iph < halfm ? iph + halfm : iph - halfm) : iph;
+            const R cf = T.up_th.coef[q];
+            const int e = (T.up_th.src[q] - lo) * mph + sp;
+            v0 = crfma(cf, U[2 * e], v0);
+            v1 = crfma(cf, U[2 * e + 1], v1);
+        }
+        V[2 * it] = v0;
+        V[2 * it + 1] = v1;
+    }
+    __syncthreads();
+    C* Ap = P.A + (static_cast<size_t>(T.par_box[par]) * P.ndir + static_cast<size_t>(r0) * nph) * 2;
+    for (int o = threadIdx.x; o < nrow * nph; o += blockDim.x) {
+        const int jr = o / nph, jph = o - jr * nph;
+        const C* row = V + static_cast<size_t>(jr) * mph * 2;
+        C a0 = zero<C>(), a1 = zero<C>();
+#pragma unroll
+        for (int k = 0; k < W; ++k) {
+            const int q = jph * W + k;
+            const int s = T.up_ph.src[q];
+            const R cf = T.up_ph.coef[q];
+            a0 = crfma(cf, row[2 * s], a0);
+            a1 = crfma(cf, row[2 * s + 1], a1);
+        }
+        Ap[2 * o] = a0;
+        Ap[2 * o + 1] = a1;
+    }
+}
+
+// Shared memory of k_m2m_sum for a tile of `rows` parent rows (bound: every
+// child row in the band).
+inline size_t m2m_sum_smem(int child_nth, int child_nph, int rows, size_t csize) {
+    return static_cast<size_t>(child_nth + rows) * child_nph * 2 * csize;
+}
+
+// L2L (and, POST, the transposed M2M) with the parent's local pattern, shifted
+// to the child's octant, staged in shared memory once per block: the same
+// arithmetic in the same order as k_l2l, every phi tap then reading shared
+// memory instead of global memory.  One block per (parent, child) pair.
+template <class R, int W, bool POST>  // both transposed stencils padded to W taps per row
+__global__ void __launch_bounds__(256)
+k_l2l_st(const DevLevelT<R>* __restrict__ lvs, DevTransT<R> T, const int2* __restrict__ pairs) {
+    using C = typename Cx<R>::T;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    const int2 pc = pairs[blockIdx.x];  // parent index, child entry
+    const DevLevelT<R> P = lvs[T.plevel];
+    const DevLevelT<R> Cl = lvs[T.plevel + 1];
+    const int pth = P.nth, pph = P.nph, cth = Cl.nth, cph = Cl.nph, halfc = Cl.nph / 2;
+    C* SB = reinterpret_cast<C*>(smraw);                    // [pth * pph][2]
+    C* S1 = SB + 2 * static_cast<size_t>(pth) * pph;        // [pth * cph][2]
+    const C* Bp = P.B + static_cast<size_t>(T.par_box[pc.x]) * P.ndir * 2;
+    const C* sh = P.shift_down + static_cast<size_t>(T.child_oct[pc.y]) * P.ndir;
+    for (int d = threadIdx.x; d < pth * pph; d += blockDim.x) {
+        C b0 = Bp[2 * d], b1 = Bp[2 * d + 1];
+        if (!POST) {
+            const C ph = sh[d];
+            b0 = cmul(ph, b0);
+            b1 = cmul(ph, b1);
+        }
+        SB[2 * d] = b0;
+        SB[2 * d + 1] = b1;
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < pth * cph; e += blockDim.x) {
+        const int ith = e / cph, jph = e - ith * cph;
+        const C* row = SB + static_cast<size_t>(ith) * pph * 2;
+        C v0 = zero<C>(), v1 = zero<C>();
+#pragma unroll
+        for (int k = 0; k < W; ++k) {
+            const int q = jph * W + k;
+            const int d = T.dn_ph.src[q];
+            const R cf = T.dn_ph.coef[q];
+            v0 = crfma(cf, row[2 * d], v0);
+            v1 = crfma(cf, row[2 * d + 1], v1);
+        }
+        S1[2 * e] = v0;
+        S1[2 * e + 1] = v1;
+    }
+    __syncthreads();
+    C* Bc = Cl.B + static_cast<size_t>(T.child_box[pc.y]) * Cl.ndir * 2;
+    for (int e = threadIdx.x; e < cth * cph; e += blockDim.x) {
+        const int jth = e / cph, jph = e - jth * cph;
+        C v0 = zero<C>(), v1 = zero<C>();
+#pragma unroll
+        for (int k = 0; k < W; ++k) {
+            const int q = jth * W + k;
+            const bool rf = T.dn_th.refl[q];
+            const int sp = rf ? (jph < halfc ? jph + halfc : jph - halfc) : jph;
+            const R cf = T.dn_th.coef[q];
+            const C* row = S1 + (static_cast<size_t>(T.dn_th.src[q]) * cph + sp) * 2;
+            v0 = crfma(cf, row[0], v0);
+            v1 = crfma(cf, row[1], v1);
+        }
+        if (POST) {
+            const C ph = Cl.shift_up[static_cast<size_t>(T.child_oct[pc.y]) * Cl.ndir + e];
+            v0 = cmul(ph, v0);
+            v1 = cmul(ph, v1);
+        }
+        Bc[2 * e] = cadd(Bc[2 * e], v0);
+        Bc[2 * e + 1] = cadd(Bc[2 * e + 1], v1);
+    }
+}
+
+inline size_t l2l_st_smem(int parent_nth, int parent_nph, int child_nph, size_t csize) {
+    return static_cast<size_t>(parent_nth) * (parent_nph + child_nph) * 2 * csize;
+}
+
 // Complex double -> far-field type (patterns, tables at setup).
 template <class C>
 __global__ void k_narrow(const double2* __restrict__ src, C* __restrict__ dst, long long n) {
