@@ -340,6 +340,8 @@ typedef struct {
                                   first in shared memory (else one interpolation per child) */
     int l2l_staged;            /* one-vector anterpolation: bit p = transition p -> p+1 stages the parent's
                                   local pattern in shared memory */
+    int near_kernel;           /* one-vector near field: 0 one tile per thread block (row and column
+                                  threads), 1 one tile per warp (see mlfma_set_near_kernel) */
 } mlfma_tuning;
 
 /* Autotuner: times the candidate launch shapes of the stages on this operator
@@ -374,6 +376,13 @@ int mlfma_get_interp_path(mlfma_handle h, int* mode);
  * memory (the same arithmetic in the same order).  Both are on after setup;
  * mlfma_autotune chooses per transition (mlfma_tuning.m2m_staged/l2l_staged). */
 int mlfma_set_staged_interp(mlfma_handle h, int mode);
+/* Near-field kernel of the one-vector product (Leaf::evalPairSols,
+ * evalNearNonNborSols, evalSelfSols, src/fmm/leaf.cpp:318-383; each stored block
+ * applied as Z and Z^T, tiles streamed by bulk copies): kind 0, one tile per
+ * thread block (row threads and column threads); kind 1 (the default), one
+ * tile per warp, each entry read from shared memory once and the row sums
+ * formed by a warp reduce-scatter.  Same partial sums, other rounding order. */
+int mlfma_set_near_kernel(mlfma_handle h, int kind);
 
 /* ---- Many independent operators of uneven size (no counterpart in the
  * reference, which holds one problem per process).  A batch refers to set-up

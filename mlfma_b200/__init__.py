@@ -269,6 +269,10 @@ class MLFMA:
         staged in shared memory (mlfma_set_staged_interp)."""
         check(lib().mlfma_set_staged_interp(self._h, int(mode)))
 
+    def set_near_kernel(self, kind: int) -> None:
+        """0: one near-field tile per thread block; 1: one per warp (mlfma_set_near_kernel)."""
+        check(lib().mlfma_set_near_kernel(self._h, int(kind)))
+
     def set_inner_operator(self, inner: "MLFMA | None") -> None:
         """Operator of the inner iterations of flexible solves (mlfma_set_inner_operator):
         same sources and tree, e.g. fewer digits or mixed precision.  None detaches it."""
@@ -425,7 +429,7 @@ class MLFMA:
                 "multi_l2l_pairs": t.multi_l2l_pairs, "product_ms_before": t.product_ms_before,
                 "product_ms_after": t.product_ms_after, "near_blocks_per_sm": t.near_blocks_per_sm,
                 "interp_path": t.interp_path, "schedule": t.schedule, "m2m_staged": t.m2m_staged,
-                "l2l_staged": t.l2l_staged}
+                "l2l_staged": t.l2l_staged, "near_kernel": t.near_kernel}
 
     @property
     def interp_path(self) -> int:

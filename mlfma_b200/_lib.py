@@ -70,7 +70,7 @@ class Tuning(ctypes.Structure):
                 ("multi_l2l_pairs", ctypes.c_int), ("product_ms_before", ctypes.c_float),
                 ("product_ms_after", ctypes.c_float), ("near_blocks_per_sm", ctypes.c_int),
                 ("interp_path", ctypes.c_int), ("schedule", ctypes.c_int), ("m2m_staged", ctypes.c_int),
-                ("l2l_staged", ctypes.c_int)]
+                ("l2l_staged", ctypes.c_int), ("near_kernel", ctypes.c_int)]
 
 
 # name -> (restype, argtypes); every symbol the header declares.
@@ -139,6 +139,7 @@ SIGNATURES = {
     "mlfma_level_transl": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _dp]),
     "mlfma_level_transl_gpu": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _dp]),
     "mlfma_set_staged_interp": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "mlfma_set_near_kernel": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "mlfma_set_inner_operator": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "mlfma_far_leaves": (ctypes.c_int, [ctypes.c_void_p, _ip, _ip, _ip]),
     "mlfma_tree_export": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _ip, ctypes.c_longlong,

@@ -741,6 +741,7 @@ int mlfma_autotune(mlfma_handle h, int nrhs, int reps, mlfma_tuning* out) {
         out->schedule = r.schedule;
         out->m2m_staged = r.m2m_staged;
         out->l2l_staged = r.l2l_staged;
+        out->near_kernel = r.near_kernel;
     }
     return MLFMA_OK;
 }
@@ -749,6 +750,12 @@ int mlfma_set_interp_path(mlfma_handle h, int mode) {
     if (!h) return fail(MLFMA_ERR_ARG, "null handle");
     if (!ready(h)) return fail(MLFMA_ERR_STATE, "mlfma_setup has not run");
     return from_msg(h->dev->set_tc(mode));
+}
+
+int mlfma_set_near_kernel(mlfma_handle h, int kind) {
+    if (!h) return fail(MLFMA_ERR_ARG, "null handle");
+    if (!ready(h)) return fail(MLFMA_ERR_STATE, "mlfma_setup has not run");
+    return from_msg(h->dev->set_near_kernel(kind));
 }
 
 int mlfma_set_staged_interp(mlfma_handle h, int mode) {

@@ -157,6 +157,7 @@ struct TuneReport {
     int schedule;                  // one-vector product: bit 0 staged M2L lists, bit 1 near field after
                                    // S2M, bit 2 two side streams for the finer levels' M2L
     int m2m_staged, l2l_staged;    // one-vector: bit p = transition p -> p + 1 on the staged kernels
+    int near_kernel;               // one-vector near field: 0 k_near_sym, 1 k_near_warp
 };
 
 // Tensor-core interpolation and anterpolation of one level transition
@@ -249,6 +250,7 @@ public:
     std::string time_stages(StageTimes* out);
     // bit 0: every transition's M2M on k_m2m_sum, bit 1: L2L on k_l2l_st (where they fit)
     std::string set_staged(int mode);
+    std::string set_near_kernel(int kind);  // 0 k_near_sym, 1 k_near_warp
     // per level l (index l): M2M into l, M2L at l, L2L out of l (ms; 0 where none)
     std::string time_levels(std::vector<float>& out);
     // Chooses launch shapes by timing them on this operator (see kernels.cu).
@@ -366,6 +368,7 @@ private:
     std::vector<int> m2m_rows_;           // one-vector M2M parent rows per block, per transition
     std::vector<int> m2m_pref_, l2l_pref_;  // per transition: 1 = staged kernels (k_m2m_sum, k_l2l_st) where they fit
     int dev_smem_ = 0;                    // opt-in shared memory per block
+    int near_kernel_ = 1;                 // one-vector near field: 0 k_near_sym, 1 k_near_warp
     int m_m2m_rows_fast_ = -1;            // many-rhs M2M grid order (-1: precision default)
     int m_l2l_pairs_ = 0;                 // many-rhs L2L column pairs per block (0: precision default)
     std::vector<int2*> l2l_pairs_;       // per parent level: (parent, child entry)

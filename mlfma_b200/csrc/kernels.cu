@@ -127,6 +127,7 @@ DeviceOp::~DeviceOp() {
 // block, so that a small operator leaves room for the kernels of others
 // running beside it.
 void DeviceOp::set_near_grid(int per_sm) {
+    if (near_kernel_ == 1) per_sm = 1;  // k_near_warp: one block per SM (its ring fills the shared memory)
     near_grid_ = std::max(1, std::min(n_near_tiles_ / 4, std::max(1, per_sm) * sms_));
 }
 
@@ -684,6 +685,8 @@ std::string DeviceOp::setup(const Plan& plan, int device, int precision, int max
                 near_slot_ = upload(plan.near_slot);
                 MLFMA_CK(cudaFuncSetAttribute(k_near_sym, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                               static_cast<int>(kSymSmemBytes)));
+                MLFMA_CK(cudaFuncSetAttribute(k_near_warp, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              static_cast<int>(kNwSmemBytes)));
                 MLFMA_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&near_occ_, k_near_sym, kSymThreads,
                                                                        kSymSmemBytes));
                 near_occ_ = std::max(1, near_occ_);
@@ -957,8 +960,12 @@ void DeviceOp::run_near(const double2* xt, cudaStream_t s) {
         cudaMemsetAsync(ynear_, 0, sizeof(double2) * n_, s);
         return;
     }
-    k_near_sym<<<near_grid_, kSymThreads, kSymSmemBytes, s>>>(near_tiles_, n_near_tiles_, near_bz_, xt, near_slot_,
-                                                             near_part_, err_dev_);
+    if (near_kernel_ == 1)
+        k_near_warp<<<near_grid_, kNwThreads, kNwSmemBytes, s>>>(near_tiles_, n_near_tiles_, near_bz_, xt, near_slot_,
+                                                                 near_part_, err_dev_);
+    else
+        k_near_sym<<<near_grid_, kSymThreads, kSymSmemBytes, s>>>(near_tiles_, n_near_tiles_, near_bz_, xt, near_slot_,
+                                                                 near_part_, err_dev_);
     k_near_reduce<<<blocks_for(static_cast<long long>(n_) * kReduceLanes, 256), 256, 0, s>>>(near_red_ptr_, near_part_,
                                                                                            n_, ynear_);
 }
@@ -1747,6 +1754,19 @@ std::string DeviceOp::set_tc(int mode) {
     return {};
 }
 
+std::string DeviceOp::set_near_kernel(int kind) {
+    if (!ready_) return "operator not set up";
+    if (kind < 0 || kind > 1) return "arg:kind must be 0 or 1";
+    MLFMA_CK(cudaSetDevice(device_));
+    MLFMA_CK(cudaStreamSynchronize(stream_));
+    near_kernel_ = kind;
+    set_near_grid(kind ? 1 : near_occ_);
+    near_per_sm_ = kind ? 1 : near_occ_;
+    drop_graphs();
+    ++generation_;
+    return {};
+}
+
 std::string DeviceOp::set_staged(int mode) {
     if (!ready_) return "operator not set up";
     if (mode < 0 || mode > 3) return "arg:mode must be 0..3";
@@ -1869,12 +1889,15 @@ std::string DeviceOp::autotune(int nr, int reps, TuneReport* rep) {
         // runs beside the far-field chain and competes with it for the SMs)
         if (n_near_tiles_) {
             float bt = 1e30f;
-            int bk = near_per_sm_;
-            for (int k = 1; k <= near_occ_; ++k) {
-                set_near_grid(k);
-                const float t = timed(product);
-                if (t < bt) { bt = t; bk = k; }
-            }
+            int bk = near_per_sm_, bkind = near_kernel_;
+            for (int kind : {0, 1})
+                for (int k = 1; k <= (kind ? 1 : near_occ_); ++k) {
+                    near_kernel_ = kind;
+                    set_near_grid(k);
+                    const float t = timed(product);
+                    if (t < bt) { bt = t; bk = k; bkind = kind; }
+                }
+            near_kernel_ = bkind;
             near_per_sm_ = bk;
             set_near_grid(bk);
         }
@@ -1949,6 +1972,7 @@ std::string DeviceOp::autotune(int nr, int reps, TuneReport* rep) {
         r.after_ms = timed(product);
     }
     r.interp_path = tc_mode();
+    r.near_kernel = near_kernel_;
     r.m2l_chunk = m2l_chunk_;
     r.m2m_staged = r.l2l_staged = 0;
     for (int p = lmin_; p < lmax_ && p < 31; ++p) {

@@ -266,6 +266,180 @@ k_near_sym(const DevNearTile* __restrict__ tiles, int ntiles, const double2* __r
     }
 }
 
+// The same tiles, stages and partial slots with one consumer warp per tile:
+// warp w of the kNwConsumers takes the block's tiles w, w + kNwConsumers, ...
+// in its own two stages of the ring (no barrier between consumer warps).
+// Lane l owns tile columns l and l + 32: their x values stay in registers and
+// their column sums accumulate in registers over the whole tile.  Rows go in
+// batches of eight: each lane forms its part of the eight row sums from the
+// same entries it read for the column sums (every entry read from shared
+// memory once), and a reduce-scatter over the warp (three halving exchanges,
+// then two butterflies) leaves row rb + ((l >> 2) & 7) complete in lanes with
+// l & 3 == 0.  A self tile's diagonal counts once, in its row.
+constexpr int kNwConsumers = 4;
+constexpr int kNwThreads = 32 * (1 + kNwConsumers);
+constexpr int kNwStages = 2 * kNwConsumers;
+constexpr size_t kNwSmemBytes = sizeof(double2) * kSymStageEntries * kNwStages;
+
+__device__ __forceinline__ double2 shfl_xor2(double2 v, int m) {
+    return make_double2(__shfl_xor_sync(0xffffffffu, v.x, m), __shfl_xor_sync(0xffffffffu, v.y, m));
+}
+
+__global__ void __launch_bounds__(kNwThreads, 1)
+k_near_warp(const DevNearTile* __restrict__ tiles, int ntiles, const double2* __restrict__ Z,
+            const double2* __restrict__ x, const int* __restrict__ slots, double2* __restrict__ part,
+            int* __restrict__ err) {
+    extern __shared__ __align__(128) unsigned char nw_smem[];
+    double2* stages = reinterpret_cast<double2*>(nw_smem);
+    __shared__ __align__(8) unsigned long long full[kNwStages], empty[kNwStages];
+    __shared__ DevNearTile hdr[kNwStages];
+    __shared__ DevNearTile hbuf[32];  // producer's header batch
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int step = gridDim.x;
+    if (tid == 0) {
+        for (int s = 0; s < kNwStages; ++s) {
+            mbar_init(smem_addr(&full[s]), 1);
+            mbar_init(smem_addr(&empty[s]), 1);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+
+    if (warp == 0) {  // ---- producer warp: as in k_near_sym, over kNwStages stages
+        int it = 0;
+        DevNearTile Tn{};
+        if (blockIdx.x + lane * step < ntiles) Tn = tiles[blockIdx.x + lane * step];
+        for (int t = blockIdx.x; t < ntiles; t += step, ++it) {
+            if ((it & 31) == 0) {
+                __syncwarp();
+                hbuf[lane] = Tn;
+                __syncwarp();
+                const int tb = t + (32 + lane) * step;
+                if (tb < ntiles) Tn = tiles[tb];
+            }
+            const DevNearTile T = hbuf[it & 31];
+            const int s = it % kNwStages;
+            if (it >= kNwStages && !mbar_wait_bounded(smem_addr(&empty[s]), ((it / kNwStages) - 1) & 1)) {
+                if (lane == 0) {
+                    atomicExch(err, 1);
+                    for (int k = 1; k <= kNwStages && k <= it; ++k)  // copies still in flight
+                        mbar_wait_bounded(smem_addr(&full[(it - k) % kNwStages]), ((it - k) / kNwStages) & 1);
+                }
+                return;
+            }
+            double2* st = stages + static_cast<size_t>(s) * kSymStageEntries;
+            int nv = 0, total;
+            long long off = 0;
+            if (T.mode == 2) {
+                if (lane < T.ni) {
+                    const int il = T.i0 + lane;
+                    nv = tile_row_len(T, lane);
+                    off = T.z + (T.kind == 0 ? static_cast<long long>(il) * T.ld : packed_row(il, T.kind)) + T.j0;
+                }
+                total = nv;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) total += __shfl_xor_sync(0xffffffffu, total, o);
+            } else {
+                total = tile_entries(T);
+            }
+            const int nslot = (T.ni + T.nj + 3) & ~3;
+            const uint32_t bytes = static_cast<uint32_t>((total + T.nj + T.ni) * sizeof(double2) + nslot * sizeof(int));
+            const uint32_t b = smem_addr(&full[s]);
+            if (lane == 0) {
+                hdr[s] = T;
+                mbar_arrive_expect_tx(b, bytes);
+            }
+            __syncwarp();
+            if (T.mode == 2) {
+                if (nv > 0) bulk_load(smem_addr(st + lane * T.nj), Z + off, static_cast<uint32_t>(nv * sizeof(double2)), b);
+            } else if (lane == 0) {
+                bulk_load(smem_addr(st), Z + T.z, static_cast<uint32_t>(total * sizeof(double2)), b);
+            }
+            if (lane == 31) bulk_load(smem_addr(st + kSymXc), x + T.c0 + T.j0, static_cast<uint32_t>(T.nj * sizeof(double2)), b);
+            if (lane == 30) bulk_load(smem_addr(st + kSymXr), x + T.r0 + T.i0, static_cast<uint32_t>(T.ni * sizeof(double2)), b);
+            if (lane == 29) bulk_load(smem_addr(st + kSymSlot), slots + T.slot, static_cast<uint32_t>(nslot * sizeof(int)), b);
+        }
+        return;
+    }
+
+    // ---- consumer warps
+    const int cw = warp - 1;
+    const int c0 = lane, c1 = lane + 32;
+    for (int it = cw, t = blockIdx.x + cw * step; t < ntiles; it += kNwConsumers, t += kNwConsumers * step) {
+        const int s = it % kNwStages;
+        const bool ok = mbar_wait_bounded(smem_addr(&full[s]), (it / kNwStages) & 1);
+        if (__any_sync(0xffffffffu, !ok)) {
+            if (lane == 0) atomicExch(err, 1);
+            return;
+        }
+        const DevNearTile T = hdr[s];
+        const double2* zt = stages + static_cast<size_t>(s) * kSymStageEntries;
+        const double2* xr = zt + kSymXr;
+        const int* sl = reinterpret_cast<const int*>(zt + kSymSlot);
+        const double2 xc0 = c0 < T.nj ? zt[kSymXc + c0] : z0();
+        const double2 xc1 = c1 < T.nj ? zt[kSymXc + c1] : z0();
+        // a row's entry at tile column c also enters column c's sum unless it is
+        // on or above a self tile's diagonal
+        const int dcol = T.j0 - T.i0;  // row r, column c is below the diagonal iff r > c + dcol
+        double2 ca0 = z0(), ca1 = z0(), cb0 = z0(), cb1 = z0();
+        for (int rb = 0; rb < T.ni; rb += 8) {
+            double2 p[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const int r = rb + j;
+                double2 za = z0(), zb = z0(), xv = z0();
+                if (r < T.ni) {
+                    const int len = tile_row_len(T, r);
+                    const double2* zr = zt + tile_row_start(T, r);
+                    if (c0 < len) za = zr[c0];
+                    if (c1 < len) zb = zr[c1];
+                    xv = xr[r];
+                }
+                p[j] = cfma(za, xc0, cmul(zb, xc1));
+                const bool ia = T.kind == 0 || r > c0 + dcol, ib = T.kind == 0 || r > c1 + dcol;
+                if (j & 1) {
+                    if (ia) cb0 = cfma(za, xv, cb0);
+                    if (ib) cb1 = cfma(zb, xv, cb1);
+                } else {
+                    if (ia) ca0 = cfma(za, xv, ca0);
+                    if (ib) ca1 = cfma(zb, xv, ca1);
+                }
+            }
+            // reduce-scatter of p[0..7] over the warp
+            const bool h4 = lane & 16, h3 = lane & 8, h2 = lane & 4;
+            double2 q[4], u[2], w;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const double2 send = h4 ? p[k] : p[k + 4];
+                const double2 keep = h4 ? p[k + 4] : p[k];
+                q[k] = cadd(keep, shfl_xor2(send, 16));
+            }
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                const double2 send = h3 ? q[k] : q[k + 2];
+                const double2 keep = h3 ? q[k + 2] : q[k];
+                u[k] = cadd(keep, shfl_xor2(send, 8));
+            }
+            {
+                const double2 send = h2 ? u[0] : u[1];
+                const double2 keep = h2 ? u[1] : u[0];
+                w = cadd(keep, shfl_xor2(send, 4));
+            }
+            w = cadd(w, shfl_xor2(w, 1));
+            w = cadd(w, shfl_xor2(w, 2));
+            const int r = rb + ((lane >> 2) & 7);
+            if ((lane & 3) == 0 && r < T.ni) {
+                const int slot = sl[r];
+                if (slot >= 0) part[slot] = w;
+            }
+        }
+        if (c0 < T.nj && sl[T.ni + c0] >= 0) part[sl[T.ni + c0]] = cadd(ca0, cb0);
+        if (c1 < T.nj && sl[T.ni + c1] >= 0) part[sl[T.ni + c1]] = cadd(ca1, cb1);
+        __syncwarp();
+        if (lane == 0) mbar_arrive(smem_addr(&empty[s]));
+    }
+}
+
 // y[t] = sum of target t's consecutive partial slots: eight lanes per target,
 // a fixed shuffle tree, so the order never changes.
 constexpr int kReduceLanes = 8;
