@@ -54,6 +54,11 @@ struct DevStencilT {
     const int* src;
     const int* refl;
     const R* coef;
+    // the same entries tap-major: entry k of row r at k * rows + r (threads
+    // on consecutive rows read consecutive words)
+    int rows;
+    const int* src_t;
+    const R* coef_t;
 };
 
 template <class R>

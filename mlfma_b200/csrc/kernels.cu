@@ -307,7 +307,14 @@ std::string DeviceOp::setup_far(const Plan& plan, FarField<R>& F, const double2*
                     refl[at] = s.refl[q];
                     coef[at] = static_cast<R>(s.refl[q] ? -s.coef[q] : s.coef[q]);
                 }
-            return DevStencilT<R>{w, upload(src), upload(refl), upload(coef)};
+            std::vector<int> src_t(src.size());
+            std::vector<R> coef_t(coef.size());
+            for (int r = 0; r < rows; ++r)
+                for (int k = 0; k < w; ++k) {
+                    src_t[static_cast<size_t>(k) * rows + r] = src[static_cast<size_t>(r) * w + k];
+                    coef_t[static_cast<size_t>(k) * rows + r] = coef[static_cast<size_t>(r) * w + k];
+                }
+            return DevStencilT<R>{w, upload(src), upload(refl), upload(coef), rows, upload(src_t), upload(coef_t)};
         };
         d.up_th = st(T.up_th, up_w_[p]);
         d.up_ph = st(T.up_ph, up_w_[p]);
@@ -413,43 +420,6 @@ std::string DeviceOp::setup_far(const Plan& plan, FarField<R>& F, const double2*
             if (e != cudaSuccess) return e;
             return cudaFuncSetAttribute(fn, attr, dev_smem - static_cast<int>(fa.sharedSizeBytes));
         };
-        // Kernels that stage in shared memory run many small blocks per SM:
-        // ask for the largest shared-memory carveout, so that their residency
-        // is set by threads and registers, not by a small default carveout.
-        auto carve = [&](const void* fn) {
-            return cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                        static_cast<int>(cudaSharedmemCarveoutMaxShared));
-        };
-        for (int tr = 0; tr < 2; ++tr) {
-            const bool t = tr != 0;
-            const void* fns[] = {
-                reinterpret_cast<const void*>(t ? k_m2m<R, 2, true> : k_m2m<R, 2, false>),
-                reinterpret_cast<const void*>(t ? k_m2m<R, 4, true> : k_m2m<R, 4, false>),
-                reinterpret_cast<const void*>(t ? k_m2m<R, 6, true> : k_m2m<R, 6, false>),
-                reinterpret_cast<const void*>(t ? k_m2m<R, 8, true> : k_m2m<R, 8, false>),
-                reinterpret_cast<const void*>(t ? k_m2m<R, 10, true> : k_m2m<R, 10, false>),
-                reinterpret_cast<const void*>(t ? k_l2l<R, 8, true> : k_l2l<R, 8, false>),
-                reinterpret_cast<const void*>(t ? k_l2l<R, 12, true> : k_l2l<R, 12, false>),
-                reinterpret_cast<const void*>(t ? k_l2l<R, 16, true> : k_l2l<R, 16, false>),
-                reinterpret_cast<const void*>(t ? k_l2l<R, 24, true> : k_l2l<R, 24, false>),
-                reinterpret_cast<const void*>(t ? k_l2l<R, 32, true> : k_l2l<R, 32, false>),
-                reinterpret_cast<const void*>(t ? k_l2l_st<R, 8, true> : k_l2l_st<R, 8, false>),
-                reinterpret_cast<const void*>(t ? k_l2l_st<R, 12, true> : k_l2l_st<R, 12, false>),
-                reinterpret_cast<const void*>(t ? k_l2l_st<R, 16, true> : k_l2l_st<R, 16, false>),
-                reinterpret_cast<const void*>(t ? k_l2l_st<R, 24, true> : k_l2l_st<R, 24, false>),
-                reinterpret_cast<const void*>(t ? k_l2l_st<R, 32, true> : k_l2l_st<R, 32, false>),
-                reinterpret_cast<const void*>(t ? k_s2m<R, true> : k_s2m<R, false>)};
-            for (const void* fn : fns) MLFMA_CK(carve(fn));
-            if constexpr (!std::is_same<R, double>::value) {
-                MLFMA_CK(carve(reinterpret_cast<const void*>(t ? k_s2m_half<R, true> : k_s2m_half<R, false>)));
-                MLFMA_CK(carve(reinterpret_cast<const void*>(t ? k_l2t_half<R, true> : k_l2t_half<R, false>)));
-            }
-        }
-        MLFMA_CK(carve(reinterpret_cast<const void*>(k_m2m_sum<R, 2>)));
-        MLFMA_CK(carve(reinterpret_cast<const void*>(k_m2m_sum<R, 4>)));
-        MLFMA_CK(carve(reinterpret_cast<const void*>(k_m2m_sum<R, 6>)));
-        MLFMA_CK(carve(reinterpret_cast<const void*>(k_m2m_sum<R, 8>)));
-        MLFMA_CK(carve(reinterpret_cast<const void*>(k_m2m_sum<R, 10>)));
         MLFMA_CK(dyn(reinterpret_cast<const void*>(k_m2m_sum<R, 2>)));
         MLFMA_CK(dyn(reinterpret_cast<const void*>(k_m2m_sum<R, 4>)));
         MLFMA_CK(dyn(reinterpret_cast<const void*>(k_m2m_sum<R, 6>)));

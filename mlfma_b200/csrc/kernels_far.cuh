@@ -345,9 +345,9 @@ k_m2m(const DevLevelT<R>* __restrict__ lvs, DevTransT<R> T, int rows) {
                 C t0 = zero<C>(), t1 = zero<C>();
 #pragma unroll
                 for (int k = 0; k < W; ++k) {
-                    const int q = jph * W + k;
-                    const int s = T.up_ph.src[q];
-                    const R cf = T.up_ph.coef[q];
+                    const int q = k * nph + jph;  // tap-major
+                    const int s = T.up_ph.src_t[q];
+                    const R cf = T.up_ph.coef_t[q];
                     t0 = crfma(cf, row[2 * s], t0);
                     t1 = crfma(cf, row[2 * s + 1], t1);
                 }
@@ -357,9 +357,9 @@ k_m2m(const DevLevelT<R>* __restrict__ lvs, DevTransT<R> T, int rows) {
             } else {
 #pragma unroll
                 for (int k = 0; k < W; ++k) {
-                    const int q = jph * W + k;
-                    const int s = T.up_ph.src[q];
-                    const R cf = T.up_ph.coef[q];
+                    const int q = k * nph + jph;  // tap-major
+                    const int s = T.up_ph.src_t[q];
+                    const R cf = T.up_ph.coef_t[q];
                     a0 = crfma(cf, row[2 * s], a0);
                     a1 = crfma(cf, row[2 * s + 1], a1);
                 }
@@ -522,9 +522,9 @@ k_l2l(const DevLevelT<R>* __restrict__ lvs, DevTransT<R> T, const int2* __restri
         C v0 = zero<C>(), v1 = zero<C>();
 #pragma unroll
         for (int k = 0; k < W; ++k) {
-            const int q = jph * W + k;
-            const int d = ith * pph + T.dn_ph.src[q];
-            const R cf = T.dn_ph.coef[q];
+            const int q = k * cph + jph;  // tap-major
+            const int d = ith * pph + T.dn_ph.src_t[q];
+            const R cf = T.dn_ph.coef_t[q];
             if (POST) {
                 v0 = crfma(cf, Bp[2 * d], v0);
                 v1 = crfma(cf, Bp[2 * d + 1], v1);
@@ -638,9 +638,9 @@ k_m2m_sum(const DevLevelT<R>* __restrict__ lvs, DevTransT<R> T, int rows) {
         C a0 = zero<C>(), a1 = zero<C>();
 #pragma unroll
         for (int k = 0; k < W; ++k) {
-            const int q = jph * W + k;
-            const int s = T.up_ph.src[q];
-            const R cf = T.up_ph.coef[q];
+            const int q = k * nph + jph;  // tap-major: consecutive jph, consecutive words
+            const int s = T.up_ph.src_t[q];
+            const R cf = T.up_ph.coef_t[q];
             a0 = crfma(cf, row[2 * s], a0);
             a1 = crfma(cf, row[2 * s + 1], a1);
         }
@@ -689,9 +689,9 @@ k_l2l_st(const DevLevelT<R>* __restrict__ lvs, DevTransT<R> T, const int2* __res
         C v0 = zero<C>(), v1 = zero<C>();
 #pragma unroll
         for (int k = 0; k < W; ++k) {
-            const int q = jph * W + k;
-            const int d = T.dn_ph.src[q];
-            const R cf = T.dn_ph.coef[q];
+            const int q = k * cph + jph;  // tap-major: consecutive jph, consecutive words
+            const int d = T.dn_ph.src_t[q];
+            const R cf = T.dn_ph.coef_t[q];
             v0 = crfma(cf, row[2 * d], v0);
             v1 = crfma(cf, row[2 * d + 1], v1);
         }

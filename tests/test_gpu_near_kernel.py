@@ -34,7 +34,7 @@ CASES = {
                                         ref_compat=0),
     "dipoles": lambda: MLFMA.dipoles(inputs.make_dipoles(8000, seed=2), PW, max_node_srcs=24, ref_compat=0),
     "large_leaves": lambda: MLFMA.dipoles(clustered(12000, 3), PW, max_node_srcs=150, ref_compat=0, self_terms=1),
-    "uneven": lambda: MLFMA.dipoles(clustered(20000, 4), PW, max_node_srcs=12, ref_compat=0),
+    "uneven": lambda: MLFMA.dipoles(clustered(20000, 4), PW, max_node_srcs=12, max_level=6, ref_compat=0),
 }
 
 
