@@ -379,7 +379,7 @@ int mlfma_set_staged_interp(mlfma_handle h, int mode);
 /* Near-field kernel of the one-vector product (Leaf::evalPairSols,
  * evalNearNonNborSols, evalSelfSols, src/fmm/leaf.cpp:318-383; each stored block
  * applied as Z and Z^T, tiles streamed by bulk copies): kind 0, one tile per
- * thread block (row threads and column threads); kind 1 (the default), one
+ * thread block (row threads and column threads; the default); kind 1, one
  * tile per warp, each entry read from shared memory once and the row sums
  * formed by a warp reduce-scatter.  Same partial sums, other rounding order. */
 int mlfma_set_near_kernel(mlfma_handle h, int kind);

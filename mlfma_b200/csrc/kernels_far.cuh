@@ -70,9 +70,17 @@ k_s2m(const DevLevelT<R>* __restrict__ lvs, const int4* __restrict__ items, cons
             a3 = cfma(xs[s + 7], v[7], a3);
         }
     }
-    for (; s < lf.nsrc; ++s) {
-        const C v = ldg_stream(r + static_cast<size_t>(s) * ne);
-        a0 = CJ ? cjfma(v, xs[s], a0) : cfma(xs[s], v, a0);
+    if (s < lf.nsrc) {  // the last sources: their loads in flight together
+        C v[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u)
+            v[u] = s + u < lf.nsrc ? ldg_stream(r + static_cast<size_t>(s + u) * ne) : zero<C>();
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            if (s + u >= lf.nsrc) break;
+            C& acc = (u & 3) == 0 ? a0 : (u & 3) == 1 ? a1 : (u & 3) == 2 ? a2 : a3;
+            acc = CJ ? cjfma(v[u], xs[s + u], acc) : cfma(xs[s + u], v[u], acc);
+        }
     }
     A[e] = cadd(cadd(a0, a1), cadd(a2, a3));
 }
@@ -98,32 +106,22 @@ k_l2t(const DevLevelT<R>* __restrict__ lvs, const int4* __restrict__ items, cons
     const int s = it.y + warp;
     const C* r = pat + (lf.pat_off + static_cast<long long>(s) * ndir) * 2;
     C a0 = zero<C>(), a1 = zero<C>(), a2 = zero<C>(), a3 = zero<C>();
-    int e = lane;
-    for (; e + 224 < ne; e += 256) {
-        C v[8];
+    // eight loads in flight per lane, the last run of the row predicated (a
+    // leaf-level row of 162-324 elements is one or two runs)
+    for (int e = lane; e < ne; e += 256) {
+        C v[8], bv[8];
 #pragma unroll
-        for (int u = 0; u < 8; ++u) v[u] = ldg_stream(r + e + 32 * u);
-        if (CJ) {
-            a0 = cjfma(v[0], Bb[e], a0);
-            a1 = cjfma(v[1], Bb[e + 32], a1);
-            a2 = cjfma(v[2], Bb[e + 64], a2);
-            a3 = cjfma(v[3], Bb[e + 96], a3);
-            a0 = cjfma(v[4], Bb[e + 128], a0);
-            a1 = cjfma(v[5], Bb[e + 160], a1);
-            a2 = cjfma(v[6], Bb[e + 192], a2);
-            a3 = cjfma(v[7], Bb[e + 224], a3);
-        } else {
-            a0 = cfma(v[0], Bb[e], a0);
-            a1 = cfma(v[1], Bb[e + 32], a1);
-            a2 = cfma(v[2], Bb[e + 64], a2);
-            a3 = cfma(v[3], Bb[e + 96], a3);
-            a0 = cfma(v[4], Bb[e + 128], a0);
-            a1 = cfma(v[5], Bb[e + 160], a1);
-            a2 = cfma(v[6], Bb[e + 192], a2);
-            a3 = cfma(v[7], Bb[e + 224], a3);
+        for (int u = 0; u < 8; ++u) {
+            const bool in = e + 32 * u < ne;
+            v[u] = in ? ldg_stream(r + e + 32 * u) : zero<C>();
+            bv[u] = in ? Bb[e + 32 * u] : zero<C>();
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            C& acc = (u & 3) == 0 ? a0 : (u & 3) == 1 ? a1 : (u & 3) == 2 ? a2 : a3;
+            acc = CJ ? cjfma(v[u], bv[u], acc) : cfma(v[u], bv[u], acc);
         }
     }
-    for (; e < ne; e += 32) a0 = CJ ? cjfma(ldg_stream(r + e), Bb[e], a0) : cfma(ldg_stream(r + e), Bb[e], a0);
     const C acc = warp_sum(cadd(cadd(a0, a1), cadd(a2, a3)));
     if (lane == 0) yfar[lf.src0 + s] = to_d2(acc);
 }
@@ -213,10 +211,19 @@ k_s2m_half(const DevLevelT<R>* __restrict__ lvs, const int4* __restrict__ items,
             }
         }
     }
-    for (; s < lf.nsrc; ++s) {
-        const C v = ldg_stream(r + static_cast<size_t>(s) * ne);
-        a0 = CJ ? cjfma(v, xs[s], a0) : cfma(xs[s], v, a0);
-        b0 = CJ ? cfma(xs[s], v, b0) : cjfma(v, xs[s], b0);
+    if (s < lf.nsrc) {  // the last sources: their loads in flight together
+        C v[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u)
+            v[u] = s + u < lf.nsrc ? ldg_stream(r + static_cast<size_t>(s + u) * ne) : zero<C>();
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            if (s + u >= lf.nsrc) break;
+            C& a = (u & 3) == 0 ? a0 : (u & 3) == 1 ? a1 : (u & 3) == 2 ? a2 : a3;
+            C& b = (u & 3) == 0 ? b0 : (u & 3) == 1 ? b1 : (u & 3) == 2 ? b2 : b3;
+            a = CJ ? cjfma(v[u], xs[s + u], a) : cfma(xs[s + u], v[u], a);
+            b = CJ ? cfma(xs[s + u], v[u], b) : cjfma(v[u], xs[s + u], b);
+        }
     }
     A[e] = cadd(cadd(a0, a1), cadd(a2, a3));
     const C b = cadd(cadd(b0, b1), cadd(b2, b3));
@@ -256,14 +263,15 @@ k_l2t_half(const DevLevelT<R>* __restrict__ lvs, const int4* __restrict__ items,
     const int s = it.y + warp;
     const C* r = hpat + lf.pat_off + static_cast<long long>(s) * ne;
     C a0 = zero<C>(), a1 = zero<C>(), a2 = zero<C>(), a3 = zero<C>();
-    int e = lane;
-    for (; e + 224 < ne; e += 256) {
+    // eight loads in flight per lane, the last run of the row predicated
+    for (int e = lane; e < ne; e += 256) {
         C v[8];
 #pragma unroll
-        for (int u = 0; u < 8; ++u) v[u] = ldg_stream(r + e + 32 * u);
+        for (int u = 0; u < 8; ++u) v[u] = e + 32 * u < ne ? ldg_stream(r + e + 32 * u) : zero<C>();
 #pragma unroll
         for (int u = 0; u < 8; ++u) {
             const int ee = e + 32 * u;
+            if (ee >= ne) continue;
             C& acc = (u & 3) == 0 ? a0 : (u & 3) == 1 ? a1 : (u & 3) == 2 ? a2 : a3;
             if (CJ) {
                 acc = cjfma(v[u], bs[ee], acc);
@@ -273,11 +281,6 @@ k_l2t_half(const DevLevelT<R>* __restrict__ lvs, const int4* __restrict__ items,
                 acc = cjfma(v[u], bp[ee], acc);
             }
         }
-    }
-    for (; e < ne; e += 32) {
-        const C v = ldg_stream(r + e);
-        a0 = CJ ? cjfma(v, bs[e], a0) : cfma(v, bs[e], a0);
-        a0 = CJ ? cfma(v, bp[e], a0) : cjfma(v, bp[e], a0);
     }
     const C acc = warp_sum(cadd(cadd(a0, a1), cadd(a2, a3)));
     if (lane == 0) yfar[lf.src0 + s] = to_d2(acc);
