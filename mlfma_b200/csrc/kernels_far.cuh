@@ -599,8 +599,13 @@ k_m2m_sum(const DevLevelT<R>* __restrict__ lvs, DevTransT<R> T, int rows) {
     }
     __syncthreads();
     const int lo = band[0], nb = band[1] - lo + 1;
-    C* U = reinterpret_cast<C*>(smraw);              // [nb * mph][2], child rows lo..lo+nb-1
-    C* V = U + 2 * static_cast<size_t>(nb) * mph;    // [nrow * mph][2]
+    // component planes (theta, phi), so that neighbouring threads read
+    // neighbouring 8- or 16-byte words of shared memory
+    const size_t nu = static_cast<size_t>(nb) * mph, nv = static_cast<size_t>(nrow) * mph;
+    C* U0 = reinterpret_cast<C*>(smraw);  // [nb * mph], child rows lo..lo+nb-1
+    C* U1 = U0 + nu;
+    C* V0 = U1 + nu;                      // [nrow * mph]
+    C* V1 = V0 + nv;
     const int c0 = T.child_ptr[par], nch = T.child_ptr[par + 1] - c0;
     for (int e = threadIdx.x; e < nb * mph; e += blockDim.x) {
         const int d = lo * mph + e;
@@ -612,8 +617,8 @@ k_m2m_sum(const DevLevelT<R>* __restrict__ lvs, DevTransT<R> T, int rows) {
             u0 = cfma(ph, Ac[2 * d], u0);
             u1 = cfma(ph, Ac[2 * d + 1], u1);
         }
-        U[2 * e] = u0;
-        U[2 * e + 1] = u1;
+        U0[e] = u0;
+        U1[e] = u1;
     }
     __syncthreads();
     for (int it = threadIdx.x; it < nrow * mph; it += blockDim.x) {
@@ -627,25 +632,26 @@ k_m2m_sum(const DevLevelT<R>* __restrict__ lvs, DevTransT<R> T, int rows) {
             const int sp = rf ? (iph < halfm ? iph + halfm : iph - halfm) : iph;
             const R cf = T.up_th.coef[q];
             const int e = (T.up_th.src[q] - lo) * mph + sp;
-            v0 = crfma(cf, U[2 * e], v0);
-            v1 = crfma(cf, U[2 * e + 1], v1);
+            v0 = crfma(cf, U0[e], v0);
+            v1 = crfma(cf, U1[e], v1);
         }
-        V[2 * it] = v0;
-        V[2 * it + 1] = v1;
+        V0[it] = v0;
+        V1[it] = v1;
     }
     __syncthreads();
     C* Ap = P.A + (static_cast<size_t>(T.par_box[par]) * P.ndir + static_cast<size_t>(r0) * nph) * 2;
     for (int o = threadIdx.x; o < nrow * nph; o += blockDim.x) {
         const int jr = o / nph, jph = o - jr * nph;
-        const C* row = V + static_cast<size_t>(jr) * mph * 2;
+        const C* row0 = V0 + static_cast<size_t>(jr) * mph;
+        const C* row1 = V1 + static_cast<size_t>(jr) * mph;
         C a0 = zero<C>(), a1 = zero<C>();
 #pragma unroll
         for (int k = 0; k < W; ++k) {
             const int q = k * nph + jph;  // tap-major: consecutive jph, consecutive words
             const int s = T.up_ph.src_t[q];
             const R cf = T.up_ph.coef_t[q];
-            a0 = crfma(cf, row[2 * s], a0);
-            a1 = crfma(cf, row[2 * s + 1], a1);
+            a0 = crfma(cf, row0[s], a0);
+            a1 = crfma(cf, row1[s], a1);
         }
         Ap[2 * o] = a0;
         Ap[2 * o + 1] = a1;
@@ -671,8 +677,12 @@ k_l2l_st(const DevLevelT<R>* __restrict__ lvs, DevTransT<R> T, const int2* __res
     const DevLevelT<R> P = lvs[T.plevel];
     const DevLevelT<R> Cl = lvs[T.plevel + 1];
     const int pth = P.nth, pph = P.nph, cth = Cl.nth, cph = Cl.nph, halfc = Cl.nph / 2;
-    C* SB = reinterpret_cast<C*>(smraw);                    // [pth * pph][2]
-    C* S1 = SB + 2 * static_cast<size_t>(pth) * pph;        // [pth * cph][2]
+    // component planes (theta, phi): neighbouring threads read neighbouring words
+    const size_t np = static_cast<size_t>(pth) * pph, nq = static_cast<size_t>(pth) * cph;
+    C* SB0 = reinterpret_cast<C*>(smraw);  // [pth * pph]
+    C* SB1 = SB0 + np;
+    C* S10 = SB1 + np;                     // [pth * cph]
+    C* S11 = S10 + nq;
     const C* Bp = P.B + static_cast<size_t>(T.par_box[pc.x]) * P.ndir * 2;
     const C* sh = P.shift_down + static_cast<size_t>(T.child_oct[pc.y]) * P.ndir;
     for (int d = threadIdx.x; d < pth * pph; d += blockDim.x) {
@@ -682,24 +692,25 @@ k_l2l_st(const DevLevelT<R>* __restrict__ lvs, DevTransT<R> T, const int2* __res
             b0 = cmul(ph, b0);
             b1 = cmul(ph, b1);
         }
-        SB[2 * d] = b0;
-        SB[2 * d + 1] = b1;
+        SB0[d] = b0;
+        SB1[d] = b1;
     }
     __syncthreads();
     for (int e = threadIdx.x; e < pth * cph; e += blockDim.x) {
         const int ith = e / cph, jph = e - ith * cph;
-        const C* row = SB + static_cast<size_t>(ith) * pph * 2;
+        const C* row0 = SB0 + static_cast<size_t>(ith) * pph;
+        const C* row1 = SB1 + static_cast<size_t>(ith) * pph;
         C v0 = zero<C>(), v1 = zero<C>();
 #pragma unroll
         for (int k = 0; k < W; ++k) {
             const int q = k * cph + jph;  // tap-major: consecutive jph, consecutive words
             const int d = T.dn_ph.src_t[q];
             const R cf = T.dn_ph.coef_t[q];
-            v0 = crfma(cf, row[2 * d], v0);
-            v1 = crfma(cf, row[2 * d + 1], v1);
+            v0 = crfma(cf, row0[d], v0);
+            v1 = crfma(cf, row1[d], v1);
         }
-        S1[2 * e] = v0;
-        S1[2 * e + 1] = v1;
+        S10[e] = v0;
+        S11[e] = v1;
     }
     __syncthreads();
     C* Bc = Cl.B + static_cast<size_t>(T.child_box[pc.y]) * Cl.ndir * 2;
@@ -712,9 +723,9 @@ k_l2l_st(const DevLevelT<R>* __restrict__ lvs, DevTransT<R> T, const int2* __res
             const bool rf = T.dn_th.refl[q];
             const int sp = rf ? (jph < halfc ? jph + halfc : jph - halfc) : jph;
             const R cf = T.dn_th.coef[q];
-            const C* row = S1 + (static_cast<size_t>(T.dn_th.src[q]) * cph + sp) * 2;
-            v0 = crfma(cf, row[0], v0);
-            v1 = crfma(cf, row[1], v1);
+            const size_t at = static_cast<size_t>(T.dn_th.src[q]) * cph + sp;
+            v0 = crfma(cf, S10[at], v0);
+            v1 = crfma(cf, S11[at], v1);
         }
         if (POST) {
             const C ph = Cl.shift_up[static_cast<size_t>(T.child_oct[pc.y]) * Cl.ndir + e];
