@@ -336,10 +336,12 @@ typedef struct {
     int schedule;              /* one-vector product: bit 0 translation lists staged in shared memory,
                                   bit 1 near field started after aggregation, bit 2 two side streams
                                   for the finer levels' translations */
-    int m2m_staged;            /* one-vector interpolation: bit p = transition p+1 -> p sums the children
-                                  first in shared memory (else one interpolation per child) */
-    int l2l_staged;            /* one-vector anterpolation: bit p = transition p -> p+1 stages the parent's
-                                  local pattern in shared memory */
+    int m2m_staged;            /* one-vector interpolation, transition p+1 -> p: bit p = children summed
+                                  first in shared memory, bit 16 + p = the same with column-stationary
+                                  phi passes; neither = one interpolation per child */
+    int l2l_staged;            /* one-vector anterpolation, transition p -> p+1: bit p = parent's local
+                                  pattern staged in shared memory, bit 16 + p = the same with
+                                  column-stationary phi passes */
     int near_kernel;           /* one-vector near field: 0 one tile per thread block (row and column
                                   threads), 1 one tile per warp (see mlfma_set_near_kernel) */
 } mlfma_tuning;
@@ -373,8 +375,10 @@ int mlfma_get_interp_path(mlfma_handle h, int* mode);
  * shifted and summed on the child grid first (one interpolation per parent,
  * all taps from shared memory; rounding-level differences from the per-child
  * kernel); bit 1, L2L with the parent's shifted local pattern staged in shared
- * memory (the same arithmetic in the same order).  Both are on after setup;
- * mlfma_autotune chooses per transition (mlfma_tuning.m2m_staged/l2l_staged). */
+ * memory (the same arithmetic in the same order); bit 2, their phi passes
+ * column-stationary (a thread keeps one output column's stencil in registers
+ * and walks the rows).  Modes 1 and 2 are on after setup; mlfma_autotune
+ * chooses per transition (mlfma_tuning.m2m_staged/l2l_staged). */
 int mlfma_set_staged_interp(mlfma_handle h, int mode);
 /* Near-field kernel of the one-vector product (Leaf::evalPairSols,
  * evalNearNonNborSols, evalSelfSols, src/fmm/leaf.cpp:318-383; each stored block

@@ -266,7 +266,8 @@ class MLFMA:
 
     def set_staged_interp(self, mode: int) -> None:
         """bit 0: M2M children summed first in shared memory; bit 1: L2L with the parent
-        staged in shared memory (mlfma_set_staged_interp)."""
+        staged in shared memory; bit 2: their phi passes column-stationary
+        (mlfma_set_staged_interp)."""
         check(lib().mlfma_set_staged_interp(self._h, int(mode)))
 
     def set_near_kernel(self, kind: int) -> None:

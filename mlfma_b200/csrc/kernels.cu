@@ -420,18 +420,25 @@ std::string DeviceOp::setup_far(const Plan& plan, FarField<R>& F, const double2*
             if (e != cudaSuccess) return e;
             return cudaFuncSetAttribute(fn, attr, dev_smem - static_cast<int>(fa.sharedSizeBytes));
         };
-        MLFMA_CK(dyn(reinterpret_cast<const void*>(k_m2m_sum<R, 2>)));
-        MLFMA_CK(dyn(reinterpret_cast<const void*>(k_m2m_sum<R, 4>)));
-        MLFMA_CK(dyn(reinterpret_cast<const void*>(k_m2m_sum<R, 6>)));
-        MLFMA_CK(dyn(reinterpret_cast<const void*>(k_m2m_sum<R, 8>)));
-        MLFMA_CK(dyn(reinterpret_cast<const void*>(k_m2m_sum<R, 10>)));
-        for (int tr = 0; tr < 2; ++tr) {
-            const bool t = tr != 0;
-            MLFMA_CK(dyn(reinterpret_cast<const void*>(t ? k_l2l_st<R, 8, true> : k_l2l_st<R, 8, false>)));
-            MLFMA_CK(dyn(reinterpret_cast<const void*>(t ? k_l2l_st<R, 12, true> : k_l2l_st<R, 12, false>)));
-            MLFMA_CK(dyn(reinterpret_cast<const void*>(t ? k_l2l_st<R, 16, true> : k_l2l_st<R, 16, false>)));
-            MLFMA_CK(dyn(reinterpret_cast<const void*>(t ? k_l2l_st<R, 24, true> : k_l2l_st<R, 24, false>)));
-            MLFMA_CK(dyn(reinterpret_cast<const void*>(t ? k_l2l_st<R, 32, true> : k_l2l_st<R, 32, false>)));
+        for (int cs = 0; cs < 2; ++cs) {
+            const bool c = cs != 0;
+            MLFMA_CK(dyn(reinterpret_cast<const void*>(c ? k_m2m_sum<R, 2, true> : k_m2m_sum<R, 2, false>)));
+            MLFMA_CK(dyn(reinterpret_cast<const void*>(c ? k_m2m_sum<R, 4, true> : k_m2m_sum<R, 4, false>)));
+            MLFMA_CK(dyn(reinterpret_cast<const void*>(c ? k_m2m_sum<R, 6, true> : k_m2m_sum<R, 6, false>)));
+            MLFMA_CK(dyn(reinterpret_cast<const void*>(c ? k_m2m_sum<R, 8, true> : k_m2m_sum<R, 8, false>)));
+            MLFMA_CK(dyn(reinterpret_cast<const void*>(c ? k_m2m_sum<R, 10, true> : k_m2m_sum<R, 10, false>)));
+        }
+        for (int v = 0; v < 4; ++v) {  // (transposed, column-stationary)
+            const void* fns[] = {
+#define MLFMA_L2L_ST_FN(WW)                                                                                  \
+    (v == 0 ? reinterpret_cast<const void*>(k_l2l_st<R, WW, false, false>)                                 \
+     : v == 1 ? reinterpret_cast<const void*>(k_l2l_st<R, WW, true, false>)                                \
+     : v == 2 ? reinterpret_cast<const void*>(k_l2l_st<R, WW, false, true>)                                \
+              : reinterpret_cast<const void*>(k_l2l_st<R, WW, true, true>))
+                MLFMA_L2L_ST_FN(8), MLFMA_L2L_ST_FN(12), MLFMA_L2L_ST_FN(16), MLFMA_L2L_ST_FN(24),
+                MLFMA_L2L_ST_FN(32)};
+#undef MLFMA_L2L_ST_FN
+            for (const void* fn : fns) MLFMA_CK(dyn(fn));
         }
     }
     if (max_rhs_ > 1) {
@@ -800,13 +807,18 @@ void DeviceOp::far_m2m(FarField<R>& F, int p, cudaStream_t s) {
     const DevTransT<R>& T = F.trans[p];
     const size_t ssum = m2m_sum_smem(nth_[p + 1], nph_[p + 1], rows, sizeof(C));
     if (!TR && m2m_pref_[p] && ssum + 1024 <= static_cast<size_t>(dev_smem_)) {
+        const bool cs = m2m_pref_[p] == 2;
+#define MLFMA_M2M_SUM(WW)                                                                           \
+    (cs ? k_m2m_sum<R, WW, true><<<grid, 256, ssum, s>>>(F.lv_dev, T, rows)                          \
+        : k_m2m_sum<R, WW, false><<<grid, 256, ssum, s>>>(F.lv_dev, T, rows))
         switch (up_w_[p]) {
-            case 2: k_m2m_sum<R, 2><<<grid, 256, ssum, s>>>(F.lv_dev, T, rows); break;
-            case 4: k_m2m_sum<R, 4><<<grid, 256, ssum, s>>>(F.lv_dev, T, rows); break;
-            case 6: k_m2m_sum<R, 6><<<grid, 256, ssum, s>>>(F.lv_dev, T, rows); break;
-            case 8: k_m2m_sum<R, 8><<<grid, 256, ssum, s>>>(F.lv_dev, T, rows); break;
-            default: k_m2m_sum<R, 10><<<grid, 256, ssum, s>>>(F.lv_dev, T, rows); break;
+            case 2: MLFMA_M2M_SUM(2); break;
+            case 4: MLFMA_M2M_SUM(4); break;
+            case 6: MLFMA_M2M_SUM(6); break;
+            case 8: MLFMA_M2M_SUM(8); break;
+            default: MLFMA_M2M_SUM(10); break;
         }
+#undef MLFMA_M2M_SUM
         return;
     }
     const size_t smem = static_cast<size_t>(8) * rows * nph_[p + 1] * 2 * sizeof(C);
@@ -840,13 +852,18 @@ void DeviceOp::far_l2l(FarField<R>& F, int p, cudaStream_t s) {
     const DevTransT<R>& T = F.trans[p];
     const size_t sst = l2l_st_smem(nth_[p], nph_[p], nph_[p + 1], sizeof(C));
     if (l2l_pref_[p] && sst + 1024 <= static_cast<size_t>(dev_smem_)) {
+        const bool cs = l2l_pref_[p] == 2;
+#define MLFMA_L2L_ST(WW)                                                                            \
+    (cs ? k_l2l_st<R, WW, TR, true><<<g, 256, sst, s>>>(F.lv_dev, T, l2l_pairs_[p])                  \
+        : k_l2l_st<R, WW, TR, false><<<g, 256, sst, s>>>(F.lv_dev, T, l2l_pairs_[p]))
         switch (dn_w_[p]) {
-            case 8: k_l2l_st<R, 8, TR><<<g, 256, sst, s>>>(F.lv_dev, T, l2l_pairs_[p]); break;
-            case 12: k_l2l_st<R, 12, TR><<<g, 256, sst, s>>>(F.lv_dev, T, l2l_pairs_[p]); break;
-            case 16: k_l2l_st<R, 16, TR><<<g, 256, sst, s>>>(F.lv_dev, T, l2l_pairs_[p]); break;
-            case 24: k_l2l_st<R, 24, TR><<<g, 256, sst, s>>>(F.lv_dev, T, l2l_pairs_[p]); break;
-            default: k_l2l_st<R, 32, TR><<<g, 256, sst, s>>>(F.lv_dev, T, l2l_pairs_[p]); break;
+            case 8: MLFMA_L2L_ST(8); break;
+            case 12: MLFMA_L2L_ST(12); break;
+            case 16: MLFMA_L2L_ST(16); break;
+            case 24: MLFMA_L2L_ST(24); break;
+            default: MLFMA_L2L_ST(32); break;
         }
+#undef MLFMA_L2L_ST
         return;
     }
     const size_t smem = static_cast<size_t>(nth_[p]) * nph_[p + 1] * 2 * sizeof(C);
@@ -1776,12 +1793,13 @@ std::string DeviceOp::set_near_kernel(int kind) {
 
 std::string DeviceOp::set_staged(int mode) {
     if (!ready_) return "operator not set up";
-    if (mode < 0 || mode > 3) return "arg:mode must be 0..3";
+    if (mode < 0 || mode > 7) return "arg:mode must be 0..7";
     MLFMA_CK(cudaSetDevice(device_));
     MLFMA_CK(cudaStreamSynchronize(stream_));
+    const int kind = (mode & 4) ? 2 : 1;
     for (int p = lmin_; p < lmax_; ++p) {
-        m2m_pref_[p] = mode & 1;
-        l2l_pref_[p] = (mode >> 1) & 1;
+        m2m_pref_[p] = (mode & 1) ? kind : 0;
+        l2l_pref_[p] = (mode & 2) ? kind : 0;
     }
     drop_graphs();
     ++generation_;
@@ -1863,7 +1881,7 @@ std::string DeviceOp::autotune(int nr, int reps, TuneReport* rep) {
             if (!npar_[p]) continue;
             float bt = 1e30f;
             int brows = m2m_rows_[p], bkind = m2m_pref_[p];
-            for (int kind : {0, 1})
+            for (int kind : {0, 1, 2})
                 for (int rows : {1, 2, 4, 8, 16, 32, 64}) {
                     if (rows > nth_[p] && rows != 1) continue;
                     const size_t need = kind ? m2m_sum_smem(nth_[p + 1], nph_[p + 1], rows, csize) + 1024
@@ -1882,7 +1900,7 @@ std::string DeviceOp::autotune(int nr, int reps, TuneReport* rep) {
             if (n_l2l_pairs_[p]) {
                 float lt = 1e30f;
                 int lkind = l2l_pref_[p];
-                for (int kind : {0, 1}) {
+                for (int kind : {0, 1, 2}) {
                     l2l_pref_[p] = kind;
                     const float t = timed([&] {
                         if (precision_ == kFp64) far_l2l<double, false>(f64_, p, s); else far_l2l<float, false>(f32_, p, s);
@@ -1982,9 +2000,9 @@ std::string DeviceOp::autotune(int nr, int reps, TuneReport* rep) {
     r.near_kernel = near_kernel_;
     r.m2l_chunk = m2l_chunk_;
     r.m2m_staged = r.l2l_staged = 0;
-    for (int p = lmin_; p < lmax_ && p < 31; ++p) {
-        if (m2m_pref_[p]) r.m2m_staged |= 1 << p;
-        if (l2l_pref_[p]) r.l2l_staged |= 1 << p;
+    for (int p = lmin_; p < lmax_ && p < 16; ++p) {
+        if (m2m_pref_[p]) r.m2m_staged |= 1 << (m2m_pref_[p] == 2 ? 16 + p : p);
+        if (l2l_pref_[p]) r.l2l_staged |= 1 << (l2l_pref_[p] == 2 ? 16 + p : p);
     }
     for (int p = lmin_; p < lmax_; ++p) r.m2m_rows[p] = m2m_rows_[p];
     if (r.multi_rows_fast == 0 && m_m2m_rows_fast_ < 0) r.multi_rows_fast = -1;

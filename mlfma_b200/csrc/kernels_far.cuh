@@ -574,7 +574,7 @@ k_l2l(const DevLevelT<R>* __restrict__ lvs, DevTransT<R> T, const int2* __restri
 // parent instead of one per child).  Block = (parent, tile of `rows` parent
 // theta rows); each child value is read from global memory once per block and
 // every stencil tap reads shared memory.
-template <class R, int W>  // taps per row: 2 * interp_order (both passes)
+template <class R, int W, bool CS>  // taps per row: 2 * interp_order (both passes); CS: column-stationary phi pass
 __global__ void __launch_bounds__(256)
 k_m2m_sum(const DevLevelT<R>* __restrict__ lvs, DevTransT<R> T, int rows) {
     using C = typename Cx<R>::T;
@@ -639,9 +639,28 @@ k_m2m_sum(const DevLevelT<R>* __restrict__ lvs, DevTransT<R> T, int rows) {
         V1[it] = v1;
     }
     __syncthreads();
+    C* Ap = P.A + (static_cast<size_t>(T.par_box[par]) * P.ndir + static_cast<size_t>(r0) * nph) * 2;
+    if (!CS) {  // one output per thread, stencil read per tap (tap-major)
+        for (int o = threadIdx.x; o < nrow * nph; o += blockDim.x) {
+            const int jr = o / nph, jph = o - jr * nph;
+            const C* row0 = V0 + static_cast<size_t>(jr) * mph;
+            const C* row1 = V1 + static_cast<size_t>(jr) * mph;
+            C a0 = zero<C>(), a1 = zero<C>();
+#pragma unroll
+            for (int k = 0; k < W; ++k) {
+                const int q = k * nph + jph;
+                const int s = T.up_ph.src_t[q];
+                const R cf = T.up_ph.coef_t[q];
+                a0 = crfma(cf, row0[s], a0);
+                a1 = crfma(cf, row1[s], a1);
+            }
+            Ap[2 * o] = a0;
+            Ap[2 * o + 1] = a1;
+        }
+        return;
+    }
     // phi pass, column-stationary: a thread keeps one output column's stencil
     // in registers and walks the tile's rows (every row uses the same stencil)
-    C* Ap = P.A + (static_cast<size_t>(T.par_box[par]) * P.ndir + static_cast<size_t>(r0) * nph) * 2;
     const int ng = max(1, static_cast<int>(blockDim.x) / nph);  // row groups
     for (int t = threadIdx.x; t < nph * ng; t += blockDim.x) {
         const int jph = t % nph, g = t / nph;
@@ -678,8 +697,8 @@ inline size_t m2m_sum_smem(int child_nth, int child_nph, int rows, size_t csize)
 // to the child's octant, staged in shared memory once per block: the same
 // arithmetic in the same order as k_l2l, every phi tap then reading shared
 // memory instead of global memory.  One block per (parent, child) pair.
-template <class R, int W, bool POST>  // both transposed stencils padded to W taps per row
-__global__ void __launch_bounds__(256, 2)
+template <class R, int W, bool POST, bool CS>  // both transposed stencils padded to W taps per row
+__global__ void __launch_bounds__(256)
 k_l2l_st(const DevLevelT<R>* __restrict__ lvs, DevTransT<R> T, const int2* __restrict__ pairs) {
     using C = typename Cx<R>::T;
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -706,9 +725,27 @@ k_l2l_st(const DevLevelT<R>* __restrict__ lvs, DevTransT<R> T, const int2* __res
         SB1[d] = b1;
     }
     __syncthreads();
+    if (!CS) {  // one output per thread, stencil read per tap (tap-major)
+        for (int e = threadIdx.x; e < pth * cph; e += blockDim.x) {
+            const int ith = e / cph, jph = e - ith * cph;
+            const C* row0 = SB0 + static_cast<size_t>(ith) * pph;
+            const C* row1 = SB1 + static_cast<size_t>(ith) * pph;
+            C v0 = zero<C>(), v1 = zero<C>();
+#pragma unroll
+            for (int k = 0; k < W; ++k) {
+                const int q = k * cph + jph;
+                const int d = T.dn_ph.src_t[q];
+                const R cf = T.dn_ph.coef_t[q];
+                v0 = crfma(cf, row0[d], v0);
+                v1 = crfma(cf, row1[d], v1);
+            }
+            S10[e] = v0;
+            S11[e] = v1;
+        }
+    }
     // phi pass, column-stationary: a thread keeps one child column's stencil in
     // registers and walks the parent's theta rows (the same stencil for each)
-    const int ng = max(1, static_cast<int>(blockDim.x) / cph);  // row groups
+    const int ng = CS ? max(1, static_cast<int>(blockDim.x) / cph) : 0;  // row groups
     for (int t = threadIdx.x; t < cph * ng; t += blockDim.x) {
         const int jph = t % cph, g = t / cph;
         int sk[W];
