@@ -341,7 +341,8 @@ typedef struct {
                                   phi passes; neither = one interpolation per child */
     int l2l_staged;            /* one-vector anterpolation, transition p -> p+1: bit p = parent's local
                                   pattern staged in shared memory, bit 16 + p = the same with
-                                  column-stationary phi passes */
+                                  column-stationary phi passes, bit 24 + p = the persistent prefetching
+                                  kernel */
     int near_kernel;           /* one-vector near field: 0 one tile per thread block (row and column
                                   threads), 1 one tile per warp (see mlfma_set_near_kernel) */
 } mlfma_tuning;
@@ -377,7 +378,8 @@ int mlfma_get_interp_path(mlfma_handle h, int* mode);
  * kernel); bit 1, L2L with the parent's shifted local pattern staged in shared
  * memory (the same arithmetic in the same order); bit 2, their phi passes
  * column-stationary (a thread keeps one output column's stencil in registers
- * and walks the rows).  Modes 1 and 2 are on after setup; mlfma_autotune
+ * and walks the rows); bit 3, L2L as a persistent kernel that prefetches the
+ * next pair's inputs with asynchronous copies while it computes one.  Modes 1 and 2 are on after setup; mlfma_autotune
  * chooses per transition (mlfma_tuning.m2m_staged/l2l_staged). */
 int mlfma_set_staged_interp(mlfma_handle h, int mode);
 /* Near-field kernel of the one-vector product (Leaf::evalPairSols,

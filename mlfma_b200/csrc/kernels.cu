@@ -440,6 +440,14 @@ std::string DeviceOp::setup_far(const Plan& plan, FarField<R>& F, const double2*
 #undef MLFMA_L2L_ST_FN
             for (const void* fn : fns) MLFMA_CK(dyn(fn));
         }
+        for (int tr = 0; tr < 2; ++tr) {
+            const bool t = tr != 0;
+            MLFMA_CK(dyn(reinterpret_cast<const void*>(t ? k_l2l_pipe<R, 8, true> : k_l2l_pipe<R, 8, false>)));
+            MLFMA_CK(dyn(reinterpret_cast<const void*>(t ? k_l2l_pipe<R, 12, true> : k_l2l_pipe<R, 12, false>)));
+            MLFMA_CK(dyn(reinterpret_cast<const void*>(t ? k_l2l_pipe<R, 16, true> : k_l2l_pipe<R, 16, false>)));
+            MLFMA_CK(dyn(reinterpret_cast<const void*>(t ? k_l2l_pipe<R, 24, true> : k_l2l_pipe<R, 24, false>)));
+            MLFMA_CK(dyn(reinterpret_cast<const void*>(t ? k_l2l_pipe<R, 32, true> : k_l2l_pipe<R, 32, false>)));
+        }
     }
     if (max_rhs_ > 1) {
         // dynamic shared memory up to the opt-in limit less the kernel's static part
@@ -851,7 +859,29 @@ void DeviceOp::far_l2l(FarField<R>& F, int p, cudaStream_t s) {
     if (!g) return;
     const DevTransT<R>& T = F.trans[p];
     const size_t sst = l2l_st_smem(nth_[p], nph_[p], nph_[p + 1], sizeof(C));
-    if (l2l_pref_[p] && sst + 1024 <= static_cast<size_t>(dev_smem_)) {
+    const size_t spipe = l2l_pipe_smem(nth_[p], nph_[p], nth_[p + 1], nph_[p + 1], sizeof(C));
+    if (l2l_pref_[p] == 3 && spipe + 1024 <= static_cast<size_t>(dev_smem_)) {
+        // persistent: as many blocks as fit on the SMs at once
+#define MLFMA_L2L_PIPE(WW)                                                                                 \
+    do {                                                                                                   \
+        const void* fn = reinterpret_cast<const void*>(k_l2l_pipe<R, WW, TR>);                             \
+        int occ = 0;                                                                                       \
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, 256, spipe) != cudaSuccess || occ < 1) \
+            occ = 1;                                                                                       \
+        const int grid = std::max(1, std::min(g, occ * sms_));                                             \
+        k_l2l_pipe<R, WW, TR><<<grid, 256, spipe, s>>>(F.lv_dev, T, l2l_pairs_[p], g);                    \
+    } while (0)
+        switch (dn_w_[p]) {
+            case 8: MLFMA_L2L_PIPE(8); break;
+            case 12: MLFMA_L2L_PIPE(12); break;
+            case 16: MLFMA_L2L_PIPE(16); break;
+            case 24: MLFMA_L2L_PIPE(24); break;
+            default: MLFMA_L2L_PIPE(32); break;
+        }
+#undef MLFMA_L2L_PIPE
+        return;
+    }
+    if (l2l_pref_[p] && l2l_pref_[p] != 3 && sst + 1024 <= static_cast<size_t>(dev_smem_)) {
         const bool cs = l2l_pref_[p] == 2;
 #define MLFMA_L2L_ST(WW)                                                                            \
     (cs ? k_l2l_st<R, WW, TR, true><<<g, 256, sst, s>>>(F.lv_dev, T, l2l_pairs_[p])                  \
@@ -1793,13 +1823,13 @@ std::string DeviceOp::set_near_kernel(int kind) {
 
 std::string DeviceOp::set_staged(int mode) {
     if (!ready_) return "operator not set up";
-    if (mode < 0 || mode > 7) return "arg:mode must be 0..7";
+    if (mode < 0 || mode > 15) return "arg:mode must be 0..15";
     MLFMA_CK(cudaSetDevice(device_));
     MLFMA_CK(cudaStreamSynchronize(stream_));
     const int kind = (mode & 4) ? 2 : 1;
     for (int p = lmin_; p < lmax_; ++p) {
         m2m_pref_[p] = (mode & 1) ? kind : 0;
-        l2l_pref_[p] = (mode & 2) ? kind : 0;
+        l2l_pref_[p] = (mode & 8) ? 3 : (mode & 2) ? kind : 0;
     }
     drop_graphs();
     ++generation_;
@@ -1900,7 +1930,7 @@ std::string DeviceOp::autotune(int nr, int reps, TuneReport* rep) {
             if (n_l2l_pairs_[p]) {
                 float lt = 1e30f;
                 int lkind = l2l_pref_[p];
-                for (int kind : {0, 1, 2}) {
+                for (int kind : {0, 1, 2, 3}) {
                     l2l_pref_[p] = kind;
                     const float t = timed([&] {
                         if (precision_ == kFp64) far_l2l<double, false>(f64_, p, s); else far_l2l<float, false>(f32_, p, s);
@@ -2000,9 +2030,9 @@ std::string DeviceOp::autotune(int nr, int reps, TuneReport* rep) {
     r.near_kernel = near_kernel_;
     r.m2l_chunk = m2l_chunk_;
     r.m2m_staged = r.l2l_staged = 0;
-    for (int p = lmin_; p < lmax_ && p < 16; ++p) {
+    for (int p = lmin_; p < lmax_ && p < 10; ++p) {
         if (m2m_pref_[p]) r.m2m_staged |= 1 << (m2m_pref_[p] == 2 ? 16 + p : p);
-        if (l2l_pref_[p]) r.l2l_staged |= 1 << (l2l_pref_[p] == 2 ? 16 + p : p);
+        if (l2l_pref_[p]) r.l2l_staged |= 1 << (l2l_pref_[p] == 3 ? 24 + p : l2l_pref_[p] == 2 ? 16 + p : p);
     }
     for (int p = lmin_; p < lmax_; ++p) r.m2m_rows[p] = m2m_rows_[p];
     if (r.multi_rows_fast == 0 && m_m2m_rows_fast_ < 0) r.multi_rows_fast = -1;

@@ -793,6 +793,125 @@ k_l2l_st(const DevLevelT<R>* __restrict__ lvs, DevTransT<R> T, const int2* __res
     }
 }
 
+// The staged L2L as a persistent, software-pipelined kernel: each block walks
+// the pairs blockIdx.x, blockIdx.x + gridDim.x, ... and, while it computes one
+// pair, the next pair's parent pattern, shift and child local pattern arrive by
+// asynchronous copies (cp.async, 8 or 16 bytes per copy) into the other half of
+// a double buffer; the child's updated local is written with plain stores.
+// Same arithmetic in the same order as k_l2l_st<..., false>.
+__device__ __forceinline__ void cp_async_elem(void* dst, const void* src, int bytes) {
+    const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(dst));
+    if (bytes == 16)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+
+template <class R, int W, bool POST>
+__global__ void __launch_bounds__(256)
+k_l2l_pipe(const DevLevelT<R>* __restrict__ lvs, DevTransT<R> T, const int2* __restrict__ pairs, int npairs) {
+    using C = typename Cx<R>::T;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    const DevLevelT<R> P = lvs[T.plevel];
+    const DevLevelT<R> Cl = lvs[T.plevel + 1];
+    const int pth = P.nth, pph = P.nph, cth = Cl.nth, cph = Cl.nph, halfc = Cl.nph / 2;
+    const int np = pth * pph, nq = pth * cph, nc = cth * cph;
+    const int nsh = POST ? nc : np;  // shift values: parent grid (before) or child grid (after, POST)
+    // per buffer: raw parent [2 np] (interleaved, as stored), shift [nsh], child [2 nc]
+    const size_t per_buf = 2 * static_cast<size_t>(np) + nsh + 2 * static_cast<size_t>(nc);
+    C* buf0 = reinterpret_cast<C*>(smraw);
+    C* SB0 = buf0 + 2 * per_buf;  // planes [np] x 2, then S1 planes [nq] x 2
+    C* SB1 = SB0 + np;
+    C* S10 = SB1 + np;
+    C* S11 = S10 + nq;
+    auto issue = [&](int pi, int b) {
+        const int2 pc = pairs[pi];
+        C* raw = buf0 + b * per_buf;
+        C* shv = raw + 2 * np;
+        C* cl = shv + nsh;
+        const C* Bp = P.B + static_cast<size_t>(T.par_box[pc.x]) * P.ndir * 2;
+        const C* sh = POST ? Cl.shift_up + static_cast<size_t>(T.child_oct[pc.y]) * Cl.ndir
+                           : P.shift_down + static_cast<size_t>(T.child_oct[pc.y]) * P.ndir;
+        const C* Bc = Cl.B + static_cast<size_t>(T.child_box[pc.y]) * Cl.ndir * 2;
+        for (int i = threadIdx.x; i < 2 * np; i += blockDim.x) cp_async_elem(raw + i, Bp + i, sizeof(C));
+        for (int i = threadIdx.x; i < nsh; i += blockDim.x) cp_async_elem(shv + i, sh + i, sizeof(C));
+        for (int i = threadIdx.x; i < 2 * nc; i += blockDim.x) cp_async_elem(cl + i, Bc + i, sizeof(C));
+    };
+    int b = 0;
+    if (static_cast<int>(blockIdx.x) < npairs) issue(blockIdx.x, 0);
+    cp_async_commit();
+    for (int pi = blockIdx.x; pi < npairs; pi += gridDim.x, b ^= 1) {
+        const int nxt = pi + gridDim.x;
+        if (nxt < npairs) issue(nxt, b ^ 1);
+        cp_async_commit();  // (possibly empty) group, so that wait_group 1 means "this pair"
+        cp_async_wait1();
+        __syncthreads();
+        const C* raw = buf0 + b * per_buf;
+        const C* shv = raw + 2 * np;
+        const C* cl = shv + nsh;
+        for (int d = threadIdx.x; d < np; d += blockDim.x) {
+            C b0 = raw[2 * d], b1 = raw[2 * d + 1];
+            if (!POST) {
+                const C ph = shv[d];
+                b0 = cmul(ph, b0);
+                b1 = cmul(ph, b1);
+            }
+            SB0[d] = b0;
+            SB1[d] = b1;
+        }
+        __syncthreads();
+        for (int e = threadIdx.x; e < nq; e += blockDim.x) {
+            const int ith = e / cph, jph = e - ith * cph;
+            const C* row0 = SB0 + static_cast<size_t>(ith) * pph;
+            const C* row1 = SB1 + static_cast<size_t>(ith) * pph;
+            C v0 = zero<C>(), v1 = zero<C>();
+#pragma unroll
+            for (int k = 0; k < W; ++k) {
+                const int q = k * cph + jph;
+                const int d = T.dn_ph.src_t[q];
+                const R cf = T.dn_ph.coef_t[q];
+                v0 = crfma(cf, row0[d], v0);
+                v1 = crfma(cf, row1[d], v1);
+            }
+            S10[e] = v0;
+            S11[e] = v1;
+        }
+        __syncthreads();
+        const int2 pc = pairs[pi];
+        C* Bc = Cl.B + static_cast<size_t>(T.child_box[pc.y]) * Cl.ndir * 2;
+        for (int e = threadIdx.x; e < nc; e += blockDim.x) {
+            const int jth = e / cph, jph = e - jth * cph;
+            C v0 = zero<C>(), v1 = zero<C>();
+#pragma unroll
+            for (int k = 0; k < W; ++k) {
+                const int q = jth * W + k;
+                const bool rf = T.dn_th.refl[q];
+                const int sp = rf ? (jph < halfc ? jph + halfc : jph - halfc) : jph;
+                const R cf = T.dn_th.coef[q];
+                const size_t at = static_cast<size_t>(T.dn_th.src[q]) * cph + sp;
+                v0 = crfma(cf, S10[at], v0);
+                v1 = crfma(cf, S11[at], v1);
+            }
+            if (POST) {
+                const C ph = shv[e];
+                v0 = cmul(ph, v0);
+                v1 = cmul(ph, v1);
+            }
+            Bc[2 * e] = cadd(cl[2 * e], v0);
+            Bc[2 * e + 1] = cadd(cl[2 * e + 1], v1);
+        }
+        __syncthreads();  // buffers and planes free for the next pair
+    }
+}
+
+inline size_t l2l_pipe_smem(int pth, int pph, int cth, int cph, size_t csize) {
+    const size_t np = static_cast<size_t>(pth) * pph, nc = static_cast<size_t>(cth) * cph;
+    const size_t per_buf = 2 * np + std::max(np, nc) + 2 * nc;
+    return (2 * per_buf + 2 * np + 2 * static_cast<size_t>(pth) * cph) * csize;
+}
+
 inline size_t l2l_st_smem(int parent_nth, int parent_nph, int child_nph, size_t csize) {
     return static_cast<size_t>(parent_nth) * (parent_nph + child_nph) * 2 * csize;
 }

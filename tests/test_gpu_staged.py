@@ -46,7 +46,7 @@ def test_staged_interp_matches_per_child_kernels(cuda_device, case, precision):
     op.set_staged_interp(0)
     y0 = op.matvec(x)
     a0 = op.matvec_adjoint(x)
-    for mode in (1, 2, 3, 5, 6, 7):
+    for mode in (1, 2, 3, 5, 6, 7, 8, 9):
         op.set_staged_interp(mode)
         y = op.matvec(x)
         assert rel(y, y0) <= tol, (mode, rel(y, y0))
