@@ -97,7 +97,6 @@ k_near_sym(const DevNearTile* __restrict__ tiles, int ntiles, const double2* __r
     __shared__ __align__(8) unsigned long long full[kSymStages], empty[kSymStages];
     __shared__ DevNearTile hdr[kSymStages];
     __shared__ DevNearTile hbuf[32];  // producer's header batch
-    __shared__ double2 rowp[2][2][kNearTileRows], colp[2][2][kNearTileCols];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int step = gridDim.x;
     if (tid == 0) {
@@ -183,16 +182,16 @@ k_near_sym(const DevNearTile* __restrict__ tiles, int ntiles, const double2* __r
         const double2* xc = zt + kSymXc;
         const double2* xr = zt + kSymXr;
         const int* sl = reinterpret_cast<const int*>(zt + kSymSlot);
-        const int b = it & 1;
-        int my_slot = -1, idx;
-        if (ct < 64) {  // row sums: two threads per row when the tile has at most 32 rows
-            const bool split = T.ni <= 32;
-            const int r = split ? (ct & 31) : ct, h = split ? (ct >> 5) : 0;
-            idx = r;
+        int my_slot = -1;
+        double2 sum;
+        if (ct < 64) {  // row sums: G adjacent lanes per row, G = 64 / rows rounded down to 1, 2, 4 or 8
+            const int G = T.ni <= 8 ? 8 : T.ni <= 16 ? 4 : T.ni <= 32 ? 2 : 1;
+            const int r = ct / G, h = ct & (G - 1);
             double2 a0 = z0(), a1 = z0(), a2 = z0(), a3 = z0();
             if (r < T.ni) {
                 const int len = tile_row_len(T, r);
-                const int k0 = split && h ? (len + 1) >> 1 : 0, k1 = split && !h ? (len + 1) >> 1 : len;
+                const int seg = (len + G - 1) / G;
+                const int k0 = min(len, h * seg), k1 = min(len, k0 + seg);
                 const int L = k1 - k0;
                 const double2* zr = zt + tile_row_start(T, r) + k0;
                 const double2* xk = xc + k0;
@@ -218,18 +217,21 @@ k_near_sym(const DevNearTile* __restrict__ tiles, int ntiles, const double2* __r
                 }
                 if (h == 0) my_slot = sl[r];
             }
-            rowp[b][h][r] = cadd(cadd(a0, a1), cadd(a2, a3));
-            if (!split) rowp[b][1][r] = z0();
-        } else {  // column sums: two threads per column when the tile has at most 32 columns
+            sum = cadd(cadd(a0, a1), cadd(a2, a3));
+            for (int o = G >> 1; o > 0; o >>= 1) {  // the row's G segments, a fixed order
+                const double2 v = make_double2(__shfl_xor_sync(0xffffffffu, sum.x, o),
+                                               __shfl_xor_sync(0xffffffffu, sum.y, o));
+                sum = cadd(sum, v);
+            }
+        } else {  // column sums: G adjacent lanes per column, G = 64 / columns rounded down to 1, 2, 4 or 8
             const int cc = ct - 64;
-            const bool split = T.nj <= 32;
-            const int c = split ? (cc & 31) : cc, h = split ? (cc >> 5) : 0;
-            idx = c;
+            const int G = T.nj <= 8 ? 8 : T.nj <= 16 ? 4 : T.nj <= 32 ? 2 : 1;
+            const int c = cc / G, h = cc & (G - 1);
             double2 a0 = z0(), a1 = z0(), a2 = z0(), a3 = z0();
             if (c < T.nj) {
                 const int rs = tile_col_start(T, c);
-                const int mid = (rs + T.ni + 1) >> 1;
-                const int ra = split && h ? mid : rs, rb = split && !h ? mid : T.ni;
+                const int seg = (max(0, T.ni - rs) + G - 1) / G;
+                const int ra = min(T.ni, rs + h * seg), rb = min(T.ni, ra + seg);
                 // walk down the column: rows nj apart, or (packed) one longer each
                 const int inc = T.mode == 1 ? 1 : 0;
                 int stride = T.mode == 1 ? T.i0 + ra + (T.kind == 2 ? 1 : 0) : T.nj;
@@ -256,13 +258,16 @@ k_near_sym(const DevNearTile* __restrict__ tiles, int ntiles, const double2* __r
                 }
                 if (h == 0) my_slot = sl[T.ni + c];
             }
-            colp[b][h][c] = cadd(cadd(a0, a1), cadd(a2, a3));
-            if (!split) colp[b][1][c] = z0();
+            sum = cadd(cadd(a0, a1), cadd(a2, a3));
+            for (int o = G >> 1; o > 0; o >>= 1) {
+                const double2 v = make_double2(__shfl_xor_sync(0xffffffffu, sum.x, o),
+                                               __shfl_xor_sync(0xffffffffu, sum.y, o));
+                sum = cadd(sum, v);
+            }
         }
-        consumers_sync();  // stage s read, partial halves complete
+        consumers_sync();  // stage s read by every consumer
         if (ct == 0) mbar_arrive(smem_addr(&empty[s]));
-        if (my_slot >= 0)
-            part[my_slot] = ct < 64 ? cadd(rowp[b][0][idx], rowp[b][1][idx]) : cadd(colp[b][0][idx], colp[b][1][idx]);
+        if (my_slot >= 0) part[my_slot] = sum;
     }
 }
 

@@ -8,6 +8,7 @@
 // the block-row form (each leaf's rows against all the sources it meets) on a
 // symmetric synthetic entry.  Run by tests/test_near_tiles.py.
 #include "plan.hpp"
+#include <algorithm>
 #include <cmath>
 #include <complex>
 #include <cstdio>
@@ -107,37 +108,45 @@ int run(int n, int maxsrc, int self_terms, double side, int seed) {
         if (total != copied || (total + T.ni + T.nj) * 16 + nslot * 4 >= (1 << 20)) { printf("tx bytes\n"); return 1; }
         auto rd = [&](int a) -> C { if (a < 0 || a >= SE || !ok[a]) { printf("read of uncopied slot %d\n", a); exit(1); } return st[a]; };
         auto rs = [&](int a) -> int { if (!slotok[a]) { printf("slot read\n"); exit(1); } return slotmem[a]; };
-        C rowp[2][64], colp[2][64]; int myslot[128], idxv[128];
+        // k_near_sym's consumers: G adjacent lanes per row (column), each a
+        // segment; the lane with h == 0 writes the group's sum
+        C gsum[128]; int myslot[128];
         for (int ct = 0; ct < 128; ++ct) {
             myslot[ct] = -1;
+            C a(0);
             if (ct < 64) {
-                const bool split = T.ni <= 32; const int r = split ? (ct & 31) : ct, h = split ? (ct >> 5) : 0; idxv[ct] = r;
-                C a(0);
+                const int G = T.ni <= 8 ? 8 : T.ni <= 16 ? 4 : T.ni <= 32 ? 2 : 1;
+                const int r = ct / G, h = ct & (G - 1);
                 if (r < T.ni) {
                     const int len = rowlen(T, r);
-                    const int k0 = split && h ? (len + 1) >> 1 : 0, k1 = split && !h ? (len + 1) >> 1 : len, L = k1 - k0;
+                    const int seg = (len + G - 1) / G;
+                    const int k0 = std::min(len, h * seg), k1 = std::min(len, k0 + seg), L = k1 - k0;
                     int q = (T.mode != 1 && !(T.nj & 1) && L > 0) ? r % L : 0;
                     for (int m = 0; m < L; ++m) { a += rd(rowstart(T, r) + k0 + q) * rd(XC + k0 + q); if (++q == L) q = 0; }
                     if (h == 0) myslot[ct] = rs(r);
                 }
-                rowp[h][r] = a; if (!split) rowp[1][r] = 0;
             } else {
-                const int cc = ct - 64; const bool split = T.nj <= 32; const int c = split ? (cc & 31) : cc, h = split ? (cc >> 5) : 0; idxv[ct] = c;
-                C a(0);
+                const int cc = ct - 64;
+                const int G = T.nj <= 8 ? 8 : T.nj <= 16 ? 4 : T.nj <= 32 ? 2 : 1;
+                const int c = cc / G, h = cc & (G - 1);
                 if (c < T.nj) {
-                    const int r0s = colstart(T, c), mid = (r0s + T.ni + 1) >> 1;
-                    const int ra = split && h ? mid : r0s, rb = split && !h ? mid : T.ni;
+                    const int r0s = colstart(T, c);
+                    const int seg = (std::max(0, T.ni - r0s) + G - 1) / G;
+                    const int ra = std::min(T.ni, r0s + h * seg), rb = std::min(T.ni, ra + seg);
                     for (int r = ra; r < rb; ++r) a += rd(rowstart(T, r) + c) * rd(XR + r);
                     if (h == 0) myslot[ct] = rs(T.ni + c);
                 }
-                colp[h][c] = a; if (!split) colp[1][c] = 0;
             }
+            gsum[ct] = a;
         }
         for (int ct = 0; ct < 128; ++ct) {
             if (myslot[ct] < 0) continue;
             if (myslot[ct] >= p.near_parts) { printf("slot value range\n"); return 1; }
-            const int id = idxv[ct];
-            part[myslot[ct]] = ct < 64 ? rowp[0][id] + rowp[1][id] : colp[0][id] + colp[1][id];
+            const int G = ct < 64 ? (T.ni <= 8 ? 8 : T.ni <= 16 ? 4 : T.ni <= 32 ? 2 : 1)
+                                  : (T.nj <= 8 ? 8 : T.nj <= 16 ? 4 : T.nj <= 32 ? 2 : 1);
+            C a(0);
+            for (int h = 0; h < G; ++h) a += gsum[ct + h];  // the group's lanes
+            part[myslot[ct]] = a;
             written[myslot[ct]]++;
         }
     }
