@@ -5,6 +5,7 @@ at):
     python -m mlfma_b200.workloads sphere_r2 --precision 1 --products 3
     python -m mlfma_b200.workloads sphere_r8 --precision 1 --staged 3 --products 2
     python -m mlfma_b200.workloads sphere_r2 --precision 1 --max-rhs 64 --interp-path 15
+    python -m mlfma_b200.workloads sphere_r2 --products 1 --solve 40
 
 sphere_r2: PEC sphere of radius 2 wavelengths, level-5 icosphere (20,480
 triangles, 30,720 RWG unknowns), root box 4 wavelengths, boxes split above 54
@@ -50,6 +51,8 @@ def main(argv=None) -> int:
     ap.add_argument("--staged", type=int, default=None, help="mlfma_set_staged_interp mode")
     ap.add_argument("--autotune", action="store_true")
     ap.add_argument("--products", type=int, default=3)
+    ap.add_argument("--solve", type=int, default=0,
+                    help="> 0: then a GMRES(50) solve of the plane-wave right-hand side, that many iterations")
     a = ap.parse_args(argv)
     import torch
 
@@ -71,6 +74,9 @@ def main(argv=None) -> int:
         for _ in range(a.products):
             op.matvec_device(x.data_ptr(), y.data_ptr(), False, 0)
     torch.cuda.synchronize()
+    if a.solve > 0:
+        b = op.rhs()
+        op.solve(b, max_iter=a.solve, tol=1e-14, restart=50, ref_givens=False)
     op.close()
     print("ok")
     return 0
