@@ -30,6 +30,8 @@ namespace {
 
 constexpr int kDotThreads = 256;
 constexpr int kDotChunk = 8192;  // vector elements per partial sum
+constexpr int kStepChunk = 1024;  // the same in the device-resident steps (more blocks in flight)
+constexpr int kUpdThreads = 128;  // k_step_update block
 
 __device__ __forceinline__ double2 cj_mul_add(double2 a, double2 b, double2 c) {
     return make_double2(fma(a.x, b.x, fma(a.y, b.y, c.x)), fma(a.x, b.y, fma(-a.y, b.x, c.y)));
@@ -185,9 +187,18 @@ __global__ void k_step_dots(StepStateD* __restrict__ st, const double2* __restri
     const int k = st->k;
     if (j <= k) {
         const double2* q = Q + static_cast<long long>(j) * n;
-        const int i0 = c * kDotChunk, i1 = min(n, i0 + kDotChunk);
-        double2 acc = make_double2(0.0, 0.0);
-        for (int i = i0 + threadIdx.x; i < i1; i += blockDim.x) acc = cj_mul_add(q[i], w[i], acc);
+        const int i0 = c * kStepChunk, i1 = min(n, i0 + kStepChunk);
+        // kStepChunk / blockDim = 4 elements per thread, loads issued together
+        double2 acc = make_double2(0.0, 0.0), acc2 = make_double2(0.0, 0.0);
+        int i = i0 + threadIdx.x;
+        for (; i + blockDim.x < i1; i += 2 * blockDim.x) {
+            const double2 qa = q[i], wa = w[i], qb = q[i + blockDim.x], wb = w[i + blockDim.x];
+            acc = cj_mul_add(qa, wa, acc);
+            acc2 = cj_mul_add(qb, wb, acc2);
+        }
+        if (i < i1) acc = cj_mul_add(q[i], w[i], acc);
+        acc.x += acc2.x;
+        acc.y += acc2.y;
         red[threadIdx.x] = acc;
         __syncthreads();
         for (int s2 = blockDim.x / 2; s2 > 0; s2 >>= 1) {
@@ -225,19 +236,38 @@ __global__ void k_step_dots(StepStateD* __restrict__ st, const double2* __restri
 __global__ void k_step_update(StepStateD* __restrict__ st, const double2* __restrict__ Q, int n,
                               const double2* __restrict__ t, double2* __restrict__ w, double* __restrict__ npart,
                               double2* __restrict__ hcols, int ldh, int norm) {
-    __shared__ double red[256];
+    __shared__ double red[kUpdThreads];
     __shared__ bool last;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int k = st->k;
     double nn = 0.0;
     if (i < n) {
-        double2 v = w[i];
-        for (int j = 0; j <= k; ++j) {
+        // four independent partial sums over the basis vectors, then in order
+        double2 u[4] = {make_double2(0.0, 0.0), make_double2(0.0, 0.0), make_double2(0.0, 0.0),
+                        make_double2(0.0, 0.0)};
+        int j = 0;
+        for (; j + 3 <= k; j += 4) {
+            double2 q[4], h[4];
+#pragma unroll
+            for (int a = 0; a < 4; ++a) {
+                q[a] = Q[static_cast<long long>(j + a) * n + i];
+                h[a] = t[j + a];
+            }
+#pragma unroll
+            for (int a = 0; a < 4; ++a) {
+                u[a].x += q[a].x * h[a].x - q[a].y * h[a].y;
+                u[a].y += q[a].x * h[a].y + q[a].y * h[a].x;
+            }
+        }
+        for (; j <= k; ++j) {
             const double2 q = Q[static_cast<long long>(j) * n + i];
             const double2 hj = t[j];
-            v.x -= q.x * hj.x - q.y * hj.y;
-            v.y -= q.x * hj.y + q.y * hj.x;
+            u[0].x += q.x * hj.x - q.y * hj.y;
+            u[0].y += q.x * hj.y + q.y * hj.x;
         }
+        double2 v = w[i];
+        v.x -= (u[0].x + u[1].x) + (u[2].x + u[3].x);
+        v.y -= (u[0].y + u[1].y) + (u[2].y + u[3].y);
         w[i] = v;
         nn = fma(v.x, v.x, v.y * v.y);
     }
@@ -300,7 +330,9 @@ std::string Gmres::ensure(int n, int ncols, int extra) {
         GM_CK(cudaMalloc(&st_, sizeof(StepStateD)));
         GM_CK(cudaMalloc(&hcols_, sizeof(double2) * static_cast<size_t>(ncols) * (ncols + 1)));
         GM_CK(cudaMalloc(&tco_, sizeof(double2) * (ncols + 1)));
-        GM_CK(cudaMalloc(&npart2_, sizeof(double) * nblk(n, 256)));
+        GM_CK(cudaMalloc(&npart2_, sizeof(double) * nblk(n, kUpdThreads)));
+        nstep_ = (n + kStepChunk - 1) / kStepChunk;
+        GM_CK(cudaMalloc(&spartial_, sizeof(double2) * static_cast<size_t>(nstep_) * (ncols + 1)));
     }
     return {};
 }
@@ -311,12 +343,13 @@ void Gmres::release_steps() {
     sgx_ = nullptr;
     sg_ = nullptr;
     sg_op_ = nullptr;
-    for (void* p : {st_, (void*)hcols_, (void*)tco_, (void*)npart2_})
+    for (void* p : {st_, (void*)hcols_, (void*)tco_, (void*)npart2_, (void*)spartial_})
         if (p) cudaFree(p);
     st_ = nullptr;
     hcols_ = nullptr;
     tco_ = nullptr;
     npart2_ = nullptr;
+    spartial_ = nullptr;
 }
 
 // The captured Arnoldi step for this operator, precision and direction
@@ -344,9 +377,9 @@ std::string Gmres::step_graph(DeviceOp& op, int prec) {
     }
     op.enqueue_apply_from_input(w_, s, prec, adj_);
     for (int pass = 0; pass < 2; ++pass) {
-        k_step_dots<<<dim3(nchunks_, cap_), kDotThreads, 0, s>>>(st, Q_, n, w_, partial_, nchunks_, tco_, hcols_, ldh,
+        k_step_dots<<<dim3(nstep_, cap_), kDotThreads, 0, s>>>(st, Q_, n, w_, spartial_, nstep_, tco_, hcols_, ldh,
                                                                   pass);
-        k_step_update<<<nblk(n, 256), 256, 0, s>>>(st, Q_, n, tco_, w_, npart2_, hcols_, ldh, pass);
+        k_step_update<<<nblk(n, kUpdThreads), kUpdThreads, 0, s>>>(st, Q_, n, tco_, w_, npart2_, hcols_, ldh, pass);
     }
     const cudaError_t ce = cudaStreamEndCapture(s, &sg_);
     if (ce != cudaSuccess) return std::string("step capture: ") + cudaGetErrorString(ce);

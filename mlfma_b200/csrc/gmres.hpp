@@ -81,6 +81,8 @@ private:
     double2* hcols_ = nullptr;   // [cap_][cap_ + 1]: Hessenberg column k at k (cap_ + 1)
     double2* tco_ = nullptr;     // [cap_]: coefficients of the current CGS pass
     double* npart2_ = nullptr;   // norm partials, one per update block
+    double2* spartial_ = nullptr;  // dot partials of the device steps, [columns][nstep_]
+    int nstep_ = 0;                // their chunks of the vector
     cudaGraph_t sg_ = nullptr;
     cudaGraphExec_t sgx_ = nullptr;
     const DeviceOp* sg_op_ = nullptr;
