@@ -53,6 +53,8 @@ def main(argv=None) -> int:
     ap.add_argument("--products", type=int, default=3)
     ap.add_argument("--solve", type=int, default=0,
                     help="> 0: then a GMRES(50) solve of the plane-wave right-hand side, that many iterations")
+    ap.add_argument("--flexible", action="store_true",
+                    help="the solve as FGMRES(30) with 50 inner iterations per outer step")
     a = ap.parse_args(argv)
     import torch
 
@@ -76,7 +78,10 @@ def main(argv=None) -> int:
     torch.cuda.synchronize()
     if a.solve > 0:
         b = op.rhs()
-        op.solve(b, max_iter=a.solve, tol=1e-14, restart=50, ref_givens=False)
+        if a.flexible:
+            op.solve(b, max_iter=a.solve, tol=1e-14, restart=30, flexible=True, inner_iters=50)
+        else:
+            op.solve(b, max_iter=a.solve, tol=1e-14, restart=50, ref_givens=False)
     op.close()
     print("ok")
     return 0
