@@ -175,40 +175,64 @@ __global__ void k_step_prep(StepStateD* __restrict__ st, double2* __restrict__ Q
 }
 
 // One CGS pass, dots: partial[j][c] = sum_{i in chunk c} conj(Q_j[i]) w[i] for
-// j <= k (block (c, j)); the last block to finish sums each j's partials in a
-// fixed order into t[j] and into column k of the Hessenberg matrix (pass 0
-// sets it, pass 1 adds).
-__global__ void k_step_dots(StepStateD* __restrict__ st, const double2* __restrict__ Q, int n,
-                            const double2* __restrict__ w, double2* __restrict__ partial, int nchunks,
-                            double2* __restrict__ t, double2* __restrict__ hcols, int ldh, int pass) {
-    __shared__ double2 red[kDotThreads];
+// j <= k.  Block (c, g) reads chunk c of w once (four elements per thread, in
+// registers) and forms the dots with the kStepCols columns j = g kStepCols ..
+// of group g; the last block to finish sums each j's partials in a fixed order
+// into t[j] and into column k of the Hessenberg matrix (pass 0 sets it, pass 1
+// adds).
+constexpr int kStepCols = 8;
+__global__ void __launch_bounds__(kDotThreads)
+k_step_dots(StepStateD* __restrict__ st, const double2* __restrict__ Q, int n, const double2* __restrict__ w,
+            double2* __restrict__ partial, int nchunks, double2* __restrict__ t, double2* __restrict__ hcols, int ldh,
+            int pass) {
+    __shared__ double2 red[kStepCols][kDotThreads];
     __shared__ bool last;
-    const int c = blockIdx.x, j = blockIdx.y;
+    const int c = blockIdx.x, j0 = blockIdx.y * kStepCols;
     const int k = st->k;
-    if (j <= k) {
-        const double2* q = Q + static_cast<long long>(j) * n;
-        const int i0 = c * kStepChunk, i1 = min(n, i0 + kStepChunk);
-        // kStepChunk / blockDim = 4 elements per thread, loads issued together
-        double2 acc = make_double2(0.0, 0.0), acc2 = make_double2(0.0, 0.0);
-        int i = i0 + threadIdx.x;
-        for (; i + blockDim.x < i1; i += 2 * blockDim.x) {
-            const double2 qa = q[i], wa = w[i], qb = q[i + blockDim.x], wb = w[i + blockDim.x];
-            acc = cj_mul_add(qa, wa, acc);
-            acc2 = cj_mul_add(qb, wb, acc2);
+    constexpr int per = kStepChunk / kDotThreads;  // elements per thread
+    if (j0 <= k) {
+        const int i0 = c * kStepChunk;
+        double2 wv[per];
+#pragma unroll
+        for (int e = 0; e < per; ++e) {
+            const int i = i0 + e * kDotThreads + threadIdx.x;
+            wv[e] = i < n ? w[i] : make_double2(0.0, 0.0);
         }
-        if (i < i1) acc = cj_mul_add(q[i], w[i], acc);
-        acc.x += acc2.x;
-        acc.y += acc2.y;
-        red[threadIdx.x] = acc;
-        __syncthreads();
-        for (int s2 = blockDim.x / 2; s2 > 0; s2 >>= 1) {
-            if (threadIdx.x < s2) {
-                red[threadIdx.x].x += red[threadIdx.x + s2].x;
-                red[threadIdx.x].y += red[threadIdx.x + s2].y;
+#pragma unroll
+        for (int jj = 0; jj < kStepCols; ++jj) {
+            const int j = j0 + jj;
+            double2 acc = make_double2(0.0, 0.0);
+            if (j <= k) {
+                const double2* q = Q + static_cast<long long>(j) * n;
+                double2 qv[per];
+#pragma unroll
+                for (int e = 0; e < per; ++e) {
+                    const int i = i0 + e * kDotThreads + threadIdx.x;
+                    qv[e] = i < n ? q[i] : make_double2(0.0, 0.0);
+                }
+#pragma unroll
+                for (int e = 0; e < per; ++e) acc = cj_mul_add(qv[e], wv[e], acc);
             }
-            __syncthreads();
+            red[jj][threadIdx.x] = acc;
         }
-        if (threadIdx.x == 0) partial[static_cast<long long>(j) * nchunks + c] = red[0];
+        __syncthreads();
+        // warp jj sums column jj's kDotThreads values: eight per lane, then a butterfly
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        if (warp < kStepCols && j0 + warp <= k) {
+            double2 a = make_double2(0.0, 0.0);
+#pragma unroll
+            for (int e = 0; e < kDotThreads / 32; ++e) {
+                const double2 v = red[warp][e * 32 + lane];
+                a.x += v.x;
+                a.y += v.y;
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                a.x += __shfl_xor_sync(0xffffffffu, a.x, o);
+                a.y += __shfl_xor_sync(0xffffffffu, a.y, o);
+            }
+            if (lane == 0) partial[static_cast<long long>(j0 + warp) * nchunks + c] = a;
+        }
     }
     __threadfence();
     __syncthreads();
@@ -377,7 +401,8 @@ std::string Gmres::step_graph(DeviceOp& op, int prec) {
     }
     op.enqueue_apply_from_input(w_, s, prec, adj_);
     for (int pass = 0; pass < 2; ++pass) {
-        k_step_dots<<<dim3(nstep_, cap_), kDotThreads, 0, s>>>(st, Q_, n, w_, spartial_, nstep_, tco_, hcols_, ldh,
+        k_step_dots<<<dim3(nstep_, (cap_ + kStepCols - 1) / kStepCols), kDotThreads, 0, s>>>(st, Q_, n, w_, spartial_,
+                                                                                          nstep_, tco_, hcols_, ldh,
                                                                   pass);
         k_step_update<<<nblk(n, kUpdThreads), kUpdThreads, 0, s>>>(st, Q_, n, tco_, w_, npart2_, hcols_, ldh, pass);
     }
