@@ -344,7 +344,8 @@ typedef struct {
                                   column-stationary phi passes, bit 24 + p = the persistent prefetching
                                   kernel */
     int near_kernel;           /* one-vector near field: 0 one tile per thread block (row and column
-                                  threads), 1 one tile per warp (see mlfma_set_near_kernel) */
+                                  threads), 1 one tile per warp from shared memory, 2 one tile per
+                                  warp from global memory (see mlfma_set_near_kernel) */
 } mlfma_tuning;
 
 /* Autotuner: times the candidate launch shapes of the stages on this operator
@@ -387,7 +388,9 @@ int mlfma_set_staged_interp(mlfma_handle h, int mode);
  * applied as Z and Z^T, tiles streamed by bulk copies): kind 0, one tile per
  * thread block (row threads and column threads; the default); kind 1, one
  * tile per warp, each entry read from shared memory once and the row sums
- * formed by a warp reduce-scatter.  Same partial sums, other rounding order. */
+ * formed by a warp reduce-scatter; kind 2, one tile per warp with the entries
+ * loaded straight from global memory into registers (no shared-memory stage).
+ * Same partial sums, other rounding order; mlfma_autotune tries all three. */
 int mlfma_set_near_kernel(mlfma_handle h, int kind);
 
 /* ---- Many independent operators of uneven size (no counterpart in the

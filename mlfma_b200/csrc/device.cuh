@@ -373,7 +373,8 @@ private:
     std::vector<int> m2m_rows_;           // one-vector M2M parent rows per block, per transition
     std::vector<int> m2m_pref_, l2l_pref_;  // per transition: 1 = staged kernels (k_m2m_sum, k_l2l_st) where they fit
     int dev_smem_ = 0;                    // opt-in shared memory per block
-    int near_kernel_ = 0;                 // one-vector near field: 0 k_near_sym, 1 k_near_warp
+    int near_kernel_ = 0;                 // one-vector near field: 0 k_near_sym, 1 k_near_warp, 2 k_near_direct
+    int near_direct_occ_ = 1;             // k_near_direct blocks per SM
     int m_m2m_rows_fast_ = -1;            // many-rhs M2M grid order (-1: precision default)
     int m_l2l_pairs_ = 0;                 // many-rhs L2L column pairs per block (0: precision default)
     std::vector<int2*> l2l_pairs_;       // per parent level: (parent, child entry)

@@ -128,6 +128,11 @@ DeviceOp::~DeviceOp() {
 // running beside it.
 void DeviceOp::set_near_grid(int per_sm) {
     if (near_kernel_ == 1) per_sm = 1;  // k_near_warp: one block per SM (its ring fills the shared memory)
+    if (near_kernel_ == 2) {            // k_near_direct: every resident warp of the grid takes tiles
+        near_grid_ = std::max(1, std::min((n_near_tiles_ + kNdThreads / 32 - 1) / (kNdThreads / 32),
+                                          std::max(1, per_sm) * sms_));
+        return;
+    }
     near_grid_ = std::max(1, std::min(n_near_tiles_ / 4, std::max(1, per_sm) * sms_));
 }
 
@@ -712,6 +717,8 @@ std::string DeviceOp::setup(const Plan& plan, int device, int precision, int max
                 MLFMA_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&near_occ_, k_near_sym, kSymThreads,
                                                                        kSymSmemBytes));
                 near_occ_ = std::max(1, near_occ_);
+                MLFMA_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&near_direct_occ_, k_near_direct, kNdThreads, 0));
+                near_direct_occ_ = std::max(1, near_direct_occ_);
                 near_per_sm_ = near_occ_;
                 MLFMA_CK(cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, device_));
                 set_near_grid(near_per_sm_);
@@ -1014,7 +1021,10 @@ void DeviceOp::run_near(const double2* xt, cudaStream_t s) {
         cudaMemsetAsync(ynear_, 0, sizeof(double2) * n_, s);
         return;
     }
-    if (near_kernel_ == 1)
+    if (near_kernel_ == 2)
+        k_near_direct<<<near_grid_, kNdThreads, 0, s>>>(near_tiles_, n_near_tiles_, near_bz_, xt, near_slot_,
+                                                         near_part_);
+    else if (near_kernel_ == 1)
         k_near_warp<<<near_grid_, kNwThreads, kNwSmemBytes, s>>>(near_tiles_, n_near_tiles_, near_bz_, xt, near_slot_,
                                                                  near_part_, err_dev_);
     else
@@ -1810,12 +1820,12 @@ std::string DeviceOp::set_tc(int mode) {
 
 std::string DeviceOp::set_near_kernel(int kind) {
     if (!ready_) return "operator not set up";
-    if (kind < 0 || kind > 1) return "arg:kind must be 0 or 1";
+    if (kind < 0 || kind > 2) return "arg:kind must be 0, 1 or 2";
     MLFMA_CK(cudaSetDevice(device_));
     MLFMA_CK(cudaStreamSynchronize(stream_));
     near_kernel_ = kind;
-    set_near_grid(kind ? 1 : near_occ_);
-    near_per_sm_ = kind ? 1 : near_occ_;
+    near_per_sm_ = kind == 2 ? near_direct_occ_ : kind == 1 ? 1 : near_occ_;
+    set_near_grid(near_per_sm_);
     drop_graphs();
     ++generation_;
     return {};
@@ -1945,8 +1955,14 @@ std::string DeviceOp::autotune(int nr, int reps, TuneReport* rep) {
         if (n_near_tiles_) {
             float bt = 1e30f;
             int bk = near_per_sm_, bkind = near_kernel_;
-            for (int kind : {0, 1})
-                for (int k = 1; k <= (kind ? 1 : near_occ_); ++k) {
+            for (int kind : {0, 1, 2})
+                for (int k : kind == 2 ? std::vector<int>{near_direct_occ_ / 2, near_direct_occ_}
+                                       : kind == 1 ? std::vector<int>{1} : [&] {
+                                             std::vector<int> v;
+                                             for (int q = 1; q <= near_occ_; ++q) v.push_back(q);
+                                             return v;
+                                         }()) {
+                    if (k < 1) continue;
                     near_kernel_ = kind;
                     set_near_grid(k);
                     const float t = timed(product);

@@ -445,6 +445,106 @@ k_near_warp(const DevNearTile* __restrict__ tiles, int ntiles, const double2* __
     }
 }
 
+// The same tiles and partial slots read straight from global memory into
+// registers: no shared-memory stage and no producer warp, so residency is set
+// by registers alone.  Warp w of the grid takes tiles w, w + (warps in the
+// grid), ...; per tile, lane l owns columns l and l + 32 (x values and column
+// sums in registers), rows go in batches of eight (each lane loads its one or
+// two entries of each of the eight rows: coalesced 16-byte loads, all sixteen
+// issued before use) and the row sums are formed by the reduce-scatter of
+// k_near_warp.  A self tile's diagonal counts once, in its row.
+constexpr int kNdThreads = 128;
+
+__device__ __forceinline__ long long tile_row_global(const DevNearTile& T, int r) {
+    if (T.mode == 0) return T.z + static_cast<long long>(r) * T.nj;
+    if (T.mode == 1) return T.z + packed_row(T.i0 + r, T.kind) - packed_row(T.i0, T.kind);
+    const int il = T.i0 + r;
+    return T.z + (T.kind == 0 ? static_cast<long long>(il) * T.ld : packed_row(il, T.kind)) + T.j0;
+}
+
+__global__ void __launch_bounds__(kNdThreads)
+k_near_direct(const DevNearTile* __restrict__ tiles, int ntiles, const double2* __restrict__ Z,
+              const double2* __restrict__ x, const int* __restrict__ slots, double2* __restrict__ part) {
+    const int lane = threadIdx.x & 31;
+    const int nwarps = gridDim.x * (kNdThreads / 32);
+    const int c0 = lane, c1 = lane + 32;
+    for (int t = blockIdx.x * (kNdThreads / 32) + (threadIdx.x >> 5); t < ntiles; t += nwarps) {
+        const DevNearTile T = tiles[t];
+        const double2* xr = x + T.r0 + T.i0;
+        const int* sl = slots + T.slot;
+        const double2 xc0 = c0 < T.nj ? x[T.c0 + T.j0 + c0] : z0();
+        const double2 xc1 = c1 < T.nj ? x[T.c0 + T.j0 + c1] : z0();
+        const int dcol = T.j0 - T.i0;  // row r, column c is below the diagonal iff r > c + dcol
+        double2 ca0 = z0(), ca1 = z0(), cb0 = z0(), cb1 = z0();
+        for (int rb = 0; rb < T.ni; rb += 8) {
+            double2 za[8], zb[8], xv[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const int r = rb + j;
+                za[j] = z0();
+                zb[j] = z0();
+                xv[j] = z0();
+                if (r < T.ni) {
+                    const int len = tile_row_len(T, r);
+                    const double2* zr = Z + tile_row_global(T, r);
+                    if (c0 < len) za[j] = __ldcs(zr + c0);
+                    if (c1 < len) zb[j] = __ldcs(zr + c1);
+                    xv[j] = xr[r];
+                }
+            }
+            double2 p[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const int r = rb + j;
+                p[j] = cfma(za[j], xc0, cmul(zb[j], xc1));
+                const bool ia = T.kind == 0 || r > c0 + dcol, ib = T.kind == 0 || r > c1 + dcol;
+                if (j & 1) {
+                    if (ia) cb0 = cfma(za[j], xv[j], cb0);
+                    if (ib) cb1 = cfma(zb[j], xv[j], cb1);
+                } else {
+                    if (ia) ca0 = cfma(za[j], xv[j], ca0);
+                    if (ib) ca1 = cfma(zb[j], xv[j], ca1);
+                }
+            }
+            // reduce-scatter of p[0..7] over the warp (as in k_near_warp)
+            const bool h4 = lane & 16, h3 = lane & 8, h2 = lane & 4;
+            double2 q[4], u[2], w;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const double2 send = h4 ? p[k] : p[k + 4];
+                const double2 keep = h4 ? p[k + 4] : p[k];
+                q[k] = cadd(keep, shfl_xor2(send, 16));
+            }
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                const double2 send = h3 ? q[k] : q[k + 2];
+                const double2 keep = h3 ? q[k + 2] : q[k];
+                u[k] = cadd(keep, shfl_xor2(send, 8));
+            }
+            {
+                const double2 send = h2 ? u[0] : u[1];
+                const double2 keep = h2 ? u[1] : u[0];
+                w = cadd(keep, shfl_xor2(send, 4));
+            }
+            w = cadd(w, shfl_xor2(w, 1));
+            w = cadd(w, shfl_xor2(w, 2));
+            const int r = rb + ((lane >> 2) & 7);
+            if ((lane & 3) == 0 && r < T.ni) {
+                const int slot = sl[r];
+                if (slot >= 0) part[slot] = w;
+            }
+        }
+        if (c0 < T.nj) {
+            const int slot = sl[T.ni + c0];
+            if (slot >= 0) part[slot] = cadd(ca0, cb0);
+        }
+        if (c1 < T.nj) {
+            const int slot = sl[T.ni + c1];
+            if (slot >= 0) part[slot] = cadd(ca1, cb1);
+        }
+    }
+}
+
 // y[t] = sum of target t's consecutive partial slots: eight lanes per target,
 // a fixed shuffle tree, so the order never changes.
 constexpr int kReduceLanes = 8;

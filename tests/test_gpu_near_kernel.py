@@ -1,6 +1,7 @@
-"""The two near-field kernels of the one-vector product (mlfma_set_near_kernel):
-one tile per thread block (row and column threads) and one tile per warp (a
-warp reduce-scatter for the row sums).  Same tiles, partial slots and per-target
+"""The near-field kernels of the one-vector product (mlfma_set_near_kernel):
+one tile per thread block (row and column threads), one tile per warp from a
+shared-memory ring, and one tile per warp read straight from global memory
+(both with a warp reduce-scatter for the row sums).  Same tiles, partial slots and per-target
 sums; products agree to FP64 rounding on RWG self tiles with their diagonal
 (self terms), dipole self tiles without it, leaves larger than a tile (row
 tiles), wide leaf-node blocks (list 3/4 partners) and products through the
@@ -44,9 +45,10 @@ def test_near_kernels_agree(cuda_device, case):
     x = cvec(op.n, 7)
     op.set_near_kernel(0)
     y0, a0 = op.matvec(x), op.matvec_adjoint(x)
-    op.set_near_kernel(1)
-    y1, a1 = op.matvec(x), op.matvec_adjoint(x)
-    assert rel(y1, y0) <= 1e-13
-    assert rel(a1, a0) <= 1e-13
-    assert np.array_equal(op.matvec(x), y1)  # deterministic: fixed summation order
+    for kind in (1, 2):
+        op.set_near_kernel(kind)
+        y1, a1 = op.matvec(x), op.matvec_adjoint(x)
+        assert rel(y1, y0) <= 1e-13, kind
+        assert rel(a1, a0) <= 1e-13, kind
+        assert np.array_equal(op.matvec(x), y1)  # deterministic: fixed summation order
     op.close()
