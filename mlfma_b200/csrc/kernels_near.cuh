@@ -88,7 +88,7 @@ __device__ __forceinline__ void consumers_sync() {
     asm volatile("bar.sync 1, %0;" ::"n"(kSymConsumers) : "memory");
 }
 
-__global__ void __launch_bounds__(kSymThreads, 6)
+__global__ void __launch_bounds__(kSymThreads, 5)
 k_near_sym(const DevNearTile* __restrict__ tiles, int ntiles, const double2* __restrict__ Z,
            const double2* __restrict__ x, const int* __restrict__ slots, double2* __restrict__ part,
            int* __restrict__ err) {

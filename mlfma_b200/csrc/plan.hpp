@@ -122,7 +122,7 @@ struct NearRow {
 //           rows nj apart in the tile.
 constexpr int kNearTileRows = 64;
 constexpr int kNearTileCols = 64;
-constexpr int kNearTileEntries = 896;
+constexpr int kNearTileEntries = 1024;
 constexpr int kNearTileRowsSplit = kNearTileEntries / kNearTileCols;  // rows of a mode-2 tile
 
 struct NearTile {
