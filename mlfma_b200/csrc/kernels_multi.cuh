@@ -131,7 +131,7 @@ __device__ __forceinline__ void cgemm_tile(int M, int N, int K, int m0, int n0, 
 // A_B[e][r] = sum_s R_s[e] x_s[r]  (Leaf::buildMpoleCoeffs, src/fmm/leaf.cpp:212-230,
 // for nr vectors).  Work item: (leaf, first row e0 of a BM-row tile).
 template <class R>
-__global__ void __launch_bounds__(kGemmThreads, 4)
+__global__ void __launch_bounds__(kGemmThreads)
 k_s2m_m(const DevLevelT<R>* __restrict__ lvs, const int2* __restrict__ items, const DevFarLeaf* __restrict__ leaves,
         const typename Cx<R>::T* __restrict__ pat, const double2* __restrict__ x, int nr) {
     using C = typename Cx<R>::T;
@@ -151,7 +151,7 @@ k_s2m_m(const DevLevelT<R>* __restrict__ lvs, const int2* __restrict__ items, co
 // y_s[r] = sum_e conj(R_s[e]) b_B[e][r]  (Leaf::evalFarSols, src/fmm/leaf.cpp:257-280).
 // Work item: (leaf, first source s0 of a BM-source tile).
 template <class R>
-__global__ void __launch_bounds__(kGemmThreads, 4)
+__global__ void __launch_bounds__(kGemmThreads)
 k_l2t_m(const DevLevelT<R>* __restrict__ lvs, const int2* __restrict__ items, const DevFarLeaf* __restrict__ leaves,
         const typename Cx<R>::T* __restrict__ pat, double2* __restrict__ yfar, int nr) {
     using C = typename Cx<R>::T;
@@ -169,7 +169,7 @@ k_l2t_m(const DevLevelT<R>* __restrict__ lvs, const int2* __restrict__ items, co
 // ------------------------------------------------------------ near field (many)
 // y_i[r] = sum_j Z_ij x_cols(j)[r] per block row (gather form, both
 // orientations stored).  Work item: (row block, first row of a BM-row tile).
-__global__ void __launch_bounds__(kGemmThreads, 4)
+__global__ void __launch_bounds__(kGemmThreads)
 k_near_m(const DevNearRow* __restrict__ rows, const int2* __restrict__ items, const double2* __restrict__ Z,
          const int* __restrict__ cols, const double2* __restrict__ x, double2* __restrict__ y, int nr) {
     __shared__ double2 As[kBK][kBM + 1];
