@@ -628,6 +628,22 @@ std::string DeviceOp::setup(const Plan& plan, int device, int precision, int max
         }
         n_leaves_ = static_cast<int>(h_leaves.size());
         leaves_ = upload(h_leaves);
+        // Largest work items first: a leaf's S2M block streams all its sources'
+        // patterns (1 to max_node_srcs of them), so launching the long blocks
+        // first keeps the last wave short.  Items write disjoint outputs; the
+        // order changes no result.
+        auto by_work = [&](std::vector<int4>& items, bool per_source) {
+            auto work = [&](const int4& it) {
+                const DevFarLeaf& f = h_leaves[it.x];
+                const long long nd = plan.levels[f.level].ndir;
+                return per_source ? static_cast<long long>(it.z) * nd : static_cast<long long>(f.nsrc) * it.z;
+            };
+            std::stable_sort(items.begin(), items.end(),
+                             [&](const int4& a, const int4& b) { return work(a) > work(b); });
+        };
+        by_work(s2m_items, false);
+        by_work(s2m_items_h, false);
+        by_work(l2t_items, true);
 
         n_s2m_items_ = static_cast<int>(s2m_items.size());
         s2m_items_ = upload(s2m_items);
