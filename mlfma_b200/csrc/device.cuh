@@ -365,6 +365,7 @@ private:
     int n_m2l_items_ = 0;
     int m2l_first_[kMaxLevels] = {}, m2l_count_[kMaxLevels] = {};  // items of each level
     std::vector<char> m2l_has_list_[kMaxLevels];  // box has a non-empty list 2
+    std::vector<int> m2l_len_[kMaxLevels];         // per level and box: list-2 length
     // Launch shapes (defaults at setup; mlfma_autotune may change them).
     int m2l_chunk_ = 128;                 // one-vector M2L directions per block
     int m2l_staged_ = 1;                  // one-vector M2L with its lists staged in shared memory

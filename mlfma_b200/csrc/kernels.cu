@@ -193,7 +193,13 @@ void DeviceOp::build_m2l_items(int max_chunk) {
         const int nchunk = (ndir_[l] + max_chunk - 1) / max_chunk;
         const int chunk = (ndir_[l] + nchunk - 1) / nchunk;
         m2l_first_[l] = static_cast<int>(items.size());
-        for (int b = 0; b < nbox_[l]; ++b) {
+        // boxes with the longest lists first (the last wave short); each box's
+        // direction chunks write their own outputs, so the order changes no result
+        std::vector<int> order(nbox_[l]);
+        for (int b = 0; b < nbox_[l]; ++b) order[b] = b;
+        std::stable_sort(order.begin(), order.end(),
+                         [&](int a, int b) { return m2l_len_[l][a] > m2l_len_[l][b]; });
+        for (int b : order) {
             if (ref_compat_ && !m2l_has_list_[l][b]) continue;
             for (int d0 = 0; d0 < ndir_[l]; d0 += chunk) items.push_back(make_int4(l, b, d0, std::min(chunk, ndir_[l] - d0)));
         }
@@ -552,7 +558,11 @@ std::string DeviceOp::setup(const Plan& plan, int device, int precision, int max
             // (repeats hit L2) and writes every local pattern once.
             traffic_.m2l += cnt * cbytes * 2.0 + 316.0 * L.ndir * cbytes;
             m2l_has_list_[l].resize(nbox_[l]);
-            for (int b = 0; b < nbox_[l]; ++b) m2l_has_list_[l][b] = L.m2l_ptr[b + 1] > L.m2l_ptr[b];
+            m2l_len_[l].resize(nbox_[l]);
+            for (int b = 0; b < nbox_[l]; ++b) {
+                m2l_has_list_[l][b] = L.m2l_ptr[b + 1] > L.m2l_ptr[b];
+                m2l_len_[l][b] = L.m2l_ptr[b + 1] - L.m2l_ptr[b];
+            }
         }
         m2l_items_ = alloc<int4>(m2l_item_capacity(8));
         build_m2l_items(128);
