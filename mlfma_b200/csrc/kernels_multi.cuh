@@ -317,6 +317,10 @@ k_m2m_m(const DevLevelT<R>* __restrict__ lvs, DevTransT<R> T, int nr, int rows_f
     for (int u = 0; u < OUT; ++u)
 #pragma unroll
         for (int j = 0; j < RPL; ++j) acc[u][j] = zero<C>();
+    if (nch == 0)  // (a listed parent has a child; kept well defined regardless)
+        for (int iph = warp; iph < mph; iph += kInterpWarps)
+#pragma unroll
+            for (int j = 0; j < RPL; ++j) sm[(iph * 32 + lane) * RPL + j] = zero<C>();
     for (int c = 0; c < nch; ++c) {
         const C* Ac = Cl.Am + static_cast<size_t>(T.child_box[c0 + c]) * Cl.ndir * 2 * nr + col;
         // weights of this row with the child's octant shift folded in: [iph][k]
@@ -334,23 +338,27 @@ k_m2m_m(const DevLevelT<R>* __restrict__ lvs, DevTransT<R> T, int nr, int rows_f
                 for (int j = 0; j < RPL; ++j)
                     if (live[j]) v[j] = cfma(f, a[16 * j], v[j]);
             }
+            // the phi pass is the same linear map for every child: sum the
+            // children's theta passes first (each entry is this thread's own)
 #pragma unroll
-            for (int j = 0; j < RPL; ++j) sm[(iph * 32 + lane) * RPL + j] = v[j];
-        }
-        __syncthreads();
-#pragma unroll
-        for (int u = 0; u < OUT; ++u) {
-            const int jph = warp + u * kInterpWarps;
-            if (jph >= nph) break;
-#pragma unroll
-            for (int k = 0; k < W; ++k) {
-                const R cf = ph_cf[jph * W + k];
-                const C* v = sm + (ph_src[jph * W + k] * 32 + lane) * RPL;
-#pragma unroll
-                for (int j = 0; j < RPL; ++j) acc[u][j] = crfma(cf, v[j], acc[u][j]);
+            for (int j = 0; j < RPL; ++j) {
+                C& o = sm[(iph * 32 + lane) * RPL + j];
+                o = c == 0 ? v[j] : cadd(o, v[j]);
             }
         }
-        __syncthreads();
+    }
+    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < OUT; ++u) {
+        const int jph = warp + u * kInterpWarps;
+        if (jph >= nph) break;
+#pragma unroll
+        for (int k = 0; k < W; ++k) {
+            const R cf = ph_cf[jph * W + k];
+            const C* v = sm + (ph_src[jph * W + k] * 32 + lane) * RPL;
+#pragma unroll
+            for (int j = 0; j < RPL; ++j) acc[u][j] = crfma(cf, v[j], acc[u][j]);
+        }
     }
     C* Ap = P.Am + (static_cast<size_t>(T.par_box[par]) * P.ndir + static_cast<size_t>(jth) * nph) * 2 * nr + col;
 #pragma unroll
