@@ -152,6 +152,8 @@ struct StepStateD {
     int k;
     unsigned cnt;
     double hn;
+    double w0;  // ||w||^2 before this step's orthogonalisation
+    int skip;   // 1: the first CGS pass kept enough of w, the second is skipped
 };
 
 // q_k = w (1 / hn) for k > 0 (q_0 is set by the cycle), and the product's input
@@ -184,9 +186,11 @@ constexpr int kStepCols = 8;
 __global__ void __launch_bounds__(kDotThreads)
 k_step_dots(StepStateD* __restrict__ st, const double2* __restrict__ Q, int n, const double2* __restrict__ w,
             double2* __restrict__ partial, int nchunks, double2* __restrict__ t, double2* __restrict__ hcols, int ldh,
-            int pass) {
+            int pass, double* __restrict__ wnorm) {
     __shared__ double2 red[kStepCols][kDotThreads];
+    __shared__ double wred[kDotThreads / 32];
     __shared__ bool last;
+    if (pass == 1 && st->skip) return;  // the whole grid: the second pass is not needed
     const int c = blockIdx.x, j0 = blockIdx.y * kStepCols;
     const int k = st->k;
     constexpr int per = kStepChunk / kDotThreads;  // elements per thread
@@ -197,6 +201,20 @@ k_step_dots(StepStateD* __restrict__ st, const double2* __restrict__ Q, int n, c
         for (int e = 0; e < per; ++e) {
             const int i = i0 + e * kDotThreads + threadIdx.x;
             wv[e] = i < n ? w[i] : make_double2(0.0, 0.0);
+        }
+        if (pass == 0 && blockIdx.y == 0) {  // ||chunk of w||^2, for the reorthogonalisation test
+            double nn = 0.0;
+#pragma unroll
+            for (int e = 0; e < per; ++e) nn = fma(wv[e].x, wv[e].x, fma(wv[e].y, wv[e].y, nn));
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) nn += __shfl_xor_sync(0xffffffffu, nn, o);
+            if ((threadIdx.x & 31) == 0) wred[threadIdx.x >> 5] = nn;
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                double a = 0.0;
+                for (int q = 0; q < kDotThreads / 32; ++q) a += wred[q];
+                wnorm[c] = a;
+            }
         }
 #pragma unroll
         for (int jj = 0; jj < kStepCols; ++jj) {
@@ -251,7 +269,14 @@ k_step_dots(StepStateD* __restrict__ st, const double2* __restrict__ Q, int n, c
         t[jj] = sum;
         h[jj] = pass ? make_double2(h[jj].x + sum.x, h[jj].y + sum.y) : sum;
     }
-    if (threadIdx.x == 0) st->cnt = 0;
+    if (threadIdx.x == 0) {
+        if (pass == 0) {
+            double a = 0.0;
+            for (int cc = 0; cc < nchunks; ++cc) a += __ldcg(wnorm + cc);
+            st->w0 = a;
+        }
+        st->cnt = 0;
+    }
 }
 
 // One CGS pass, update: w -= sum_{j <= k} Q_j t[j].  The second pass also
@@ -259,9 +284,10 @@ k_step_dots(StepStateD* __restrict__ st, const double2* __restrict__ Q, int n, c
 // h[k+1] = (||w||^2, 0), hn = ||w||, and the step index moves on.
 __global__ void k_step_update(StepStateD* __restrict__ st, const double2* __restrict__ Q, int n,
                               const double2* __restrict__ t, double2* __restrict__ w, double* __restrict__ npart,
-                              double2* __restrict__ hcols, int ldh, int norm) {
+                              double2* __restrict__ hcols, int ldh, int pass) {
     __shared__ double red[kUpdThreads];
     __shared__ bool last;
+    if (pass == 1 && st->skip) return;  // the whole grid
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int k = st->k;
     double nn = 0.0;
@@ -295,7 +321,6 @@ __global__ void k_step_update(StepStateD* __restrict__ st, const double2* __rest
         w[i] = v;
         nn = fma(v.x, v.x, v.y * v.y);
     }
-    if (!norm) return;
     red[threadIdx.x] = nn;
     __syncthreads();
     for (int s2 = blockDim.x / 2; s2 > 0; s2 >>= 1) {
@@ -311,10 +336,16 @@ __global__ void k_step_update(StepStateD* __restrict__ st, const double2* __rest
     __threadfence();
     double acc = 0.0;
     for (int b = 0; b < static_cast<int>(gridDim.x); ++b) acc += __ldcg(npart + b);
+    st->cnt = 0;
+    // Twice is enough: a second pass only when the first one cancelled more
+    // than half of ||w||^2 (||w_1|| <= ||w_0|| / sqrt 2).
+    if (pass == 0) {
+        st->skip = acc > 0.5 * st->w0 ? 1 : 0;
+        if (!st->skip) return;
+    }
     hcols[static_cast<long long>(k) * ldh + k + 1] = make_double2(acc, 0.0);
     st->hn = sqrt(acc);
     st->k = k + 1;
-    st->cnt = 0;
 }
 
 }  // namespace
@@ -357,6 +388,7 @@ std::string Gmres::ensure(int n, int ncols, int extra) {
         GM_CK(cudaMalloc(&npart2_, sizeof(double) * nblk(n, kUpdThreads)));
         nstep_ = (n + kStepChunk - 1) / kStepChunk;
         GM_CK(cudaMalloc(&spartial_, sizeof(double2) * static_cast<size_t>(nstep_) * (ncols + 1)));
+        GM_CK(cudaMalloc(&swnorm_, sizeof(double) * nstep_));
     }
     return {};
 }
@@ -367,8 +399,9 @@ void Gmres::release_steps() {
     sgx_ = nullptr;
     sg_ = nullptr;
     sg_op_ = nullptr;
-    for (void* p : {st_, (void*)hcols_, (void*)tco_, (void*)npart2_, (void*)spartial_})
+    for (void* p : {st_, (void*)hcols_, (void*)tco_, (void*)npart2_, (void*)spartial_, (void*)swnorm_})
         if (p) cudaFree(p);
+    swnorm_ = nullptr;
     st_ = nullptr;
     hcols_ = nullptr;
     tco_ = nullptr;
@@ -403,7 +436,7 @@ std::string Gmres::step_graph(DeviceOp& op, int prec) {
     for (int pass = 0; pass < 2; ++pass) {
         k_step_dots<<<dim3(nstep_, (cap_ + kStepCols - 1) / kStepCols), kDotThreads, 0, s>>>(st, Q_, n, w_, spartial_,
                                                                                           nstep_, tco_, hcols_, ldh,
-                                                                  pass);
+                                                                                          pass, swnorm_);
         k_step_update<<<nblk(n, kUpdThreads), kUpdThreads, 0, s>>>(st, Q_, n, tco_, w_, npart2_, hcols_, ldh, pass);
     }
     const cudaError_t ce = cudaStreamEndCapture(s, &sg_);

@@ -83,6 +83,7 @@ private:
     double* npart2_ = nullptr;   // norm partials, one per update block
     double2* spartial_ = nullptr;  // dot partials of the device steps, [columns][nstep_]
     int nstep_ = 0;                // their chunks of the vector
+    double* swnorm_ = nullptr;     // ||w||^2 partials of the device steps, [nstep_]
     cudaGraph_t sg_ = nullptr;
     cudaGraphExec_t sgx_ = nullptr;
     const DeviceOp* sg_op_ = nullptr;
