@@ -280,7 +280,12 @@ int mlfma_matvec_multi_device(mlfma_handle h, int nrhs, const void* d_x, void* d
  * src/solver.cpp:116-146, for many b): each system has its own Krylov basis
  * and Givens rotations (unitary; ref_givens is ignored) and stops on its own
  * tolerance.  b and x: nrhs x n complex host buffers, caller order; info:
- * nrhs records (may be NULL).  refine as in mlfma_gmres. */
+ * nrhs records (may be NULL).  refine as in mlfma_gmres.  flexible = 1:
+ * FGMRES(restart) per right-hand side with FP64 outer spaces, each outer
+ * step's inner solves (inner_iters iterations on the operator's own far
+ * field) run for all right-hand sides together; iterations counts a system's
+ * inner iterations, refinements its outer steps.  precond and an inner
+ * operator serve mlfma_gmres only. */
 int mlfma_gmres_multi(mlfma_handle h, int nrhs, const double* b, double* x, const mlfma_solver_opts* opts,
                       mlfma_solve_info* info);
 /* Per-stage CUDA-event time of one product on nrhs right-hand sides. */
@@ -335,7 +340,9 @@ typedef struct {
     int interp_path;           /* interpolation/anterpolation kernels chosen (see mlfma_set_interp_path) */
     int schedule;              /* one-vector product: bit 0 translation lists staged in shared memory,
                                   bit 1 near field started after aggregation, bit 2 two side streams
-                                  for the finer levels' translations */
+                                  for the finer levels' translations, bit 3 the far-field chain's
+                                  kernels launched as programmatic dependent launches (each kernel's
+                                  blocks scheduled while its predecessor drains) */
     int m2m_staged;            /* one-vector interpolation, transition p+1 -> p: bit p = children summed
                                   first in shared memory, bit 16 + p = the same with column-stationary
                                   phi passes; neither = one interpolation per child */
@@ -392,6 +399,15 @@ int mlfma_set_staged_interp(mlfma_handle h, int mode);
  * loaded straight from global memory into registers (no shared-memory stage).
  * Same partial sums, other rounding order; mlfma_autotune tries all three. */
 int mlfma_set_near_kernel(mlfma_handle h, int kind);
+
+/* The one-vector product's schedule, as mlfma_tuning.schedule reports it (no
+ * counterpart in the reference, which runs the stages one after another on
+ * one thread): bit 0 translation lists staged in shared memory, bit 1 near
+ * field started after aggregation, bit 2 two side streams for the finer
+ * levels' translations, bit 3 the far-field chain's kernels launched as
+ * programmatic dependent launches.  Results are unchanged up to rounding
+ * order (bit 3 changes nothing).  MLFMA_ERR_ARG outside 0..15. */
+int mlfma_set_schedule(mlfma_handle h, int schedule);
 
 /* ---- Many independent operators of uneven size (no counterpart in the
  * reference, which holds one problem per process).  A batch refers to set-up

@@ -270,6 +270,10 @@ class MLFMA:
         (mlfma_set_staged_interp)."""
         check(lib().mlfma_set_staged_interp(self._h, int(mode)))
 
+    def set_schedule(self, schedule: int) -> None:
+        """One-vector product schedule bits, as autotune() reports them (mlfma_set_schedule)."""
+        check(lib().mlfma_set_schedule(self._h, int(schedule)))
+
     def set_near_kernel(self, kind: int) -> None:
         """0: one near-field tile per thread block; 1: one per warp (mlfma_set_near_kernel)."""
         check(lib().mlfma_set_near_kernel(self._h, int(kind)))
@@ -308,13 +312,15 @@ class MLFMA:
                                               int(accumulate), ctypes.c_void_p(stream)))
 
     def solve_multi(self, B, max_iter: int = 500, tol: float = 1e-6, restart: int = 0, refine: bool = False,
-                    inner_tol: float = 0.0, raise_on_fail: bool = False):
-        """GMRES on the rows of B (nrhs x n) at once; returns (X, [SolveResult])."""
+                    inner_tol: float = 0.0, raise_on_fail: bool = False, flexible: bool = False,
+                    inner_iters: int = 0):
+        """GMRES on the rows of B (nrhs x n) at once; returns (X, [SolveResult]).
+        flexible: FGMRES(restart) per row, inner solves of inner_iters iterations run together."""
         bv = self._cmat(B)
         nr = bv.shape[0]
         x = np.zeros_like(bv)
         o = SolverOpts(max_iter=max_iter, tol=tol, restart=restart, ref_givens=0, refine=int(refine),
-                       inner_tol=inner_tol)
+                       inner_tol=inner_tol, flexible=int(flexible), inner_iters=inner_iters)
         infos = (SolveInfo * nr)()
         code = lib().mlfma_gmres_multi(self._h, nr, bv.view(np.float64).ctypes.data_as(_dp),
                                        x.view(np.float64).ctypes.data_as(_dp), ctypes.byref(o), infos)

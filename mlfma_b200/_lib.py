@@ -140,6 +140,7 @@ SIGNATURES = {
     "mlfma_level_transl_gpu": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _dp]),
     "mlfma_set_staged_interp": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "mlfma_set_near_kernel": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "mlfma_set_schedule": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "mlfma_set_inner_operator": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "mlfma_far_leaves": (ctypes.c_int, [ctypes.c_void_p, _ip, _ip, _ip]),
     "mlfma_tree_export": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _ip, ctypes.c_longlong,

@@ -497,8 +497,8 @@ int mlfma_gmres_multi(mlfma_handle h, int nrhs, const double* b, double* x, cons
         o.inner_iters = opts->inner_iters;
         o.precond = opts->precond;
     }
-    if (o.flexible || o.precond)
-        return fail(MLFMA_ERR_ARG, "flexible and preconditioned GMRES run one right-hand side at a time (mlfma_gmres)");
+    if (o.precond)
+        return fail(MLFMA_ERR_ARG, "preconditioned GMRES runs one right-hand side at a time (mlfma_gmres)");
     if (cudaSetDevice(h->device) != cudaSuccess) return fail(MLFMA_ERR_CUDA, "cudaSetDevice failed");
     int code = ensure_multi_staging(h);
     if (code != MLFMA_OK) return code;
@@ -756,6 +756,12 @@ int mlfma_set_near_kernel(mlfma_handle h, int kind) {
     if (!h) return fail(MLFMA_ERR_ARG, "null handle");
     if (!ready(h)) return fail(MLFMA_ERR_STATE, "mlfma_setup has not run");
     return from_msg(h->dev->set_near_kernel(kind));
+}
+
+int mlfma_set_schedule(mlfma_handle h, int schedule) {
+    if (!h) return fail(MLFMA_ERR_ARG, "null handle");
+    if (!ready(h)) return fail(MLFMA_ERR_STATE, "mlfma_setup has not run");
+    return from_msg(h->dev->set_schedule(schedule));
 }
 
 int mlfma_set_staged_interp(mlfma_handle h, int mode) {

@@ -160,7 +160,8 @@ struct TuneReport {
     int near_blocks_per_sm;        // one-vector near field: persistent blocks per SM
     int interp_path;               // tensor-core interpolation: bit 0 one vector, bit 1 many
     int schedule;                  // one-vector product: bit 0 staged M2L lists, bit 1 near field after
-                                   // S2M, bit 2 two side streams for the finer levels' M2L
+                                   // S2M, bit 2 two side streams for the finer levels' M2L, bit 3
+                                   // chain kernels as programmatic dependent launches
     int m2m_staged, l2l_staged;    // one-vector: bit p = transition p -> p + 1 on the staged kernels
     int near_kernel;               // one-vector near field: 0 k_near_sym, 1 k_near_warp
 };
@@ -255,6 +256,7 @@ public:
     std::string time_stages(StageTimes* out);
     // bit 0: every transition's M2M on k_m2m_sum, bit 1: L2L on k_l2l_st (where they fit)
     std::string set_staged(int mode);
+    std::string set_schedule(int schedule);
     std::string set_near_kernel(int kind);  // 0 k_near_sym, 1 k_near_warp
     // per level l (index l): M2M into l, M2L at l, L2L out of l (ms; 0 where none)
     std::string time_levels(std::vector<float>& out);
@@ -318,11 +320,13 @@ private:
     template <class R, bool TR> void run_far_overlap_t(FarField<R>& F, const double2* xt, cudaStream_t s,
                                                        cudaStream_t s2, bool near_late);
     void run_far_overlap(const double2* xt, cudaStream_t s, cudaStream_t s2, int prec, bool tr, bool late);
+    // pdl: launched as a programmatic dependent launch (the predecessor on s
+    // is a kernel of the chain, and the only one this launch depends on)
     template <class R, bool TR> void far_s2m(FarField<R>& F, const double2* xt, cudaStream_t s);
-    template <class R, bool TR> void far_m2m(FarField<R>& F, int p, cudaStream_t s);
-    template <class R, bool TR> void far_m2l(FarField<R>& F, int lo, int hi, cudaStream_t s);
-    template <class R, bool TR> void far_l2l(FarField<R>& F, int p, cudaStream_t s);
-    template <class R, bool TR> void far_l2t(FarField<R>& F, cudaStream_t s);
+    template <class R, bool TR> void far_m2m(FarField<R>& F, int p, cudaStream_t s, bool pdl = false);
+    template <class R, bool TR> void far_m2l(FarField<R>& F, int lo, int hi, cudaStream_t s, bool pdl = false);
+    template <class R, bool TR> void far_l2l(FarField<R>& F, int p, cudaStream_t s, bool pdl = false);
+    template <class R, bool TR> void far_l2t(FarField<R>& F, cudaStream_t s, bool pdl = false);
     void run_far(const double2* xt, cudaStream_t s, int stage = -1, int prec = -1, bool tr = false);
     void run_near(const double2* xt, cudaStream_t s);
     void enqueue_core(cudaStream_t s, int prec, bool tr);   // xt_ -> yfar_, ynear_
@@ -371,6 +375,7 @@ private:
     int m2l_staged_ = 1;                  // one-vector M2L with its lists staged in shared memory
     bool near_late_ = false;              // near field after S2M (overlapping the latency-bound stages)
     int m2l_streams_ = 1;                 // side streams for the finer levels' translations
+    bool chain_pdl_ = false;              // far-field chain kernels as programmatic dependent launches
     std::vector<int> m2m_rows_;           // one-vector M2M parent rows per block, per transition
     std::vector<int> m2m_pref_, l2l_pref_;  // per transition: 1 = staged kernels (k_m2m_sum, k_l2l_st) where they fit
     int dev_smem_ = 0;                    // opt-in shared memory per block

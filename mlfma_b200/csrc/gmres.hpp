@@ -134,6 +134,12 @@ public:
                       std::vector<SolveResult>& res);
 
 private:
+    // opts.flexible: FGMRES(restart) per column, FP64 outer spaces, each outer
+    // step's inner solves run together (inner_iters GMRES iterations on the
+    // operator's own far field, complex float on a mixed operator).
+    std::string solve_flexible(DeviceOp& op, int nr, const double2* d_b_user, double2* d_x_user, const SolveOpts& o,
+                               std::vector<SolveResult>& res);
+    void cgs_pass_q(const double2* Q, double2* w, int ncols, cudaStream_t s, double2* h, bool add);
     std::string ensure(int n, int nr, int ncols);
     void release();
     std::string norms(const double2* v, cudaStream_t s, std::vector<double>& out);
@@ -146,6 +152,8 @@ private:
     double2 *Q_ = nullptr, *w_ = nullptr, *b_ = nullptr, *x_ = nullptr, *r_ = nullptr;
     double2 *h_ = nullptr, *y_ = nullptr, *partial_ = nullptr, *xo_ = nullptr, *bo_ = nullptr;
     double *npartial_ = nullptr, *scale_ = nullptr;
+    double2 *V_ = nullptr, *Z_ = nullptr;  // flexible: outer bases ([mo + 1] and [mo] vectors of [n][nr])
+    int vcap_ = 0;                         // their capacity (outer steps)
 };
 
 }  // namespace mlfma

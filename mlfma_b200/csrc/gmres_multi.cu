@@ -168,7 +168,10 @@ void GmresMulti::release() {
         if (p) cudaFree(p);
     Q_ = w_ = b_ = x_ = r_ = h_ = y_ = partial_ = xo_ = bo_ = nullptr;
     npartial_ = scale_ = nullptr;
-    n_ = nr_ = cap_ = 0;
+    for (void* p : {(void*)V_, (void*)Z_})
+        if (p) cudaFree(p);
+    V_ = Z_ = nullptr;
+    n_ = nr_ = cap_ = vcap_ = 0;
 }
 
 std::string GmresMulti::ensure(int n, int nr, int ncols) {
@@ -207,12 +210,14 @@ std::string GmresMulti::norms(const double2* v, cudaStream_t s, std::vector<doub
 }
 
 // One CGS pass over columns 0..ncols-1: h (+)= Q^H w ; w -= Q h_pass.
-void GmresMulti::cgs_pass(int ncols, cudaStream_t s, bool add) {
+void GmresMulti::cgs_pass(int ncols, cudaStream_t s, bool add) { cgs_pass_q(Q_, w_, ncols, s, h_, add); }
+
+void GmresMulti::cgs_pass_q(const double2* Q, double2* w, int ncols, cudaStream_t s, double2* h, bool add) {
     const long long ld = static_cast<long long>(n_) * nr_;
-    k_mdot<<<dim3(nchunks_, ncols), kThreads, 0, s>>>(Q_, ld, w_, n_, nr_, partial_, nchunks_);
+    k_mdot<<<dim3(nchunks_, ncols), kThreads, 0, s>>>(Q, ld, w, n_, nr_, partial_, nchunks_);
     k_mreduce<<<nblk(static_cast<long long>(ncols) * nr_, 128), 128, 0, s>>>(partial_, nchunks_, ncols, nr_, y_, 0);
-    k_msub_qh<<<nblk(ld, 256), 256, 0, s>>>(Q_, ld, ncols, y_, w_, ld, nr_);
-    k_mreduce<<<nblk(static_cast<long long>(ncols) * nr_, 128), 128, 0, s>>>(partial_, nchunks_, ncols, nr_, h_,
+    k_msub_qh<<<nblk(ld, 256), 256, 0, s>>>(Q, ld, ncols, y_, w, ld, nr_);
+    k_mreduce<<<nblk(static_cast<long long>(ncols) * nr_, 128), 128, 0, s>>>(partial_, nchunks_, ncols, nr_, h,
                                                                              add ? 1 : 0);
 }
 
@@ -353,6 +358,7 @@ std::string GmresMulti::solve(DeviceOp& op, int nr, const double2* d_b_user, dou
     if (nr < 1 || nr > op.max_rhs()) return "arg:nrhs must be between 1 and the operator's max_rhs";
     const int m = o.restart > 0 ? o.restart : o.max_iter;
     if (m < 1 || o.max_iter < 1) return "arg:max_iter and restart must be positive";
+    if (o.flexible) return solve_flexible(op, nr, d_b_user, d_x_user, o, res);
     std::string err = ensure(n, nr, m + 1);
     if (!err.empty()) return err;
     cudaStream_t s = op.stream();
@@ -426,6 +432,184 @@ std::string GmresMulti::solve(DeviceOp& op, int nr, const double2* d_b_user, dou
         res[r].true_residual = bnorm[r] > 0 ? rn[r] / bnorm[r] : 0.0;
         res[r].residual = refine ? res[r].true_residual : est[r];
         res[r].converged = bnorm[r] == 0.0 || rn[r] <= tol_abs[r] * (1.0 + 1e-12) || (!refine && done[r]);
+        res[r].seconds = secs;
+    }
+    return {};
+}
+
+// Flexible GMRES on many right-hand sides (Gmres::solve_flexible, one column
+// at a time there).  Each column r has its own FP64 outer space: basis V_r,
+// preconditioned directions Z_r, Hessenberg matrix, unitary rotations and
+// residual.  Outer step k solves A z = v_k for every working column at once:
+// inner_iters GMRES iterations from zero on the operator's own far field
+// (complex float on a mixed operator), through the batched cycles above, so
+// the columns share every inner product launch; then w = A z_k in FP64 (the
+// batched FP64 product), CGS2 against the column's V, and the columns' Givens
+// rotations on the host.  x_r = Z_r y_r exactly after each cycle, and the
+// stopping test is the FP64 residual.  A column that meets its tolerance is
+// frozen (zero directions) while the others go on; iterations counts a
+// column's inner iterations and refinements its outer steps.
+std::string GmresMulti::solve_flexible(DeviceOp& op, int nr, const double2* d_b_user, double2* d_x_user,
+                                       const SolveOpts& o, std::vector<SolveResult>& res) {
+    using cd = std::complex<double>;
+    const auto t_start = std::chrono::steady_clock::now();
+    const int n = op.n();
+    const int mo = o.restart > 0 ? o.restart : o.max_iter;
+    const int mi = o.inner_iters > 0 ? o.inner_iters : 20;
+    if (mo < 1 || o.max_iter < 1) return "arg:max_iter and restart must be positive";
+    if (o.inner && o.inner != &op) return "arg:an inner operator serves the one-right-hand-side flexible solve";
+    std::string err = ensure(n, nr, std::max(mi, mo) + 1);
+    if (!err.empty()) return err;
+    const long long ld = static_cast<long long>(n) * nr;
+    if (vcap_ < mo) {
+        for (void* p : {(void*)V_, (void*)Z_})
+            if (p) cudaFree(p);
+        V_ = Z_ = nullptr;
+        vcap_ = 0;
+        GMM_CK(cudaMalloc(&V_, sizeof(double2) * ld * (mo + 1)));
+        GMM_CK(cudaMalloc(&Z_, sizeof(double2) * ld * mo));
+        vcap_ = mo;
+    }
+    cudaStream_t s = op.stream();
+    const int prec_in = op.precision();
+    res.assign(nr, SolveResult{});
+    k_mgather<<<nblk(ld, 256), 256, 0, s>>>(d_b_user, op.perm(), bo_, n, nr);
+    std::vector<double> bnorm;
+    err = norms(bo_, s, bnorm);
+    if (!err.empty()) return err;
+    std::vector<double> tol_abs(nr), beta = bnorm, sc(nr);
+    std::vector<char> conv(nr, 0), active(nr, 0);
+    std::vector<int> iters(nr, 0), outer(nr, 0), kr(nr, 0);
+    for (int r = 0; r < nr; ++r) {
+        if (!std::isfinite(bnorm[r])) return "nonfinite:right-hand side";
+        tol_abs[r] = o.tol * bnorm[r];
+        conv[r] = bnorm[r] == 0.0;
+    }
+    GMM_CK(cudaMemsetAsync(xo_, 0, sizeof(double2) * ld, s));
+    GMM_CK(cudaMemcpyAsync(r_, bo_, sizeof(double2) * ld, cudaMemcpyDeviceToDevice, s));  // r = b (x = 0)
+    std::vector<std::vector<cd>> H(nr), cs(nr), sn(nr), g(nr);
+    std::vector<double2> hh(static_cast<size_t>(mo + 2) * nr);
+    for (;;) {
+        int nact = 0;
+        for (int r = 0; r < nr; ++r) {
+            active[r] = !conv[r] && beta[r] > 0.0 && iters[r] < o.max_iter;
+            sc[r] = active[r] ? 1.0 / beta[r] : 0.0;
+            kr[r] = 0;
+            nact += active[r];
+            if (active[r]) {
+                H[r].assign(static_cast<size_t>(mo + 1) * mo, cd(0));
+                cs[r].assign(mo, cd(0));
+                sn[r].assign(mo, cd(0));
+                g[r].assign(mo + 1, cd(0));
+                g[r][0] = beta[r];
+            }
+        }
+        if (nact == 0) break;
+        GMM_CK(cudaMemcpyAsync(scale_, sc.data(), sizeof(double) * nr, cudaMemcpyHostToDevice, s));
+        k_mscale<<<nblk(ld, 256), 256, 0, s>>>(r_, scale_, V_, ld, nr);  // v_0 = r / beta, zero when frozen
+        for (int k = 0; k < mo && nact > 0; ++k) {
+            double2* vk = V_ + static_cast<long long>(k) * ld;
+            double2* zk = Z_ + static_cast<long long>(k) * ld;
+            // inner solves A z = v_k from zero (||v_k|| = 1 in every working column)
+            std::vector<char> idone(nr);
+            std::vector<double> ib(nr), itol(nr), iest(nr, 0.0);
+            std::vector<int> it(nr, 0);
+            int maxit = 0;
+            for (int r = 0; r < nr; ++r) {
+                idone[r] = !active[r];
+                ib[r] = active[r] ? 1.0 : 0.0;
+                itol[r] = active[r] && o.inner_tol > 0 ? o.inner_tol : 0.0;
+                if (active[r]) maxit = std::max(maxit, std::min(mi, o.max_iter - iters[r]));
+            }
+            GMM_CK(cudaMemcpyAsync(b_, vk, sizeof(double2) * ld, cudaMemcpyDeviceToDevice, s));
+            err = cycles(op, prec_in, mi, std::max(1, maxit), ib, itol, idone, it, iest);
+            if (!err.empty()) return err;
+            GMM_CK(cudaMemcpyAsync(zk, x_, sizeof(double2) * ld, cudaMemcpyDeviceToDevice, s));
+            // w = A z_k in FP64, orthogonalised against v_0..v_k of its column
+            op.apply_tree_multi(zk, w_, nr, s, kFp64);
+            cgs_pass_q(V_, w_, k + 1, s, h_, false);
+            cgs_pass_q(V_, w_, k + 1, s, h_, true);
+            k_mnorm2<<<nchunks_, kThreads, 0, s>>>(w_, n, nr, npartial_);
+            k_msum<<<1, kMaxRhs, 0, s>>>(npartial_, nchunks_, nr, h_ + static_cast<size_t>(k + 1) * nr);
+            GMM_CK(cudaMemcpyAsync(hh.data(), h_, sizeof(double2) * (k + 2) * nr, cudaMemcpyDeviceToHost, s));
+            GMM_CK(cudaStreamSynchronize(s));
+            for (int r = 0; r < nr; ++r) {
+                sc[r] = 0.0;
+                if (!active[r]) continue;
+                iters[r] += it[r];
+                ++outer[r];
+                const double hn = std::sqrt(hh[static_cast<size_t>(k + 1) * nr + r].x);
+                if (!std::isfinite(hn)) return "nonfinite:Arnoldi";
+                std::vector<cd> hc(k + 2);
+                for (int i = 0; i <= k; ++i)
+                    hc[i] = cd(hh[static_cast<size_t>(i) * nr + r].x, hh[static_cast<size_t>(i) * nr + r].y);
+                hc[k + 1] = hn;
+                for (int i = 0; i < k; ++i) {  // previous unitary rotations
+                    const cd a = hc[i], b = hc[i + 1];
+                    hc[i] = cs[r][i] * a + sn[r][i] * b;
+                    hc[i + 1] = -std::conj(sn[r][i]) * a + cs[r][i] * b;
+                }
+                const double az = std::abs(hc[k]);
+                const double t = std::sqrt(az * az + std::norm(hc[k + 1]));
+                cd c, sg;
+                if (az == 0.0) { c = 0.0; sg = 1.0; } else { c = az / t; sg = (hc[k] / az) * std::conj(hc[k + 1]) / t; }
+                hc[k] = c * hc[k] + sg * hc[k + 1];
+                g[r][k + 1] = -std::conj(sg) * g[r][k];
+                g[r][k] = c * g[r][k];
+                cs[r][k] = c;
+                sn[r][k] = sg;
+                for (int i = 0; i <= k; ++i) H[r][static_cast<size_t>(k) * (mo + 1) + i] = hc[i];
+                kr[r] = k + 1;
+                if (!(std::abs(g[r][k + 1]) > tol_abs[r]) || hn == 0.0 || iters[r] >= o.max_iter) {
+                    active[r] = 0;
+                    --nact;
+                } else {
+                    sc[r] = 1.0 / hn;
+                }
+            }
+            if (nact > 0 && k + 1 < mo) {
+                GMM_CK(cudaMemcpyAsync(scale_, sc.data(), sizeof(double) * nr, cudaMemcpyHostToDevice, s));
+                k_mscale<<<nblk(ld, 256), 256, 0, s>>>(w_, scale_, V_ + static_cast<long long>(k + 1) * ld, ld, nr);
+            }
+        }
+        // x += Z y per column, R y = g
+        int kmax = 0;
+        for (int r = 0; r < nr; ++r) kmax = std::max(kmax, kr[r]);
+        if (kmax > 0) {
+            std::vector<double2> yd(static_cast<size_t>(kmax) * nr, make_double2(0.0, 0.0));
+            for (int r = 0; r < nr; ++r) {
+                const int kk = kr[r];
+                std::vector<cd> yv(kk);
+                for (int i = kk - 1; i >= 0; --i) {
+                    cd acc = g[r][i];
+                    for (int j = i + 1; j < kk; ++j) acc -= H[r][static_cast<size_t>(j) * (mo + 1) + i] * yv[j];
+                    yv[i] = acc / H[r][static_cast<size_t>(i) * (mo + 1) + i];
+                }
+                for (int i = 0; i < kk; ++i) yd[static_cast<size_t>(i) * nr + r] = make_double2(-yv[i].real(), -yv[i].imag());
+            }
+            GMM_CK(cudaMemcpyAsync(y_, yd.data(), sizeof(double2) * yd.size(), cudaMemcpyHostToDevice, s));
+            k_msub_qh<<<nblk(ld, 256), 256, 0, s>>>(Z_, ld, kmax, y_, xo_, ld, nr);
+        }
+        // true FP64 residual
+        op.apply_tree_multi(xo_, w_, nr, s, kFp64);
+        k_msub<<<nblk(ld, 256), 256, 0, s>>>(bo_, w_, r_, ld);
+        err = norms(r_, s, beta);
+        if (!err.empty()) return err;
+        for (int r = 0; r < nr; ++r) {
+            if (!std::isfinite(beta[r])) return "nonfinite:residual";
+            if (beta[r] <= tol_abs[r]) conv[r] = 1;
+        }
+        if (o.restart <= 0) break;
+    }
+    k_mscatter<<<nblk(ld, 256), 256, 0, s>>>(xo_, op.perm(), d_x_user, n, nr);
+    GMM_CK(cudaStreamSynchronize(s));
+    const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
+    for (int r = 0; r < nr; ++r) {
+        res[r].iterations = iters[r];
+        res[r].refinements = outer[r];
+        res[r].true_residual = bnorm[r] > 0 ? beta[r] / bnorm[r] : 0.0;
+        res[r].residual = res[r].true_residual;
+        res[r].converged = bnorm[r] == 0.0 || beta[r] <= tol_abs[r] * (1.0 + 1e-12);
         res[r].seconds = secs;
     }
     return {};

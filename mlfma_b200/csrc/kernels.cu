@@ -48,6 +48,24 @@ namespace mlfma {
 
 namespace {
 
+// Launch kernel k on s; with pdl as a programmatic dependent launch (its blocks
+// may be scheduled while the predecessor on s drains; the far-field kernels
+// wait for it in chain_wait before touching its data).
+template <typename... P, typename... A>
+void launch_k(bool pdl, void (*k)(P...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, A... args) {
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cfg.attrs = at;
+    cfg.numAttrs = pdl ? 1 : 0;
+    cudaLaunchKernelEx(&cfg, k, static_cast<P>(args)...);
+}
+
 // xt[t] = x[perm[t]] (conjugated when cj)
 __global__ void k_gather(const double2* __restrict__ x, const int* __restrict__ perm,
                          double2* __restrict__ xt, int n, int cj) {
@@ -840,7 +858,7 @@ void DeviceOp::far_s2m(FarField<R>& F, const double2* xt, cudaStream_t s) {
 }
 
 template <class R, bool TR>
-void DeviceOp::far_m2m(FarField<R>& F, int p, cudaStream_t s) {
+void DeviceOp::far_m2m(FarField<R>& F, int p, cudaStream_t s, bool pdl) {
     using C = typename Cx<R>::T;
     if (npar_[p] == 0) return;
     const int rows = m2m_rows_[p];
@@ -849,9 +867,8 @@ void DeviceOp::far_m2m(FarField<R>& F, int p, cudaStream_t s) {
     const size_t ssum = m2m_sum_smem(nth_[p + 1], nph_[p + 1], rows, sizeof(C));
     if (!TR && m2m_pref_[p] && ssum + 1024 <= static_cast<size_t>(dev_smem_)) {
         const bool cs = m2m_pref_[p] == 2;
-#define MLFMA_M2M_SUM(WW)                                                                           \
-    (cs ? k_m2m_sum<R, WW, true><<<grid, 256, ssum, s>>>(F.lv_dev, T, rows)                          \
-        : k_m2m_sum<R, WW, false><<<grid, 256, ssum, s>>>(F.lv_dev, T, rows))
+#define MLFMA_M2M_SUM(WW) \
+    launch_k(pdl, cs ? k_m2m_sum<R, WW, true> : k_m2m_sum<R, WW, false>, grid, 256, ssum, s, F.lv_dev, T, rows)
         switch (up_w_[p]) {
             case 2: MLFMA_M2M_SUM(2); break;
             case 4: MLFMA_M2M_SUM(4); break;
@@ -864,29 +881,27 @@ void DeviceOp::far_m2m(FarField<R>& F, int p, cudaStream_t s) {
     }
     const size_t smem = static_cast<size_t>(8) * rows * nph_[p + 1] * 2 * sizeof(C);
     switch (up_w_[p]) {
-        case 2: k_m2m<R, 2, TR><<<grid, 128, smem, s>>>(F.lv_dev, T, rows); break;
-        case 4: k_m2m<R, 4, TR><<<grid, 128, smem, s>>>(F.lv_dev, T, rows); break;
-        case 6: k_m2m<R, 6, TR><<<grid, 128, smem, s>>>(F.lv_dev, T, rows); break;
-        case 8: k_m2m<R, 8, TR><<<grid, 128, smem, s>>>(F.lv_dev, T, rows); break;
-        default: k_m2m<R, 10, TR><<<grid, 128, smem, s>>>(F.lv_dev, T, rows); break;
+        case 2: launch_k(pdl, k_m2m<R, 2, TR>, grid, 128, smem, s, F.lv_dev, T, rows); break;
+        case 4: launch_k(pdl, k_m2m<R, 4, TR>, grid, 128, smem, s, F.lv_dev, T, rows); break;
+        case 6: launch_k(pdl, k_m2m<R, 6, TR>, grid, 128, smem, s, F.lv_dev, T, rows); break;
+        case 8: launch_k(pdl, k_m2m<R, 8, TR>, grid, 128, smem, s, F.lv_dev, T, rows); break;
+        default: launch_k(pdl, k_m2m<R, 10, TR>, grid, 128, smem, s, F.lv_dev, T, rows); break;
     }
 }
 
 // M2L of levels lo..hi (their items are contiguous, level by level).
 template <class R, bool TR>
-void DeviceOp::far_m2l(FarField<R>& F, int lo, int hi, cudaStream_t s) {
+void DeviceOp::far_m2l(FarField<R>& F, int lo, int hi, cudaStream_t s, bool pdl) {
     if (lo > hi) return;
     const int first = m2l_first_[lo];
     const int count = m2l_first_[hi] + m2l_count_[hi] - first;
     if (count <= 0) return;
-    if (m2l_staged_)
-        k_m2l_staged<R, TR><<<count, 128, 0, s>>>(F.lv_dev, m2l_items_ + first, ref_compat_ ? 0 : 1);
-    else
-        k_m2l<R, TR><<<count, 128, 0, s>>>(F.lv_dev, m2l_items_ + first, ref_compat_ ? 0 : 1);
+    launch_k(pdl, m2l_staged_ ? k_m2l_staged<R, TR> : k_m2l<R, TR>, count, 128, 0, s, F.lv_dev, m2l_items_ + first,
+             ref_compat_ ? 0 : 1);
 }
 
 template <class R, bool TR>
-void DeviceOp::far_l2l(FarField<R>& F, int p, cudaStream_t s) {
+void DeviceOp::far_l2l(FarField<R>& F, int p, cudaStream_t s, bool pdl) {
     using C = typename Cx<R>::T;
     const int g = n_l2l_pairs_[p];
     if (!g) return;
@@ -902,7 +917,7 @@ void DeviceOp::far_l2l(FarField<R>& F, int p, cudaStream_t s) {
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, 256, spipe) != cudaSuccess || occ < 1) \
             occ = 1;                                                                                       \
         const int grid = std::max(1, std::min(g, occ * sms_));                                             \
-        k_l2l_pipe<R, WW, TR><<<grid, 256, spipe, s>>>(F.lv_dev, T, l2l_pairs_[p], g);                    \
+        launch_k(pdl, k_l2l_pipe<R, WW, TR>, grid, 256, spipe, s, F.lv_dev, T, l2l_pairs_[p], g);          \
     } while (0)
         switch (dn_w_[p]) {
             case 8: MLFMA_L2L_PIPE(8); break;
@@ -916,9 +931,9 @@ void DeviceOp::far_l2l(FarField<R>& F, int p, cudaStream_t s) {
     }
     if (l2l_pref_[p] && l2l_pref_[p] != 3 && sst + 1024 <= static_cast<size_t>(dev_smem_)) {
         const bool cs = l2l_pref_[p] == 2;
-#define MLFMA_L2L_ST(WW)                                                                            \
-    (cs ? k_l2l_st<R, WW, TR, true><<<g, 256, sst, s>>>(F.lv_dev, T, l2l_pairs_[p])                  \
-        : k_l2l_st<R, WW, TR, false><<<g, 256, sst, s>>>(F.lv_dev, T, l2l_pairs_[p]))
+#define MLFMA_L2L_ST(WW)                                                                             \
+    launch_k(pdl, cs ? k_l2l_st<R, WW, TR, true> : k_l2l_st<R, WW, TR, false>, g, 256, sst, s, F.lv_dev, T, \
+             l2l_pairs_[p])
         switch (dn_w_[p]) {
             case 8: MLFMA_L2L_ST(8); break;
             case 12: MLFMA_L2L_ST(12); break;
@@ -931,22 +946,22 @@ void DeviceOp::far_l2l(FarField<R>& F, int p, cudaStream_t s) {
     }
     const size_t smem = static_cast<size_t>(nth_[p]) * nph_[p + 1] * 2 * sizeof(C);
     switch (dn_w_[p]) {
-        case 8: k_l2l<R, 8, TR><<<g, 256, smem, s>>>(F.lv_dev, T, l2l_pairs_[p]); break;
-        case 12: k_l2l<R, 12, TR><<<g, 256, smem, s>>>(F.lv_dev, T, l2l_pairs_[p]); break;
-        case 16: k_l2l<R, 16, TR><<<g, 256, smem, s>>>(F.lv_dev, T, l2l_pairs_[p]); break;
-        case 24: k_l2l<R, 24, TR><<<g, 256, smem, s>>>(F.lv_dev, T, l2l_pairs_[p]); break;
-        default: k_l2l<R, 32, TR><<<g, 256, smem, s>>>(F.lv_dev, T, l2l_pairs_[p]); break;
+        case 8: launch_k(pdl, k_l2l<R, 8, TR>, g, 256, smem, s, F.lv_dev, T, l2l_pairs_[p]); break;
+        case 12: launch_k(pdl, k_l2l<R, 12, TR>, g, 256, smem, s, F.lv_dev, T, l2l_pairs_[p]); break;
+        case 16: launch_k(pdl, k_l2l<R, 16, TR>, g, 256, smem, s, F.lv_dev, T, l2l_pairs_[p]); break;
+        case 24: launch_k(pdl, k_l2l<R, 24, TR>, g, 256, smem, s, F.lv_dev, T, l2l_pairs_[p]); break;
+        default: launch_k(pdl, k_l2l<R, 32, TR>, g, 256, smem, s, F.lv_dev, T, l2l_pairs_[p]); break;
     }
 }
 
 template <class R, bool TR>
-void DeviceOp::far_l2t(FarField<R>& F, cudaStream_t s) {
+void DeviceOp::far_l2t(FarField<R>& F, cudaStream_t s, bool pdl) {
     if (!n_l2t_items_) return;
     if constexpr (std::is_same<R, double>::value)
-        k_l2t<R, !TR><<<n_l2t_items_, kL2TThreads, 0, s>>>(F.lv_dev, l2t_items_, leaves_, F.pat, yfar_);
+        launch_k(pdl, k_l2t<R, !TR>, n_l2t_items_, kL2TThreads, 0, s, F.lv_dev, l2t_items_, leaves_, F.pat, yfar_);
     else
-        k_l2t_half<R, !TR><<<n_l2t_items_, kL2TThreads, 2 * sizeof(typename Cx<R>::T) * max_leaf_ndir_, s>>>(
-            F.lv_dev, l2t_items_, leaves_, F.hpat, yfar_);
+        launch_k(pdl, k_l2t_half<R, !TR>, n_l2t_items_, kL2TThreads, 2 * sizeof(typename Cx<R>::T) * max_leaf_ndir_, s,
+                 F.lv_dev, l2t_items_, leaves_, F.hpat, yfar_);
 }
 
 // stage: -1 all, 0 S2M, 1 M2M, 2 M2L, 3 L2L, 4 L2T, in sequence on s.
@@ -992,6 +1007,9 @@ void DeviceOp::run_far_overlap_t(FarField<R>& F, const double2* xt, cudaStream_t
     const bool tcf = std::is_same<R, float>::value && !TR;
     const bool tc_up = tcf && (tc_mode_ & 1), tc_dn = tcf && (tc_mode_ & 4);
     far_s2m<R, TR>(F, xt, s);
+    // chain: the last operation on s is a kernel of the chain (a programmatic
+    // dependent launch may follow it), not a memset or a join of side streams
+    bool chain = (std::is_same<R, double>::value ? n_s2m_items_ : n_s2m_items_h_) > 0;
     cudaEventRecord(ev_level_[lmax_], s);
     if (near_late) {
         cudaStreamWaitEvent(side_, ev_level_[lmax_], 0);
@@ -999,7 +1017,8 @@ void DeviceOp::run_far_overlap_t(FarField<R>& F, const double2* xt, cudaStream_t
         cudaEventRecord(ev_join_, side_);
     }
     for (int p = lmax_ - 1; p >= lmin_; --p) {
-        if (tc_up) far_m2m_tc(p, 1, s); else far_m2m<R, TR>(F, p, s);
+        if (tc_up) far_m2m_tc(p, 1, s); else far_m2m<R, TR>(F, p, s, chain_pdl_ && chain);
+        chain = chain || npar_[p] > 0;
         cudaEventRecord(ev_level_[p], s);
     }
     cudaStream_t ms[2] = {s2, side3_};
@@ -1013,13 +1032,15 @@ void DeviceOp::run_far_overlap_t(FarField<R>& F, const double2* xt, cudaStream_t
     }
     cudaEventRecord(ev_m2l_done_, s2);
     if (nms > 1) cudaEventRecord(ev_m2l_done2_, side3_);
-    far_m2l<R, TR>(F, lmin_, lmin_, s);
+    far_m2l<R, TR>(F, lmin_, lmin_, s, chain_pdl_ && chain);
     cudaStreamWaitEvent(s, ev_m2l_done_, 0);
     if (nms > 1) cudaStreamWaitEvent(s, ev_m2l_done2_, 0);
+    chain = false;  // the join: the next launch depends on more than one kernel
     for (int p = lmin_; p < lmax_; ++p) {
-        if (tc_dn) far_l2l_tc(p, 1, s); else far_l2l<R, TR>(F, p, s);
+        if (tc_dn) far_l2l_tc(p, 1, s); else far_l2l<R, TR>(F, p, s, chain_pdl_ && chain);
+        chain = chain || n_l2l_pairs_[p] > 0;
     }
-    far_l2t<R, TR>(F, s);
+    far_l2t<R, TR>(F, s, chain_pdl_ && chain);
 }
 
 void DeviceOp::run_far(const double2* xt, cudaStream_t s, int stage, int prec, bool tr) {
@@ -1857,6 +1878,20 @@ std::string DeviceOp::set_near_kernel(int kind) {
     return {};
 }
 
+std::string DeviceOp::set_schedule(int schedule) {
+    if (!ready_) return "operator not set up";
+    if (schedule < 0 || schedule > 15) return "arg:schedule must be 0..15";
+    MLFMA_CK(cudaSetDevice(device_));
+    MLFMA_CK(cudaStreamSynchronize(stream_));
+    m2l_staged_ = schedule & 1;
+    near_late_ = (schedule & 2) != 0;
+    m2l_streams_ = (schedule & 4) ? 2 : 1;
+    chain_pdl_ = (schedule & 8) != 0;
+    drop_graphs();
+    ++generation_;
+    return {};
+}
+
 std::string DeviceOp::set_staged(int mode) {
     if (!ready_) return "operator not set up";
     if (mode < 0 || mode > 15) return "arg:mode must be 0..15";
@@ -2003,20 +2038,23 @@ std::string DeviceOp::autotune(int nr, int reps, TuneReport* rep) {
         // early or after S2M, one or two side streams for the finer translations
         {
             float bt = 1e30f;
-            int bst = m2l_staged_, bnl = near_late_ ? 1 : 0, bms = m2l_streams_;
+            int bst = m2l_staged_, bnl = near_late_ ? 1 : 0, bms = m2l_streams_, bpdl = chain_pdl_ ? 1 : 0;
             for (int st : {0, 1})
                 for (int nl : {0, 1})
-                    for (int ms : {1, 2}) {
-                        m2l_staged_ = st;
-                        near_late_ = nl != 0;
-                        m2l_streams_ = ms;
-                        const float t = timed(product);
-                        if (t < bt) { bt = t; bst = st; bnl = nl; bms = ms; }
-                    }
+                    for (int ms : {1, 2})
+                        for (int pd : {0, 1}) {
+                            m2l_staged_ = st;
+                            near_late_ = nl != 0;
+                            m2l_streams_ = ms;
+                            chain_pdl_ = pd != 0;
+                            const float t = timed(product);
+                            if (t < bt) { bt = t; bst = st; bnl = nl; bms = ms; bpdl = pd; }
+                        }
             m2l_staged_ = bst;
             near_late_ = bnl != 0;
             m2l_streams_ = bms;
-            r.schedule = bst | (bnl << 1) | ((bms - 1) << 2);
+            chain_pdl_ = bpdl != 0;
+            r.schedule = bst | (bnl << 1) | ((bms - 1) << 2) | (bpdl << 3);
         }
         // interpolation and anterpolation: tensor cores or CUDA cores (the
         // complex-float far field), timed on the whole product

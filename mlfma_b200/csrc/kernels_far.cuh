@@ -16,6 +16,20 @@
 namespace mlfma {
 namespace {
 
+// Programmatic dependent launch.  The far-field chain's kernels after the first
+// are launched with programmatic stream serialization, so that a kernel's
+// blocks are scheduled while its predecessor on the stream is still draining
+// its last wave.  Every chain kernel therefore starts with griddepcontrol.wait,
+// which returns once the predecessor grid has completed and its writes are
+// visible (a no-op for a kernel launched without the attribute): nothing a
+// predecessor writes is read, and nothing it reads is overwritten, before it.
+// Only then does the kernel let its own successor launch, so at most one
+// kernel's blocks wait ahead of the running one.
+__device__ __forceinline__ void chain_wait() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // ------------------------------------------------------------ S2M
 // a_B[e] = sum_n x_n R_n[e]  (Leaf::buildMpoleCoeffs, src/fmm/leaf.cpp:212-230).
 // One block per work item (leaf, run of at most kS2MThreads elements), all leaf
@@ -32,6 +46,7 @@ template <class R, bool CJ>
 __global__ void __launch_bounds__(kS2MThreads)
 k_s2m(const DevLevelT<R>* __restrict__ lvs, const int4* __restrict__ items, const DevFarLeaf* __restrict__ leaves,
       const typename Cx<R>::T* __restrict__ pat, const double2* __restrict__ x) {
+    chain_wait();
     using C = typename Cx<R>::T;
     extern __shared__ unsigned char smraw[];
     C* xs = reinterpret_cast<C*>(smraw);
@@ -96,6 +111,7 @@ template <class R, bool CJ>
 __global__ void __launch_bounds__(kL2TThreads)
 k_l2t(const DevLevelT<R>* __restrict__ lvs, const int4* __restrict__ items, const DevFarLeaf* __restrict__ leaves,
       const typename Cx<R>::T* __restrict__ pat, double2* __restrict__ yfar) {
+    chain_wait();
     using C = typename Cx<R>::T;
     const int4 it = items[blockIdx.x];  // leaf, first source, source count
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -167,6 +183,7 @@ template <class R, bool CJ>
 __global__ void __launch_bounds__(kS2MThreads)
 k_s2m_half(const DevLevelT<R>* __restrict__ lvs, const int4* __restrict__ items, const DevFarLeaf* __restrict__ leaves,
       const typename Cx<R>::T* __restrict__ hpat, const double2* __restrict__ x) {
+    chain_wait();
     using C = typename Cx<R>::T;
     extern __shared__ unsigned char smraw[];
     C* xs = reinterpret_cast<C*>(smraw);
@@ -241,6 +258,7 @@ template <class R, bool CJ>
 __global__ void __launch_bounds__(kL2TThreads)
 k_l2t_half(const DevLevelT<R>* __restrict__ lvs, const int4* __restrict__ items, const DevFarLeaf* __restrict__ leaves,
            const typename Cx<R>::T* __restrict__ hpat, double2* __restrict__ yfar) {
+    chain_wait();
     using C = typename Cx<R>::T;
     extern __shared__ unsigned char smraw[];
     const int4 it = items[blockIdx.x];  // leaf, first source, source count
@@ -299,6 +317,7 @@ k_l2t_half(const DevLevelT<R>* __restrict__ lvs, const int4* __restrict__ items,
 template <class R, int W, bool POST>  // taps per row: 2 * interp_order (both passes)
 __global__ void __launch_bounds__(128)
 k_m2m(const DevLevelT<R>* __restrict__ lvs, DevTransT<R> T, int rows) {
+    chain_wait();
     using C = typename Cx<R>::T;
     extern __shared__ unsigned char smraw[];
     C* sm = reinterpret_cast<C*>(smraw);
@@ -385,6 +404,7 @@ k_m2m(const DevLevelT<R>* __restrict__ lvs, DevTransT<R> T, int rows) {
 template <class R, bool TR>
 __global__ void __launch_bounds__(128)
 k_m2l(const DevLevelT<R>* __restrict__ lvs, const int4* __restrict__ items, int zero_empty) {
+    chain_wait();
     using C = typename Cx<R>::T;
     const int4 it = items[blockIdx.x];  // level, box, first direction, count
     if (static_cast<int>(threadIdx.x) >= it.w) return;
@@ -443,6 +463,7 @@ constexpr int kM2LStage = 256;  // list entries staged per round (list 2 holds a
 template <class R, bool TR>
 __global__ void __launch_bounds__(128)
 k_m2l_staged(const DevLevelT<R>* __restrict__ lvs, const int4* __restrict__ items, int zero_empty) {
+    chain_wait();
     using C = typename Cx<R>::T;
     constexpr int U = sizeof(R) == 4 ? 8 : 6;
     __shared__ int s_src[kM2LStage], s_off[kM2LStage];
@@ -511,6 +532,7 @@ k_m2l_staged(const DevLevelT<R>* __restrict__ lvs, const int4* __restrict__ item
 template <class R, int W, bool POST>  // both transposed stencils padded to W taps per row
 __global__ void __launch_bounds__(256)
 k_l2l(const DevLevelT<R>* __restrict__ lvs, DevTransT<R> T, const int2* __restrict__ pairs) {
+    chain_wait();
     using C = typename Cx<R>::T;
     extern __shared__ unsigned char smraw[];
     C* sm = reinterpret_cast<C*>(smraw);
@@ -577,6 +599,7 @@ k_l2l(const DevLevelT<R>* __restrict__ lvs, DevTransT<R> T, const int2* __restri
 template <class R, int W, bool CS>  // taps per row: 2 * interp_order (both passes); CS: column-stationary phi pass
 __global__ void __launch_bounds__(256)
 k_m2m_sum(const DevLevelT<R>* __restrict__ lvs, DevTransT<R> T, int rows) {
+    chain_wait();
     using C = typename Cx<R>::T;
     extern __shared__ __align__(16) unsigned char smraw[];
     __shared__ int band[2];
@@ -700,6 +723,7 @@ inline size_t m2m_sum_smem(int child_nth, int child_nph, int rows, size_t csize)
 template <class R, int W, bool POST, bool CS>  // both transposed stencils padded to W taps per row
 __global__ void __launch_bounds__(256)
 k_l2l_st(const DevLevelT<R>* __restrict__ lvs, DevTransT<R> T, const int2* __restrict__ pairs) {
+    chain_wait();
     using C = typename Cx<R>::T;
     extern __shared__ __align__(16) unsigned char smraw[];
     const int2 pc = pairs[blockIdx.x];  // parent index, child entry
@@ -812,6 +836,7 @@ __device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_g
 template <class R, int W, bool POST>
 __global__ void __launch_bounds__(256)
 k_l2l_pipe(const DevLevelT<R>* __restrict__ lvs, DevTransT<R> T, const int2* __restrict__ pairs, int npairs) {
+    chain_wait();
     using C = typename Cx<R>::T;
     extern __shared__ __align__(16) unsigned char smraw[];
     const DevLevelT<R> P = lvs[T.plevel];

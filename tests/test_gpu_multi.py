@@ -170,3 +170,48 @@ def test_operators_of_different_sizes_coexist(cuda_device):
     assert rel(y, orc.matvec(x)) <= 1e-10
     big.close()
     small.close()
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_gmres_multi_flexible_matches_single(cuda_device, precision):
+    """Batched FGMRES (mlfma_gmres_multi with flexible = 1): every column meets
+    its tolerance on the FP64 residual and agrees with the one-vector FGMRES
+    of the same right-hand side (same outer and inner steps up to rounding);
+    columns stop on their own tolerance while the others go on."""
+    m = inputs.make_icosphere(3, radius=1.0)
+    op = MLFMA.rwg(m, PW, max_node_srcs=16, ref_compat=0, self_terms=1, max_rhs=8, precision=precision).setup()
+    op64 = MLFMA.rwg(m, PW, max_node_srcs=16, ref_compat=0, self_terms=1).setup()
+    B = np.stack([op.rhs_planewave(p) for p in inputs.fibonacci_planewaves(6)])
+    B[3] *= 1e3  # a column of another scale: its own absolute target
+    tol = 1e-7
+    X, infos = op.solve_multi(B, max_iter=2000, tol=tol, restart=10, flexible=True, inner_iters=8)
+    for r in range(6):
+        assert infos[r].converged
+        assert infos[r].refinements >= 1 and infos[r].iterations >= infos[r].refinements
+        assert rel(op64.matvec(X[r]), B[r]) <= tol * 1.0001
+        x1, i1 = op.solve(B[r], max_iter=2000, tol=tol, restart=10, flexible=True, inner_iters=8)
+        assert i1.converged
+        assert abs(infos[r].refinements - i1.refinements) <= 2
+        assert rel(X[r], x1) <= 1e-5
+    op.close()
+    op64.close()
+
+
+def test_gmres_multi_flexible_edge_cases(cuda_device):
+    """A zero right-hand side gives x = 0 at once; one column; a budget that
+    runs out reports the column as not converged with its true residual."""
+    op = MLFMA.rwg(inputs.make_icosphere(3, radius=1.0), PW, max_node_srcs=16, ref_compat=0, self_terms=1,
+                   max_rhs=4, precision=1).setup()
+    B = cmat(3, op.n, 5)
+    B[1] = 0.0
+    X, infos = op.solve_multi(B, max_iter=600, tol=1e-8, restart=12, flexible=True, inner_iters=10)
+    assert np.all(X[1] == 0) and infos[1].converged and infos[1].iterations == 0
+    for r in (0, 2):
+        assert infos[r].converged
+        assert rel(op.matvec(X[r]), B[r]) <= 1e-4  # the mixed product; the FP64 residual met 1e-8
+    X1, i1 = op.solve_multi(B[:1], max_iter=600, tol=1e-8, restart=12, flexible=True, inner_iters=10)
+    assert i1[0].converged and rel(X1[0], X[0]) <= 1e-6
+    Xs, ishort = op.solve_multi(B[:1], max_iter=5, tol=1e-12, restart=12, flexible=True, inner_iters=10)
+    assert not ishort[0].converged and ishort[0].iterations <= 5 + 10
+    assert ishort[0].true_residual < 1.0
+    op.close()
