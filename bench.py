@@ -12,9 +12,11 @@ matrix-vector product y = A x on one right-hand side.
 
 `value` is device-resident throughput (x and y already in HBM), timed with
 CUDA events on the launching stream; `e2e` is the same product through the
-C-ABI host-buffer call mlfma_matvec (called through ctypes, pointers prepared
-once), with the host->device copy of x and the device->host copy of y (pinned
-buffers) inside the timed region.  The operator
+C-ABI host-buffer call mlfma_matvec_mapped (called through ctypes, pointers
+prepared once) on pinned host buffers: its first kernel reads x and its last
+kernel writes y across the bus inside the timed region, and the call
+synchronises before it returns.  `e2e.copy_path` times mlfma_matvec on the
+same buffers (cudaMemcpyAsync in, product, cudaMemcpyAsync out).  The operator
 reads 0.41 GB per matvec, more than the 126 MB L2, so no flush runs between
 steps.  With N > 1 every rank runs an independent replica of the product
 (there is no data exchange on this path); rank 0 reports N * K / max time.
@@ -253,23 +255,31 @@ def measure(torch, dev, rank, world, args, precision: int, clocks=None) -> dict:
     xp.copy_(xh)
     xn, yn = xp.numpy(), yp.numpy()
     dp = ctypes.POINTER(ctypes.c_double)
-    c_matvec, handle = _lib.lib().mlfma_matvec, op._h
+    handle = _lib.lib(), op._h
     px, py = xn.view(np.float64).ctypes.data_as(dp), yn.view(np.float64).ctypes.data_as(dp)
 
-    def e2e_step():
-        rc = c_matvec(handle, px, py, 0)
-        if rc:
-            raise RuntimeError(f"mlfma_matvec returned {rc}")
+    def e2e_time(fn, name):
+        def e2e_step():
+            rc = fn(handle[1], px, py, 0)
+            if rc:
+                raise RuntimeError(f"{name} returned {rc}")
 
-    for _ in range(args.warmup):
-        e2e_step()
-    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    f0.record(stream)
-    for _ in range(args.steps):
-        e2e_step()
-    f1.record(stream)
-    torch.cuda.synchronize(dev)
-    e2e_ms = f0.elapsed_time(f1) / args.steps
+        for _ in range(args.warmup):
+            e2e_step()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        for _ in range(args.steps):
+            e2e_step()
+        f1.record(stream)
+        torch.cuda.synchronize(dev)
+        return f0.elapsed_time(f1) / args.steps
+
+    # mlfma_matvec_mapped: the gather and final kernels read x and write y in
+    # the pinned buffers across the bus (the transfers inside the kernels);
+    # mlfma_matvec: copies in and out around the device product
+    e2e_ms = e2e_time(handle[0].mlfma_matvec_mapped, "mlfma_matvec_mapped")
+    e2e_mapped_ok = bool(np.array_equal(yn, y_dev))
+    e2e_copy_ms = e2e_time(handle[0].mlfma_matvec, "mlfma_matvec")
     clk = clocks.stop() if clocks is not None else None
 
     # Per-stage device times (stages launched back to back on the operator's stream).
@@ -314,10 +324,10 @@ def measure(torch, dev, rank, world, args, precision: int, clocks=None) -> dict:
                      dense_residual=dres)
         op.close()
     if world > 1:
-        t = torch.tensor([ms, e2e_ms], device=dev, dtype=torch.float64)
+        t = torch.tensor([ms, e2e_ms, e2e_copy_ms], device=dev, dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms, e2e_ms = float(t[0]), float(t[1])
-    return dict(ms=ms, e2e_ms=e2e_ms, stages=avg, traffic=traffic, stats=st, setup_s=setup_s, n=n, y=y_dev,
+        ms, e2e_ms, e2e_copy_ms = float(t[0]), float(t[1]), float(t[2])
+    return dict(ms=ms, e2e_ms=e2e_ms, e2e_copy_ms=e2e_copy_ms, e2e_mapped_ok=e2e_mapped_ok, stages=avg, traffic=traffic, stats=st, setup_s=setup_s, n=n, y=y_dev,
                 clocks=clk, solve=solve, tuning=tuning, dense_err=dense_err)
 
 
@@ -889,7 +899,12 @@ def main():
                                                  "near_blocks_per_sm": r64["tuning"]["near_blocks_per_sm"],
                                                  "m2m_rows": [v for v in r64["tuning"]["m2m_rows"] if v]}}),
             "e2e": {"value": world * 1000.0 / e2e_ms, "unit": UNIT, "h2d_bytes_per_step": n * 16,
-                    "d2h_bytes_per_step": n * 16},
+                    "d2h_bytes_per_step": n * 16, "call": "mlfma_matvec_mapped",
+                    "what": "pinned host buffers; x read and y written across the bus by the product's first and "
+                            "last kernels, synchronised every call",
+                    "equals_device_product": r64["e2e_mapped_ok"],
+                    "copy_path": {"value": world * 1000.0 / r64["e2e_copy_ms"], "call": "mlfma_matvec",
+                                  "what": "the same buffers through cudaMemcpyAsync in and out"}},
             "gpu_launches": int(st.get("launches_per_matvec", 0)) * args.steps,
             "roofline": roofline(r64["stages"], r64["traffic"], ""),
             "stage_ms": r64["stages"],

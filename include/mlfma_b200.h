@@ -193,6 +193,15 @@ int mlfma_matvec(mlfma_handle h, const double* x, double* y, int accumulate);
  * on the GPU (issue them on one stream, or order the streams). */
 int mlfma_matvec_device(mlfma_handle h, const void* d_x, void* d_y, int accumulate, void* stream);
 
+/* mlfma_matvec (Solver::evalRvec, src/solver.cpp:41-57) on page-locked host
+ * buffers that the device addresses directly (cudaHostAlloc / cudaMallocHost
+ * memory, or cudaHostRegister'd memory, each covering the n complex values):
+ * no separate copies; the gather kernel reads x and the final kernel writes y
+ * across the bus, each in one contiguous run per warp.  Returns when y is
+ * complete.  MLFMA_ERR_ARG when the first or the last value of x or y is not
+ * in such memory. */
+int mlfma_matvec_mapped(mlfma_handle h, const double* x, double* y, int accumulate);
+
 /* Solve A x = b with GMRES on the device; b and x host buffers (Solver::solve,
  * src/solver.cpp:116-146).  x is overwritten (initial guess 0).  On a mixed
  * operator with opts->refine = 1 the answer meets tol on the FP64 residual. */

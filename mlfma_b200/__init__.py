@@ -240,6 +240,11 @@ class MLFMA:
         check(lib().mlfma_matvec_device(self._h, ctypes.c_void_p(x_ptr), ctypes.c_void_p(y_ptr),
                                         int(accumulate), ctypes.c_void_p(stream)))
 
+    def matvec_mapped(self, x_ptr: int, y_ptr: int, accumulate: bool = False) -> None:
+        """y = A x on page-locked, device-mapped host buffers given by address
+        (e.g. torch pin_memory tensors): no separate copies (mlfma_matvec_mapped)."""
+        check(lib().mlfma_matvec_mapped(self._h, ctypes.cast(x_ptr, _dp), ctypes.cast(y_ptr, _dp), int(accumulate)))
+
     def solve(self, b=None, max_iter: int = 500, tol: float = 1e-6, restart: int = 0,
               ref_givens: bool = True, raise_on_fail: bool = False, refine: bool = False, inner_tol: float = 0.0,
               flexible: bool = False, inner_iters: int = 0, precond: bool = False):

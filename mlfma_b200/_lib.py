@@ -85,6 +85,7 @@ SIGNATURES = {
     "mlfma_get_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Stats)]),
     "mlfma_rhs": (ctypes.c_int, [ctypes.c_void_p, _dp]),
     "mlfma_matvec": (ctypes.c_int, [ctypes.c_void_p, _dp, _dp, ctypes.c_int]),
+    "mlfma_matvec_mapped": (ctypes.c_int, [ctypes.c_void_p, _dp, _dp, ctypes.c_int]),
     "mlfma_matvec_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
                                            ctypes.c_void_p]),
     "mlfma_gmres": (ctypes.c_int, [ctypes.c_void_p, _dp, _dp, ctypes.POINTER(SolverOpts),

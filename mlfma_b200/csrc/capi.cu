@@ -246,6 +246,46 @@ int mlfma_matvec(mlfma_handle h, const double* x, double* y, int accumulate) {
     return MLFMA_OK;
 }
 
+namespace {
+// Device address of the page-locked, mapped host range [p, p + bytes), or null
+// when its first or last byte is not in such memory.
+void* mapped_range(const void* p, size_t bytes) {
+    cudaPointerAttributes a{}, b{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    const char* last = static_cast<const char*>(p) + bytes - 1;
+    if (cudaPointerGetAttributes(&b, last) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    if (a.type != cudaMemoryTypeHost || b.type != cudaMemoryTypeHost || !a.devicePointer || !b.devicePointer)
+        return nullptr;
+    if (static_cast<const char*>(b.devicePointer) != static_cast<const char*>(a.devicePointer) + (bytes - 1))
+        return nullptr;
+    return a.devicePointer;
+}
+}  // namespace
+
+int mlfma_matvec_mapped(mlfma_handle h, const double* x, double* y, int accumulate) {
+    if (!h || !x || !y) return fail(MLFMA_ERR_ARG, "null argument");
+    if (!ready(h)) return fail(MLFMA_ERR_STATE, "mlfma_setup has not run");
+    if (cudaSetDevice(h->device) != cudaSuccess) return fail(MLFMA_ERR_CUDA, "cudaSetDevice failed");
+    const size_t bytes = sizeof(double2) * h->plan.n;
+    void* dx = mapped_range(x, bytes);
+    void* dy = mapped_range(y, bytes);
+    if (!dx || !dy) return fail(MLFMA_ERR_ARG, "x and y must be page-locked host memory mapped for the device");
+    cudaStream_t s = h->dev->stream();
+    std::string e = h->dev->matvec_mapped(static_cast<const double2*>(dx), static_cast<double2*>(dy), accumulate != 0, s);
+    if (!e.empty()) return fail(MLFMA_ERR_CUDA, e);
+    const cudaError_t ce = cudaStreamSynchronize(s);
+    if (ce != cudaSuccess) return fail(MLFMA_ERR_CUDA, cudaGetErrorString(ce));
+    e = h->dev->device_error();
+    if (!e.empty()) return fail(MLFMA_ERR_CUDA, e);
+    return MLFMA_OK;
+}
+
 int mlfma_matvec_device(mlfma_handle h, const void* d_x, void* d_y, int accumulate, void* stream) {
     if (!h || !d_x || !d_y) return fail(MLFMA_ERR_ARG, "null argument");
     if (!ready(h)) return fail(MLFMA_ERR_STATE, "mlfma_setup has not run");

@@ -215,6 +215,11 @@ public:
     // adj: y = A^H x (needs ref_compat = 0).
     std::string matvec_device(const double2* x, double2* y, bool accumulate, cudaStream_t stream, int prec = -1,
                               bool adj = false);
+    // The same product on host buffers the device can address (pinned,
+    // mapped; device-side addresses of them): the gather kernel reads x and
+    // the finishing kernel writes y in caller order straight over the bus
+    // (coalesced), no separate copies.
+    std::string matvec_mapped(const double2* x, double2* y, bool accumulate, cudaStream_t stream);
 
     // Non-empty when a kernel of this operator gave up a bounded wait (its
     // results since then are not valid); read after the stream is synchronised.
@@ -422,6 +427,7 @@ private:
     long long near_entries_ = 0;
 
     int* perm_ = nullptr;
+    int* tpos_ = nullptr;  // inverse of perm_: caller index -> tree position
     DevSources src_{};         // source geometry (setup kernels, far field)
     double2* xt_ = nullptr;    // tree-ordered input
     double2* yfar_ = nullptr;  // tree-ordered far result (before C k)

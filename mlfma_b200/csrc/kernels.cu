@@ -96,6 +96,26 @@ __global__ void k_finish(const double2* __restrict__ yfar, const double2* __rest
     y[o] = accumulate ? cadd(y[o], v) : v;
 }
 
+// The boundary kernels of a product on mapped host buffers, indexed by the
+// caller's order so that every warp reads x and writes y in one contiguous
+// run across the bus: xt[tpos[c]] = x[c]; y[c] (+)= ck (yfar + ynear)[tpos[c]]
+// + loads xt (the same value k_finish forms).
+__global__ void k_gather_caller(const double2* __restrict__ x, const int* __restrict__ tpos,
+                                double2* __restrict__ xt, int n) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < n) xt[tpos[c]] = x[c];
+}
+__global__ void k_finish_caller(const double2* __restrict__ yfar, const double2* __restrict__ ynear,
+                                const int* __restrict__ tpos, double2* __restrict__ y, int n, double2 ck,
+                                int accumulate, const double2* __restrict__ xt, const double2* __restrict__ loads) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    const int t = tpos[c];
+    double2 v = cmul(ck, cadd(yfar[t], ynear[t]));
+    if (loads) v = cfma(loads[t], xt[t], v);
+    y[c] = accumulate ? cadd(y[c], v) : v;
+}
+
 inline int blocks_for(long long n, int bs) { return static_cast<int>((n + bs - 1) / bs); }
 
 template <class C> C host_c(const cplx& v);
@@ -552,6 +572,11 @@ std::string DeviceOp::setup(const Plan& plan, int device, int precision, int max
         const cplx ck = cplx(0, -kC0 * kMu0 / (4.0 * kPi)) * plan.pw.wavenum;
         ck_ = make_double2(ck.real(), ck.imag());
         perm_ = upload(plan.perm);
+        {
+            std::vector<int> tpos(plan.perm.size());
+            for (size_t t = 0; t < plan.perm.size(); ++t) tpos[plan.perm[t]] = static_cast<int>(t);
+            tpos_ = upload(tpos);
+        }
         xt_ = alloc<double2>(n_);
         yfar_ = alloc<double2>(n_);
         ynear_ = alloc<double2>(n_);
@@ -1174,6 +1199,20 @@ std::string DeviceOp::matvec_device(const double2* x, double2* y, bool accumulat
     launch_core(s, prec, adj);
     k_finish<<<blocks_for(n_, 256), 256, 0, s>>>(yfar_, ynear_, perm_, y, n_, ck_, accumulate ? 1 : 0, xt_,
                                                  has_loads_ ? loads_ : nullptr, adj ? 1 : 0);
+    MLFMA_CK(cudaGetLastError());
+    return {};
+}
+
+std::string DeviceOp::matvec_mapped(const double2* x, double2* y, bool accumulate, cudaStream_t stream) {
+    if (!ready_) return "operator not set up";
+    cudaStream_t s = stream ? stream : stream_;
+    MLFMA_CK(cudaSetDevice(device_));
+    std::string e = ensure_graph(precision_, false);
+    if (!e.empty()) return e;
+    k_gather_caller<<<blocks_for(n_, 256), 256, 0, s>>>(x, tpos_, xt_, n_);
+    launch_core(s, precision_, false);
+    k_finish_caller<<<blocks_for(n_, 256), 256, 0, s>>>(yfar_, ynear_, tpos_, y, n_, ck_, accumulate ? 1 : 0, xt_,
+                                                        has_loads_ ? loads_ : nullptr);
     MLFMA_CK(cudaGetLastError());
     return {};
 }
