@@ -122,6 +122,29 @@ public:
         return t;
     }
 
+    // The one-vector product's schedule: the bits mlfma_tuning.schedule reports.
+    void setSchedule(int schedule) { check(mlfma_set_schedule(h_, schedule)); }
+
+    // evalRvec on page-locked host buffers the device addresses directly
+    // (cudaHostAlloc / cudaMallocHost / cudaHostRegister memory of n values).
+    void evalRvecMapped(const cplx* lvec, cplx* rvec, bool accumulate = false) {
+        check(mlfma_matvec_mapped(h_, reinterpret_cast<const double*>(lvec), reinterpret_cast<double*>(rvec),
+                                  accumulate ? 1 : 0));
+    }
+
+    // nrhs systems at once (B: nrhs x n, caller order), GMRES or, with
+    // opts.flexible, FGMRES per system; infos may be null.
+    std::vector<cplx> solveMulti(int nrhs, const std::vector<cplx>& B, const mlfma_solver_opts& opts,
+                                 std::vector<mlfma_solve_info>* infos = nullptr) {
+        std::vector<cplx> X(B.size());
+        std::vector<mlfma_solve_info> inf(static_cast<size_t>(nrhs));
+        const int code = mlfma_gmres_multi(h_, nrhs, reinterpret_cast<const double*>(B.data()),
+                                           reinterpret_cast<double*>(X.data()), &opts, inf.data());
+        if (code != MLFMA_OK && code != MLFMA_ERR_NOT_CONVERGED) check(code);
+        if (infos) *infos = inf;
+        return X;
+    }
+
     mlfma_handle handle() const { return h_; }
 
 private:

@@ -77,6 +77,16 @@ def test_device_calls_before_setup_are_state_errors():
     with pytest.raises(MlfmaError) as e:
         op.dense_rows([0, 1], np.zeros(50))
     assert e.value.code == _lib.MLFMA_ERR_STATE
+    x = np.zeros(50, dtype=np.complex128)
+    with pytest.raises(MlfmaError) as e:
+        op.matvec_mapped(x.ctypes.data, x.ctypes.data)
+    assert e.value.code == _lib.MLFMA_ERR_STATE
+    with pytest.raises(MlfmaError) as e:
+        op.set_schedule(1)
+    assert e.value.code == _lib.MLFMA_ERR_STATE
+    with pytest.raises(MlfmaError) as e:
+        op.solve_multi(np.zeros((2, 50)), flexible=True)
+    assert e.value.code == _lib.MLFMA_ERR_STATE
     op.close()
 
 
@@ -89,6 +99,8 @@ def test_null_arguments():
     assert L.mlfma_dense_rows(None, 1, None, None, None) == _lib.MLFMA_ERR_ARG
     assert L.mlfma_check_bounded_wait(0, None) == _lib.MLFMA_ERR_ARG
     assert L.mlfma_batch_create(0, None, None) == _lib.MLFMA_ERR_ARG
+    assert L.mlfma_matvec_mapped(None, None, None, 0) == _lib.MLFMA_ERR_ARG
+    assert L.mlfma_set_schedule(None, 0) == _lib.MLFMA_ERR_ARG
 
 
 def test_host_plan_stats_without_gpu():
