@@ -19,7 +19,9 @@ synchronises before it returns.  `e2e.copy_path` times mlfma_matvec on the
 same buffers (cudaMemcpyAsync in, product, cudaMemcpyAsync out).  The operator
 reads 0.41 GB per matvec, more than the 126 MB L2, so no flush runs between
 steps.  With N > 1 every rank runs an independent replica of the product
-(there is no data exchange on this path); rank 0 reports N * K / max time.
+(there is no data exchange on this path); rank 0 reports N * K / max time,
+and the secondary blocks (many right-hand sides, many problems, adjoint,
+8-wavelength sphere) run only when N = 1.
 
 `dense_check` (and `dense_rel_err` / `dense_residual` in the mixed and solve
 blocks) states the relative error of the product, and the residual of each
@@ -861,12 +863,16 @@ def main():
 
     r64 = measure(torch, dev, rank, world, args, precision=0, clocks=ClockSampler(local_rank))
     rmx = None if args.no_mixed else measure(torch, dev, rank, world, args, precision=1)
+    # The secondary legs (many right-hand sides, many problems, the adjoint
+    # gradient, the 8-wavelength sphere) run with one process only: the
+    # replicas of a multi-GPU run report the headline product.
+    solo = world == 1
     bat = None
-    if not args.no_batched:
+    if not args.no_batched and solo:
         bat = {p: measure_batched(torch, dev, args, p) for p in ((0, 1) if not args.no_mixed else (0,))}
-    probs = None if args.no_batched else measure_problems(torch, dev, args)
-    adj = None if args.no_adjoint else measure_adjoint(torch, dev, args)
-    large = None if args.no_large else measure_large(torch, dev, args)
+    probs = None if args.no_batched or not solo else measure_problems(torch, dev, args)
+    adj = None if args.no_adjoint or not solo else measure_adjoint(torch, dev, args)
+    large = None if args.no_large or not solo else measure_large(torch, dev, args)
 
     if rank == 0:
         cpu = None
